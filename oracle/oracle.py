@@ -1,0 +1,259 @@
+"""Python front end of the test oracle (TEST INFRASTRUCTURE ONLY).
+
+Two CPU backends with one interface:
+
+* ``ref``   — the reference's own C functions compiled in place from the
+              reference tree (``oracle/_ref/libdenise_ref.so``, built by
+              ``oracle/Makefile``; ``libdenise_ref_fast.so`` is the -O3 timing
+              build used only as the CPU baseline),
+* ``port``  — this repository's C restatement (``oracle/_ref/libdsh_oracle.so``),
+              in FP32 (``fp64=False``, bit-identical to ``ref``) or FP64.
+
+Array conventions: grid fields are numpy float32 ``[NY, NX]``; traces
+``[ntr, NT]``; source tables ``[8, nsrc]`` (grid x, grid y, 0, tshift, fc, amp,
+angle, type); receiver tables ``[2, ntr]`` int32 grid indices (1-based, as the
+reference's ``recpos``).  Only tests, the smoke check and the CPU-baseline leg
+of bench.py import this module.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_DIR = os.path.join(HERE, "_ref")
+
+FIELD = {"vy": 0, "sxy": 1, "syz": 2, "vyp1": 3, "uy": 4, "uyx": 5, "uip": 6, "ujp": 7, "rho": 8, "vs": 9,
+         "fipjp": 10, "f": 11, "Ws": 12, "Wr": 13, "We": 14, "g_u": 15, "g_rho": 16, "hess_u": 17,
+         "hess_rho": 18, "taus": 19, "tausipjp": 20}
+PML = ["K_x", "a_x", "b_x", "K_x_half", "a_x_half", "b_x_half", "K_y", "a_y", "b_y", "K_y_half", "a_y_half",
+       "b_y_half", "d_x", "d_x_half", "d_y", "d_y_half"]
+
+
+class Params(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("nx", "ny", "nt", "fdorder", "maxrelerror", "fw", "free_surf", "l",
+                                      "quellart", "eprecond")] + \
+               [(n, C.c_float) for n in ("dh", "dt", "damping", "fpml", "npower", "k_max_pml")] + \
+               [("fl", C.c_float * 8)]
+
+
+@dataclass
+class Model:
+    """One SH model and its time-stepping settings (mirrors the reference's .inp keys)."""
+    nx: int
+    ny: int
+    nt: int
+    dh: float
+    dt: float
+    vs: np.ndarray
+    rho: np.ndarray
+    qs: np.ndarray | None = None
+    fdorder: int = 4
+    maxrelerror: int = 1
+    fw: int = 20
+    free_surf: int = 1
+    l: int = 0
+    fl: tuple = ()
+    quellart: int = 1
+    eprecond: int = 1
+    damping: float | None = None
+    fpml: float = 30.0
+    npower: float = 4.0
+    k_max_pml: float = 1.0
+    extra: dict = field(default_factory=dict)
+
+    def params(self) -> Params:
+        p = Params()
+        p.nx, p.ny, p.nt = self.nx, self.ny, self.nt
+        p.fdorder, p.maxrelerror, p.fw, p.free_surf = self.fdorder, self.maxrelerror, self.fw, self.free_surf
+        p.l, p.quellart, p.eprecond = self.l, self.quellart, self.eprecond
+        p.dh, p.dt = self.dh, self.dt
+        p.damping = float(self.damping if self.damping is not None else float(np.max(self.vs)))
+        p.fpml, p.npower, p.k_max_pml = self.fpml, self.npower, self.k_max_pml
+        for i, v in enumerate(self.fl[:8]):
+            p.fl[i] = v
+        return p
+
+
+def build(reference: str | None = None, quiet: bool = True) -> None:
+    """Build the oracle libraries (the reference part only if its tree exists)."""
+    targets = ["port"]
+    ref = reference or os.environ.get("DSH_REFERENCE", "/root/reference")
+    if os.path.isdir(os.path.join(ref, "src")):
+        targets.insert(0, "ref")
+    out = subprocess.run(["make", "-C", HERE, f"REF={ref}", *targets], capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
+
+
+def available(kind: str) -> bool:
+    name = {"ref": "libdenise_ref.so", "ref_fast": "libdenise_ref_fast.so", "port": "libdsh_oracle.so"}[kind]
+    return os.path.exists(os.path.join(REF_DIR, name))
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _ptr(a, t=C.c_float):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+class Oracle:
+    """A CPU oracle session for one model (one process-wide session per backend)."""
+
+    def __init__(self, model: Model, kind: str = "ref", fp64: bool = False, fd12_compat: bool = True):
+        self.kind, self.fp64, self.m = kind, fp64, model
+        lib = {"ref": "libdenise_ref.so", "ref_fast": "libdenise_ref_fast.so", "port": "libdsh_oracle.so"}[kind]
+        path = os.path.join(REF_DIR, lib)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        self.lib = C.CDLL(path)
+        self.pre = "refh_" if kind.startswith("ref") else "dsho_"
+        if fp64 and not kind == "port":
+            raise ValueError("FP64 runs exist only for the restatement")
+        self._fn("init").restype = C.c_int
+        self._fn("residual").argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_double)]
+        vs, rho = _f32(model.vs), _f32(model.rho)
+        qs = _f32(model.qs) if model.qs is not None else np.ones_like(vs)
+        self._keep = (vs, rho, qs)
+        self.params = model.params()
+        if self.pre == "dsho_":
+            self.lib.dsho_set_fd12_compat(int(fd12_compat))
+            rc = self.lib.dsho_init(C.byref(self.params), _ptr(vs), _ptr(rho), _ptr(qs), int(fp64))
+        else:
+            rc = self.lib.refh_init(C.byref(self.params), _ptr(vs), _ptr(rho), _ptr(qs))
+        if rc != 0:
+            raise ValueError(f"oracle init failed ({rc})")
+        self.ntr = 0
+
+    def _fn(self, name):
+        return getattr(self.lib, self.pre + name)
+
+    # --- coefficients -------------------------------------------------
+    def hc(self):
+        out = np.zeros(7, np.float32)
+        self._fn("get_hc")(_ptr(out))
+        return out
+
+    def cnorm(self):
+        out = np.zeros(2, np.float32)
+        self._fn("get_cnorm")(_ptr(out))
+        return out
+
+    def pml(self, name):
+        out = np.zeros(2 * self.m.fw, np.float32)
+        rc = self._fn("get_pml")(PML.index(name), _ptr(out))
+        if rc != 0:
+            raise ValueError(name)
+        return out
+
+    def sls(self):
+        outs = [np.zeros(max(self.m.l, 1), np.float32) for _ in range(4)]
+        self._fn("get_sls")(*[_ptr(o) for o in outs])
+        return [o[: self.m.l] for o in outs]
+
+    def field(self, name, l: int | None = None, f64: bool = False):
+        code = FIELD[name] if l is None else {"r": 100, "q": 200, "dip": 300, "d": 400}[name] + l
+        if f64:
+            out = np.zeros((self.m.ny, self.m.nx), np.float64)
+            rc = self.lib.dsho_get_field_f64(code, _ptr(out, C.c_double))
+        else:
+            out = np.zeros((self.m.ny, self.m.nx), np.float32)
+            rc = self._fn("get_field")(code, _ptr(out))
+        if rc != 0:
+            raise ValueError(name)
+        return out
+
+    def psi(self, which):
+        idx = ["psi_sxy_x", "psi_vyx", "psi_syz_y", "psi_vyy"].index(which)
+        shape = (self.m.ny, 2 * self.m.fw) if idx < 2 else (2 * self.m.fw, self.m.nx)
+        out = np.zeros(shape, np.float32)
+        rc = self._fn("get_psi")(idx, _ptr(out))
+        if rc != 0:
+            raise ValueError(which)
+        return out
+
+    def wavelet(self, srcpos8):
+        sp = _f32(srcpos8)
+        nsrc = sp.shape[1]
+        out = np.zeros((nsrc, self.m.nt), np.float32)
+        self._fn("wavelet")(nsrc, _ptr(sp), _ptr(out))
+        return out
+
+    # --- time loops ---------------------------------------------------
+    def forward(self, srcpos8, recpos, signals=None, nsteps=None, store=False, hessian=False):
+        sp = _f32(srcpos8)
+        rp = np.ascontiguousarray(recpos, dtype=np.int32)
+        nsrc, ntr = sp.shape[1], rp.shape[1]
+        nsteps = self.m.nt if nsteps is None else nsteps
+        seis = np.zeros((max(ntr, 1), self.m.nt), np.float32)
+        sig = _f32(signals) if signals is not None else None
+        self._keep_fwd = (sp, rp, sig)
+        if self.fp64:
+            s64 = np.zeros((max(ntr, 1), self.m.nt), np.float64)
+            rc = self.lib.dsho_forward_f64(nsrc, _ptr(sp), _ptr(sig) if sig is not None else None, ntr,
+                                           _ptr(rp, C.c_int), nsteps, int(store), int(hessian), _ptr(s64, C.c_double))
+            seis = s64
+        else:
+            rc = self._fn("forward")(nsrc, _ptr(sp), _ptr(sig) if sig is not None else None, ntr,
+                                     _ptr(rp, C.c_int), nsteps, int(store), int(hessian), _ptr(seis))
+        if rc != 0:
+            raise RuntimeError("oracle forward failed")
+        self.ntr = ntr
+        return seis[:ntr]
+
+    def residual(self, obs):
+        ob = _f32(obs)
+        res = np.zeros((self.ntr, self.m.nt), np.float32)
+        l2 = C.c_double(0.0)
+        rc = self._fn("residual")(ob.ctypes.data, res.ctypes.data, C.byref(l2))
+        if rc != 0:
+            raise RuntimeError("oracle residual failed")
+        return res, l2.value
+
+    def adjoint(self, adj=None, nsteps=None):
+        nsteps = self.m.nt if nsteps is None else nsteps
+        a = _f32(adj) if adj is not None else None
+        rc = self._fn("adjoint")(_ptr(a) if a is not None else None, nsteps)
+        if rc != 0:
+            raise RuntimeError("oracle adjoint failed")
+
+    def eprecond_scale(self):
+        self._fn("eprecond_scale")()
+
+    def convert(self, wu, wrho):
+        a, b = _f32(wu), _f32(wrho)
+        gv, gr = np.zeros_like(a), np.zeros_like(b)
+        self._fn("convert")(_ptr(a), _ptr(b), _ptr(gv), _ptr(gr))
+        return gv, gr
+
+    def hessian_out(self):
+        hv = np.zeros((self.m.ny, self.m.nx), np.float32)
+        hr = np.zeros_like(hv)
+        self._fn("hessian_out")(_ptr(hv), _ptr(hr))
+        return hv, hr
+
+    def psource(self, nt, sxx, syy, srcpos8, signals):
+        a, b, sp, sig = _f32(sxx).copy(), _f32(syy).copy(), _f32(srcpos8), _f32(signals)
+        self._fn("psource")(nt, _ptr(a), _ptr(b), sp.shape[1], _ptr(sp), _ptr(sig))
+        return a, b
+
+    def shot_gradient(self, srcpos8, recpos, obs, signals=None, nsteps=None):
+        """Forward + residual + adjoint + eprecond scaling for one shot (denise.c:875-1694).
+
+        Returns dict(seis, res, l2, g_u, g_rho, Ws, Wr, We)."""
+        seis = self.forward(srcpos8, recpos, signals=signals, nsteps=nsteps, store=True)
+        res, l2 = self.residual(obs)
+        self.adjoint(nsteps=nsteps)
+        out = {"seis": seis, "res": res, "l2": l2, "Ws": self.field("Ws"), "Wr": self.field("Wr")}
+        self.eprecond_scale()
+        out.update(g_u=self.field("g_u"), g_rho=self.field("g_rho"), We=self.field("We"))
+        return out
+
+    def close(self):
+        self._fn("free")()

@@ -1,0 +1,581 @@
+/*
+ * ref_harness.c — TEST ORACLE ONLY.
+ *
+ * Drives the reference's own compiled CPU functions (update_v_PML,
+ * update_s_elastic_PML, update_s_visc_PML, seismo_ssg, eprecond, eprecond1,
+ * hess_save, hessian, matcopy, av_mue, av_tau, prepare_update_s, PML_pro,
+ * holbergcoeff, wavelet, calc_res, zero_fdveps*) through the same per-shot
+ * time loops that the reference's main program runs for one MPI rank
+ * (NPROCX=NPROCY=1).  The reference sources are compiled in place by
+ * oracle/Makefile into oracle/_ref/; nothing here is linked into the product.
+ *
+ * The loop bodies restated here follow:
+ *   forward loop         src/denise.c:1179-1346
+ *   residual             src/denise.c:1364-1428 (calc_res with LNORM=2)
+ *   adjoint loop         src/denise.c:1452-1654 (correlation :1580-1625)
+ *   eprecond scaling     src/denise.c:1665-1678
+ *   shot summation       src/denise.c:1689-1694
+ *   gradient conversion  src/denise.c:1743-1813 (INVMAT=0, INVMAT1=1)
+ *   normalisers C_vs/C_rho  src/denise.c:778-816
+ *   Hessian output conversion src/hessian_out.c:20-31 (file output omitted)
+ * All arrays crossing this API are dense row-major [NY][NX] (index j*NX+i for
+ * grid point (i+1, j+1)); seismograms are [ntr][NT].
+ */
+#include "fd.h"
+
+/* reference globals referenced here (defined by the reference's globvar.h) */
+extern float DT, DH, DAMPING, FPML, *FL, TIME;
+extern int NX, NY, NXG, NYG, NT, FDORDER, MAXRELERROR, FW, FREE_SURF, BOUNDARY, L;
+extern int IDX, IDY, NPROCX, NPROCY, MYID, POS[3], INDEX[5], INVMAT1, INVMAT, GRAD_FORM;
+extern int QUELLART, QUELLTYP, QUELLTYPB, EPRECOND, DTINV, SEISMO, NDT, HESSIAN;
+extern int IENDX, IENDY, NP, NPROC;
+extern int TRKILL, TIMEWIN, RTM, OFFSET_MUTE, NORMALIZE;
+extern float npower, k_max_PML, C_vs, C_rho;
+extern FILE *FP;
+
+typedef struct {
+    int nx, ny, nt, fdorder, maxrelerror, fw, free_surf, l, quellart, eprecond;
+    float dh, dt, damping, fpml, npower, k_max_pml;
+    float fl[8];
+} refh_params;
+
+static int nd;
+static float **pvy, **psxy, **psyz, **pvyp1, **pvym1, **uy, **uyx, **utty;
+static float **prho, **pu, **puip, **pujp, **absorb_coeff;
+static float ***pr, ***pp, ***pq, ***dip, ***d, ***e;
+static float **ptaus, **ptausipjp, **fipjp, **f, **g;
+static float *peta, *etaip, *etajm, *bip, *bjm, *cip, *cjm;
+static float *hc;
+static float *d_x, *K_x, *alpha_prime_x, *a_x, *b_x, *d_x_half, *K_x_half, *alpha_prime_x_half, *a_x_half, *b_x_half;
+static float *d_y, *K_y, *alpha_prime_y, *a_y, *b_y, *d_y_half, *K_y_half, *alpha_prime_y_half, *a_y_half, *b_y_half;
+static float **psi_syz_y, **psi_sxy_x, **psi_vyy, **psi_vyx;
+static float **Ws, **Wr, **We, **g_u_shot, **g_rho_shot, **hessian_u, **hessian_rho;
+static float *fwd_rho_y, *fwd_y, *fwd_u;         /* forward_prop_* of denise.c:467-478 */
+static float ***hess_eyy, ***hess_eyx, ***hess_utty;
+static int fwd_stored = 0, hess_alloc = 0, alive = 0;
+static int cur_ntr = 0;
+static int **recpos_loc = NULL;
+static float **sectionvy = NULL, **sectionvydiff = NULL, **sectionvydata = NULL, **sectionvydiffold = NULL;
+
+static void harness_free_shot(void)
+{
+    if (recpos_loc) { free_imatrix(recpos_loc, 1, 3, 1, cur_ntr); recpos_loc = NULL; }
+    if (sectionvy) { free_matrix(sectionvy, 1, cur_ntr, 1, NT); sectionvy = NULL; }
+    if (sectionvydiff) { free_matrix(sectionvydiff, 1, cur_ntr, 1, NT); sectionvydiff = NULL; }
+    if (sectionvydata) { free_matrix(sectionvydata, 1, cur_ntr, 1, NT); sectionvydata = NULL; }
+    if (sectionvydiffold) { free_matrix(sectionvydiffold, 1, cur_ntr, 1, NT); sectionvydiffold = NULL; }
+    cur_ntr = 0;
+}
+
+void refh_free(void)
+{
+    if (!alive) return;
+    harness_free_shot();
+    free_matrix(pvy, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(psxy, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(psyz, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(pvyp1, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(pvym1, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(uy, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(uyx, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(utty, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(prho, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(pu, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(puip, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(pujp, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(absorb_coeff, 1, NY, 1, NX);
+    free_matrix(Ws, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(Wr, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(We, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(g_u_shot, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(g_rho_shot, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(hessian_u, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(hessian_rho, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    if (L) {
+        free_f3tensor(pr, -nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        free_f3tensor(pp, -nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        free_f3tensor(pq, -nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        free_f3tensor(dip, -nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        free_f3tensor(d, -nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        free_f3tensor(e, -nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        free_matrix(ptaus, -nd + 1, NY + nd, -nd + 1, NX + nd);
+        free_matrix(ptausipjp, -nd + 1, NY + nd, -nd + 1, NX + nd);
+        free_matrix(fipjp, -nd + 1, NY + nd, -nd + 1, NX + nd);
+        free_matrix(f, -nd + 1, NY + nd, -nd + 1, NX + nd);
+        free_matrix(g, -nd + 1, NY + nd, -nd + 1, NX + nd);
+        free_vector(peta, 1, L); free_vector(etaip, 1, L); free_vector(etajm, 1, L);
+        free_vector(bip, 1, L); free_vector(bjm, 1, L); free_vector(cip, 1, L); free_vector(cjm, 1, L);
+        free_vector(FL, 1, L);
+    }
+    free_vector(hc, 0, 6);
+    if (FW > 0) {
+        free_vector(d_x, 1, 2 * FW); free_vector(K_x, 1, 2 * FW); free_vector(alpha_prime_x, 1, 2 * FW);
+        free_vector(a_x, 1, 2 * FW); free_vector(b_x, 1, 2 * FW);
+        free_vector(d_x_half, 1, 2 * FW); free_vector(K_x_half, 1, 2 * FW); free_vector(alpha_prime_x_half, 1, 2 * FW);
+        free_vector(a_x_half, 1, 2 * FW); free_vector(b_x_half, 1, 2 * FW);
+        free_vector(d_y, 1, 2 * FW); free_vector(K_y, 1, 2 * FW); free_vector(alpha_prime_y, 1, 2 * FW);
+        free_vector(a_y, 1, 2 * FW); free_vector(b_y, 1, 2 * FW);
+        free_vector(d_y_half, 1, 2 * FW); free_vector(K_y_half, 1, 2 * FW); free_vector(alpha_prime_y_half, 1, 2 * FW);
+        free_vector(a_y_half, 1, 2 * FW); free_vector(b_y_half, 1, 2 * FW);
+        free_matrix(psi_syz_y, 1, 2 * FW, 1, NX);
+        free_matrix(psi_sxy_x, 1, NY, 1, 2 * FW);
+        free_matrix(psi_vyy, 1, 2 * FW, 1, NX);
+        free_matrix(psi_vyx, 1, NY, 1, 2 * FW);
+    }
+    if (fwd_stored) {
+        free_vector(fwd_rho_y, 1, NX * NY * NT);
+        free_vector(fwd_y, 1, NX * NY * NT);
+        free_vector(fwd_u, 1, NX * NY * NT);
+        fwd_stored = 0;
+    }
+    if (hess_alloc) {
+        free_f3tensor(hess_eyy, 1, NY, 1, NX, 1, NT);
+        free_f3tensor(hess_eyx, 1, NY, 1, NX, 1, NT);
+        free_f3tensor(hess_utty, 1, NY, 1, NX, 1, NT);
+        hess_alloc = 0;
+    }
+    alive = 0;
+}
+
+/* Sets the reference globals for one rank and builds every coefficient the
+ * time loop consumes, in the order of denise.c:598-627 and :726-743. */
+int refh_init(const refh_params *p, const float *vs, const float *rho, const float *qs)
+{
+    int i, j, l;
+    refh_free();
+    FP = stderr;
+    NX = NXG = p->nx; NY = NYG = p->ny; NT = p->nt;
+    FDORDER = p->fdorder; MAXRELERROR = p->maxrelerror; FW = p->fw; FREE_SURF = p->free_surf;
+    L = p->l; QUELLART = p->quellart; EPRECOND = p->eprecond;
+    DH = p->dh; DT = p->dt; DAMPING = p->damping; FPML = p->fpml; npower = p->npower; k_max_PML = p->k_max_pml;
+    TIME = NT * DT;
+    BOUNDARY = 0; IDX = IDY = 1; NPROCX = NPROCY = 1; NP = NPROC = 1; MYID = 0;
+    POS[1] = POS[2] = 0; INDEX[1] = INDEX[2] = INDEX[3] = INDEX[4] = 0;
+    IENDX = NX; IENDY = NY;
+    INVMAT1 = 1; INVMAT = 0; GRAD_FORM = 2; QUELLTYPB = 2; DTINV = 1; SEISMO = 1; NDT = 1; HESSIAN = 0;
+    TRKILL = 0; TIMEWIN = 0; RTM = 0; OFFSET_MUTE = 0; NORMALIZE = 0;
+    if (L > 0) {
+        FL = vector(1, L);
+        for (l = 1; l <= L; l++) FL[l] = p->fl[l - 1];
+    }
+    nd = FDORDER / 2 + 1;
+
+    pvy = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    psxy = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    psyz = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    pvyp1 = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    pvym1 = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    uy = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    uyx = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    utty = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    prho = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    pu = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    puip = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    pujp = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    absorb_coeff = matrix(1, NY, 1, NX);
+    Ws = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    Wr = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    We = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    g_u_shot = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    g_rho_shot = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    hessian_u = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    hessian_rho = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    if (L) {
+        pr = f3tensor(-nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        pp = f3tensor(-nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        pq = f3tensor(-nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        dip = f3tensor(-nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        d = f3tensor(-nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        e = f3tensor(-nd + 1, NY + nd, -nd + 1, NX + nd, 1, L);
+        ptaus = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+        ptausipjp = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+        fipjp = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+        f = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+        g = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+        peta = vector(1, L); etaip = vector(1, L); etajm = vector(1, L);
+        bip = vector(1, L); bjm = vector(1, L); cip = vector(1, L); cjm = vector(1, L);
+    }
+    /* CPML arrays: denise.c:528-555 */
+    if (FW > 0) {
+        d_x = vector(1, 2 * FW); K_x = vector(1, 2 * FW); alpha_prime_x = vector(1, 2 * FW);
+        a_x = vector(1, 2 * FW); b_x = vector(1, 2 * FW);
+        d_x_half = vector(1, 2 * FW); K_x_half = vector(1, 2 * FW); alpha_prime_x_half = vector(1, 2 * FW);
+        a_x_half = vector(1, 2 * FW); b_x_half = vector(1, 2 * FW);
+        d_y = vector(1, 2 * FW); K_y = vector(1, 2 * FW); alpha_prime_y = vector(1, 2 * FW);
+        a_y = vector(1, 2 * FW); b_y = vector(1, 2 * FW);
+        d_y_half = vector(1, 2 * FW); K_y_half = vector(1, 2 * FW); alpha_prime_y_half = vector(1, 2 * FW);
+        a_y_half = vector(1, 2 * FW); b_y_half = vector(1, 2 * FW);
+        psi_syz_y = matrix(1, 2 * FW, 1, NX);
+        psi_sxy_x = matrix(1, NY, 1, 2 * FW);
+        psi_vyy = matrix(1, 2 * FW, 1, NX);
+        psi_vyx = matrix(1, NY, 1, 2 * FW);
+    }
+    alive = 1;
+
+    hc = holbergcoeff();                                  /* denise.c:598 */
+
+    /* model: readmod.c:82-99 (u=vs, rho, taus=2/qs; eta=DT/pts) */
+    for (j = 1; j <= NY; j++)
+        for (i = 1; i <= NX; i++) {
+            pu[j][i] = vs[(j - 1) * NX + (i - 1)];
+            prho[j][i] = rho[(j - 1) * NX + (i - 1)];
+            if (L) ptaus[j][i] = 2.0 / qs[(j - 1) * NX + (i - 1)];
+        }
+    if (L) {
+        for (l = 1; l <= L; l++) {
+            float pts = 1.0 / (2.0 * PI * FL[l]);
+            peta[l] = DT / pts;
+        }
+    }
+
+    if (FW > 0)                                           /* denise.c:626-627 */
+        PML_pro(d_x, K_x, alpha_prime_x, a_x, b_x, d_x_half, K_x_half, alpha_prime_x_half, a_x_half, b_x_half,
+                d_y, K_y, alpha_prime_y, a_y, b_y, d_y_half, K_y_half, alpha_prime_y_half, a_y_half, b_y_half);
+
+    /* per-iteration preparation: denise.c:726-743 */
+    if (L) matcopy(prho, pu, ptaus);
+    else matcopy_elastic(prho, pu);
+    av_mue(pu, puip, pujp, prho);
+    if (L) av_tau(ptaus, ptausipjp);
+    if (L) prepare_update_s(etajm, etaip, peta, fipjp, pujp, puip, prho, ptaus, ptausipjp, f, g, bip, bjm, cip, cjm, dip, d, e);
+
+    /* normalisers: denise.c:778-816 (first iteration) */
+    {
+        float Vs_avg = 0.0, rho_avg = 0.0;
+        int Lcount = 1;
+        for (i = 1; i <= NX; i = i + IDX)
+            for (j = 1; j <= NY; j = j + IDY) {
+                Vs_avg += pu[j][i];
+                rho_avg += prho[j][i];
+                Lcount++;
+            }
+        Lcount--;
+        Vs_avg /= Lcount;
+        rho_avg /= Lcount;
+        C_vs = Vs_avg;
+        C_rho = rho_avg;
+    }
+    /* Hessian accumulators start at zero (matrix() zero-fills; denise.c:673-674) */
+    return 0;
+}
+
+/* Coefficient export (for parity of the product's own host-side setup). */
+void refh_get_hc(float *out7) { int i; for (i = 0; i <= 6; i++) out7[i] = hc[i]; }
+void refh_get_cnorm(float *out2) { out2[0] = C_vs; out2[1] = C_rho; }
+
+/* which: 0..9 = K_x a_x b_x K_x_half a_x_half b_x_half K_y a_y b_y K_y_half;
+ * 10 a_y_half 11 b_y_half 12 d_x 13 d_x_half 14 d_y 15 d_y_half */
+int refh_get_pml(int which, float *out)
+{
+    float *v[] = {K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half,
+                  d_x, d_x_half, d_y, d_y_half};
+    int i;
+    if (FW <= 0 || which < 0 || which > 15) return -1;
+    for (i = 1; i <= 2 * FW; i++) out[i - 1] = v[which][i];
+    return 0;
+}
+
+/* Dense [NY][NX] export of a grid field.
+ * 0 vy 1 sxy 2 syz 3 vyp1 4 uy 5 uyx 6 uip 7 ujp 8 rho 9 u(vs) 10 fipjp 11 f
+ * 12 Ws 13 Wr 14 We 15 g_u_shot 16 g_rho_shot 17 hessian_u 18 hessian_rho 19 taus 20 tausipjp
+ * 100+l: r[.][.][l+1]; 200+l: q[.][.][l+1]; 300+l: dip[l+1]; 400+l: d[l+1] */
+int refh_get_field(int which, float *out)
+{
+    float **m = NULL;
+    float ***t = NULL;
+    int i, j, l = 0;
+    switch (which) {
+    case 0: m = pvy; break;  case 1: m = psxy; break; case 2: m = psyz; break;
+    case 3: m = pvyp1; break; case 4: m = uy; break; case 5: m = uyx; break;
+    case 6: m = puip; break; case 7: m = pujp; break; case 8: m = prho; break;
+    case 9: m = pu; break;
+    case 10: m = L ? fipjp : NULL; break; case 11: m = L ? f : NULL; break;
+    case 12: m = Ws; break; case 13: m = Wr; break; case 14: m = We; break;
+    case 15: m = g_u_shot; break; case 16: m = g_rho_shot; break;
+    case 17: m = hessian_u; break; case 18: m = hessian_rho; break;
+    case 19: m = L ? ptaus : NULL; break; case 20: m = L ? ptausipjp : NULL; break;
+    default:
+        if (!L) return -1;
+        l = which % 100 + 1;
+        if (l > L) return -1;
+        if (which >= 100 && which < 200) t = pr;
+        else if (which >= 200 && which < 300) t = pq;
+        else if (which >= 300 && which < 400) t = dip;
+        else if (which >= 400 && which < 500) t = d;
+        else return -1;
+    }
+    if (!m && !t) return -1;
+    for (j = 1; j <= NY; j++)
+        for (i = 1; i <= NX; i++)
+            out[(j - 1) * NX + (i - 1)] = m ? m[j][i] : t[j][i][l];
+    return 0;
+}
+
+void refh_get_sls(float *bip_o, float *bjm_o, float *cip_o, float *cjm_o)
+{
+    int l;
+    for (l = 1; l <= L; l++) { bip_o[l - 1] = bip[l]; bjm_o[l - 1] = bjm[l]; cip_o[l - 1] = cip[l]; cjm_o[l - 1] = cjm[l]; }
+}
+
+/* psi export: 0 psi_sxy_x [NY][2FW], 1 psi_vyx [NY][2FW], 2 psi_syz_y [2FW][NX], 3 psi_vyy [2FW][NX] */
+int refh_get_psi(int which, float *out)
+{
+    int i, j;
+    if (FW <= 0) return -1;
+    if (which == 0 || which == 1) {
+        float **m = which == 0 ? psi_sxy_x : psi_vyx;
+        for (j = 1; j <= NY; j++) for (i = 1; i <= 2 * FW; i++) out[(j - 1) * 2 * FW + i - 1] = m[j][i];
+    } else if (which == 2 || which == 3) {
+        float **m = which == 2 ? psi_syz_y : psi_vyy;
+        for (j = 1; j <= 2 * FW; j++) for (i = 1; i <= NX; i++) out[(j - 1) * NX + i - 1] = m[j][i];
+    } else return -1;
+    return 0;
+}
+
+/* Ricker (or other QUELLART) wavelets through the reference's wavelet():
+ * srcpos rows 4..6 = tshift, fc, amp (wavelet.c:33-45). out: [nsrc][NT] */
+int refh_wavelet(int nsrc, const float *srcpos8, float *out)
+{
+    float **sp = matrix(1, 8, 1, nsrc);
+    float **sig;
+    int k, r, n;
+    for (r = 1; r <= 8; r++) for (k = 1; k <= nsrc; k++) sp[r][k] = srcpos8[(r - 1) * nsrc + (k - 1)];
+    sig = wavelet(sp, nsrc, 1);
+    for (k = 1; k <= nsrc; k++) for (n = 1; n <= NT; n++) out[(k - 1) * NT + (n - 1)] = sig[k][n];
+    free_matrix(sig, 1, nsrc, 1, NT);
+    free_matrix(sp, 1, 8, 1, nsrc);
+    return 0;
+}
+
+static void zero_state(void)
+{
+    if (L) zero_fdveps_visc(-nd + 1, NY + nd, -nd + 1, NX + nd, pvy, psyz, psxy, uy, pvyp1,
+                            psi_sxy_x, psi_vyx, psi_syz_y, psi_vyy, pr, pp, pq);
+    else zero_fdveps(-nd + 1, NY + nd, -nd + 1, NX + nd, pvy, psyz, psxy, uy, pvyp1,
+                     psi_sxy_x, psi_vyx, psi_syz_y, psi_vyy);
+}
+
+static void step_stress(void)
+{
+    if (L)
+        update_s_visc_PML(1, NX, 1, NY, pvy, uy, uyx, psyz, psxy, pujp, puip, prho, hc, 0,
+                          pr, pp, pq, fipjp, f, g, bip, bjm, cip, cjm, d, e, dip,
+                          K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half,
+                          psi_vyy, psi_vyx);
+    else
+        update_s_elastic_PML(1, NX, 1, NY, pvy, uy, uyx, psyz, psxy, pu, puip, pujp, absorb_coeff, prho, hc, 0,
+                             K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half,
+                             psi_vyy, psi_vyx);
+}
+
+/*
+ * One shot forward: denise.c:1126-1346.
+ *   srcpos8: [8][nsrc] rows as srcpos_loc (grid x, grid y, 0, tshift, fc, amp, angle, type)
+ *   signals: [nsrc][NT] source time functions (or NULL -> reference wavelet())
+ *   recpos:  [2][ntr] grid x, grid y
+ *   nsteps:  number of steps to run (<= NT); store: keep forward_prop_* for the adjoint
+ *   hessian: run hess_save each step and hessian() at the end (denise.c:1312-1315, :1350-1352)
+ *   seis:    [ntr][NT] output (columns beyond nsteps stay 0)
+ */
+int refh_forward(int nsrc, const float *srcpos8, const float *signals_in, int ntr, const int *recpos,
+                 int nsteps, int store, int hessian_on, float *seis)
+{
+    float **sp, **signals;
+    int i, j, k, r, nt, hin, hin1, imat, imat1, imat2;
+    if (!alive) return -1;
+    if (nsteps > NT) nsteps = NT;
+    harness_free_shot();
+    cur_ntr = ntr;
+    recpos_loc = imatrix(1, 3, 1, ntr > 0 ? ntr : 1);
+    for (k = 1; k <= ntr; k++) {
+        recpos_loc[1][k] = recpos[k - 1];
+        recpos_loc[2][k] = recpos[ntr + k - 1];
+        recpos_loc[3][k] = k;
+    }
+    sectionvy = matrix(1, ntr > 0 ? ntr : 1, 1, NT);
+    cur_ntr = ntr > 0 ? ntr : 1;
+    sp = matrix(1, 8, 1, nsrc);
+    for (r = 1; r <= 8; r++) for (k = 1; k <= nsrc; k++) sp[r][k] = srcpos8[(r - 1) * nsrc + (k - 1)];
+    if (signals_in) {
+        signals = matrix(1, nsrc, 1, NT);
+        for (k = 1; k <= nsrc; k++) for (nt = 1; nt <= NT; nt++) signals[k][nt] = signals_in[(k - 1) * NT + nt - 1];
+    } else {
+        signals = wavelet(sp, nsrc, 1);
+    }
+
+    zero_state();
+    /* per-shot gradient / energy accumulators: denise.c:1138-1161 */
+    for (i = 1; i <= NX; i++)
+        for (j = 1; j <= NY; j++) {
+            g_rho_shot[j][i] = 0.0; g_u_shot[j][i] = 0.0;
+            Ws[j][i] = 0.0; Wr[j][i] = 0.0; We[j][i] = 0.0;
+        }
+    if (store && !fwd_stored) {
+        fwd_rho_y = vector(1, NX * NY * NT);
+        fwd_y = vector(1, NX * NY * NT);
+        fwd_u = vector(1, NX * NY * NT);
+        fwd_stored = 1;
+    }
+    if (hessian_on && !hess_alloc) {
+        hess_eyy = f3tensor(1, NY, 1, NX, 1, NT);
+        hess_eyx = f3tensor(1, NY, 1, NX, 1, NT);
+        hess_utty = f3tensor(1, NY, 1, NX, 1, NT);
+        hess_alloc = 1;
+    }
+    hin = 1; hin1 = 1; imat = 1; imat1 = 1; imat2 = 1;
+    for (nt = 1; nt <= nsteps; nt++) {
+        update_v_PML(1, NX, 1, NY, nt, pvy, pvyp1, pvym1, utty, psyz, psxy, prho, sp, signals, nsrc, absorb_coeff,
+                     hc, 0, 0, K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half,
+                     b_y_half, psi_syz_y, psi_sxy_x);
+        step_stress();
+        if (ntr > 0) seismo_ssg(nt, ntr, recpos_loc, sectionvy, pvy, psyz, pu, hc);
+        if (nt == hin1) {
+            if (store) {                                  /* denise.c:1261-1301 */
+                for (i = 1; i <= NX; i++) for (j = 1; j <= NY; j++) fwd_rho_y[imat1++] = pvyp1[j][i];
+                for (i = 1; i <= NX; i++) for (j = 1; j <= NY; j++) fwd_y[imat++] = uy[j][i];
+                for (i = 1; i <= NX; i++) for (j = 1; j <= NY; j++) fwd_u[imat2++] = uyx[j][i];
+            }
+            if (hessian_on) hess_save(hin, uy, uyx, pvyp1, hess_eyy, hess_eyx, hess_utty);
+            if ((EPRECOND == 1) || (EPRECOND == 3)) eprecond(Ws, pvy);
+            hin++;
+            hin1 = hin1 + DTINV;
+        }
+    }
+    if (hessian_on) hessian(nsteps, hess_eyy, hess_eyx, hess_utty, hessian_u, hessian_rho);
+    for (k = 1; k <= ntr; k++) for (nt = 1; nt <= NT; nt++) seis[(k - 1) * NT + nt - 1] = sectionvy[k][nt];
+    free_matrix(signals, 1, nsrc, 1, NT);
+    free_matrix(sp, 1, 8, 1, nsrc);
+    return 0;
+}
+
+/* Residual and L2 (calc_res.c, LNORM=2, GRAD_FORM=2): obs [ntr][NT]; res out [ntr][NT]
+ * (time-reversed); the reference also overwrites obs sample 1 with the synthetic one. */
+int refh_residual(const float *obs, float *res, double *l2)
+{
+    int k, nt, ntr = cur_ntr;
+    if (!sectionvy) return -1;
+    sectionvydata = matrix(1, ntr, 1, NT);
+    sectionvydiff = matrix(1, ntr, 1, NT);
+    sectionvydiffold = matrix(1, ntr, 1, NT);
+    for (k = 1; k <= ntr; k++) for (nt = 1; nt <= NT; nt++) sectionvydata[k][nt] = obs[(k - 1) * NT + nt - 1];
+    {
+        int **recpos_glob = recpos_loc;
+        float **srcdummy = matrix(1, 8, 1, 1);
+        *l2 = calc_res(sectionvydata, sectionvy, sectionvydiff, sectionvydiffold, ntr, NT, 2, 0.0, 0, 1, 1, ntr,
+                       recpos_glob, recpos_loc, srcdummy, 1, 1, 1);
+        free_matrix(srcdummy, 1, 8, 1, 1);
+    }
+    for (k = 1; k <= ntr; k++) for (nt = 1; nt <= NT; nt++) res[(k - 1) * NT + nt - 1] = sectionvydiff[k][nt];
+    return 0;
+}
+
+/*
+ * Adjoint loop with correlation: denise.c:1452-1654, nsteps <= NT
+ * (for a full run nsteps = NT; the snapshot index follows :1582 with NTDTINV = nsteps).
+ * adj: [ntr][NT] adjoint source (time-reversed residual) or NULL -> last refh_residual output.
+ */
+int refh_adjoint(const float *adj, int nsteps)
+{
+    int i, j, k, nt, hin, imat, ntr = cur_ntr, NTD;
+    float **srcpos_loc_back, **sig;
+    if (!fwd_stored) return -1;
+    if (nsteps > NT) nsteps = NT;
+    NTD = nsteps;
+    srcpos_loc_back = matrix(1, 6, 1, ntr);
+    for (i = 1; i <= ntr; i++) {
+        srcpos_loc_back[1][i] = recpos_loc[1][i];
+        srcpos_loc_back[2][i] = recpos_loc[2][i];
+    }
+    sig = matrix(1, ntr, 1, NT);
+    for (k = 1; k <= ntr; k++) for (nt = 1; nt <= NT; nt++)
+        sig[k][nt] = adj ? adj[(k - 1) * NT + nt - 1] : sectionvydiff[k][nt];
+    zero_state();
+    hin = 1;
+    for (nt = 1; nt <= nsteps; nt++) {
+        update_v_PML(1, NX, 1, NY, nt, pvy, pvyp1, pvym1, utty, psyz, psxy, prho, srcpos_loc_back, sig, ntr,
+                     absorb_coeff, hc, 0, 1, K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half,
+                     a_y_half, b_y_half, psi_syz_y, psi_sxy_x);
+        step_stress();
+        /* DTINV=1: every step is a stored step (DTINV_help[NT-nt+1]==1) */
+        imat = ((NX * NY * NTD) - hin * NX * NY) + 1;
+        for (i = 1; i <= NX; i++)
+            for (j = 1; j <= NY; j++) {
+                g_rho_shot[j][i] += (pvyp1[j][i] * fwd_rho_y[imat]);
+                g_u_shot[j][i] += (fwd_u[imat] * psxy[j][i]) + (fwd_y[imat] * psyz[j][i]);
+                imat++;
+            }
+        if (EPRECOND == 1) eprecond(Wr, pvy);
+        hin++;
+    }
+    free_matrix(sig, 1, ntr, 1, NT);
+    free_matrix(srcpos_loc_back, 1, 6, 1, ntr);
+    return 0;
+}
+
+/* eprecond1 + per-shot scaling: denise.c:1665-1678 */
+int refh_eprecond_scale(void)
+{
+    int i, j;
+    if ((EPRECOND == 1) || (EPRECOND == 3)) {
+        eprecond1(We, Ws, Wr);
+        for (i = 1; i <= NX; i = i + IDX)
+            for (j = 1; j <= NY; j = j + IDY) {
+                g_u_shot[j][i] = g_u_shot[j][i] / (We[j][i] * C_vs * C_vs);
+                g_rho_shot[j][i] = g_rho_shot[j][i] / (We[j][i] * C_rho * C_rho);
+            }
+    }
+    return 0;
+}
+
+/* Gradient conversion, denise.c:1743-1813 (INVMAT=0, INVMAT1=1):
+ * waveconv_u / waveconv_rho are the shot sums [NY][NX]; outputs g_vs, g_rho. */
+int refh_convert(const float *wu, const float *wrho, float *g_vs, float *g_rho)
+{
+    int i, j;
+    for (i = 1; i <= NX; i++)
+        for (j = 1; j <= NY; j++) {
+            int o = (j - 1) * NX + (i - 1);
+            float waveconv_u = wu[o], waveconv_rho = wrho[o];
+            float waveconv_mu, waveconv_rho_s;
+            waveconv_mu = -DT * waveconv_u;
+            waveconv_u = 2.0 * prho[j][i] * pu[j][i] * waveconv_mu;
+            waveconv_rho_s = -DT * waveconv_rho;
+            waveconv_rho = (pu[j][i] * pu[j][i] * waveconv_mu) + waveconv_rho_s;
+            g_vs[o] = waveconv_u;
+            g_rho[o] = waveconv_rho;
+        }
+    return 0;
+}
+
+/* Hessian output conversion, hessian_out.c:20-31 (INVMAT1=1), applied to the
+ * accumulated hessian_u / hessian_rho; outputs H_vs, H_rho. */
+int refh_hessian_out(float *h_vs, float *h_rho)
+{
+    int i, j;
+    for (i = 1; i <= NX; i++)
+        for (j = 1; j <= NY; j++) {
+            float hu = hessian_u[j][i], hr = hessian_rho[j][i];
+            hr += pu[j][i] * pu[j][i] * pu[j][i] * pu[j][i] * hu;
+            hu = 4.0 * prho[j][i] * prho[j][i] * pu[j][i] * pu[j][i] * hu;
+            h_vs[(j - 1) * NX + i - 1] = hu;
+            h_rho[(j - 1) * NX + i - 1] = hr;
+        }
+    return 0;
+}
+
+/* P-SV explosive source of the reference (psource.c), run in isolation on
+ * dense [NY][NX] sxx/syy fields. srcpos8 [8][nsrc], signals [nsrc][NT]. */
+int refh_psource(int nt, float *sxx, float *syy, int nsrc, const float *srcpos8, const float *signals_in)
+{
+    float **a = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd), **b = matrix(-nd + 1, NY + nd, -nd + 1, NX + nd);
+    float **sp = matrix(1, 8, 1, nsrc), **sig = matrix(1, nsrc, 1, NT);
+    int i, j, k, r, n;
+    for (j = 1; j <= NY; j++) for (i = 1; i <= NX; i++) { a[j][i] = sxx[(j - 1) * NX + i - 1]; b[j][i] = syy[(j - 1) * NX + i - 1]; }
+    for (r = 1; r <= 8; r++) for (k = 1; k <= nsrc; k++) sp[r][k] = srcpos8[(r - 1) * nsrc + (k - 1)];
+    for (k = 1; k <= nsrc; k++) for (n = 1; n <= NT; n++) sig[k][n] = signals_in[(k - 1) * NT + n - 1];
+    psource(nt, a, b, sp, sig, nsrc);
+    for (j = 1; j <= NY; j++) for (i = 1; i <= NX; i++) { sxx[(j - 1) * NX + i - 1] = a[j][i]; syy[(j - 1) * NX + i - 1] = b[j][i]; }
+    free_matrix(a, -nd + 1, NY + nd, -nd + 1, NX + nd); free_matrix(b, -nd + 1, NY + nd, -nd + 1, NX + nd);
+    free_matrix(sp, 1, 8, 1, nsrc); free_matrix(sig, 1, nsrc, 1, NT);
+    return 0;
+}
