@@ -1,0 +1,44 @@
+/* dsh_dispatch.h — kernel selection by FD order, relaxation count and mode. */
+#pragma once
+#include "dsh_kernels.cuh"
+
+namespace dsh {
+using KFn = void (*)(StepArgs, int);
+
+#define DSH_DECLARE_FD(N)                  \
+    KFn v_kernel_fd##N(int flags);         \
+    KFn s_kernel_fd##N(int l, int flags);
+DSH_DECLARE_FD(2)
+DSH_DECLARE_FD(4)
+DSH_DECLARE_FD(6)
+DSH_DECLARE_FD(8)
+DSH_DECLARE_FD(10)
+DSH_DECLARE_FD(12)
+#undef DSH_DECLARE_FD
+
+inline KFn v_kernel(int fdo, int flags)
+{
+    switch (fdo) {
+    case 2: return v_kernel_fd2(flags);
+    case 4: return v_kernel_fd4(flags);
+    case 6: return v_kernel_fd6(flags);
+    case 8: return v_kernel_fd8(flags);
+    case 10: return v_kernel_fd10(flags);
+    case 12: return v_kernel_fd12(flags);
+    default: return nullptr;
+    }
+}
+
+inline KFn s_kernel(int fdo, int l, int flags)
+{
+    switch (fdo) {
+    case 2: return s_kernel_fd2(l, flags);
+    case 4: return s_kernel_fd4(l, flags);
+    case 6: return s_kernel_fd6(l, flags);
+    case 8: return s_kernel_fd8(l, flags);
+    case 10: return s_kernel_fd10(l, flags);
+    case 12: return s_kernel_fd12(l, flags);
+    default: return nullptr;
+    }
+}
+}  // namespace dsh

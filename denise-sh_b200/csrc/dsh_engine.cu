@@ -1,0 +1,1138 @@
+/*
+ * dsh_engine.cu — device-resident engine behind include/dsh.h.
+ *
+ * One context = one model on one GPU with `max_shots` shot slots advanced
+ * together (grid z = slot).  A pass (forward, forward with storage, forward
+ * with Hessian accumulation, adjoint) is a loop over NT steps of
+ *     v_step -> inject_sample -> s_step
+ * replayed from a CUDA graph that holds `chunk` steps; the kernels read the
+ * step number from a device counter that the graph's last node advances, so
+ * one small graph serves every step of every pass.
+ *
+ * Reference correspondence (src/...): forward loop denise.c:1179-1346,
+ * residual calc_res.c:94-232, adjoint loop denise.c:1452-1654, energy
+ * preconditioning eprecond1.c + denise.c:1665-1678, shot sum :1689-1694,
+ * conversion :1743-1813, Hessian hessian.c:91-94 + hessian_out.c:20-31.
+ */
+#include "dsh.h"
+#include "dsh_dispatch.h"
+#include "dsh_setup.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <vector>
+
+using namespace dsh;
+
+namespace {
+
+enum Pass { P_FWD_PLAIN = 0, P_FWD_STORE = 1, P_FWD_HESS = 2, P_ADJ = 3 };
+
+constexpr int RED_BLOCKS = 296;        /* 2 x 148 SMs for reductions */
+constexpr int RED_THREADS = 256;
+
+long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+/* ---------------- epilogue kernels ---------------- */
+
+/* Residual of one slot, stored as the adjoint source of step t (1-based):
+ * res[r][t-1] = syn(NT-t+1) - obs(NT-t+1), with the first observed sample
+ * replaced by the synthetic one (calc_res.c:115,172-177).  Also the per-block
+ * partial sums of res^2 (double) for a deterministic L2. */
+__global__ void residual_kernel(int nt_total, const int *rec_off, const float *seis, const long long *seis_off,
+                                const float *obs, const long long *obs_off, float *res, double *part)
+{
+    const int s = blockIdx.y;
+    const int ntr = rec_off[s + 1] - rec_off[s];
+    const long long n = (long long)ntr * nt_total;
+    const float *syn = seis + seis_off[s];
+    const float *ob = obs + obs_off[s];
+    float *rs = res + seis_off[s];
+    double acc = 0.0;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx / nt_total);
+        const int t = (int)(idx % nt_total) + 1;       /* adjoint step */
+        const int tf = nt_total - t + 1;                /* forward sample */
+        const float sy = syn[(long long)(tf - 1) * ntr + r];
+        const float od = (tf == 1) ? sy : ob[(long long)r * nt_total + (tf - 1)];
+        const float v = sy - od;
+        rs[(long long)r * nt_total + (t - 1)] = v;
+        acc += (double)v * (double)v;
+    }
+    __shared__ double sh[RED_THREADS];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(long long)s * gridDim.x + blockIdx.x] = sh[0];
+}
+
+__global__ void reduce_parts(const double *part, int nparts, int nslots, double *out)
+{
+    const int s = blockIdx.x;
+    __shared__ double sh[RED_THREADS];
+    double acc = 0.0;
+    for (int k = threadIdx.x; k < nparts; k += blockDim.x) acc += part[(long long)s * nparts + k];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0 && s < nslots) out[s] = sh[0];
+}
+
+struct EpiArgs {
+    int nx, ny, pitch;
+    long long slot_stride;
+    float *ws, *wr, *we, *gu, *grho;
+    unsigned *wemax;
+    float cvs, crho, dh;
+    int eprecond;
+};
+
+/* We = sqrt(Ws*Wr) (EPRECOND=1) or sqrt(Ws)*(asinh((xmax-x)/y)-asinh((xmin-x)/y))
+ * (EPRECOND=3, Plessix & Mulder), and its maximum (eprecond1.c:17-57). */
+__global__ void eprecond_we_kernel(EpiArgs a)
+{
+    const int s = blockIdx.y;
+    const long long so = (long long)s * a.slot_stride;
+    const long long n = (long long)a.nx * a.ny;
+    float mx = 0.0f;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % a.nx) + 1, j = (int)(idx / a.nx) + 1;
+        const long long o = so + (long long)(j - 1) * a.pitch + (i - 1 + HX);
+        float we;
+        if (a.eprecond == 1) {
+            we = sqrtf(a.ws[o] * a.wr[o]);
+        } else {
+            const float x = i * a.dh, y = j * a.dh, xmin = a.dh, xmax = a.nx * a.dh;
+            we = (float)(sqrt((double)a.ws[o]) * (asinh((double)((xmax - x) / y)) - asinh((double)((xmin - x) / y))));
+        }
+        a.we[o] = we;
+        if (we > mx) mx = we;
+    }
+    /* float max of non-negative values == unsigned max of their bits */
+    for (int off = 16; off > 0; off >>= 1) mx = fmaxf(mx, __shfl_down_sync(0xffffffffu, mx, off));
+    if ((threadIdx.x & 31) == 0 && mx > 0.0f) atomicMax(a.wemax + s, __float_as_uint(mx));
+}
+
+/* We += 0.005*max(We); per-shot gradients /= We*C^2 (eprecond1.c:59-73, denise.c:1670-1675) */
+__global__ void eprecond_scale_kernel(EpiArgs a)
+{
+    const int s = blockIdx.y;
+    const long long so = (long long)s * a.slot_stride;
+    const long long n = (long long)a.nx * a.ny;
+    const float eps = 0.005f;
+    const float mx = __uint_as_float(a.wemax[s]);
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % a.nx) + 1, j = (int)(idx / a.nx) + 1;
+        const long long o = so + (long long)(j - 1) * a.pitch + (i - 1 + HX);
+        const float we = a.we[o] + (eps * mx);
+        a.we[o] = we;
+        a.gu[o] = a.gu[o] / (we * a.cvs * a.cvs);
+        a.grho[o] = a.grho[o] / (we * a.crho * a.crho);
+    }
+}
+
+/* sum += per-shot field, slots in shot order (denise.c:1689-1694) */
+__global__ void shot_sum_kernel(int nx, int ny, int pitch, long long slot_stride, int nslots, const float *a_u,
+                                const float *a_r, float *sum_u, float *sum_r)
+{
+    const long long n = (long long)nx * ny;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nx) + 1, j = (int)(idx / nx) + 1;
+        const long long o = (long long)(j - 1) * pitch + (i - 1 + HX);
+        float su = sum_u[o], sr = sum_r[o];
+        for (int s = 0; s < nslots; s++) {
+            su = su + a_u[(long long)s * slot_stride + o];
+            sr = sr + a_r[(long long)s * slot_stride + o];
+        }
+        sum_u[o] = su;
+        sum_r[o] = sr;
+    }
+}
+
+/* waveconv_mu = -DT*sum_u; g_vs = 2 rho vs mu (double, as the reference's
+ * double literal promotes it); g_rho = vs^2 mu - DT*sum_rho (denise.c:1752-1800) */
+__global__ void convert_kernel(int nx, int ny, int pitch, float dt, const float *vs, const float *rho,
+                               const float *sum_u, const float *sum_r, float *g_vs, float *g_rho)
+{
+    const long long n = (long long)nx * ny;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nx) + 1, j = (int)(idx / nx) + 1;
+        const long long o = (long long)(j - 1) * pitch + (i - 1 + HX);
+        const float u = vs[o], r = rho[o];
+        const float mu = -dt * sum_u[o];
+        const float gv = (float)(2.0 * (double)r * (double)u * (double)mu);
+        const float rho_s = -dt * sum_r[o];
+        const float gr = (u * u * mu) + rho_s;
+        g_vs[idx] = gv;
+        g_rho[idx] = gr;
+    }
+}
+
+/* hessian_out.c:20-31: H_rho += vs^4 H_mu; H_vs = 4 rho^2 vs^2 H_mu (double) */
+__global__ void hessian_convert_kernel(int nx, int ny, int pitch, const float *vs, const float *rho, const float *hu,
+                                       const float *hr, float *h_vs, float *h_rho)
+{
+    const long long n = (long long)nx * ny;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nx) + 1, j = (int)(idx / nx) + 1;
+        const long long o = (long long)(j - 1) * pitch + (i - 1 + HX);
+        const float u = vs[o], r = rho[o];
+        float a = hu[o], b = hr[o];
+        b += u * u * u * u * a;
+        a = (float)(4.0 * (double)r * (double)r * (double)u * (double)u * (double)a);
+        h_vs[idx] = a;
+        h_rho[idx] = b;
+    }
+}
+
+/* [NT][ntr] (device seismogram layout) -> [ntr][NT] */
+__global__ void seis_transpose_kernel(int nt_total, const int *rec_off, const float *in, const long long *in_off,
+                                      float *out, const long long *out_off)
+{
+    const int s = blockIdx.y;
+    const int ntr = rec_off[s + 1] - rec_off[s];
+    const long long n = (long long)ntr * nt_total;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx / nt_total), t = (int)(idx % nt_total);
+        out[out_off[s] + idx] = in[in_off[s] + (long long)t * ntr + r];
+    }
+}
+
+/* dense pitched interior field of slot s -> [ny][nx] */
+__global__ void gather_dense_kernel(int nx, int ny, int pitch, const float *src, float *dst)
+{
+    const long long n = (long long)nx * ny;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nx), j = (int)(idx / nx);
+        dst[idx] = src[(long long)j * pitch + i + HX];
+    }
+}
+
+__global__ void set_int_kernel(int *p, int v) { *p = v; }
+
+}  // namespace
+
+/* ======================= context ======================= */
+
+struct dsh_ctx {
+    dsh_params p;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    cudaStream_t own_st = nullptr;
+    int H = 0, hy = 0, pitch = 0, S = 1, chunk = 32;
+    long long fstride = 0, dstride = 0, slot_stride = 0;
+    long long o_vy, o_sxy, o_syz, o_r, o_q, o_pvxx, o_psxx, o_pvyy, o_psyy, o_state_end;
+    long long o_ws, o_wr, o_we, o_gu, o_grho, o_hu, o_hrho;
+    float *slab = nullptr;
+    float *model = nullptr;               /* brho uip ujp fipjp f dip[L] d[L] vs rho */
+    float *m_brho, *m_uip, *m_ujp, *m_fipjp, *m_f, *m_dip, *m_d, *m_vs, *m_rho;
+    float *pml = nullptr;
+    float *sums = nullptr;                /* sum_u, sum_rho, out_a, out_b (dense pitched) */
+    float hc[7] = {0}, bip[4] = {0}, bjm[4] = {0}, cip[4] = {0}, cjm[4] = {0}, cnorm[2] = {0};
+    int model_set = 0;
+    float *fwd = nullptr;
+    long long fwd_slot_stride = 0, fwd_step_stride = 0;
+    size_t fwd_bytes = 0;
+    /* geometry */
+    int *d_geo = nullptr;
+    long long geo_cap = 0;
+    int *d_fgrp_off, *d_agrp_off, *d_grp_pt, *d_grp_beg, *d_src_id, *d_rec_off, *d_rec_pt;
+    long long *d_offs = nullptr;          /* sig_off[S], seis_off[S], obs_off[S], out_off[S] */
+    float *d_sig = nullptr, *d_seis = nullptr, *d_res = nullptr, *d_obs = nullptr, *d_tmp = nullptr;
+    float *d_out = nullptr;               /* 2 x [ny][nx] dense outputs */
+    long long cap_sig = 0, cap_seis = 0, cap_obs = 0;
+    int geo_version = 0;
+    int *d_nt = nullptr, *d_status = nullptr;
+    double *d_part = nullptr, *d_l2 = nullptr;
+    unsigned *d_wemax = nullptr;
+    std::vector<int> ntr_b;
+    std::map<long long, cudaGraphExec_t> graphs;
+    cudaEvent_t ev[4];
+    dsh_stats stats;
+    long long launches = 0;
+    int last_cuda = 0;
+};
+
+static int fail_cuda(dsh_ctx *c, cudaError_t e)
+{
+    if (c) c->last_cuda = (int)e;
+    fprintf(stderr, "dsh: CUDA error %d (%s)\n", (int)e, cudaGetErrorString(e));
+    return DSH_ERR_CUDA;
+}
+#define CK(x)                                              \
+    do {                                                   \
+        cudaError_t e_ = (x);                              \
+        if (e_ != cudaSuccess) return fail_cuda(ctx, e_);  \
+    } while (0)
+
+extern "C" void dsh_params_default(dsh_params *p)
+{
+    memset(p, 0, sizeof(*p));
+    p->fdorder = 4;
+    p->maxrelerror = 1;
+    p->fw = 20;
+    p->free_surf = 1;
+    p->npower = 4.0f;
+    p->k_max_pml = 1.0f;
+    p->fpml = 30.0f;
+    p->quellart = 1;
+    p->eprecond = 1;
+    p->max_shots = 1;
+    p->compat_fd12 = 1;
+}
+
+extern "C" const char *dsh_error_string(int s)
+{
+    switch (s) {
+    case DSH_OK: return "ok";
+    case DSH_ERR_PARAM: return "invalid parameter";
+    case DSH_ERR_CUDA: return "CUDA error";
+    case DSH_ERR_OOM: return "out of device memory or budget";
+    case DSH_ERR_UNSTABLE: return "simulation is unstable (non-finite wavefield)";
+    case DSH_ERR_STATE: return "call out of order";
+    case DSH_ERR_TIMEOUT: return "device wait timed out";
+    default: return "unknown status";
+    }
+}
+
+static int check_params(const dsh_params *p)
+{
+    if (p->nx < 1 || p->ny < 1 || p->nt < 1) return DSH_ERR_PARAM;
+    if (p->fdorder < 2 || p->fdorder > 12 || (p->fdorder & 1)) return DSH_ERR_PARAM;
+    if (p->maxrelerror < 0 || p->maxrelerror > 4) return DSH_ERR_PARAM;
+    if (p->fw < 0 || p->fw > DSH_MAX_FW || p->fw > p->nx || p->fw > p->ny) return DSH_ERR_PARAM;
+    if (p->l < 0 || p->l > DSH_MAX_L) return DSH_ERR_PARAM;
+    if (!(p->dh > 0) || !(p->dt > 0)) return DSH_ERR_PARAM;
+    for (int l = 0; l < p->l; l++)
+        if (!(p->fl[l] > 0)) return DSH_ERR_PARAM;
+    if (p->eprecond != 0 && p->eprecond != 1 && p->eprecond != 3) return DSH_ERR_PARAM;
+    if (p->max_shots < 1 || p->max_shots > 65535) return DSH_ERR_PARAM;
+    if (p->quellart != 1 && p->quellart != 2 && p->quellart != 3 && p->quellart != 4 && p->quellart != 5 &&
+        p->quellart != 6)
+        return DSH_ERR_PARAM;
+    return DSH_OK;
+}
+
+extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
+{
+    int rc = check_params(p);
+    if (rc != DSH_OK) { if (status) *status = rc; return nullptr; }
+    dsh_ctx *ctx = new dsh_ctx();
+    ctx->p = *p;
+    ctx->dev = device;
+    auto bail = [&](int code) { if (status) *status = code; dsh_destroy(ctx); return (dsh_ctx *)nullptr; };
+    if (cudaSetDevice(device) != cudaSuccess) return bail(DSH_ERR_CUDA);
+    if (cudaStreamCreateWithFlags(&ctx->own_st, cudaStreamNonBlocking) != cudaSuccess) return bail(DSH_ERR_CUDA);
+    ctx->st = ctx->own_st;
+    for (int k = 0; k < 4; k++) cudaEventCreate(&ctx->ev[k]);
+    const int nx = p->nx, ny = p->ny, L = p->l, fw = p->fw;
+    ctx->H = p->fdorder / 2;
+    ctx->hy = ctx->H;
+    ctx->pitch = (int)round_up(nx + 32, 32);
+    ctx->S = p->max_shots;
+    ctx->fstride = round_up((long long)(ny + 2 * ctx->hy) * ctx->pitch, 32);
+    ctx->dstride = round_up((long long)ny * ctx->pitch, 32);
+    long long o = 0;
+    ctx->o_vy = o; o += ctx->fstride;
+    ctx->o_sxy = o; o += ctx->fstride;
+    ctx->o_syz = o; o += ctx->fstride;
+    ctx->o_r = o; o += (long long)L * ctx->dstride;
+    ctx->o_q = o; o += (long long)L * ctx->dstride;
+    ctx->o_pvxx = o; o += round_up((long long)ny * 2 * fw + 4, 32);
+    ctx->o_psxx = o; o += round_up((long long)ny * 2 * fw + 4, 32);
+    ctx->o_pvyy = o; o += round_up((long long)2 * fw * ctx->pitch + 4, 32);
+    ctx->o_psyy = o; o += round_up((long long)2 * fw * ctx->pitch + 4, 32);
+    ctx->o_state_end = o;
+    ctx->o_ws = o; o += ctx->dstride;
+    ctx->o_wr = o; o += ctx->dstride;
+    ctx->o_we = o; o += ctx->dstride;
+    ctx->o_gu = o; o += ctx->dstride;
+    ctx->o_grho = o; o += ctx->dstride;
+    ctx->o_hu = o; o += ctx->dstride;
+    ctx->o_hrho = o; o += ctx->dstride;
+    ctx->slot_stride = o;
+    if (cudaMalloc(&ctx->slab, (size_t)ctx->S * ctx->slot_stride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    const long long nmodel = (long long)(7 + 2 * L) * ctx->dstride;
+    if (cudaMalloc(&ctx->model, (size_t)nmodel * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    cudaMemset(ctx->model, 0, (size_t)nmodel * sizeof(float));
+    float *m = ctx->model;
+    ctx->m_brho = m; m += ctx->dstride;
+    ctx->m_uip = m; m += ctx->dstride;
+    ctx->m_ujp = m; m += ctx->dstride;
+    ctx->m_fipjp = m; m += ctx->dstride;
+    ctx->m_f = m; m += ctx->dstride;
+    ctx->m_dip = m; m += (long long)L * ctx->dstride;
+    ctx->m_d = m; m += (long long)L * ctx->dstride;
+    ctx->m_vs = m; m += ctx->dstride;
+    ctx->m_rho = m;
+    if (cudaMalloc(&ctx->pml, 12 * (size_t)(2 * DSH_MAX_FW + 1) * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->sums, 4 * (size_t)ctx->dstride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->d_out, 2 * (size_t)nx * ny * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->d_nt, 2 * sizeof(int)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    ctx->d_status = ctx->d_nt + 1;
+    cudaMemset(ctx->d_nt, 0, 2 * sizeof(int));
+    if (cudaMalloc(&ctx->d_part, (size_t)ctx->S * RED_BLOCKS * sizeof(double)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->d_l2, (size_t)ctx->S * sizeof(double)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->d_wemax, (size_t)ctx->S * sizeof(unsigned)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->d_offs, 4 * (size_t)ctx->S * sizeof(long long)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaDeviceSynchronize() != cudaSuccess) return bail(DSH_ERR_CUDA);
+    memset(&ctx->stats, 0, sizeof(ctx->stats));
+    if (status) *status = DSH_OK;
+    return ctx;
+}
+
+static void drop_graphs(dsh_ctx *ctx)
+{
+    for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
+    ctx->graphs.clear();
+}
+
+extern "C" int dsh_destroy(dsh_ctx *ctx)
+{
+    if (!ctx) return DSH_OK;
+    cudaSetDevice(ctx->dev);
+    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    drop_graphs(ctx);
+    cudaFree(ctx->slab); cudaFree(ctx->model); cudaFree(ctx->pml); cudaFree(ctx->sums); cudaFree(ctx->fwd);
+    cudaFree(ctx->d_geo); cudaFree(ctx->d_offs); cudaFree(ctx->d_sig); cudaFree(ctx->d_seis); cudaFree(ctx->d_res);
+    cudaFree(ctx->d_obs); cudaFree(ctx->d_tmp); cudaFree(ctx->d_out); cudaFree(ctx->d_nt); cudaFree(ctx->d_part); cudaFree(ctx->d_l2);
+    cudaFree(ctx->d_wemax);
+    for (int k = 0; k < 4; k++) if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+    if (ctx->own_st) cudaStreamDestroy(ctx->own_st);
+    delete ctx;
+    return DSH_OK;
+}
+
+static int upload_field(dsh_ctx *ctx, float *dst, const float *src)
+{
+    CK(cudaMemcpy2DAsync(dst + HX, (size_t)ctx->pitch * sizeof(float), src, (size_t)ctx->p.nx * sizeof(float),
+                         (size_t)ctx->p.nx * sizeof(float), ctx->p.ny, cudaMemcpyHostToDevice, ctx->st));
+    return DSH_OK;
+}
+
+extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, const float *qs)
+{
+    if (!ctx || !vs || !rho || (ctx->p.l > 0 && !qs)) return DSH_ERR_PARAM;
+    CK(cudaSetDevice(ctx->dev));
+    const dsh_params &p = ctx->p;
+    const int L = p.l;
+    const size_t n = (size_t)p.nx * p.ny;
+    for (size_t k = 0; k < n; k++) {
+        if (!std::isfinite(vs[k]) || !std::isfinite(rho[k]) || vs[k] < 0 || rho[k] < 0) return DSH_ERR_PARAM;
+        if (L > 0 && !(qs[k] > 0)) return DSH_ERR_PARAM;
+    }
+    std::vector<float> brho(n), uip(n), ujp(n), fipjp(L ? n : 1), f(L ? n : 1), dip(L ? n * L : 1), d(L ? n * L : 1);
+    if (dsh_setup_holberg(p.fdorder, p.maxrelerror, ctx->hc) != 0) return DSH_ERR_PARAM;
+    if (dsh_setup_model(p.nx, p.ny, L, p.fl, p.dt, vs, rho, qs, brho.data(), uip.data(), ujp.data(),
+                        L ? fipjp.data() : nullptr, L ? f.data() : nullptr, L ? dip.data() : nullptr,
+                        L ? d.data() : nullptr, ctx->bip, ctx->bjm, ctx->cip, ctx->cjm, ctx->cnorm) != 0)
+        return DSH_ERR_PARAM;
+    dsh_pml pml;
+    float damping = p.damping;
+    if (!(damping > 0)) damping = *std::max_element(vs, vs + n);
+    dsh_setup_pml(p.nx, p.ny, p.fw, p.dh, p.dt, damping, p.fpml, p.npower, p.k_max_pml, &pml);
+    const float *vecs[12] = {pml.K_x, pml.a_x, pml.b_x, pml.K_x_half, pml.a_x_half, pml.b_x_half,
+                             pml.K_y, pml.a_y, pml.b_y, pml.K_y_half, pml.a_y_half, pml.b_y_half};
+    const size_t vlen = 2 * DSH_MAX_FW + 1;
+    std::vector<float> pmlh(12 * vlen);
+    for (int k = 0; k < 12; k++) memcpy(&pmlh[k * vlen], vecs[k], vlen * sizeof(float));
+    CK(cudaMemcpyAsync(ctx->pml, pmlh.data(), pmlh.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    int rc;
+    if ((rc = upload_field(ctx, ctx->m_brho, brho.data())) != DSH_OK) return rc;
+    if ((rc = upload_field(ctx, ctx->m_uip, uip.data())) != DSH_OK) return rc;
+    if ((rc = upload_field(ctx, ctx->m_ujp, ujp.data())) != DSH_OK) return rc;
+    if ((rc = upload_field(ctx, ctx->m_vs, vs)) != DSH_OK) return rc;
+    if ((rc = upload_field(ctx, ctx->m_rho, rho)) != DSH_OK) return rc;
+    if (L > 0) {
+        if ((rc = upload_field(ctx, ctx->m_fipjp, fipjp.data())) != DSH_OK) return rc;
+        if ((rc = upload_field(ctx, ctx->m_f, f.data())) != DSH_OK) return rc;
+        for (int l = 0; l < L; l++) {
+            if ((rc = upload_field(ctx, ctx->m_dip + (long long)l * ctx->dstride, dip.data() + l * n)) != DSH_OK) return rc;
+            if ((rc = upload_field(ctx, ctx->m_d + (long long)l * ctx->dstride, d.data() + l * n)) != DSH_OK) return rc;
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->st));   /* host staging vectors go out of scope */
+    ctx->model_set = 1;
+    return DSH_OK;
+}
+
+/* ---------------- geometry of one batch ---------------- */
+
+static bool in_grid(const dsh_params &p, int i, int j) { return i >= 0 && i <= p.nx + 1 && j >= 0 && j <= p.ny + 1; }
+
+/* Uploads sources, receivers, forward signals and (optionally) observed data
+ * of shots[0..nb) into slots 0..nb). */
+static int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_host, const float *obs_dev,
+                        long long obs_dev_off)
+{
+    const dsh_params &p = ctx->p;
+    const int NT = p.nt;
+    std::vector<int> fgrp_off(nb + 1), agrp_off(nb + 1), rec_off(nb + 1), grp_pt, grp_beg, src_id, rec_pt;
+    std::vector<long long> sig_off(ctx->S, 0), seis_off(ctx->S, 0), obs_off(ctx->S, 0), out_off(ctx->S, 0);
+    long long nsig = 0, nseis = 0;
+    ctx->ntr_b.assign(nb, 0);
+    auto pt_of = [&](int i, int j) { return (int)((long long)(j - 1 + ctx->hy) * ctx->pitch + (i - 1 + HX)); };
+    /* forward groups: type-3 sources by point, in source order */
+    for (int s = 0; s < nb; s++) {
+        const dsh_shot &sh = shots[s];
+        if (sh.nsrc < 0 || sh.ntr < 0 || (sh.nsrc > 0 && !sh.srcpos) || (sh.ntr > 0 && !sh.recpos)) return DSH_ERR_PARAM;
+        fgrp_off[s] = (int)grp_pt.size();
+        std::map<int, int> gidx;
+        std::vector<std::vector<int>> members;
+        std::vector<int> pts;
+        for (int k = 0; k < sh.nsrc; k++) {
+            const int i = (int)sh.srcpos[0 * sh.nsrc + k], j = (int)sh.srcpos[1 * sh.nsrc + k];
+            if (!in_grid(p, i, j)) return DSH_ERR_PARAM;
+            if ((int)sh.srcpos[7 * sh.nsrc + k] != 3) continue;
+            const int pt = pt_of(i, j);
+            auto it = gidx.find(pt);
+            if (it == gidx.end()) { gidx[pt] = (int)pts.size(); pts.push_back(pt); members.push_back({k}); }
+            else members[it->second].push_back(k);
+        }
+        for (size_t g = 0; g < pts.size(); g++) {
+            grp_pt.push_back(pts[g]);
+            grp_beg.push_back((int)src_id.size());
+            for (int k : members[g]) src_id.push_back(k);
+        }
+        sig_off[s] = nsig;
+        nsig += (long long)sh.nsrc * NT;
+    }
+    fgrp_off[nb] = (int)grp_pt.size();
+    /* adjoint groups: receivers by point */
+    for (int s = 0; s < nb; s++) {
+        const dsh_shot &sh = shots[s];
+        agrp_off[s] = (int)grp_pt.size();
+        rec_off[s] = (int)rec_pt.size();
+        std::map<int, int> gidx;
+        std::vector<std::vector<int>> members;
+        std::vector<int> pts;
+        for (int r = 0; r < sh.ntr; r++) {
+            const int i = sh.recpos[r], j = sh.recpos[sh.ntr + r];
+            if (!in_grid(p, i, j)) return DSH_ERR_PARAM;
+            const int pt = pt_of(i, j);
+            rec_pt.push_back(pt);
+            auto it = gidx.find(pt);
+            if (it == gidx.end()) { gidx[pt] = (int)pts.size(); pts.push_back(pt); members.push_back({r}); }
+            else members[it->second].push_back(r);
+        }
+        for (size_t g = 0; g < pts.size(); g++) {
+            grp_pt.push_back(pts[g]);
+            grp_beg.push_back((int)src_id.size());
+            for (int r : members[g]) src_id.push_back(r);
+        }
+        ctx->ntr_b[s] = sh.ntr;
+        seis_off[s] = nseis;
+        out_off[s] = nseis;
+        obs_off[s] = obs_dev ? obs_dev_off + nseis : nseis;
+        nseis += (long long)sh.ntr * NT;
+    }
+    agrp_off[nb] = (int)grp_pt.size();
+    rec_off[nb] = (int)rec_pt.size();
+    grp_beg.push_back((int)src_id.size());
+    /* pad offset tables to S slots */
+    fgrp_off.resize(ctx->S + 1, fgrp_off[nb]);
+    agrp_off.resize(ctx->S + 1, agrp_off[nb]);
+    rec_off.resize(ctx->S + 1, rec_off[nb]);
+
+    /* one int buffer: fgrp_off[S+1] agrp_off[S+1] rec_off[S+1], then four
+     * equally sized sub-arrays grp_pt, grp_beg, src_id, rec_pt */
+    bool realloc = false;
+    const long long maxlen = (long long)std::max({grp_pt.size(), grp_beg.size(), src_id.size(), rec_pt.size()}) + 1;
+    const long long head = 3LL * (ctx->S + 1);
+    if (head + 4 * maxlen > ctx->geo_cap) {
+        cudaFree(ctx->d_geo);
+        ctx->d_geo = nullptr;
+        ctx->geo_cap = head + 4 * std::max(maxlen, 2 * ((ctx->geo_cap - head) / 4 + 1));
+        CK(cudaMalloc(&ctx->d_geo, (size_t)ctx->geo_cap * sizeof(int)));
+        realloc = true;
+    }
+    const long long cp = (ctx->geo_cap - head) / 4;
+    ctx->d_fgrp_off = ctx->d_geo;
+    ctx->d_agrp_off = ctx->d_geo + (ctx->S + 1);
+    ctx->d_rec_off = ctx->d_geo + 2 * (ctx->S + 1);
+    ctx->d_grp_pt = ctx->d_geo + head;
+    ctx->d_grp_beg = ctx->d_grp_pt + cp;
+    ctx->d_src_id = ctx->d_grp_beg + cp;
+    ctx->d_rec_pt = ctx->d_src_id + cp;
+    std::vector<int> hostgeo((size_t)ctx->geo_cap, 0);
+    memcpy(&hostgeo[0], fgrp_off.data(), (ctx->S + 1) * sizeof(int));
+    memcpy(&hostgeo[ctx->S + 1], agrp_off.data(), (ctx->S + 1) * sizeof(int));
+    memcpy(&hostgeo[2 * (ctx->S + 1)], rec_off.data(), (ctx->S + 1) * sizeof(int));
+    if (!grp_pt.empty()) memcpy(&hostgeo[head], grp_pt.data(), grp_pt.size() * sizeof(int));
+    memcpy(&hostgeo[head + cp], grp_beg.data(), grp_beg.size() * sizeof(int));
+    if (!src_id.empty()) memcpy(&hostgeo[head + 2 * cp], src_id.data(), src_id.size() * sizeof(int));
+    if (!rec_pt.empty()) memcpy(&hostgeo[head + 3 * cp], rec_pt.data(), rec_pt.size() * sizeof(int));
+    CK(cudaMemcpyAsync(ctx->d_geo, hostgeo.data(), (size_t)ctx->geo_cap * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+
+    /* signals */
+    if (nsig > ctx->cap_sig) {
+        cudaFree(ctx->d_sig);
+        ctx->cap_sig = std::max(nsig, 2 * ctx->cap_sig);
+        CK(cudaMalloc(&ctx->d_sig, (size_t)ctx->cap_sig * sizeof(float)));
+        realloc = true;
+    }
+    if (nsig > 0) {
+        std::vector<float> sig((size_t)nsig);
+        for (int s = 0; s < nb; s++) {
+            const dsh_shot &sh = shots[s];
+            if (sh.nsrc == 0) continue;
+            float *dst = &sig[(size_t)sig_off[s]];
+            if (sh.signals) memcpy(dst, sh.signals, (size_t)sh.nsrc * NT * sizeof(float));
+            else if (p.quellart == 3 || dsh_setup_wavelet(p.quellart, NT, p.dt, sh.nsrc, sh.srcpos, dst) != 0)
+                return DSH_ERR_PARAM;
+        }
+        CK(cudaMemcpyAsync(ctx->d_sig, sig.data(), (size_t)nsig * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    /* seismograms, residuals, observed data, transposed output */
+    const long long nseis_cap = std::max(nseis, 1LL);
+    if (nseis_cap > ctx->cap_seis) {
+        cudaFree(ctx->d_seis); cudaFree(ctx->d_res); cudaFree(ctx->d_tmp);
+        ctx->cap_seis = std::max(nseis_cap, 2 * ctx->cap_seis);
+        CK(cudaMalloc(&ctx->d_seis, (size_t)ctx->cap_seis * sizeof(float)));
+        CK(cudaMalloc(&ctx->d_res, (size_t)ctx->cap_seis * sizeof(float)));
+        CK(cudaMalloc(&ctx->d_tmp, (size_t)ctx->cap_seis * sizeof(float)));
+        realloc = true;
+    }
+    if (obs_host) {
+        if (nseis_cap > ctx->cap_obs) {
+            cudaFree(ctx->d_obs);
+            ctx->cap_obs = std::max(nseis_cap, 2 * ctx->cap_obs);
+            CK(cudaMalloc(&ctx->d_obs, (size_t)ctx->cap_obs * sizeof(float)));
+        }
+        if (nseis > 0)
+            CK(cudaMemcpyAsync(ctx->d_obs, obs_host, (size_t)nseis * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    }
+    std::vector<long long> offs(4 * (size_t)ctx->S);
+    memcpy(&offs[0], sig_off.data(), ctx->S * sizeof(long long));
+    memcpy(&offs[ctx->S], seis_off.data(), ctx->S * sizeof(long long));
+    memcpy(&offs[2 * ctx->S], obs_off.data(), ctx->S * sizeof(long long));
+    memcpy(&offs[3 * ctx->S], out_off.data(), ctx->S * sizeof(long long));
+    CK(cudaMemcpyAsync(ctx->d_offs, offs.data(), offs.size() * sizeof(long long), cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (realloc) { drop_graphs(ctx); ctx->geo_version++; }
+    return DSH_OK;
+}
+
+/* ---------------- passes ---------------- */
+
+static StepArgs step_args(dsh_ctx *ctx, Pass pass)
+{
+    const dsh_params &p = ctx->p;
+    StepArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nx = p.nx; a.ny = p.ny; a.pitch = ctx->pitch; a.hy = ctx->hy; a.fw = p.fw; a.free_surf = p.free_surf;
+    a.l = p.l; a.fd12_compat = p.compat_fd12;
+    a.nt_last = p.nt; a.nt_total = p.nt; a.nt_base = ctx->d_nt;
+    a.fstride = ctx->fstride; a.dstride = ctx->dstride; a.slot_stride = ctx->slot_stride;
+    for (int k = 0; k < 7; k++) a.hc[k] = ctx->hc[k];
+    a.dt = p.dt; a.dh = p.dh;
+    a.dhi_el = p.dt / p.dh;
+    a.dhi_visc = (float)(1.0 / (double)p.dh);
+    a.dthalbe = (float)((double)p.dt / 2.0);
+    const size_t vlen = 2 * DSH_MAX_FW + 1;
+    const float *pm = ctx->pml;
+    a.pml.K_x = pm; a.pml.a_x = pm + vlen; a.pml.b_x = pm + 2 * vlen;
+    a.pml.K_x_half = pm + 3 * vlen; a.pml.a_x_half = pm + 4 * vlen; a.pml.b_x_half = pm + 5 * vlen;
+    a.pml.K_y = pm + 6 * vlen; a.pml.a_y = pm + 7 * vlen; a.pml.b_y = pm + 8 * vlen;
+    a.pml.K_y_half = pm + 9 * vlen; a.pml.a_y_half = pm + 10 * vlen; a.pml.b_y_half = pm + 11 * vlen;
+    float *sl = ctx->slab;
+    a.vy = sl + ctx->o_vy; a.sxy = sl + ctx->o_sxy; a.syz = sl + ctx->o_syz;
+    a.r = sl + ctx->o_r; a.q = sl + ctx->o_q;
+    a.psi_vxx = sl + ctx->o_pvxx; a.psi_sxx = sl + ctx->o_psxx;
+    a.psi_vyy_v = sl + ctx->o_pvyy; a.psi_syy = sl + ctx->o_psyy;
+    a.gu = sl + ctx->o_gu; a.grho = sl + ctx->o_grho; a.hu = sl + ctx->o_hu; a.hrho = sl + ctx->o_hrho;
+    a.brho = ctx->m_brho; a.uip = ctx->m_uip; a.ujp = ctx->m_ujp; a.fipjp = ctx->m_fipjp; a.f = ctx->m_f;
+    a.dip = ctx->m_dip; a.d = ctx->m_d;
+    for (int l = 0; l < 4; l++) { a.bip[l] = ctx->bip[l]; a.bjm[l] = ctx->bjm[l]; a.cip[l] = ctx->cip[l]; a.cjm[l] = ctx->cjm[l]; }
+    a.fwd_slot_stride = ctx->fwd_slot_stride;
+    a.fwd_step_stride = ctx->fwd_step_stride;
+    a.status = ctx->d_status;
+    switch (pass) {
+    case P_FWD_PLAIN:
+        break;
+    case P_FWD_STORE:
+        a.fwd = ctx->fwd; a.fwd_k0 = 0;
+        if (p.eprecond == 1 || p.eprecond == 3) a.ws = sl + ctx->o_ws;
+        break;
+    case P_FWD_HESS:
+        break;
+    case P_ADJ:
+        a.fwd = ctx->fwd; a.fwd_k0 = p.nt;
+        if (p.eprecond == 1) a.ws = sl + ctx->o_wr;
+        break;
+    }
+    return a;
+}
+
+static InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
+{
+    InjectArgs a;
+    memset(&a, 0, sizeof(a));
+    a.nt_base = ctx->d_nt;
+    a.nt_last = ctx->p.nt;
+    a.nt_total = ctx->p.nt;
+    a.slot_stride = ctx->slot_stride;
+    a.vy = ctx->slab + ctx->o_vy;
+    a.grp_pt = ctx->d_grp_pt; a.grp_beg = ctx->d_grp_beg; a.src_id = ctx->d_src_id;
+    a.rec_off = ctx->d_rec_off; a.rec_pt = ctx->d_rec_pt;
+    a.seis = ctx->d_seis; a.seis_off = ctx->d_offs + ctx->S;
+    if (pass == P_ADJ) {
+        a.grp_off = ctx->d_agrp_off;
+        a.sig = ctx->d_res; a.sig_off = ctx->d_offs + ctx->S;   /* residual [ntr][NT] at the seismogram offsets */
+        a.sig_ss = ctx->p.nt; a.sig_ts = 1;
+        a.sample = 0;
+    } else {
+        a.grp_off = ctx->d_fgrp_off;
+        a.sig = ctx->d_sig; a.sig_off = ctx->d_offs;
+        a.sig_ss = ctx->p.nt; a.sig_ts = 1;
+        a.sample = (pass == P_FWD_HESS) ? 0 : 1;
+    }
+    return a;
+}
+
+static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chunk, long long *nlaunch)
+{
+    const dsh_params &p = ctx->p;
+    int vflags = 0, sflags = 0;
+    switch (pass) {
+    case P_FWD_PLAIN: break;
+    case P_FWD_STORE: sflags = SF_STRAIN_OUT; break;
+    case P_FWD_HESS: vflags = VF_HESS; sflags = SF_HESS; break;
+    case P_ADJ: vflags = VF_ADJOINT | VF_CORR; sflags = SF_CORR; break;
+    }
+    KFn vk = v_kernel(p.fdorder, vflags), sk = s_kernel(p.fdorder, p.l, sflags);
+    if (!vk || !sk) return DSH_ERR_PARAM;
+    StepArgs sa = step_args(ctx, pass);
+    InjectArgs ia = inject_args(ctx, pass);
+    dim3 block(BX, BY, 1);
+    dim3 grid((unsigned)((p.nx + 4 * BX - 1) / (4 * BX)), (unsigned)((p.ny + BY - 1) / BY), (unsigned)nb);
+    for (int k = 0; k < nsteps_in_chunk; k++) {
+        int off = k;
+        void *args[2] = {&sa, &off};
+        CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
+        void *iargs[2] = {&ia, &off};
+        CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
+        CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
+        *nlaunch += 3;
+    }
+    advance_step<<<1, 1, 0, ctx->st>>>(ctx->d_nt, nsteps_in_chunk);
+    *nlaunch += 1;
+    CK(cudaGetLastError());
+    return DSH_OK;
+}
+
+static int run_pass(dsh_ctx *ctx, Pass pass, int nb)
+{
+    const int NT = ctx->p.nt;
+    const int K = std::min(ctx->chunk, NT);
+    const long long key = ((long long)pass << 40) | ((long long)nb << 20) | (long long)ctx->geo_version;
+    set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
+    ctx->launches += 1;
+    static const bool use_graphs = getenv("DSH_NO_GRAPHS") == nullptr;
+    const int nchunks = (NT + K - 1) / K;
+    long long per_chunk = 0;
+    if (!use_graphs) {
+        for (int c = 0; c < nchunks; c++) {
+            long long nl = 0;
+            int rc = launch_step_chunk(ctx, pass, nb, K, &nl);
+            if (rc != DSH_OK) return rc;
+            ctx->launches += nl;
+        }
+        return DSH_OK;
+    }
+    auto it = ctx->graphs.find(key);
+    cudaGraphExec_t exec;
+    if (it == ctx->graphs.end()) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+        int rc = launch_step_chunk(ctx, pass, nb, K, &per_chunk);
+        cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
+        if (rc != DSH_OK) return rc;
+        CK(e);
+        CK(cudaGraphInstantiate(&exec, g, 0));
+        cudaGraphDestroy(g);
+        ctx->graphs[key] = exec;
+    } else {
+        exec = it->second;
+    }
+    per_chunk = 3LL * K + 1;
+    for (int c = 0; c < nchunks; c++) CK(cudaGraphLaunch(exec, ctx->st));
+    ctx->launches += per_chunk * nchunks;
+    return DSH_OK;
+}
+
+/* zero the wavefield state of slots [0, nb) (zero_fdveps(_visc)); with
+ * accumulators also the per-shot energies, gradients and Hessian sums */
+static int zero_slots(dsh_ctx *ctx, int nb, bool accumulators)
+{
+    const size_t w = (size_t)(accumulators ? ctx->slot_stride : ctx->o_state_end) * sizeof(float);
+    CK(cudaMemset2DAsync(ctx->slab, (size_t)ctx->slot_stride * sizeof(float), 0, w, nb, ctx->st));
+    return DSH_OK;
+}
+
+static int check_status(dsh_ctx *ctx)
+{
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    if (h) {
+        cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->st);
+        cudaStreamSynchronize(ctx->st);
+        return DSH_ERR_UNSTABLE;
+    }
+    return DSH_OK;
+}
+
+static int ensure_storage(dsh_ctx *ctx)
+{
+    const dsh_params &p = ctx->p;
+    ctx->fwd_step_stride = 3 * ctx->dstride;
+    ctx->fwd_slot_stride = (long long)p.nt * ctx->fwd_step_stride;
+    const size_t need = (size_t)ctx->S * ctx->fwd_slot_stride * sizeof(float);
+    if (p.mem_budget > 0 && (long long)need > p.mem_budget) return DSH_ERR_OOM;
+    if (ctx->fwd && ctx->fwd_bytes >= need) return DSH_OK;
+    cudaFree(ctx->fwd);
+    ctx->fwd = nullptr;
+    ctx->fwd_bytes = 0;
+    if (cudaMalloc(&ctx->fwd, need) != cudaSuccess) { cudaGetLastError(); return DSH_ERR_OOM; }
+    ctx->fwd_bytes = need;
+    drop_graphs(ctx);
+    ctx->geo_version++;
+    return DSH_OK;
+}
+
+static dim3 epi_grid(dsh_ctx *ctx, int nb)
+{
+    const long long n = (long long)ctx->p.nx * ctx->p.ny;
+    return dim3((unsigned)std::min<long long>((n + 255) / 256, 4 * 148), (unsigned)nb, 1);
+}
+
+static int copy_seis_out(dsh_ctx *ctx, int nb, float *host_out, float *dev_out)
+{
+    long long tot = 0;
+    for (int s = 0; s < nb; s++) tot += (long long)ctx->ntr_b[s] * ctx->p.nt;
+    if (tot == 0) return DSH_OK;
+    float *dst = dev_out ? dev_out : ctx->d_tmp;
+    seis_transpose_kernel<<<dim3(256, nb), 256, 0, ctx->st>>>(ctx->p.nt, ctx->d_rec_off, ctx->d_seis, ctx->d_offs + ctx->S,
+                                                             dst, ctx->d_offs + 3 * ctx->S);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    if (host_out) CK(cudaMemcpyAsync(host_out, ctx->d_tmp, (size_t)tot * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    return DSH_OK;
+}
+
+static long long batch_seis_len(dsh_ctx *ctx, const dsh_shot *shots, int nb)
+{
+    long long t = 0;
+    for (int s = 0; s < nb; s++) t += (long long)shots[s].ntr * ctx->p.nt;
+    return t;
+}
+
+static int forward_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *seis_host, float *seis_dev)
+{
+    if (!ctx || !shots || nshots < 0) return DSH_ERR_PARAM;
+    if (!ctx->model_set) return DSH_ERR_STATE;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    ctx->launches = 0;
+    long long out = 0;
+    for (int b0 = 0; b0 < nshots; b0 += ctx->S) {
+        const int nb = std::min(ctx->S, nshots - b0);
+        int rc = upload_batch(ctx, shots + b0, nb, nullptr, nullptr, 0);
+        if (rc != DSH_OK) return rc;
+        if ((rc = zero_slots(ctx, nb, false)) != DSH_OK) return rc;
+        if ((rc = run_pass(ctx, P_FWD_PLAIN, nb)) != DSH_OK) return rc;
+        if ((rc = copy_seis_out(ctx, nb, seis_host ? seis_host + out : nullptr, seis_dev ? seis_dev + out : nullptr)) != DSH_OK)
+            return rc;
+        out += batch_seis_len(ctx, shots + b0, nb);
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    ctx->stats.ms_forward = ms; ctx->stats.ms_adjoint = 0; ctx->stats.ms_total = ms;
+    ctx->stats.kernel_launches = ctx->launches;
+    ctx->stats.point_updates = (long long)ctx->p.nx * ctx->p.ny * ctx->p.nt * nshots;
+    ctx->stats.storage_bytes = 0;
+    ctx->stats.checkpoint_interval = 0;
+    return check_status(ctx);
+}
+
+extern "C" int dsh_forward(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *seis_out)
+{
+    return forward_impl(ctx, shots, nshots, seis_out, nullptr);
+}
+
+extern "C" int dsh_forward_device(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *seis_dev)
+{
+    return forward_impl(ctx, shots, nshots, nullptr, seis_dev);
+}
+
+static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const float *obs_host, const float *obs_dev,
+                         float *g_vs_host, float *g_rho_host, float *g_vs_dev, float *g_rho_dev, double *l2,
+                         float *seis_host, float *ws_host, float *wr_host)
+{
+    if (!ctx || !shots || nshots < 1 || (!obs_host && !obs_dev)) return DSH_ERR_PARAM;
+    if (!ctx->model_set) return DSH_ERR_STATE;
+    CK(cudaSetDevice(ctx->dev));
+    int rc = ensure_storage(ctx);
+    if (rc != DSH_OK) return rc;
+    const dsh_params &p = ctx->p;
+    const long long n = (long long)p.nx * p.ny;
+    float *sum_u = ctx->sums, *sum_r = ctx->sums + ctx->dstride;
+    CK(cudaMemsetAsync(ctx->sums, 0, 2 * (size_t)ctx->dstride * sizeof(float), ctx->st));
+    ctx->launches = 0;
+    double l2_total = 0.0;
+    float ms_f = 0, ms_a = 0;
+    long long out = 0;
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    for (int b0 = 0; b0 < nshots; b0 += ctx->S) {
+        const int nb = std::min(ctx->S, nshots - b0);
+        const float *obs_h = obs_host ? obs_host + out : nullptr;
+        if ((rc = upload_batch(ctx, shots + b0, nb, obs_h, obs_dev, out)) != DSH_OK) return rc;
+        const float *obs_base = obs_dev ? obs_dev : ctx->d_obs;
+        if ((rc = zero_slots(ctx, nb, true)) != DSH_OK) return rc;
+        cudaEvent_t e0, e1, e2;
+        cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
+        cudaEventRecord(e0, ctx->st);
+        if ((rc = run_pass(ctx, P_FWD_STORE, nb)) != DSH_OK) return rc;
+        cudaEventRecord(e1, ctx->st);
+        /* residual + L2 */
+        residual_kernel<<<dim3(RED_BLOCKS, nb), RED_THREADS, 0, ctx->st>>>(p.nt, ctx->d_rec_off, ctx->d_seis,
+                                                                          ctx->d_offs + ctx->S, obs_base,
+                                                                          ctx->d_offs + 2 * ctx->S, ctx->d_res, ctx->d_part);
+        reduce_parts<<<nb, RED_THREADS, 0, ctx->st>>>(ctx->d_part, RED_BLOCKS, nb, ctx->d_l2);
+        ctx->launches += 2;
+        CK(cudaGetLastError());
+        if (seis_host) {
+            if ((rc = copy_seis_out(ctx, nb, seis_host + out, nullptr)) != DSH_OK) return rc;
+        }
+        if ((rc = zero_slots(ctx, nb, false)) != DSH_OK) return rc;
+        if ((rc = run_pass(ctx, P_ADJ, nb)) != DSH_OK) return rc;
+        cudaEventRecord(e2, ctx->st);
+        if (ws_host || wr_host) {
+            for (int s = 0; s < nb; s++) {
+                if (ws_host) {
+                    gather_dense_kernel<<<256, 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch,
+                                                                  ctx->slab + s * ctx->slot_stride + ctx->o_ws, ctx->d_out);
+                    CK(cudaMemcpyAsync(ws_host + (size_t)(b0 + s) * n, ctx->d_out, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+                }
+                if (wr_host) {
+                    gather_dense_kernel<<<256, 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch,
+                                                                  ctx->slab + s * ctx->slot_stride + ctx->o_wr, ctx->d_out + n);
+                    CK(cudaMemcpyAsync(wr_host + (size_t)(b0 + s) * n, ctx->d_out + n, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+                }
+                CK(cudaStreamSynchronize(ctx->st));
+            }
+        }
+        if (p.eprecond == 1 || p.eprecond == 3) {
+            EpiArgs ea;
+            ea.nx = p.nx; ea.ny = p.ny; ea.pitch = ctx->pitch; ea.slot_stride = ctx->slot_stride;
+            ea.ws = ctx->slab + ctx->o_ws; ea.wr = ctx->slab + ctx->o_wr; ea.we = ctx->slab + ctx->o_we;
+            ea.gu = ctx->slab + ctx->o_gu; ea.grho = ctx->slab + ctx->o_grho;
+            ea.wemax = ctx->d_wemax; ea.cvs = ctx->cnorm[0]; ea.crho = ctx->cnorm[1]; ea.dh = p.dh;
+            ea.eprecond = p.eprecond;
+            CK(cudaMemsetAsync(ctx->d_wemax, 0, (size_t)nb * sizeof(unsigned), ctx->st));
+            eprecond_we_kernel<<<epi_grid(ctx, nb), 256, 0, ctx->st>>>(ea);
+            eprecond_scale_kernel<<<epi_grid(ctx, nb), 256, 0, ctx->st>>>(ea);
+            ctx->launches += 2;
+        }
+        shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
+                                                               ctx->slab + ctx->o_gu, ctx->slab + ctx->o_grho, sum_u, sum_r);
+        ctx->launches++;
+        CK(cudaGetLastError());
+        std::vector<double> l2b(nb);
+        CK(cudaMemcpyAsync(l2b.data(), ctx->d_l2, nb * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+        for (int s = 0; s < nb; s++) l2_total += l2b[s];
+        float a = 0, b = 0;
+        cudaEventElapsedTime(&a, e0, e1);
+        cudaEventElapsedTime(&b, e1, e2);
+        ms_f += a; ms_a += b;
+        cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2);
+        out += batch_seis_len(ctx, shots + b0, nb);
+    }
+    float *gv = g_vs_dev ? g_vs_dev : ctx->d_out;
+    float *gr = g_rho_dev ? g_rho_dev : ctx->d_out + n;
+    convert_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, p.dt, ctx->m_vs, ctx->m_rho, sum_u,
+                                                          sum_r, gv, gr);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    if (g_vs_host) CK(cudaMemcpyAsync(g_vs_host, gv, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    if (g_rho_host) CK(cudaMemcpyAsync(g_rho_host, gr, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    ctx->stats.ms_forward = ms_f; ctx->stats.ms_adjoint = ms_a; ctx->stats.ms_total = ms;
+    ctx->stats.kernel_launches = ctx->launches;
+    ctx->stats.point_updates = 2LL * p.nx * p.ny * p.nt * nshots;
+    ctx->stats.storage_bytes = (long long)ctx->fwd_bytes;
+    ctx->stats.checkpoint_interval = 0;
+    if (l2) *l2 = l2_total;
+    return check_status(ctx);
+}
+
+extern "C" int dsh_gradient(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const float *obs, float *g_vs,
+                            float *g_rho, double *l2, float *seis_out, float *ws, float *wr)
+{
+    if (!obs) return DSH_ERR_PARAM;
+    return gradient_impl(ctx, shots, nshots, obs, nullptr, g_vs, g_rho, nullptr, nullptr, l2, seis_out, ws, wr);
+}
+
+extern "C" int dsh_gradient_device(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const float *obs_dev,
+                                   float *g_vs_dev, float *g_rho_dev, double *l2)
+{
+    if (!obs_dev) return DSH_ERR_PARAM;
+    return gradient_impl(ctx, shots, nshots, nullptr, obs_dev, nullptr, nullptr, g_vs_dev, g_rho_dev, l2, nullptr,
+                         nullptr, nullptr);
+}
+
+extern "C" int dsh_hessian_diag(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *h_vs, float *h_rho)
+{
+    if (!ctx || !shots || nshots < 1) return DSH_ERR_PARAM;
+    if (!ctx->model_set) return DSH_ERR_STATE;
+    CK(cudaSetDevice(ctx->dev));
+    const dsh_params &p = ctx->p;
+    const long long n = (long long)p.nx * p.ny;
+    float *sum_u = ctx->sums, *sum_r = ctx->sums + ctx->dstride;
+    CK(cudaMemsetAsync(ctx->sums, 0, 2 * (size_t)ctx->dstride * sizeof(float), ctx->st));
+    CK(cudaEventRecord(ctx->ev[0], ctx->st));
+    ctx->launches = 0;
+    int rc;
+    for (int b0 = 0; b0 < nshots; b0 += ctx->S) {
+        const int nb = std::min(ctx->S, nshots - b0);
+        if ((rc = upload_batch(ctx, shots + b0, nb, nullptr, nullptr, 0)) != DSH_OK) return rc;
+        if ((rc = zero_slots(ctx, nb, true)) != DSH_OK) return rc;
+        if ((rc = run_pass(ctx, P_FWD_HESS, nb)) != DSH_OK) return rc;
+        shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
+                                                               ctx->slab + ctx->o_hu, ctx->slab + ctx->o_hrho, sum_u, sum_r);
+        ctx->launches++;
+        CK(cudaStreamSynchronize(ctx->st));
+    }
+    hessian_convert_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->m_vs, ctx->m_rho, sum_u,
+                                                                  sum_r, ctx->d_out, ctx->d_out + n);
+    ctx->launches++;
+    CK(cudaGetLastError());
+    if (h_vs) CK(cudaMemcpyAsync(h_vs, ctx->d_out, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    if (h_rho) CK(cudaMemcpyAsync(h_rho, ctx->d_out + n, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaEventRecord(ctx->ev[1], ctx->st));
+    CK(cudaEventSynchronize(ctx->ev[1]));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    ctx->stats.ms_forward = ms; ctx->stats.ms_adjoint = 0; ctx->stats.ms_total = ms;
+    ctx->stats.kernel_launches = ctx->launches;
+    ctx->stats.point_updates = (long long)p.nx * p.ny * p.nt * nshots;
+    return check_status(ctx);
+}
+
+extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
+{
+    if (!ctx || !out || shot < 0 || shot >= ctx->S) return DSH_ERR_PARAM;
+    CK(cudaSetDevice(ctx->dev));
+    const dsh_params &p = ctx->p;
+    const long long n = (long long)p.nx * p.ny;
+    const float *base = ctx->slab + (long long)shot * ctx->slot_stride;
+    const float *src;
+    int pitch = ctx->pitch;
+    switch (which) {
+    case 0: src = base + ctx->o_vy + (long long)ctx->hy * pitch; break;
+    case 1: src = base + ctx->o_sxy + (long long)ctx->hy * pitch; break;
+    case 2: src = base + ctx->o_syz + (long long)ctx->hy * pitch; break;
+    case 12: src = base + ctx->o_ws; break;
+    case 13: src = base + ctx->o_wr; break;
+    case 14: src = base + ctx->o_we; break;
+    case 15: src = base + ctx->o_gu; break;
+    case 16: src = base + ctx->o_grho; break;
+    case 17: src = base + ctx->o_hu; break;
+    case 18: src = base + ctx->o_hrho; break;
+    default: {
+        const int l = which % 100;
+        if (l >= p.l) return DSH_ERR_PARAM;
+        if (which >= 100 && which < 200) src = base + ctx->o_r + (long long)l * ctx->dstride;
+        else if (which >= 200 && which < 300) src = base + ctx->o_q + (long long)l * ctx->dstride;
+        else return DSH_ERR_PARAM;
+    }
+    }
+    CK(cudaMemcpy2DAsync(out, (size_t)p.nx * sizeof(float), src + HX, (size_t)pitch * sizeof(float),
+                         (size_t)p.nx * sizeof(float), p.ny, cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    (void)n;
+    return DSH_OK;
+}
+
+extern "C" int dsh_get_stats(dsh_ctx *ctx, dsh_stats *out)
+{
+    if (!ctx || !out) return DSH_ERR_PARAM;
+    *out = ctx->stats;
+    return DSH_OK;
+}
+
+extern "C" int dsh_set_stream(dsh_ctx *ctx, void *stream)
+{
+    if (!ctx) return DSH_ERR_PARAM;
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaStreamSynchronize(ctx->st));
+    ctx->st = stream ? (cudaStream_t)stream : ctx->own_st;
+    return DSH_OK;
+}
+
+extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3)
+{
+    if (!ctx || !out_ms3 || pass < 0 || pass > 3 || nsteps < 1 || nsteps > ctx->p.nt) return DSH_ERR_PARAM;
+    if (!ctx->model_set || ctx->ntr_b.empty() || ((pass == P_FWD_STORE || pass == P_ADJ) && !ctx->fwd)) return DSH_ERR_STATE;
+    CK(cudaSetDevice(ctx->dev));
+    const dsh_params &p = ctx->p;
+    const int nb = (int)ctx->ntr_b.size();
+    int vflags = 0, sflags = 0;
+    if (pass == P_FWD_STORE) sflags = SF_STRAIN_OUT;
+    if (pass == P_FWD_HESS) { vflags = VF_HESS; sflags = SF_HESS; }
+    if (pass == P_ADJ) { vflags = VF_ADJOINT | VF_CORR; sflags = SF_CORR; }
+    KFn vk = v_kernel(p.fdorder, vflags), sk = s_kernel(p.fdorder, p.l, sflags);
+    if (!vk || !sk) return DSH_ERR_PARAM;
+    StepArgs sa = step_args(ctx, (Pass)pass);
+    InjectArgs ia = inject_args(ctx, (Pass)pass);
+    dim3 block(BX, BY, 1);
+    dim3 grid((unsigned)((p.nx + 4 * BX - 1) / (4 * BX)), (unsigned)((p.ny + BY - 1) / BY), (unsigned)nb);
+    std::vector<cudaEvent_t> ev(6 * nsteps);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
+    for (int k = 0; k < nsteps; k++) {
+        int off = k;
+        void *args[2] = {&sa, &off};
+        void *iargs[2] = {&ia, &off};
+        CK(cudaEventRecord(ev[6 * k + 0], ctx->st));
+        CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
+        CK(cudaEventRecord(ev[6 * k + 1], ctx->st));
+        CK(cudaEventRecord(ev[6 * k + 2], ctx->st));
+        CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
+        CK(cudaEventRecord(ev[6 * k + 3], ctx->st));
+        CK(cudaEventRecord(ev[6 * k + 4], ctx->st));
+        CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
+        CK(cudaEventRecord(ev[6 * k + 5], ctx->st));
+    }
+    CK(cudaStreamSynchronize(ctx->st));
+    double acc[3] = {0, 0, 0};
+    for (int k = 0; k < nsteps; k++)
+        for (int q = 0; q < 3; q++) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[6 * k + 2 * q], ev[6 * k + 2 * q + 1]);
+            acc[q] += ms;
+        }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (int q = 0; q < 3; q++) out_ms3[q] = (float)(acc[q] / nsteps);
+    return check_status(ctx);
+}

@@ -1,0 +1,41 @@
+/* dsh_inst.cuh — instantiates the step kernels of one FD order (included by
+ * dsh_fd<N>.cu so the orders compile in parallel). */
+#pragma once
+#include "dsh_dispatch.h"
+
+#define DSH_INSTANTIATE_FD(N)                                                                 \
+    namespace dsh {                                                                           \
+    KFn v_kernel_fd##N(int flags)                                                             \
+    {                                                                                         \
+        switch (flags) {                                                                      \
+        case 0: return v_step<N, 0>;                                                          \
+        case VF_HESS: return v_step<N, VF_HESS>;                                              \
+        case VF_ADJOINT | VF_CORR: return v_step<N, VF_ADJOINT | VF_CORR>;                    \
+        case VF_ACC_OUT: return v_step<N, VF_ACC_OUT>;                                        \
+        case VF_ADJOINT | VF_ACC_OUT: return v_step<N, VF_ADJOINT | VF_ACC_OUT>;              \
+        default: return nullptr;                                                              \
+        }                                                                                     \
+    }                                                                                         \
+    template <int L>                                                                          \
+    static KFn s_pick_##N(int flags)                                                          \
+    {                                                                                         \
+        switch (flags) {                                                                      \
+        case 0: return s_step<N, L, 0>;                                                       \
+        case SF_STRAIN_OUT: return s_step<N, L, SF_STRAIN_OUT>;                               \
+        case SF_HESS: return s_step<N, L, SF_HESS>;                                           \
+        case SF_CORR: return s_step<N, L, SF_CORR>;                                           \
+        default: return nullptr;                                                              \
+        }                                                                                     \
+    }                                                                                         \
+    KFn s_kernel_fd##N(int l, int flags)                                                      \
+    {                                                                                         \
+        switch (l) {                                                                          \
+        case 0: return s_pick_##N<0>(flags);                                                  \
+        case 1: return s_pick_##N<1>(flags);                                                  \
+        case 2: return s_pick_##N<2>(flags);                                                  \
+        case 3: return s_pick_##N<3>(flags);                                                  \
+        case 4: return s_pick_##N<4>(flags);                                                  \
+        default: return nullptr;                                                              \
+        }                                                                                     \
+    }                                                                                         \
+    }

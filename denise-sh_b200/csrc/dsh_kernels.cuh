@@ -1,0 +1,461 @@
+/*
+ * dsh_kernels.cuh — sm_100a kernels of the SH time step.
+ *
+ * Layout in HBM (one "slot" per concurrently advanced shot):
+ *   haloed fields vy, sxy, syz   [ny + 2*hy][pitch], element (i,j) at
+ *                                 (j-1+hy)*pitch + (i-1+hx); the halo stays 0
+ *   interior fields (model coefficients, memory variables, energies,
+ *   gradients, stored forward wavefields)   [ny][pitch], element at
+ *                                 (j-1)*pitch + (i-1+hx)
+ *   CPML memory psi: x strips [ny][2fw], y strips [2fw][pitch]
+ * hx = 8 and pitch % 32 == 0, so the four x-consecutive points a thread owns
+ * start on a 16-byte boundary and every row access is a float4.
+ *
+ * Arithmetic: every point is computed with the reference's expression order
+ * (src/update_v_PML.c, src/update_s_elastic_PML.c, src/update_s_visc_PML.c)
+ * and the file is compiled with -fmad=false, so no multiply-add is fused:
+ * results are bit-identical to the reference's FP32 CPU code.
+ */
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace dsh {
+
+constexpr int HX = 8;            /* left halo / alignment columns */
+constexpr int BX = 32;           /* threads per block along x (4 points each) */
+constexpr int BY = 8;            /* threads per block along depth */
+
+/* flags of the velocity kernel */
+constexpr int VF_ADJOINT = 1;    /* sw=1: vyp1 = old vy (update_v_PML.c:189-192) */
+constexpr int VF_ACC_OUT = 2;    /* write vyp1 (acceleration or old vy) to acc_out */
+constexpr int VF_CORR = 4;       /* g_rho += vyp1 * stored forward acceleration (denise.c:1589) */
+constexpr int VF_HESS = 8;       /* H_rho += acc^2 (hessian.c:93) */
+/* flags of the stress kernel */
+constexpr int SF_STRAIN_OUT = 1; /* write uy = vyy, uyx = vyx (GRAD_FORM=2) */
+constexpr int SF_ENERGY = 2;     /* unused: the energy W += vy^2 (eprecond.c:11) runs when ws != nullptr */
+constexpr int SF_CORR = 4;       /* g_u += uyx_fwd*sxy + uy_fwd*syz (denise.c:1609) */
+constexpr int SF_HESS = 8;       /* H_u += uy^2 + (0.5 uyx)^2 (hessian.c:92) */
+
+struct PmlCoef {                 /* device copies, index 1..2fw */
+    const float *K_x, *a_x, *b_x, *K_x_half, *a_x_half, *b_x_half;
+    const float *K_y, *a_y, *b_y, *K_y_half, *a_y_half, *b_y_half;
+};
+
+struct StepArgs {
+    int nx, ny, pitch, hy, fw, free_surf, l;
+    int fd12_compat;
+    int nt_last;                 /* last valid step of this pass (1-based) */
+    int nt_total;                /* NT of the pass (for the Hessian's nt < NTDTINV) */
+    const int *nt_base;          /* device step counter; step = *nt_base + nt_off */
+    long long fstride;           /* floats per haloed field */
+    long long dstride;           /* floats per interior field */
+    long long slot_stride;       /* floats between consecutive shot slots */
+    float hc[7];
+    float dt, dh, dhi_el, dhi_visc, dthalbe;
+    PmlCoef pml;
+    /* per-slot state (slot 0 base; slot s at + s*slot_stride) */
+    float *vy, *sxy, *syz, *r, *q, *psi_vxx, *psi_vyy_v, *psi_sxx, *psi_syy;
+    float *ws, *gu, *grho, *hu, *hrho;
+    /* model (shared by all slots) */
+    const float *brho, *uip, *ujp, *fipjp, *f, *dip, *d;
+    float bip[4], bjm[4], cip[4], cjm[4];
+    /* stored forward wavefields: slot s, stored step k (0-based) at
+       fwd + s*fwd_slot_stride + k*fwd_step_stride (+ 0/1/2 * dstride for acc/uy/uyx) */
+    float *fwd;
+    long long fwd_slot_stride, fwd_step_stride;
+    int fwd_step_of_nt_sign;     /* +1: store step nt at k=nt-1-k0; -1: read k = ntd - nt */
+    int fwd_k0;                  /* forward: k = nt - 1 - fwd_k0; adjoint: k = fwd_k0 - nt */
+    /* compat outputs (Layer-1): explicit vyp1/uy/uyx haloed fields */
+    float *out_acc, *out_uy, *out_uyx;
+    int *status;                 /* device error word (non-finite detection) */
+};
+
+__device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ float get(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+__device__ __forceinline__ void set(float4 &v, int k, float x)
+{
+    if (k == 0) v.x = x; else if (k == 1) v.y = x; else if (k == 2) v.z = x; else v.w = x;
+}
+
+/* store the lanes of v that lie inside the grid (i0+k <= nx) */
+__device__ __forceinline__ void st4m(float *p, float4 v, int nvalid)
+{
+    if (nvalid >= 4) { st4(p, v); return; }
+    if (nvalid > 0) p[0] = v.x;
+    if (nvalid > 1) p[1] = v.y;
+    if (nvalid > 2) p[2] = v.z;
+}
+
+/*
+ * Velocity half-step (update_v_PML.c:51-198 for FDORDER = FDO): per point
+ *   sxy_x = sum_m hc[m] (sxy[i+m-1] - sxy[i-m]),  syy_y = sum_m hc[m] (syz[j+m-1] - syz[j-m])
+ *   CPML strips: psi = b*psi + a*d;  d = d/K + psi   (full-grid profiles)
+ *   vy += b*DT*(sxy_x+syy_y)/DH with b = 1/rho
+ * Thread = 4 x-consecutive points of one row; block = 128 x 8 points; z = shot slot.
+ */
+template <int FDO, int FLAGS>
+__global__ void __launch_bounds__(BX *BY) v_step(StepArgs a, int nt_off)
+{
+    constexpr int H = FDO / 2;
+    constexpr int NL = (H + 3) / 4;          /* float4s left of the own vector (needs H)   */
+    constexpr int NR = (H - 1 + 3) / 4;      /* float4s right of the own vector (needs H-1) */
+    constexpr int NXS = 4 * (NL + 1 + NR);
+    const int nt = *a.nt_base + nt_off;
+    if (nt > a.nt_last) return;
+    const int i0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x);
+    const int j = 1 + blockIdx.y * BY + threadIdx.y;
+    if (i0 > a.nx || j > a.ny) return;
+    const int slot = blockIdx.z;
+    const long long so = (long long)slot * a.slot_stride;
+    const int pitch = a.pitch;
+    const int col0 = i0 - 1 + HX;
+    const long long hrow = (long long)(j - 1 + a.hy) * pitch;
+    const long long drow = (long long)(j - 1) * pitch;
+
+    /* x taps of sxy: xs[p] = sxy[i0 - 4*NL + p] */
+    float xs[NXS];
+    {
+        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
+#pragma unroll
+        for (int v = 0; v < NL + 1 + NR; v++) {
+            float4 t = ldg4(row + 4 * v);
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+    }
+    /* y taps of syz: rows j-H .. j+H-1 */
+    float4 ys[2 * H];
+    {
+        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * pitch + col0;
+#pragma unroll
+        for (int r = 0; r < 2 * H; r++) ys[r] = ldg4(col + (long long)r * pitch);
+    }
+    const float4 b4 = ldg4(a.brho + drow + col0);
+    float4 vy4 = ld4(a.vy + so + hrow + col0);
+    float4 acc4 = make_float4(0.f, 0.f, 0.f, 0.f), old4 = vy4;
+    const int nvalid = min(4, a.nx - i0 + 1);
+
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int i = i0 + k;
+        float sxy_x, syy_y;
+#pragma unroll
+        for (int m = 1; m <= H; m++) {
+            const int my = (FDO == 12 && m == 6 && a.fd12_compat) ? 5 : m;
+            float tx = a.hc[m] * (xs[4 * NL + k + m - 1] - xs[4 * NL + k - m]);
+            float ty = a.hc[my] * (get(ys[H + m - 1], k) - get(ys[H - m], k));
+            if (m == 1) { sxy_x = tx; syy_y = ty; }
+            else { sxy_x = sxy_x + tx; syy_y = syy_y + ty; }
+        }
+        const int fw = a.fw;
+        if (fw > 0 && i <= a.nx) {
+            if (i <= fw) {
+                float *p = a.psi_vxx + so + (long long)(j - 1) * 2 * fw + (i - 1);
+                float ps = __ldg(a.pml.b_x + i) * *p + __ldg(a.pml.a_x + i) * sxy_x;
+                *p = ps;
+                sxy_x = sxy_x / __ldg(a.pml.K_x + i) + ps;
+            }
+            if (i >= a.nx - fw + 1) {
+                const int h1 = i - a.nx + 2 * fw;
+                float *p = a.psi_vxx + so + (long long)(j - 1) * 2 * fw + (h1 - 1);
+                float ps = __ldg(a.pml.b_x + h1) * *p + __ldg(a.pml.a_x + h1) * sxy_x;
+                *p = ps;
+                sxy_x = sxy_x / __ldg(a.pml.K_x + h1) + ps;
+            }
+            if (!a.free_surf && j <= fw) {
+                float *p = a.psi_vyy_v + so + (long long)(j - 1) * pitch + (col0 + k);
+                float ps = __ldg(a.pml.b_y + j) * *p + __ldg(a.pml.a_y + j) * syy_y;
+                *p = ps;
+                syy_y = syy_y / __ldg(a.pml.K_y + j) + ps;
+            }
+            if (j >= a.ny - fw + 1) {
+                const int h1 = j - a.ny + 2 * fw;
+                float *p = a.psi_vyy_v + so + (long long)(h1 - 1) * pitch + (col0 + k);
+                float ps = __ldg(a.pml.b_y + h1) * *p + __ldg(a.pml.a_y + h1) * syy_y;
+                *p = ps;
+                syy_y = syy_y / __ldg(a.pml.K_y + h1) + ps;
+            }
+        }
+        const float b = get(b4, k);
+        const float s = sxy_x + syy_y;
+        if (!(FLAGS & VF_ADJOINT)) set(acc4, k, b * s / a.dh);
+        set(vy4, k, get(vy4, k) + b * a.dt * s / a.dh);
+    }
+    st4m(a.vy + so + hrow + col0, vy4, nvalid);
+
+    if (FLAGS & VF_ACC_OUT) st4m(a.out_acc + so + hrow + col0, (FLAGS & VF_ADJOINT) ? old4 : acc4, nvalid);
+    if (FLAGS & VF_CORR) {          /* adjoint: g_rho += vyp1 * forward acceleration of step NT-nt+1 */
+        const long long k = (long long)a.fwd_k0 - nt;
+        const float *fa = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
+        const float4 f4 = ldg4(fa);
+        float *g = a.grho + so + drow + col0;
+        float4 g4 = ld4(g);
+        g4.x = g4.x + (old4.x * f4.x); g4.y = g4.y + (old4.y * f4.y);
+        g4.z = g4.z + (old4.z * f4.z); g4.w = g4.w + (old4.w * f4.w);
+        st4m(g, g4, nvalid);
+    }
+    if (!(FLAGS & VF_ADJOINT) && a.fwd && !(FLAGS & VF_CORR)) {   /* forward storage of vyp1 */
+        const long long k = (long long)nt - 1 - a.fwd_k0;
+        st4m(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4, nvalid);
+    }
+    if ((FLAGS & VF_HESS) && nt < a.nt_total) {
+        float *h = a.hrho + so + drow + col0;
+        float4 h4 = ld4(h);
+        h4.x = h4.x + (acc4.x * acc4.x); h4.y = h4.y + (acc4.y * acc4.y);
+        h4.z = h4.z + (acc4.z * acc4.z); h4.w = h4.w + (acc4.w * acc4.w);
+        st4m(h, h4, nvalid);
+    }
+}
+
+/*
+ * Stress half-step with CPML and, for L > 0, L standard-linear-solid memory
+ * variables (update_s_elastic_PML.c:104-158, update_s_visc_PML.c:131-209):
+ *   vyx = (sum_m hc[m] (vy[i+m]-vy[i-m+1])) * dhi,   vyy likewise in depth
+ *   CPML on the half grid (the viscoelastic top strip uses full-grid profiles)
+ *   elastic: sxy += uip*vyx, syz += ujp*vyy  (dhi = DT/DH)
+ *   visc:    sxy += fipjp*vyx + DT/2*sum r;  r_l = bip_l (r_l cip_l - dip_l vyx);
+ *            sxy += DT/2*sum r_new (same for syz / q)   (dhi = 1/DH)
+ */
+template <int FDO, int L, int FLAGS>
+__global__ void __launch_bounds__(BX *BY) s_step(StepArgs a, int nt_off)
+{
+    constexpr int H = FDO / 2;
+    constexpr int NL = (H - 1 + 3) / 4;      /* needs vy[i0-(H-1)] */
+    constexpr int NR = (H + 3) / 4;          /* needs vy[i0+3+H]   */
+    constexpr int NXS = 4 * (NL + 1 + NR);
+    const int nt = *a.nt_base + nt_off;
+    if (nt > a.nt_last) return;
+    const int i0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x);
+    const int j = 1 + blockIdx.y * BY + threadIdx.y;
+    if (i0 > a.nx || j > a.ny) return;
+    const int slot = blockIdx.z;
+    const long long so = (long long)slot * a.slot_stride;
+    const int pitch = a.pitch;
+    const int col0 = i0 - 1 + HX;
+    const long long hrow = (long long)(j - 1 + a.hy) * pitch;
+    const long long drow = (long long)(j - 1) * pitch;
+    const int nvalid = min(4, a.nx - i0 + 1);
+
+    float xs[NXS];
+    {
+        const float *row = a.vy + so + hrow + col0 - 4 * NL;
+#pragma unroll
+        for (int v = 0; v < NL + 1 + NR; v++) {
+            float4 t = ldg4(row + 4 * v);
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+    }
+    /* rows j-H+1 .. j+H: ys[r] = vy row (j - H + 1 + r) */
+    float4 ys[2 * H];
+    {
+        const float *col = a.vy + so + (long long)(j - 1 + a.hy - H + 1) * pitch + col0;
+#pragma unroll
+        for (int r = 0; r < 2 * H; r++) ys[r] = ldg4(col + (long long)r * pitch);
+    }
+    const float dhi = (L > 0) ? a.dhi_visc : a.dhi_el;
+    float4 vyx4 = make_float4(0.f, 0.f, 0.f, 0.f), vyy4 = vyx4;
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const int i = i0 + k;
+        float vyx, vyy;
+#pragma unroll
+        for (int m = 1; m <= H; m++) {
+            float tx = a.hc[m] * (xs[4 * NL + k + m] - xs[4 * NL + k - m + 1]);
+            float ty = a.hc[m] * (get(ys[H - 1 + m], k) - get(ys[H - m], k));
+            if (m == 1) { vyx = tx; vyy = ty; }
+            else { vyx = vyx + tx; vyy = vyy + ty; }
+        }
+        vyx = vyx * dhi;
+        vyy = vyy * dhi;
+        const int fw = a.fw;
+        if (fw > 0 && i <= a.nx) {
+            if (i <= fw) {
+                float *p = a.psi_sxx + so + (long long)(j - 1) * 2 * fw + (i - 1);
+                float ps = __ldg(a.pml.b_x_half + i) * *p + __ldg(a.pml.a_x_half + i) * vyx;
+                *p = ps;
+                vyx = vyx / __ldg(a.pml.K_x_half + i) + ps;
+            }
+            if (i >= a.nx - fw + 1) {
+                const int h1 = i - a.nx + 2 * fw;
+                float *p = a.psi_sxx + so + (long long)(j - 1) * 2 * fw + (h1 - 1);
+                float ps = __ldg(a.pml.b_x_half + h1) * *p + __ldg(a.pml.a_x_half + h1) * vyx;
+                *p = ps;
+                vyx = vyx / __ldg(a.pml.K_x_half + h1) + ps;
+            }
+            if (!a.free_surf && j <= fw) {
+                float *p = a.psi_syy + so + (long long)(j - 1) * pitch + (col0 + k);
+                if (L > 0) {
+                    float ps = __ldg(a.pml.b_y + j) * *p + __ldg(a.pml.a_y + j) * vyy;
+                    *p = ps;
+                    vyy = vyy / __ldg(a.pml.K_y + j) + ps;
+                } else {
+                    float ps = __ldg(a.pml.b_y_half + j) * *p + __ldg(a.pml.a_y_half + j) * vyy;
+                    *p = ps;
+                    vyy = vyy / __ldg(a.pml.K_y_half + j) + ps;
+                }
+            }
+            if (j >= a.ny - fw + 1) {
+                const int h1 = j - a.ny + 2 * fw;
+                float *p = a.psi_syy + so + (long long)(h1 - 1) * pitch + (col0 + k);
+                float ps = __ldg(a.pml.b_y_half + h1) * *p + __ldg(a.pml.a_y_half + h1) * vyy;
+                *p = ps;
+                vyy = vyy / __ldg(a.pml.K_y_half + h1) + ps;
+            }
+        }
+        set(vyx4, k, vyx);
+        set(vyy4, k, vyy);
+    }
+
+    float *sxy_p = a.sxy + so + hrow + col0;
+    float *syz_p = a.syz + so + hrow + col0;
+    float4 sxy4 = ld4(sxy_p), syz4 = ld4(syz_p);
+    if (L == 0) {
+        const float4 uip4 = ldg4(a.uip + drow + col0), ujp4 = ldg4(a.ujp + drow + col0);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            set(sxy4, k, get(sxy4, k) + get(uip4, k) * get(vyx4, k));
+            set(syz4, k, get(syz4, k) + get(ujp4, k) * get(vyy4, k));
+        }
+    } else {
+        const float4 fipjp4 = ldg4(a.fipjp + drow + col0), f4 = ldg4(a.f + drow + col0);
+        float4 rr[L > 0 ? L : 1], qq[L > 0 ? L : 1];
+        float4 sumr4 = make_float4(0.f, 0.f, 0.f, 0.f), sumq4 = sumr4;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            rr[l] = ld4(a.r + so + l * a.dstride + drow + col0);
+            qq[l] = ld4(a.q + so + l * a.dstride + drow + col0);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                set(sumr4, k, get(sumr4, k) + get(rr[l], k));
+                set(sumq4, k, get(sumq4, k) + get(qq[l], k));
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            set(sxy4, k, get(sxy4, k) + ((get(fipjp4, k) * get(vyx4, k)) + (a.dthalbe * get(sumr4, k))));
+            set(syz4, k, get(syz4, k) + ((get(f4, k) * get(vyy4, k)) + (a.dthalbe * get(sumq4, k))));
+        }
+        sumr4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        sumq4 = sumr4;
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            const float4 dip4 = ldg4(a.dip + l * a.dstride + drow + col0);
+            const float4 d4 = ldg4(a.d + l * a.dstride + drow + col0);
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                float rn = a.bip[l] * (get(rr[l], k) * a.cip[l] - (get(dip4, k) * get(vyx4, k)));
+                float qn = a.bjm[l] * (get(qq[l], k) * a.cjm[l] - (get(d4, k) * get(vyy4, k)));
+                set(rr[l], k, rn);
+                set(qq[l], k, qn);
+                set(sumr4, k, get(sumr4, k) + rn);
+                set(sumq4, k, get(sumq4, k) + qn);
+            }
+            st4m(a.r + so + l * a.dstride + drow + col0, rr[l], nvalid);
+            st4m(a.q + so + l * a.dstride + drow + col0, qq[l], nvalid);
+        }
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            set(sxy4, k, get(sxy4, k) + (a.dthalbe * get(sumr4, k)));
+            set(syz4, k, get(syz4, k) + (a.dthalbe * get(sumq4, k)));
+        }
+    }
+    st4m(sxy_p, sxy4, nvalid);
+    st4m(syz_p, syz4, nvalid);
+    if (!(isfinite(sxy4.x) && isfinite(sxy4.y) && isfinite(sxy4.z) && isfinite(sxy4.w) && isfinite(syz4.x) &&
+          isfinite(syz4.y) && isfinite(syz4.z) && isfinite(syz4.w) && isfinite(xs[4 * NL])))
+        atomicOr(a.status, 1);
+
+    if (FLAGS & SF_STRAIN_OUT) {
+        if (a.out_uy) {               /* compat fields */
+            st4m(a.out_uy + so + hrow + col0, vyy4, nvalid);
+            st4m(a.out_uyx + so + hrow + col0, vyx4, nvalid);
+        } else {                      /* forward storage: uy at +dstride, uyx at +2*dstride */
+            const long long k = (long long)nt - 1 - a.fwd_k0;
+            float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
+            st4m(base + a.dstride, vyy4, nvalid);
+            st4m(base + 2 * a.dstride, vyx4, nvalid);
+        }
+    }
+    if (a.ws) {                       /* energy W += vy^2; vy at the point is xs[4NL+k] */
+        float *w = a.ws + so + drow + col0;
+        float4 w4 = ld4(w);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float v = xs[4 * NL + k];
+            set(w4, k, get(w4, k) + v * v);
+        }
+        st4m(w, w4, nvalid);
+    }
+    if (FLAGS & SF_CORR) {
+        const long long k = (long long)a.fwd_k0 - nt;
+        const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
+        const float4 fy = ldg4(base + a.dstride), fu = ldg4(base + 2 * a.dstride);
+        float *g = a.gu + so + drow + col0;
+        float4 g4 = ld4(g);
+#pragma unroll
+        for (int kk = 0; kk < 4; kk++)
+            set(g4, kk, get(g4, kk) + ((get(fu, kk) * get(sxy4, kk)) + (get(fy, kk) * get(syz4, kk))));
+        st4m(g, g4, nvalid);
+    }
+    if ((FLAGS & SF_HESS) && nt < a.nt_total) {
+        float *h = a.hu + so + drow + col0;
+        float4 h4 = ld4(h);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const float eyy = get(vyy4, k), eyx = 0.5f * get(vyx4, k);
+            set(h4, k, get(h4, k) + ((eyy * eyy) + (eyx * eyx)));
+        }
+        st4m(h, h4, nvalid);
+    }
+}
+
+/* Source injection then receiver sampling for one step, one block per slot
+ * (update_v_PML.c:564-583, seismo_ssg.c:17-27).  Sources at the same grid
+ * point are grouped so their additions keep the reference's order. */
+struct InjectArgs {
+    const int *nt_base;
+    int nt_last;
+    int nt_total;
+    long long slot_stride;
+    float *vy;
+    /* per slot s: groups [grp_off[s], grp_off[s+1]) with point offset grp_pt[g]
+       and source ids src_id[grp_beg[g] .. grp_beg[g+1]) */
+    const int *grp_off, *grp_pt, *grp_beg, *src_id;
+    const float *sig;             /* signal of source id sid at step nt: sig[sig_off[s] + sid*sig_ss + (nt-1)*sig_ts] */
+    const long long *sig_off;
+    long long sig_ss, sig_ts;
+    int reverse_time;             /* unused (the adjoint signal is stored time-reversed) */
+    /* receivers: slot s has rec_n[s] receivers at rec_pt[rec_off[s] + r] */
+    const int *rec_off, *rec_pt;
+    float *seis;                  /* slot s: seis[seis_off[s] + (nt-1)*ntr_s + r] */
+    const long long *seis_off;
+    int sample;
+};
+
+static __global__ void inject_sample(InjectArgs a, int nt_off)
+{
+    const int nt = *a.nt_base + nt_off;
+    if (nt > a.nt_last) return;
+    const int s = blockIdx.x;
+    float *vy = a.vy + (long long)s * a.slot_stride;
+    const int g0 = a.grp_off[s], g1 = a.grp_off[s + 1];
+    for (int g = g0 + threadIdx.x; g < g1; g += blockDim.x) {
+        const int pt = a.grp_pt[g];
+        float v = vy[pt];
+        for (int e = a.grp_beg[g]; e < a.grp_beg[g + 1]; e++)
+            v = v + a.sig[a.sig_off[s] + (long long)a.src_id[e] * a.sig_ss + (long long)(nt - 1) * a.sig_ts];
+        vy[pt] = v;
+    }
+    if (!a.sample) return;
+    __syncthreads();
+    const int r0 = a.rec_off[s], r1 = a.rec_off[s + 1], ntr = r1 - r0;
+    float *seis = a.seis + a.seis_off[s] + (long long)(nt - 1) * ntr;
+    for (int r = threadIdx.x; r < ntr; r += blockDim.x) seis[r] = vy[a.rec_pt[r0 + r]];
+}
+
+/* advance the device step counter of a captured chunk */
+static __global__ void advance_step(int *nt_base, int by) { *nt_base += by; }
+
+}  // namespace dsh

@@ -1,0 +1,285 @@
+/*
+ * dsh_setup.c — host-side coefficient generation for the SH engine.
+ *
+ * Every coefficient is computed with the same C types (float storage, double
+ * libm calls and double literals) and the same operation order as the
+ * reference, so the device kernels see bit-identical inputs.  Compiled as C
+ * (C++ would pick float overloads of pow/exp/log) with -ffp-contract=off.
+ */
+#include "dsh_setup.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define DSH_PI (3.141592653589793)
+
+/* Operator coefficients of the staggered first derivative, per half-order
+ * (FDORDER/2 = 1..6) and error level.  Level 0 is the Taylor operator (exact
+ * fractions); levels 1..4 are Holberg's (1987) optimised operators for a
+ * maximum group-velocity error of 0.1, 0.5, 1 and 3 %.  Column 0 is the
+ * minimum number of grid points per shortest wavelength of that operator.
+ * The reference tabulates the same published numbers in holbergcoeff.c:25-66. */
+static const double OPERATORS[5][6][7] = {
+    {{23.0, 1.0, 0, 0, 0, 0, 0},
+     {8.0, 9.0 / 8.0, -1.0 / 24.0, 0, 0, 0, 0},
+     {6.0, 75.0 / 64.0, -25.0 / 384.0, 3.0 / 640.0, 0, 0, 0},
+     {5.0, 1225.0 / 1024.0, -245.0 / 3072.0, 49.0 / 5120.0, -5.0 / 7168.0, 0, 0},
+     {5.0, 19845.0 / 16384.0, -735.0 / 8192.0, 567.0 / 40960.0, -405.0 / 229376.0, 35.0 / 294912.0, 0},
+     {4.0, 160083.0 / 131072.0, -12705.0 / 131072.0, 22869.0 / 1310720.0, -5445.0 / 1835008.0,
+      847.0 / 2359296.0, -63.0 / 2883584.0}},
+    {{49.7, 1.0010, 0, 0, 0, 0, 0},
+     {8.32, 1.1382, -0.046414, 0, 0, 0, 0},
+     {4.77, 1.1965, -0.078804, 0.0081781, 0, 0, 0},
+     {3.69, 1.2257, -0.099537, 0.018063, -0.0026274, 0, 0},
+     {3.19, 1.2415, -0.11231, 0.026191, -0.0064682, 0.001191, 0},
+     {2.91, 1.2508, -0.12034, 0.032131, -0.010142, 0.0029857, -0.00066667}},
+    {{22.2, 1.0050, 0, 0, 0, 0, 0},
+     {5.65, 1.1534, -0.052806, 0, 0, 0, 0},
+     {3.74, 1.2111, -0.088313, 0.011768, 0, 0, 0},
+     {3.11, 1.2367, -0.10815, 0.023113, -0.0046905, 0, 0},
+     {2.80, 1.2496, -0.11921, 0.031130, -0.0093272, 0.0025161, 0},
+     {2.62, 1.2568, -0.12573, 0.036423, -0.013132, 0.0047484, -0.0015979}},
+    {{15.8, 1.0100, 0, 0, 0, 0, 0},
+     {4.80, 1.1640, -0.057991, 0, 0, 0, 0},
+     {3.39, 1.2192, -0.094070, 0.014608, 0, 0, 0},
+     {2.90, 1.2422, -0.11269, 0.026140, -0.0064054, 0, 0},
+     {2.65, 1.2534, -0.12257, 0.033755, -0.011081, 0.0036784, 0},
+     {2.51, 1.2596, -0.12825, 0.038550, -0.014763, 0.0058619, -0.0024538}},
+    {{9.16, 1.0300, 0, 0, 0, 0, 0},
+     {3.47, 1.1876, -0.072518, 0, 0, 0, 0},
+     {2.91, 1.2341, -0.10569, 0.022589, 0, 0, 0},
+     {2.61, 1.2516, -0.12085, 0.032236, -0.011459, 0, 0},
+     {2.45, 1.2596, -0.12829, 0.038533, -0.014681, 0.0072580, 0},
+     {2.36, 1.2640, -0.13239, 0.042217, -0.017803, 0.0081959, -0.0051848}},
+};
+
+int dsh_setup_holberg(int fdorder, int maxrelerror, float hc[7])
+{
+    int k;
+    if (fdorder < 2 || fdorder > 12 || (fdorder & 1) || maxrelerror < 0 || maxrelerror > 4) return -1;
+    for (k = 0; k < 7; k++) hc[k] = (float)OPERATORS[maxrelerror][fdorder / 2 - 1][k];
+    return 0;
+}
+
+double dsh_setup_dt_limit(int fdorder, int maxrelerror, float dh, float vmax)
+{
+    float hc[7];
+    double gamma = 0.0;
+    int k;
+    if (dsh_setup_holberg(fdorder, maxrelerror, hc) != 0 || vmax <= 0) return 0.0;
+    for (k = 1; k <= 6; k++) gamma += fabs(hc[k]);
+    return dh / (sqrt(2.0) * gamma * vmax);
+}
+
+/* One C-PML node: damping d = d0 * x^npower, stretching K, frequency shift
+ * alpha = alpha_max*(1-x) + 0.1*alpha_max (x = normalised depth into the
+ * layer), recursion coefficients b = exp(-(d/K + alpha)*dt) and
+ * a = d*(b-1)/(K*(d + K*alpha)).  The reference guards a with the integer
+ * abs() of d, so a stays 0 where |d| < 1 (PML_pro.c:151-152); kept as is. */
+static void pml_node(float abscissa, float thickness, float d0, float npower, float k_max, float alpha_max,
+                     float dt, int clamp_alpha, float *d, float *K, float *a, float *b)
+{
+    float alpha = 0.0f, xn;
+    *K = 1.0;
+    if (abscissa >= 0.0) {
+        xn = abscissa / thickness;
+        *d = d0 * pow(xn, npower);
+        *K = 1.0 + (k_max - 1.0) * pow(xn, npower);
+        alpha = alpha_max * (1.0 - xn) + 0.1 * alpha_max;
+    }
+    if (clamp_alpha && alpha < 0.0) alpha = 0.0;
+    *b = exp(-(*d / *K + alpha) * dt);
+    if (abs((int)*d) > 1.0e-6) *a = *d * (*b - 1.0) / (*K * (*d + *K * alpha));
+}
+
+void dsh_setup_pml(int nx, int ny, int fw, float dh, float dt, float damping, float fpml, float npower,
+                   float k_max_pml, dsh_pml *o)
+{
+    const float alpha_max = 2.0 * DSH_PI * (fpml / 2.0);
+    float thickness, d0, origin_lo, origin_hi_x, origin_hi_y, pos, abscissa;
+    int i, h;
+    memset(o, 0, sizeof(*o));
+    if (fw <= 0) return;
+    thickness = fw * dh;
+    d0 = -(npower + 1) * damping * log((float)0.001) / (2.0 * thickness);
+    origin_lo = thickness;
+    origin_hi_x = (nx - 1) * dh - thickness;
+    origin_hi_y = (ny - 1) * dh - thickness;
+
+    for (i = 1; i <= fw; i++) {                 /* left / top strip, index i */
+        pos = dh * (i - 1);
+        abscissa = origin_lo - pos;
+        pml_node(abscissa, thickness, d0, npower, k_max_pml, alpha_max, dt, 1, &o->d_x[i], &o->K_x[i], &o->a_x[i],
+                 &o->b_x[i]);
+        abscissa = origin_lo - (pos + dh / 2.0);
+        pml_node(abscissa, thickness, d0, npower, k_max_pml, alpha_max, dt, 1, &o->d_x_half[i], &o->K_x_half[i],
+                 &o->a_x_half[i], &o->b_x_half[i]);
+        abscissa = origin_lo - pos;
+        pml_node(abscissa, thickness, d0, npower, k_max_pml, alpha_max, dt, 0, &o->d_y[i], &o->K_y[i], &o->a_y[i],
+                 &o->b_y[i]);
+        abscissa = origin_lo - (pos + dh / 2.0);
+        pml_node(abscissa, thickness, d0, npower, k_max_pml, alpha_max, dt, 0, &o->d_y_half[i], &o->K_y_half[i],
+                 &o->a_y_half[i], &o->b_y_half[i]);
+    }
+    for (i = nx - fw + 1; i <= nx; i++) {       /* right strip, index h = fw+1..2fw */
+        h = i - nx + 2 * fw;
+        pos = dh * (i - 1);
+        abscissa = pos - origin_hi_x;
+        pml_node(abscissa, thickness, d0, npower, k_max_pml, alpha_max, dt, 1, &o->d_x[h], &o->K_x[h], &o->a_x[h],
+                 &o->b_x[h]);
+        abscissa = pos + dh / 2.0 - origin_hi_x;
+        pml_node(abscissa, thickness, d0, npower, k_max_pml, alpha_max, dt, 1, &o->d_x_half[h], &o->K_x_half[h],
+                 &o->a_x_half[h], &o->b_x_half[h]);
+    }
+    for (i = ny - fw + 1; i <= ny; i++) {       /* bottom strip */
+        h = i - ny + 2 * fw;
+        pos = dh * (i - 1);
+        abscissa = pos - origin_hi_y;
+        pml_node(abscissa, thickness, d0, npower, k_max_pml, alpha_max, dt, 0, &o->d_y[h], &o->K_y[h], &o->a_y[h],
+                 &o->b_y[h]);
+        abscissa = pos + dh / 2.0 - origin_hi_y;
+        pml_node(abscissa, thickness, d0, npower, k_max_pml, alpha_max, dt, 0, &o->d_y_half[h], &o->K_y_half[h],
+                 &o->a_y_half[h], &o->b_y_half[h]);
+    }
+}
+
+/* periodic neighbour of the one-rank model halo */
+static size_t nb(int nx, int ny, int i, int j)
+{
+    if (i > nx) i -= nx;
+    if (j > ny) j -= ny;
+    return (size_t)(j - 1) * nx + (i - 1);
+}
+
+int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const float *vs, const float *rho,
+                    const float *qs, float *brho, float *uip, float *ujp, float *fipjp, float *f, float *dip,
+                    float *d, float *bip, float *bjm, float *cip, float *cjm, float *cnorm)
+{
+    const size_t n = (size_t)nx * ny;
+    float *mu_ip = NULL, *mu_jp = NULL, *taus = NULL, *tausipjp = NULL;
+    size_t k;
+    int i, j, m;
+    if (nx < 1 || ny < 1 || l < 0 || l > DSH_MAX_L) return -1;
+
+    if (brho)
+        for (k = 0; k < n; k++) {
+            float b = 1.0 / rho[k];
+            if (rho[k] < 1e-20) b = 0.0;
+            brho[k] = b;
+        }
+
+    /* shear modulus mu = rho*vs^2 and its harmonic means at (i+1/2, j) and
+     * (i, j+1/2); zero if either side is zero */
+    mu_ip = uip ? uip : (float *)malloc(n * sizeof(float));
+    mu_jp = ujp ? ujp : (float *)malloc(n * sizeof(float));
+    if (!mu_ip || !mu_jp) return -1;
+    for (j = 1; j <= ny; j++)
+        for (i = 1; i <= nx; i++) {
+            size_t c = nb(nx, ny, i, j), e = nb(nx, ny, i + 1, j), s = nb(nx, ny, i, j + 1);
+            float mu_c = rho[c] * vs[c] * vs[c];
+            float mu_e = rho[e] * vs[e] * vs[e];
+            float mu_s = rho[s] * vs[s] * vs[s];
+            mu_ip[c] = 2.0 / ((1.0 / mu_c) + (1.0 / mu_e));
+            mu_jp[c] = 2.0 / ((1.0 / mu_c) + (1.0 / mu_s));
+            if ((mu_c == 0.0) || (mu_e == 0.0)) mu_ip[c] = 0.0;
+            if ((mu_c == 0.0) || (mu_s == 0.0)) mu_jp[c] = 0.0;
+        }
+
+    if (l > 0) {
+        float eta[DSH_MAX_L], tau_sls[DSH_MAX_L], omega, sumu = 0.0;
+        taus = (float *)malloc(n * sizeof(float));
+        tausipjp = (float *)malloc(n * sizeof(float));
+        if (!taus || !tausipjp) { free(taus); free(tausipjp); return -1; }
+        /* relaxation times and eta = DT/tau_l (readmod.c:30-33) */
+        for (m = 0; m < l; m++) {
+            tau_sls[m] = 1.0 / (2.0 * DSH_PI * fl[m]);
+            eta[m] = dt / tau_sls[m];
+        }
+        for (k = 0; k < n; k++) taus[k] = 2.0 / qs[k];
+        for (j = 1; j <= ny; j++)
+            for (i = 1; i <= nx; i++)
+                tausipjp[nb(nx, ny, i, j)] = 0.25 * (taus[nb(nx, ny, i, j)] + taus[nb(nx, ny, i + 1, j)] +
+                                                     taus[nb(nx, ny, i, j + 1)] + taus[nb(nx, ny, i + 1, j + 1)]);
+        /* relaxed-modulus correction at the reference frequency FL[1] */
+        omega = 2.0 * DSH_PI * fl[0];
+        for (m = 0; m < l; m++)
+            sumu = sumu + ((omega * omega * tau_sls[m] * tau_sls[m]) /
+                           (1.0 + omega * omega * tau_sls[m] * tau_sls[m]));
+        for (m = 0; m < l; m++) {
+            if (bip) bip[m] = 1.0 / (1.0 + (eta[m] * 0.5));
+            if (bjm) bjm[m] = 1.0 / (1.0 + (eta[m] * 0.5));
+            if (cip) cip[m] = 1.0 - (eta[m] * 0.5);
+            if (cjm) cjm[m] = 1.0 - (eta[m] * 0.5);
+        }
+        for (k = 0; k < n; k++) {
+            float mujp = mu_jp[k] / (1.0 + sumu * taus[k]);
+            float muip = mu_ip[k] / (1.0 + sumu * tausipjp[k]);
+            if (fipjp) fipjp[k] = muip * dt * (1.0 + l * tausipjp[k]);
+            if (f) f[k] = mujp * dt * (1.0 + l * taus[k]);
+            for (m = 0; m < l; m++) {
+                if (dip) dip[(size_t)m * n + k] = muip * eta[m] * tausipjp[k];
+                if (d) d[(size_t)m * n + k] = mujp * eta[m] * taus[k];
+            }
+        }
+        free(taus);
+        free(tausipjp);
+    }
+    if (!uip) free(mu_ip);
+    if (!ujp) free(mu_jp);
+
+    if (cnorm) {   /* means in the reference's loop order (x outer, depth inner) */
+        float vs_sum = 0.0, rho_sum = 0.0;
+        int cnt = 0;
+        for (i = 1; i <= nx; i++)
+            for (j = 1; j <= ny; j++) {
+                vs_sum += vs[(size_t)(j - 1) * nx + i - 1];
+                rho_sum += rho[(size_t)(j - 1) * nx + i - 1];
+                cnt++;
+            }
+        vs_sum /= cnt;
+        rho_sum /= cnt;
+        cnorm[0] = vs_sum;
+        cnorm[1] = rho_sum;
+    }
+    return 0;
+}
+
+int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *srcpos8, float *out)
+{
+    int it, s;
+    for (it = 1; it <= nt; it++) {
+        float t = (float)it * dt;
+        for (s = 0; s < nsrc; s++) {
+            float tshift = srcpos8[3 * nsrc + s], fc = srcpos8[4 * nsrc + s], amp_scale = srcpos8[5 * nsrc + s];
+            float ts = 1.0 / fc, tau, ag, amp;
+            switch (quellart) {
+            case 1:   /* Ricker, centred at 1.5/fc after tshift */
+                tau = DSH_PI * (t - 1.5 * ts - tshift) / (1.5 * ts);
+                amp = (((1.0 - 4.0 * tau * tau) * exp(-2.0 * tau * tau)));
+                break;
+            case 2:   /* one-period two-sine pulse */
+                if ((t < tshift) || (t > (tshift + ts))) amp = 0.0;
+                else amp = ((sin(2.0 * DSH_PI * (t - tshift) * fc) - 0.5 * sin(4.0 * DSH_PI * (t - tshift) * fc)));
+                break;
+            case 4:   /* sine cubed */
+                if ((t < tshift) || (t > (tshift + ts))) amp = 0.0;
+                else amp = pow(sin(DSH_PI * (t + tshift) / ts), 3.0);
+                break;
+            case 5:   /* first derivative of a Gaussian */
+                ts = 1.2 / fc;
+                ag = DSH_PI * DSH_PI * fc * fc;
+                amp = -2.0 * ag * (t - ts) * exp(-ag * (t - ts) * (t - ts));
+                break;
+            case 6:   /* spike at sample 1 + round(tshift/dt) */
+                amp = 0.0;
+                if (it == 1 + (int)floor(tshift / dt + 0.5)) amp = 1.0;
+                break;
+            default:
+                return -1;
+            }
+            out[(size_t)s * nt + it - 1] = amp * amp_scale;
+        }
+    }
+    return 0;
+}

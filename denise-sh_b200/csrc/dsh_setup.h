@@ -1,0 +1,54 @@
+/*
+ * dsh_setup.h — host-side coefficient generation (plain C, FP32 with the
+ * reference's float/double mixture so every coefficient is bit-identical to
+ * the one the reference's CPU code computes).
+ */
+#ifndef DSH_SETUP_H
+#define DSH_SETUP_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSH_MAX_FW 256
+#define DSH_MAX_L 4
+
+/* CPML profile vectors, index 1..2*fw (entry 0 unused). */
+typedef struct dsh_pml {
+    float K_x[2 * DSH_MAX_FW + 1], a_x[2 * DSH_MAX_FW + 1], b_x[2 * DSH_MAX_FW + 1];
+    float K_x_half[2 * DSH_MAX_FW + 1], a_x_half[2 * DSH_MAX_FW + 1], b_x_half[2 * DSH_MAX_FW + 1];
+    float K_y[2 * DSH_MAX_FW + 1], a_y[2 * DSH_MAX_FW + 1], b_y[2 * DSH_MAX_FW + 1];
+    float K_y_half[2 * DSH_MAX_FW + 1], a_y_half[2 * DSH_MAX_FW + 1], b_y_half[2 * DSH_MAX_FW + 1];
+    float d_x[2 * DSH_MAX_FW + 1], d_x_half[2 * DSH_MAX_FW + 1], d_y[2 * DSH_MAX_FW + 1], d_y_half[2 * DSH_MAX_FW + 1];
+} dsh_pml;
+
+/* Staggered-grid operator hc[1..6] (hc[0] = minimum points per wavelength). */
+int dsh_setup_holberg(int fdorder, int maxrelerror, float hc[7]);
+
+/* C-PML profiles for an nx x ny grid (src/PML_pro.c:65-295). */
+void dsh_setup_pml(int nx, int ny, int fw, float dh, float dt, float damping, float fpml, float npower,
+                   float k_max_pml, dsh_pml *out);
+
+/* Model-dependent coefficients for dense [ny][nx] inputs.  Outputs (dense
+ * [ny][nx] unless noted; pass NULL for what is not needed):
+ *   brho  1/rho as the velocity update forms it (0 where rho < 1e-20)
+ *   uip, ujp  harmonic shear-modulus averages with the periodic one-rank halo
+ *   for l > 0: fipjp, f, dip [l][ny][nx], d [l][ny][nx], bip/bjm/cip/cjm [l]
+ *   cnorm[2]  C_vs, C_rho */
+int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const float *vs, const float *rho,
+                    const float *qs, float *brho, float *uip, float *ujp, float *fipjp, float *f, float *dip,
+                    float *d, float *bip, float *bjm, float *cip, float *cjm, float *cnorm);
+
+/* Source time functions (src/wavelet.c:26-84): out [nsrc][nt]. */
+int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *srcpos8, float *out);
+
+/* Largest stable DT of the staggered scheme (src/checkfd_ssg_elastic.c):
+ * DH / (sqrt(2) * sum|hc| * vmax). */
+double dsh_setup_dt_limit(int fdorder, int maxrelerror, float dh, float vmax);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,328 @@
+"""dsh — Python host interface of the B200 SH time-stepping / FWI-gradient engine.
+
+A thin ctypes layer over the in-tree C-ABI library ``libdsh.so`` (declared in
+``include/dsh.h``).  It mirrors the reference's per-shot workflow
+(src/denise.c): set a model, model shots forward, or compute the energy-
+preconditioned vs/rho gradient of the L2 waveform misfit and the
+pseudo-Hessian diagonal.  There is no CPU fallback: if the CUDA library is
+missing or no GPU is visible, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libdsh.so")
+
+DSH_OK = 0
+ERRORS = {-1: "invalid parameter", -2: "CUDA error", -3: "out of device memory or budget",
+          -4: "simulation is unstable (non-finite wavefield)", -5: "call out of order", -6: "device wait timed out"}
+
+FIELD = {"vy": 0, "sxy": 1, "syz": 2, "Ws": 12, "Wr": 13, "We": 14, "g_u": 15, "g_rho": 16, "hess_u": 17,
+         "hess_rho": 18}
+
+
+class DshError(RuntimeError):
+    def __init__(self, code: int, what: str = ""):
+        super().__init__(f"{what}: {ERRORS.get(code, code)} ({code})")
+        self.code = code
+
+
+class Params(C.Structure):
+    """Mirror of ``dsh_params`` (include/dsh.h)."""
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nt", C.c_int), ("dh", C.c_float), ("dt", C.c_float),
+                ("fdorder", C.c_int), ("maxrelerror", C.c_int), ("fw", C.c_int), ("free_surf", C.c_int),
+                ("damping", C.c_float), ("fpml", C.c_float), ("npower", C.c_float), ("k_max_pml", C.c_float),
+                ("l", C.c_int), ("fl", C.c_float * 8), ("quellart", C.c_int), ("eprecond", C.c_int),
+                ("max_shots", C.c_int), ("compat_fd12", C.c_int), ("mem_budget", C.c_longlong)]
+
+
+class ShotC(C.Structure):
+    _fields_ = [("nsrc", C.c_int), ("srcpos", C.POINTER(C.c_float)), ("signals", C.POINTER(C.c_float)),
+                ("ntr", C.c_int), ("recpos", C.POINTER(C.c_int))]
+
+
+class Stats(C.Structure):
+    _fields_ = [("ms_forward", C.c_double), ("ms_adjoint", C.c_double), ("ms_total", C.c_double),
+                ("kernel_launches", C.c_longlong), ("point_updates", C.c_longlong),
+                ("storage_bytes", C.c_longlong), ("checkpoint_interval", C.c_int)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the CUDA engine; raises if it has not been built (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} not built (run __graft_entry__.build() or make -C denise-sh_b200/csrc)")
+        L = C.CDLL(LIB_PATH)
+        L.dsh_create.restype = C.c_void_p
+        L.dsh_create.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(C.c_int)]
+        L.dsh_destroy.argtypes = [C.c_void_p]
+        L.dsh_error_string.restype = C.c_char_p
+        L.dsh_set_model.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_forward.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_void_p]
+        L.dsh_forward_device.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_void_p]
+        L.dsh_gradient.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                   C.POINTER(C.c_double), C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_gradient_device.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.POINTER(C.c_double)]
+        L.dsh_hessian_diag.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_void_p, C.c_void_p]
+        L.dsh_get_field.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.dsh_get_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+        L.dsh_params_default.argtypes = [C.POINTER(Params)]
+        L.dsh_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+        L.dsh_profile_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.dsh_setup_holberg.argtypes = [C.c_int, C.c_int, C.c_void_p]
+        L.dsh_setup_pml.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                    C.c_float, C.c_float, C.c_void_p]
+        L.dsh_setup_model.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_float] + [C.c_void_p] * 15
+        L.dsh_setup_wavelet.argtypes = [C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
+        L.dsh_setup_dt_limit.restype = C.c_double
+        L.dsh_setup_dt_limit.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float]
+        _lib = L
+    return _lib
+
+
+def _check(code, what):
+    if code != DSH_OK:
+        raise DshError(code, what)
+
+
+def _fptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float)) if a is not None else None
+
+
+@dataclass
+class Shot:
+    """One shot: source table [8, nsrc] (grid x, grid y, 0, tshift, fc, amp, angle, type),
+    receivers [2, ntr] (grid x, grid y), optional signals [nsrc, nt]."""
+    srcpos: np.ndarray
+    recpos: np.ndarray
+    signals: np.ndarray | None = None
+
+    def __post_init__(self):
+        self.srcpos = np.ascontiguousarray(self.srcpos, np.float32)
+        self.recpos = np.ascontiguousarray(self.recpos, np.int32)
+        if self.signals is not None:
+            self.signals = np.ascontiguousarray(self.signals, np.float32)
+
+    @property
+    def ntr(self):
+        return self.recpos.shape[1]
+
+
+def point_source(ix: int, iy: int, fc: float, amp: float = 1.0, tshift: float = 0.0) -> np.ndarray:
+    """Source table of one vertical point force (type 3) at grid (ix, iy)."""
+    sp = np.zeros((8, 1), np.float32)
+    sp[:, 0] = [ix, iy, 0.0, tshift, fc, amp, 0.0, 3.0]
+    return sp
+
+
+def _shots_c(shots):
+    arr = (ShotC * len(shots))()
+    for k, s in enumerate(shots):
+        arr[k].nsrc = s.srcpos.shape[1]
+        arr[k].srcpos = _fptr(s.srcpos)
+        arr[k].signals = _fptr(s.signals)
+        arr[k].ntr = s.ntr
+        arr[k].recpos = s.recpos.ctypes.data_as(C.POINTER(C.c_int))
+    return arr
+
+
+def make_params(nx, ny, nt, dh, dt, **kw) -> Params:
+    p = Params()
+    lib().dsh_params_default(C.byref(p))
+    p.nx, p.ny, p.nt, p.dh, p.dt = nx, ny, nt, dh, dt
+    fl = kw.pop("fl", ())
+    for k, v in kw.items():
+        if not hasattr(p, k):
+            raise KeyError(k)
+        setattr(p, k, v)
+    for i, v in enumerate(fl):
+        p.fl[i] = v
+    return p
+
+
+class Engine:
+    """A device context for one model (``dsh_ctx``)."""
+
+    def __init__(self, params: Params, device: int = 0):
+        self.p = params
+        st = C.c_int(0)
+        self.h = lib().dsh_create(C.byref(params), device, C.byref(st))
+        if not self.h:
+            raise DshError(st.value, "dsh_create")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dsh_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def shape(self):
+        return (self.p.ny, self.p.nx)
+
+    def set_model(self, vs, rho, qs=None):
+        self._vs = np.ascontiguousarray(vs, np.float32)
+        self._rho = np.ascontiguousarray(rho, np.float32)
+        self._qs = np.ascontiguousarray(qs, np.float32) if qs is not None else None
+        _check(lib().dsh_set_model(self.h, self._vs.ctypes.data, self._rho.ctypes.data,
+                                   self._qs.ctypes.data if self._qs is not None else None), "dsh_set_model")
+
+    def forward(self, shots):
+        shots = list(shots)
+        total = sum(s.ntr for s in shots) * self.p.nt
+        out = np.zeros(max(total, 1), np.float32)
+        arr = _shots_c(shots)
+        _check(lib().dsh_forward(self.h, arr, len(shots), out.ctypes.data), "dsh_forward")
+        return _split(out, shots, self.p.nt)
+
+    def gradient(self, shots, obs, want_seis=False, want_energy=False):
+        """obs: list of [ntr, nt] arrays (one per shot).  Returns a dict with
+        g_vs, g_rho, l2 (and seis, Ws, Wr if asked)."""
+        shots = list(shots)
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(o, np.float32).ravel() for o in obs]))
+        ny, nx = self.shape
+        gv = np.zeros((ny, nx), np.float32)
+        gr = np.zeros((ny, nx), np.float32)
+        l2 = C.c_double(0)
+        seis = np.zeros(max(flat.size, 1), np.float32) if want_seis else None
+        ws = np.zeros((len(shots), ny, nx), np.float32) if want_energy else None
+        wr = np.zeros((len(shots), ny, nx), np.float32) if want_energy else None
+        arr = _shots_c(shots)
+        _check(lib().dsh_gradient(self.h, arr, len(shots), flat.ctypes.data, gv.ctypes.data, gr.ctypes.data,
+                                  C.byref(l2), seis.ctypes.data if want_seis else None,
+                                  ws.ctypes.data if want_energy else None, wr.ctypes.data if want_energy else None),
+               "dsh_gradient")
+        out = {"g_vs": gv, "g_rho": gr, "l2": l2.value}
+        if want_seis:
+            out["seis"] = _split(seis, shots, self.p.nt)
+        if want_energy:
+            out["Ws"], out["Wr"] = ws, wr
+        return out
+
+    def gradient_device(self, shots, obs_dev_ptr: int, g_vs_ptr: int, g_rho_ptr: int) -> float:
+        """Device-resident gradient (pointers from e.g. torch tensors)."""
+        arr = _shots_c(list(shots))
+        l2 = C.c_double(0)
+        _check(lib().dsh_gradient_device(self.h, arr, len(arr), obs_dev_ptr, g_vs_ptr, g_rho_ptr, C.byref(l2)),
+               "dsh_gradient_device")
+        return l2.value
+
+    def forward_device(self, shots, seis_dev_ptr: int):
+        arr = _shots_c(list(shots))
+        _check(lib().dsh_forward_device(self.h, arr, len(arr), seis_dev_ptr), "dsh_forward_device")
+
+    def hessian_diag(self, shots):
+        shots = list(shots)
+        ny, nx = self.shape
+        hv = np.zeros((ny, nx), np.float32)
+        hr = np.zeros((ny, nx), np.float32)
+        _check(lib().dsh_hessian_diag(self.h, _shots_c(shots), len(shots), hv.ctypes.data, hr.ctypes.data),
+               "dsh_hessian_diag")
+        return hv, hr
+
+    def field(self, name, shot=0, l=None):
+        code = FIELD[name] if l is None else {"r": 100, "q": 200}[name] + l
+        out = np.zeros(self.shape, np.float32)
+        _check(lib().dsh_get_field(self.h, shot, code, out.ctypes.data), "dsh_get_field")
+        return out
+
+    def set_stream(self, stream_handle: int | None):
+        """Run on a caller's CUDA stream (e.g. torch.cuda.Stream().cuda_stream)."""
+        _check(lib().dsh_set_stream(self.h, stream_handle), "dsh_set_stream")
+
+    PASSES = {"forward": 0, "forward_store": 1, "forward_hessian": 2, "adjoint": 3}
+
+    def profile_step(self, pass_name: str, nsteps: int) -> dict:
+        """Mean device ms per launch of the velocity, injection and stress kernels."""
+        out = np.zeros(3, np.float32)
+        _check(lib().dsh_profile_step(self.h, self.PASSES[pass_name], nsteps, out.ctypes.data), "dsh_profile_step")
+        return {"v_step": float(out[0]), "inject_sample": float(out[1]), "s_step": float(out[2])}
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(lib().dsh_get_stats(self.h, C.byref(s)), "dsh_get_stats")
+        return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+def _split(flat, shots, nt):
+    out, o = [], 0
+    for s in shots:
+        n = s.ntr * nt
+        out.append(flat[o:o + n].reshape(s.ntr, nt))
+        o += n
+    return out
+
+
+# ---------------- host-side coefficient helpers (for parity checks) ----------------
+
+def holberg(fdorder: int, maxrelerror: int) -> np.ndarray:
+    hc = np.zeros(7, np.float32)
+    _check(lib().dsh_setup_holberg(fdorder, maxrelerror, hc.ctypes.data), "dsh_setup_holberg")
+    return hc
+
+
+PML_NAMES = ["K_x", "a_x", "b_x", "K_x_half", "a_x_half", "b_x_half", "K_y", "a_y", "b_y", "K_y_half",
+             "a_y_half", "b_y_half", "d_x", "d_x_half", "d_y", "d_y_half"]
+MAX_FW = 256
+
+
+def pml_profiles(nx, ny, fw, dh, dt, damping, fpml, npower=4.0, k_max_pml=1.0) -> dict:
+    buf = np.zeros(16 * (2 * MAX_FW + 1), np.float32)
+    lib().dsh_setup_pml(nx, ny, fw, dh, dt, damping, fpml, npower, k_max_pml, buf.ctypes.data)
+    v = buf.reshape(16, 2 * MAX_FW + 1)
+    return {n: v[k, 1:2 * fw + 1].copy() for k, n in enumerate(PML_NAMES)}
+
+
+def model_coefficients(vs, rho, qs=None, l=0, fl=(), dt=1e-4) -> dict:
+    vs = np.ascontiguousarray(vs, np.float32)
+    rho = np.ascontiguousarray(rho, np.float32)
+    ny, nx = vs.shape
+    n = nx * ny
+    qs = np.ascontiguousarray(qs if qs is not None else np.ones_like(vs), np.float32)
+    flv = np.zeros(8, np.float32)
+    flv[:len(fl)] = fl
+    out = {k: np.zeros((ny, nx), np.float32) for k in ("brho", "uip", "ujp", "fipjp", "f")}
+    dip = np.zeros((max(l, 1), ny, nx), np.float32)
+    d = np.zeros((max(l, 1), ny, nx), np.float32)
+    sls = [np.zeros(4, np.float32) for _ in range(4)]
+    cn = np.zeros(2, np.float32)
+    rc = lib().dsh_setup_model(nx, ny, l, flv.ctypes.data, dt, vs.ctypes.data, rho.ctypes.data, qs.ctypes.data,
+                               out["brho"].ctypes.data, out["uip"].ctypes.data, out["ujp"].ctypes.data,
+                               out["fipjp"].ctypes.data, out["f"].ctypes.data, dip.ctypes.data, d.ctypes.data,
+                               *[x.ctypes.data for x in sls], cn.ctypes.data)
+    _check(rc, "dsh_setup_model")
+    out.update(dip=dip[:l], d=d[:l], bip=sls[0][:l], bjm=sls[1][:l], cip=sls[2][:l], cjm=sls[3][:l], cnorm=cn)
+    return out
+
+
+def wavelet(quellart: int, nt: int, dt: float, srcpos8) -> np.ndarray:
+    sp = np.ascontiguousarray(srcpos8, np.float32)
+    out = np.zeros((sp.shape[1], nt), np.float32)
+    _check(lib().dsh_setup_wavelet(quellart, nt, dt, sp.shape[1], sp.ctypes.data, out.ctypes.data),
+           "dsh_setup_wavelet")
+    return out
+
+
+def dt_limit(fdorder: int, maxrelerror: int, dh: float, vmax: float) -> float:
+    return lib().dsh_setup_dt_limit(fdorder, maxrelerror, dh, vmax)

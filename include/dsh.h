@@ -1,0 +1,158 @@
+/*
+ * dsh.h — C ABI of the B200 SH time-stepping / FWI-gradient engine.
+ *
+ * Drop-in for the hot path of DENISE-SH's single-rank (NPROCX=NPROCY=1)
+ * program: the per-shot forward loop (src/denise.c:1179-1346), the residual
+ * (src/calc_res.c, LNORM=2), the adjoint back-propagation with vs/rho
+ * correlation (src/denise.c:1452-1654), energy preconditioning
+ * (src/eprecond.c, src/eprecond1.c, src/denise.c:1665-1678), the shot sum and
+ * gradient conversion (src/denise.c:1689-1694, :1743-1813) and the
+ * pseudo-Hessian diagonal (src/hess_save.c, src/hessian.c, src/hessian_out.c).
+ * Each of these runs as sm_100a CUDA kernels on device-resident wavefields;
+ * results are bit-identical to the reference's FP32 CPU code built without
+ * fused multiply-add (see the parity tests), except the float-accumulated L2
+ * misfit, which is summed in double here.
+ *
+ * Conventions
+ *   grid fields        dense row-major [ny][nx]; element (i,j) of the reference
+ *                      (1-based, i along x, j along depth) is at (j-1)*nx+(i-1)
+ *   source table       [8][nsrc] floats, the rows of the reference's srcpos_loc
+ *                      (src/splitsrc.c:20-29): grid x, grid y, 0, tshift, fc,
+ *                      amplitude, angle, source type (3 = vertical force; only
+ *                      type 3 injects in the forward pass, src/update_v_PML.c:569)
+ *   receiver table     [2][ntr] ints: grid x, grid y (src/receiver.c:40-41)
+ *   traces             per shot [ntr][nt], concatenated shot after shot
+ * Every entry point returns DSH_OK (0) or a negative DSH_ERR_* code and never
+ * aborts the process.  A context is not thread-safe; use one per host thread.
+ */
+#ifndef DSH_H
+#define DSH_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DSH_OK 0
+#define DSH_ERR_PARAM (-1)     /* invalid parameter or size */
+#define DSH_ERR_CUDA (-2)      /* a CUDA call failed */
+#define DSH_ERR_OOM (-3)       /* device allocation failed or budget too small */
+#define DSH_ERR_UNSTABLE (-4)  /* non-finite wavefield detected (src/denise.c:1183-1185) */
+#define DSH_ERR_STATE (-5)     /* call out of order (e.g. no model set) */
+#define DSH_ERR_TIMEOUT (-6)   /* a bounded device wait expired */
+
+/* Time-stepping parameters: the keys of the reference's .inp/.json files
+ * that the hot path reads (src/read_par.c, src/globvar.h). */
+typedef struct dsh_params {
+    int nx, ny;               /* NX, NY: interior grid points */
+    int nt;                   /* NT = iround(TIME/DT) (src/denise.c:231) */
+    float dh, dt;             /* DH, DT */
+    int fdorder;              /* FDORDER: 2, 4, 6, 8, 10, 12 */
+    int maxrelerror;          /* MAXRELERROR 0..4 (0 = Taylor, 1..4 = Holberg) */
+    int fw;                   /* FW: CPML width in grid points (0 = none) */
+    int free_surf;            /* FREE_SURF: 1 disables the top CPML strip */
+    float damping;            /* DAMPING: CPML reference velocity (m/s) */
+    float fpml;               /* FPML: CPML frequency (Hz) */
+    float npower, k_max_pml;  /* npower, k_max_PML */
+    int l;                    /* L: relaxation mechanisms (0 = elastic, <= 4) */
+    float fl[8];              /* FL[1..L]: relaxation frequencies (Hz) */
+    int quellart;             /* QUELLART: source wavelet (1 Ricker, 2, 4, 5, 6); 3 = caller supplies signals */
+    int eprecond;             /* EPRECOND: 0 or 1 (energy preconditioning) */
+    int max_shots;            /* shots advanced together in one launch (>= 1) */
+    int compat_fd12;          /* 1: reuse hc[5] in the 6th y term of the FDORDER=12 velocity
+                                 operator, as src/update_v_PML.c:469 does */
+    long long mem_budget;     /* device bytes for stored forward wavefields; 0 = as
+                                 needed (full storage); smaller budgets select
+                                 checkpoint-and-recompute */
+} dsh_params;
+
+/* One shot (one source gather). */
+typedef struct dsh_shot {
+    int nsrc;
+    const float *srcpos;      /* [8][nsrc] host */
+    const float *signals;     /* [nsrc][nt] host, or NULL: computed from srcpos + quellart
+                                 (src/wavelet.c:26-84) */
+    int ntr;
+    const int *recpos;        /* [2][ntr] host */
+} dsh_shot;
+
+typedef struct dsh_ctx dsh_ctx;
+
+/* Fills a dsh_params with the values the reference's example parameter
+ * file uses for keys the caller does not set (FDORDER 4, MAXRELERROR 1,
+ * FW 20, FREE_SURF 1, npower 4, k_max_PML 1, EPRECOND 1, QUELLART 1). */
+void dsh_params_default(dsh_params *p);
+
+/* Creates a context on CUDA device `device`. */
+dsh_ctx *dsh_create(const dsh_params *p, int device, int *status);
+int dsh_destroy(dsh_ctx *ctx);
+const char *dsh_error_string(int status);
+
+/* Sets the model (host arrays [ny][nx]: vs in m/s, rho in kg/m^3, qs quality
+ * factor, ignored when L=0) and builds every coefficient the kernels read:
+ * Holberg operator (src/holbergcoeff.c), CPML profiles (src/PML_pro.c),
+ * harmonic shear-modulus averages with the one-rank periodic model halo
+ * (src/matcopy_elastic.c, src/av_mue.c), tau averages (src/av_tau.c),
+ * SLS coefficients (src/prepare_update_s.c) and the C_vs / C_rho means
+ * (src/denise.c:778-816). */
+int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, const float *qs);
+
+/* Forward modelling of nshots shots; seis_out receives the vertical-velocity
+ * seismograms (src/seismo_ssg.c), per shot [ntr][nt]. */
+int dsh_forward(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *seis_out);
+
+/* FWI gradient over nshots shots: forward + residual against obs (per shot
+ * [ntr][nt]) + adjoint with correlation + per-shot energy preconditioning +
+ * shot sum + conversion to (vs, rho).  Outputs (any may be NULL):
+ *   g_vs, g_rho [ny][nx]   gradients (waveconv_u, waveconv_rho after :1813)
+ *   l2                     sum over shots of the residual L2 (double accumulation)
+ *   seis_out               synthetic seismograms, per shot [ntr][nt]
+ *   ws, wr                 [nshots][ny][nx] forward / adjoint energies */
+int dsh_gradient(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const float *obs, float *g_vs, float *g_rho,
+                 double *l2, float *seis_out, float *ws, float *wr);
+
+/* Pseudo-Hessian diagonal (src/hessian.c:91-94 summed over shots, then the
+ * (vs, rho) conversion of src/hessian_out.c:20-31). */
+int dsh_hessian_diag(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *h_vs, float *h_rho);
+
+/* Device-resident variant of dsh_gradient for callers that keep data in HBM:
+ * obs_dev is a device array [nshots][ntr][nt]; outputs are device arrays
+ * (g_vs_dev, g_rho_dev [ny][nx]); l2 is a host double.  Shots' geometry is
+ * host data as above (uploaded once per distinct geometry). */
+int dsh_gradient_device(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const float *obs_dev, float *g_vs_dev,
+                        float *g_rho_dev, double *l2);
+
+/* Device-resident forward: seis_dev receives [nshots][ntr][nt]. */
+int dsh_forward_device(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *seis_dev);
+
+/* Inspection of the last run (tests and tools): copies a wavefield of shot
+ * slot `shot` to host [ny][nx].  which: 0 vy, 1 sxy, 2 syz, 100+l r_l, 200+l q_l,
+ * 12 Ws, 13 Wr, 14 We, 15 per-shot g_u (scaled), 16 per-shot g_rho (scaled). */
+int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out);
+
+/* Runs the context's work on the caller's CUDA stream (a cudaStream_t passed
+ * as void*; NULL restores the context's own stream), so callers can order it
+ * with their own work and time it with events on that stream. */
+int dsh_set_stream(dsh_ctx *ctx, void *stream);
+
+/* Per-kernel timing: re-runs `nsteps` steps of pass `pass` (0 forward,
+ * 1 forward with storage, 2 forward with Hessian sums, 3 adjoint) of the
+ * last batch with a CUDA event pair around every kernel (no graph) and
+ * returns the mean device time per launch in ms: out[0] velocity step,
+ * out[1] injection/sampling, out[2] stress step.  Call it after a
+ * dsh_gradient on the same shots; it overwrites the wavefield state. */
+int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
+
+/* Statistics of the last dsh_forward / dsh_gradient call. */
+typedef struct dsh_stats {
+    double ms_forward, ms_adjoint, ms_total;   /* device time (CUDA events) */
+    long long kernel_launches;                  /* kernels of this library launched */
+    long long point_updates;                    /* grid-point time steps advanced (all passes) */
+    long long storage_bytes;                    /* device bytes used for forward storage */
+    int checkpoint_interval;                    /* 0 = full storage */
+} dsh_stats;
+int dsh_get_stats(dsh_ctx *ctx, dsh_stats *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,215 @@
+"""Parity of the CUDA path (through the C ABI) with the reference.
+
+Bit-exact: seismograms, per-shot energies, preconditioned and converted
+gradients, Hessian diagonal and final wavefields, against (a) the golden
+fixtures that the reference's own compiled functions produced and (b) the CPU
+oracle (the restatement pinned to those fixtures) on randomised cases over
+every FD order, relaxation count, boundary setting, grid shapes that are not a
+multiple of the 4-point vector width, and multi-shot batches.  The L2 misfit
+is summed in double on the device (the reference accumulates in float), so it
+is compared with a relative tolerance of 1e-5."""
+import numpy as np
+import pytest
+
+import dsh
+import oracle as O
+from conftest import GOLDEN_CASES, golden, oracle_model
+
+pytestmark = pytest.mark.gpu
+
+L2_RTOL = 1e-5
+
+
+def engine_from(d, max_shots=1, **kw):
+    p = dsh.make_params(nx=int(d["nx"]), ny=int(d["ny"]), nt=int(d["nt"]), dh=float(d["dh"]), dt=float(d["dt"]),
+                        fdorder=int(d["fdorder"]), fw=int(d["fw"]), free_surf=int(d["free_surf"]), l=int(d["l"]),
+                        fl=tuple(float(x) for x in d["fl"]), damping=float(d["damping"]), fpml=float(d["fpml"]),
+                        max_shots=max_shots, **kw)
+    e = dsh.Engine(p)
+    e.set_model(d["vs"], d["rho"], d["qs"] if int(d["l"]) else None)
+    return e
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_golden_forward(name):
+    d = golden(name)
+    shot = dsh.Shot(d["srcpos"], d["recpos"])
+    with engine_from(d) as e:
+        seis = e.forward([shot])[0]
+        assert e.stats()["kernel_launches"] > 0
+    assert np.array_equal(seis, d["seis_plain"])
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_golden_gradient(name):
+    d = golden(name)
+    shot = dsh.Shot(d["srcpos"], d["recpos"])
+    with engine_from(d) as e:
+        out = e.gradient([shot], [d["obs"]], want_seis=True, want_energy=True)
+        end = {k: e.field(k) for k in ("vy", "sxy", "syz")}
+        We = e.field("We")
+        gu, gr = e.field("g_u"), e.field("g_rho")
+    assert np.array_equal(out["seis"][0], d["seis"])
+    assert np.array_equal(out["Ws"][0], d["Ws"])
+    assert np.array_equal(out["Wr"][0], d["Wr"])
+    assert np.array_equal(We, d["We"])
+    assert np.array_equal(gu, d["g_u"])
+    assert np.array_equal(gr, d["g_rho"])
+    assert np.array_equal(out["g_vs"], d["g_vs"])
+    assert np.array_equal(out["g_rho"], d["g_rhoc"])
+    for k in ("vy", "sxy", "syz"):
+        assert np.array_equal(end[k], d["adj_" + k]), k
+    assert abs(out["l2"] - float(d["l2"])) <= L2_RTOL * float(d["l2"])
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_golden_hessian(name):
+    d = golden(name)
+    shot = dsh.Shot(d["srcpos"], d["recpos"])
+    with engine_from(d) as e:
+        hv, hr = e.hessian_diag([shot])
+        vy = e.field("vy")
+    assert np.array_equal(hv, d["hess_vs"])
+    assert np.array_equal(hr, d["hess_rho"])
+    assert np.array_equal(vy, d["fwd_vy"])
+
+
+def _case(seed, nx, ny, nt, fdo, L, fs, fw, nshots=1):
+    rng = np.random.default_rng(seed)
+    vs = (200.0 + 40.0 * rng.standard_normal((ny, nx))).clip(120, 320).astype(np.float32)
+    rho = (1800.0 + 80.0 * rng.standard_normal((ny, nx))).astype(np.float32)
+    qs = rng.uniform(20.0, 60.0, (ny, nx)).astype(np.float32)
+    fl = (7.5, 30.0, 120.0, 240.0)[:L]
+    d = dict(nx=nx, ny=ny, nt=nt, dh=0.5, dt=np.float32(2e-4), fdorder=fdo, fw=fw, free_surf=fs, l=L,
+             fl=np.array(fl, np.float32), damping=np.float32(vs.max()), fpml=np.float32(30.0), vs=vs, rho=rho, qs=qs)
+    shots = []
+    for s in range(nshots):
+        sp = np.zeros((8, 2), np.float32)
+        sp[:, 0] = [int(rng.integers(2, nx)), 2 + s % 3, 0, -0.01, 60.0, 1.0, 0, 3]
+        sp[:, 1] = [int(rng.integers(2, nx)), 1, 0, -0.012, 45.0, -0.5, 0, 3 if s % 2 == 0 else 1]
+        rec = np.array([rng.integers(1, nx + 1, 5), [1, 1, 0, ny, max(1, ny // 2)]], np.int32)
+        shots.append(dsh.Shot(sp, rec))
+    return d, shots
+
+
+def _oracle_gradient(d, shots, obs):
+    """Reference shot loop on the CPU oracle: per-shot preconditioned gradients
+    summed in shot order (denise.c:1689-1694), then converted."""
+    m = oracle_model(d)
+    su = np.zeros((m.ny, m.nx), np.float32)
+    sr = np.zeros((m.ny, m.nx), np.float32)
+    l2 = 0.0
+    seis = []
+    for sh, ob in zip(shots, obs):
+        o = O.Oracle(m, "port")
+        g = o.shot_gradient(sh.srcpos, sh.recpos, ob)
+        su = su + g["g_u"]
+        sr = sr + g["g_rho"]
+        l2 += g["l2"]
+        seis.append(g["seis"])
+        o.close()
+    o = O.Oracle(m, "port")
+    gv, gr = o.convert(su, sr)
+    o.close()
+    return gv, gr, l2, seis
+
+
+@pytest.mark.parametrize("fdo", [2, 4, 6, 8, 10, 12])
+@pytest.mark.parametrize("L,fs", [(0, 1), (1, 0), (2, 1), (3, 0), (4, 1)])
+def test_random_cases_vs_oracle(fdo, L, fs):
+    d, shots = _case(1000 + 7 * fdo + L, nx=37 + fdo, ny=31 + L, nt=140, fdo=fdo, L=L, fs=fs, fw=6)
+    m = oracle_model(d)
+    o = O.Oracle(m, "port")
+    seis_ref = o.forward(shots[0].srcpos, shots[0].recpos)
+    o.close()
+    obs = [(seis_ref * np.float32(0.6) + np.float32(1e-3)).astype(np.float32)]
+    gv, gr, l2, seis = _oracle_gradient(d, shots, obs)
+    with engine_from(d) as e:
+        s_gpu = e.forward(shots)[0]
+        out = e.gradient(shots, obs)
+    assert np.array_equal(s_gpu, seis_ref)
+    assert np.array_equal(out["g_vs"], gv)
+    assert np.array_equal(out["g_rho"], gr)
+    assert abs(out["l2"] - l2) <= L2_RTOL * abs(l2)
+
+
+@pytest.mark.parametrize("max_shots", [1, 2, 5])
+def test_multi_shot_batches(max_shots):
+    d, shots = _case(77, nx=61, ny=45, nt=160, fdo=8, L=2, fs=1, fw=8, nshots=5)
+    m = oracle_model(d)
+    obs = []
+    for sh in shots:
+        o = O.Oracle(m, "port")
+        obs.append((o.forward(sh.srcpos, sh.recpos) * np.float32(1.1)).astype(np.float32))
+        o.close()
+    gv, gr, l2, seis = _oracle_gradient(d, shots, obs)
+    with engine_from(d, max_shots=max_shots) as e:
+        fwd = e.forward(shots)
+        out = e.gradient(shots, obs)
+    for a, b in zip(fwd, seis):
+        assert np.array_equal(a, b)
+    assert np.array_equal(out["g_vs"], gv)
+    assert np.array_equal(out["g_rho"], gr)
+    assert abs(out["l2"] - l2) <= L2_RTOL * abs(l2)
+
+
+def test_multi_shot_hessian_sum():
+    """Per shot the Hessian is bit-exact; the reference chains one float
+    accumulator through all shots while shots advance concurrently here, so
+    the multi-shot sum agrees to float rounding."""
+    d, shots = _case(78, nx=40, ny=36, nt=120, fdo=4, L=0, fs=1, fw=6, nshots=3)
+    m = oracle_model(d)
+    hv = np.zeros((m.ny, m.nx), np.float64)
+    for sh in shots:
+        with engine_from(d) as e:
+            h1, _ = e.hessian_diag([sh])
+        o = O.Oracle(m, "port")
+        o.forward(sh.srcpos, sh.recpos, hessian=True)
+        h_ref, _ = o.hessian_out()
+        o.close()
+        assert np.array_equal(h1, h_ref)
+        hv += h1
+    with engine_from(d, max_shots=3) as e:
+        hs, _ = e.hessian_diag(shots)
+    assert np.allclose(hs, hv, rtol=1e-5, atol=0)
+
+
+@pytest.mark.parametrize("ep", [0, 3])
+def test_eprecond_off_and_plessix_mulder(ep):
+    """EPRECOND=0 (no energy scaling) is bit-exact; EPRECOND=3 (Plessix &
+    Mulder receiver approximation, eprecond1.c:35-58) calls asinh, whose last
+    bit may differ between CUDA and glibc, so it is compared to 1e-6."""
+    d, shots = _case(79, nx=44, ny=30, nt=100, fdo=4, L=0, fs=1, fw=6)
+    md = oracle_model(d)
+    md.eprecond = ep
+    o = O.Oracle(md, "port")
+    obs = (o.forward(shots[0].srcpos, shots[0].recpos) * np.float32(0.5)).astype(np.float32)
+    o.close()
+    o = O.Oracle(md, "port")
+    g = o.shot_gradient(shots[0].srcpos, shots[0].recpos, obs)
+    gv0, gr0 = o.convert(g["g_u"], g["g_rho"])
+    o.close()
+    with engine_from(d, eprecond=ep) as e:
+        out = e.gradient(shots, [obs])
+    if ep == 0:
+        assert np.array_equal(out["g_vs"], gv0)
+        assert np.array_equal(out["g_rho"], gr0)
+    else:
+        assert np.allclose(out["g_vs"], gv0, rtol=1e-6, atol=1e-6 * np.abs(gv0).max())
+        assert np.allclose(out["g_rho"], gr0, rtol=1e-6, atol=1e-6 * np.abs(gr0).max())
+
+
+def test_unstable_model_reports_error():
+    """DT far above the stability limit: the engine returns DSH_ERR_UNSTABLE
+    (the reference aborts on a NaN probe, denise.c:1183-1185)."""
+    d, shots = _case(80, nx=40, ny=32, nt=400, fdo=4, L=0, fs=1, fw=6)
+    d["dt"] = np.float32(5e-3)
+    with engine_from(d) as e:
+        with pytest.raises(dsh.DshError) as ei:
+            e.forward(shots)
+        assert ei.value.code == -4
+        # the context stays usable after the error
+        d2 = dict(d)
+    d2["dt"] = np.float32(2e-4)
+    with engine_from(d2) as e:
+        assert np.all(np.isfinite(e.forward(shots)[0]))
