@@ -6,8 +6,9 @@ fixtures that the reference's own compiled functions produced and (b) the CPU
 oracle (the restatement pinned to those fixtures) on randomised cases over
 every FD order, relaxation count, boundary setting, grid shapes that are not a
 multiple of the 4-point vector width, and multi-shot batches.  The L2 misfit
-is summed in double on the device (the reference accumulates in float), so it
-is compared with a relative tolerance of 1e-5."""
+is summed in double on the device while the reference adds its n terms one by
+one in float, so it is compared within the float summation bound
+(n-1)*2^-24 relative (non-negative terms)."""
 import numpy as np
 import pytest
 
@@ -17,7 +18,8 @@ from conftest import GOLDEN_CASES, golden, oracle_model
 
 pytestmark = pytest.mark.gpu
 
-L2_RTOL = 1e-5
+def l2_tol(nterms):
+    return max(nterms - 1, 1) * 2.0 ** -24
 
 
 def engine_from(d, max_shots=1, **kw):
@@ -59,7 +61,7 @@ def test_golden_gradient(name):
     assert np.array_equal(out["g_rho"], d["g_rhoc"])
     for k in ("vy", "sxy", "syz"):
         assert np.array_equal(end[k], d["adj_" + k]), k
-    assert abs(out["l2"] - float(d["l2"])) <= L2_RTOL * float(d["l2"])
+    assert abs(out["l2"] - float(d["l2"])) <= l2_tol(d["obs"].size) * float(d["l2"])
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
@@ -130,7 +132,7 @@ def test_random_cases_vs_oracle(fdo, L, fs):
     assert np.array_equal(s_gpu, seis_ref)
     assert np.array_equal(out["g_vs"], gv)
     assert np.array_equal(out["g_rho"], gr)
-    assert abs(out["l2"] - l2) <= L2_RTOL * abs(l2)
+    assert abs(out["l2"] - l2) <= l2_tol(obs[0].size) * abs(l2)
 
 
 @pytest.mark.parametrize("max_shots", [1, 2, 5])
@@ -150,7 +152,7 @@ def test_multi_shot_batches(max_shots):
         assert np.array_equal(a, b)
     assert np.array_equal(out["g_vs"], gv)
     assert np.array_equal(out["g_rho"], gr)
-    assert abs(out["l2"] - l2) <= L2_RTOL * abs(l2)
+    assert abs(out["l2"] - l2) <= l2_tol(sum(o.size for o in obs)) * abs(l2)
 
 
 def test_multi_shot_hessian_sum():

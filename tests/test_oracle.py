@@ -85,3 +85,24 @@ def test_restatement_matches_reference_random(fdo, L):
         o.close()
     for k in outs["ref"]:
         assert np.array_equal(outs["ref"][k], outs["port"][k]), k
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference not compiled here")
+@pytest.mark.parametrize("ep", [0, 1, 3])
+def test_restatement_eprecond_variants(ep):
+    m = _rand_model(7, 44, 30, 100, 4, 0, fs=1, fw=6)
+    m.eprecond = ep
+    src = np.zeros((8, 1), np.float32)
+    src[:, 0] = [20, 2, 0, -0.01, 60.0, 1.0, 0, 3]
+    rec = np.array([[5, 15, 25, 35], [1, 1, 1, 1]], np.int32)
+    outs = {}
+    for kind in ("ref", "port"):
+        o = O.Oracle(m, kind)
+        obs = (o.forward(src, rec) * np.float32(0.5)).astype(np.float32)
+        o.close()
+        o = O.Oracle(m, kind)
+        g = o.shot_gradient(src, rec, obs)
+        outs[kind] = (g["We"], g["g_u"], g["g_rho"], g["Wr"])
+        o.close()
+    for a, b in zip(outs["ref"], outs["port"]):
+        assert np.array_equal(a, b)
