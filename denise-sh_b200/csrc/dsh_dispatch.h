@@ -6,7 +6,7 @@ namespace dsh {
 using KFn = void (*)(StepArgs, int);
 
 #define DSH_DECLARE_FD(N)                  \
-    KFn v_kernel_fd##N(int flags);         \
+    KFn v_kernel_fd##N(int flags, bool p2); \
     KFn s_kernel_fd##N(int l, int flags);
 DSH_DECLARE_FD(2)
 DSH_DECLARE_FD(4)
@@ -16,15 +16,15 @@ DSH_DECLARE_FD(10)
 DSH_DECLARE_FD(12)
 #undef DSH_DECLARE_FD
 
-inline KFn v_kernel(int fdo, int flags)
+inline KFn v_kernel(int fdo, int flags, bool p2)
 {
     switch (fdo) {
-    case 2: return v_kernel_fd2(flags);
-    case 4: return v_kernel_fd4(flags);
-    case 6: return v_kernel_fd6(flags);
-    case 8: return v_kernel_fd8(flags);
-    case 10: return v_kernel_fd10(flags);
-    case 12: return v_kernel_fd12(flags);
+    case 2: return v_kernel_fd2(flags, p2);
+    case 4: return v_kernel_fd4(flags, p2);
+    case 6: return v_kernel_fd6(flags, p2);
+    case 8: return v_kernel_fd8(flags, p2);
+    case 10: return v_kernel_fd10(flags, p2);
+    case 12: return v_kernel_fd12(flags, p2);
     default: return nullptr;
     }
 }

@@ -247,6 +247,8 @@ struct dsh_ctx {
     int *d_geo = nullptr;
     long long geo_cap = 0;
     int *d_fgrp_off, *d_agrp_off, *d_grp_pt, *d_grp_beg, *d_src_id, *d_rec_off, *d_rec_pt;
+    int *d_ftile, *d_atile, *d_rtile, *d_gpk, *d_rpk, *d_rid;
+    int ntiles = 0, fused_inject = 0;
     long long *d_offs = nullptr;          /* sig_off[S], seis_off[S], obs_off[S], out_off[S] */
     float *d_sig = nullptr, *d_seis = nullptr, *d_res = nullptr, *d_obs = nullptr, *d_tmp = nullptr;
     float *d_out = nullptr;               /* 2 x [ny][nx] dense outputs */
@@ -317,6 +319,7 @@ static int check_params(const dsh_params *p)
         if (!(p->fl[l] > 0)) return DSH_ERR_PARAM;
     if (p->eprecond != 0 && p->eprecond != 1 && p->eprecond != 3) return DSH_ERR_PARAM;
     if (p->max_shots < 1 || p->max_shots > 65535) return DSH_ERR_PARAM;
+    if (p->nx > 65000 || p->ny > 65000) return DSH_ERR_PARAM;
     if (p->quellart != 1 && p->quellart != 2 && p->quellart != 3 && p->quellart != 4 && p->quellart != 5 &&
         p->quellart != 6)
         return DSH_ERR_PARAM;
@@ -471,108 +474,153 @@ extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, co
 static bool in_grid(const dsh_params &p, int i, int j) { return i >= 0 && i <= p.nx + 1 && j >= 0 && j <= p.ny + 1; }
 
 /* Uploads sources, receivers, forward signals and (optionally) observed data
- * of shots[0..nb) into slots 0..nb). */
+ * of shots[0..nb) into slots 0..nb).  Sources at one grid point form a group
+ * (members in source order); groups and receivers are also listed per thread
+ * block tile for the fused injection/sampling of the velocity kernel. */
 static int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_host, const float *obs_dev,
                         long long obs_dev_off)
 {
     const dsh_params &p = ctx->p;
-    const int NT = p.nt;
-    std::vector<int> fgrp_off(nb + 1), agrp_off(nb + 1), rec_off(nb + 1), grp_pt, grp_beg, src_id, rec_pt;
-    std::vector<long long> sig_off(ctx->S, 0), seis_off(ctx->S, 0), obs_off(ctx->S, 0), out_off(ctx->S, 0);
+    const int NT = p.nt, S = ctx->S;
+    const int gx = (p.nx + 4 * BX - 1) / (4 * BX), gy = (p.ny + BY - 1) / BY, T = gx * gy;
+    std::vector<int> fgrp_off(S + 1), agrp_off(S + 1), rec_off(S + 1);
+    std::vector<int> ftile(S * (T + 1)), atile(S * (T + 1)), rtile(S * (T + 1));
+    std::vector<int> grp_pt, grp_beg, src_id, rec_pt, gpk, rpk, rid;
+    std::vector<long long> sig_off(S, 0), seis_off(S, 0), obs_off(S, 0), out_off(S, 0);
     long long nsig = 0, nseis = 0;
+    bool fused = true;
     ctx->ntr_b.assign(nb, 0);
     auto pt_of = [&](int i, int j) { return (int)((long long)(j - 1 + ctx->hy) * ctx->pitch + (i - 1 + HX)); };
-    /* forward groups: type-3 sources by point, in source order */
+    auto tile_of = [&](int i, int j) {
+        if (i < 1 || i > p.nx || j < 1 || j > p.ny) return -1;
+        return ((j - 1) / BY) * gx + (i - 1) / (4 * BX);
+    };
+    struct Grp { int i, j, tile; std::vector<int> members; };
+    /* appends groups (sorted by tile, stable) and fills the tile table of slot s */
+    auto emit = [&](std::vector<Grp> &gs, int *tab) {
+        std::stable_sort(gs.begin(), gs.end(), [](const Grp &x, const Grp &y) { return x.tile < y.tile; });
+        size_t k = 0;
+        for (int t = 0; t <= T; t++) {
+            while (k < gs.size() && gs[k].tile < t) k++;
+            tab[t] = (int)grp_pt.size() + (int)k;
+        }
+        for (auto &g : gs) {
+            grp_pt.push_back(pt_of(g.i, g.j));
+            gpk.push_back((g.j << 16) | (g.i & 0xffff));
+            grp_beg.push_back((int)src_id.size());
+            for (int m : g.members) src_id.push_back(m);
+        }
+    };
+    auto group = [&](int n, auto pos_i, auto pos_j, auto use) {
+        std::map<int, int> idx;
+        std::vector<Grp> gs;
+        for (int k = 0; k < n; k++) {
+            if (!use(k)) continue;
+            const int i = pos_i(k), j = pos_j(k);
+            const int key = pt_of(i, j);
+            auto it = idx.find(key);
+            if (it == idx.end()) { idx[key] = (int)gs.size(); gs.push_back({i, j, tile_of(i, j), {k}}); }
+            else gs[it->second].members.push_back(k);
+            if (tile_of(i, j) < 0) fused = false;
+        }
+        return gs;
+    };
     for (int s = 0; s < nb; s++) {
         const dsh_shot &sh = shots[s];
         if (sh.nsrc < 0 || sh.ntr < 0 || (sh.nsrc > 0 && !sh.srcpos) || (sh.ntr > 0 && !sh.recpos)) return DSH_ERR_PARAM;
+        for (int k = 0; k < sh.nsrc; k++)
+            if (!in_grid(p, (int)sh.srcpos[k], (int)sh.srcpos[sh.nsrc + k])) return DSH_ERR_PARAM;
+        for (int r = 0; r < sh.ntr; r++)
+            if (!in_grid(p, sh.recpos[r], sh.recpos[sh.ntr + r])) return DSH_ERR_PARAM;
+    }
+    /* forward groups: type-3 sources (update_v_PML.c:569) */
+    for (int s = 0; s < S; s++) {
         fgrp_off[s] = (int)grp_pt.size();
-        std::map<int, int> gidx;
-        std::vector<std::vector<int>> members;
-        std::vector<int> pts;
-        for (int k = 0; k < sh.nsrc; k++) {
-            const int i = (int)sh.srcpos[0 * sh.nsrc + k], j = (int)sh.srcpos[1 * sh.nsrc + k];
-            if (!in_grid(p, i, j)) return DSH_ERR_PARAM;
-            if ((int)sh.srcpos[7 * sh.nsrc + k] != 3) continue;
-            const int pt = pt_of(i, j);
-            auto it = gidx.find(pt);
-            if (it == gidx.end()) { gidx[pt] = (int)pts.size(); pts.push_back(pt); members.push_back({k}); }
-            else members[it->second].push_back(k);
+        std::vector<Grp> gs;
+        if (s < nb) {
+            const dsh_shot &sh = shots[s];
+            gs = group(sh.nsrc, [&](int k) { return (int)sh.srcpos[k]; },
+                       [&](int k) { return (int)sh.srcpos[sh.nsrc + k]; },
+                       [&](int k) { return (int)sh.srcpos[7 * sh.nsrc + k] == 3; });
+            sig_off[s] = nsig;
+            nsig += (long long)sh.nsrc * NT;
         }
-        for (size_t g = 0; g < pts.size(); g++) {
-            grp_pt.push_back(pts[g]);
-            grp_beg.push_back((int)src_id.size());
-            for (int k : members[g]) src_id.push_back(k);
-        }
-        sig_off[s] = nsig;
-        nsig += (long long)sh.nsrc * NT;
+        emit(gs, &ftile[s * (T + 1)]);
     }
-    fgrp_off[nb] = (int)grp_pt.size();
-    /* adjoint groups: receivers by point */
-    for (int s = 0; s < nb; s++) {
-        const dsh_shot &sh = shots[s];
+    fgrp_off[S] = (int)grp_pt.size();
+    /* adjoint groups: receivers inject the residual (update_v_PML.c:576-583) */
+    for (int s = 0; s < S; s++) {
         agrp_off[s] = (int)grp_pt.size();
-        rec_off[s] = (int)rec_pt.size();
-        std::map<int, int> gidx;
-        std::vector<std::vector<int>> members;
-        std::vector<int> pts;
-        for (int r = 0; r < sh.ntr; r++) {
-            const int i = sh.recpos[r], j = sh.recpos[sh.ntr + r];
-            if (!in_grid(p, i, j)) return DSH_ERR_PARAM;
-            const int pt = pt_of(i, j);
-            rec_pt.push_back(pt);
-            auto it = gidx.find(pt);
-            if (it == gidx.end()) { gidx[pt] = (int)pts.size(); pts.push_back(pt); members.push_back({r}); }
-            else members[it->second].push_back(r);
+        std::vector<Grp> gs;
+        if (s < nb) {
+            const dsh_shot &sh = shots[s];
+            gs = group(sh.ntr, [&](int r) { return sh.recpos[r]; }, [&](int r) { return sh.recpos[sh.ntr + r]; },
+                       [](int) { return true; });
         }
-        for (size_t g = 0; g < pts.size(); g++) {
-            grp_pt.push_back(pts[g]);
-            grp_beg.push_back((int)src_id.size());
-            for (int r : members[g]) src_id.push_back(r);
-        }
-        ctx->ntr_b[s] = sh.ntr;
-        seis_off[s] = nseis;
-        out_off[s] = nseis;
-        obs_off[s] = obs_dev ? obs_dev_off + nseis : nseis;
-        nseis += (long long)sh.ntr * NT;
+        emit(gs, &atile[s * (T + 1)]);
     }
-    agrp_off[nb] = (int)grp_pt.size();
-    rec_off[nb] = (int)rec_pt.size();
+    agrp_off[S] = (int)grp_pt.size();
     grp_beg.push_back((int)src_id.size());
-    /* pad offset tables to S slots */
-    fgrp_off.resize(ctx->S + 1, fgrp_off[nb]);
-    agrp_off.resize(ctx->S + 1, agrp_off[nb]);
-    rec_off.resize(ctx->S + 1, rec_off[nb]);
+    /* receivers: original order (fallback kernel) and per tile (fused sampling) */
+    for (int s = 0; s < S; s++) {
+        rec_off[s] = (int)rec_pt.size();
+        std::vector<std::pair<int, int>> ent;       /* (tile, r) */
+        if (s < nb) {
+            const dsh_shot &sh = shots[s];
+            for (int r = 0; r < sh.ntr; r++) {
+                const int i = sh.recpos[r], j = sh.recpos[sh.ntr + r];
+                rec_pt.push_back(pt_of(i, j));
+                ent.push_back({tile_of(i, j), r});
+            }
+            std::stable_sort(ent.begin(), ent.end(), [](auto &x, auto &y) { return x.first < y.first; });
+            ctx->ntr_b[s] = sh.ntr;
+            seis_off[s] = nseis;
+            out_off[s] = nseis;
+            obs_off[s] = obs_dev ? obs_dev_off + nseis : nseis;
+            nseis += (long long)sh.ntr * NT;
+        }
+        size_t k = 0;
+        for (int t = 0; t <= T; t++) {
+            while (k < ent.size() && ent[k].first < t) k++;
+            rtile[s * (T + 1) + t] = (int)rpk.size() + (int)k;
+        }
+        for (auto &e : ent) {
+            const int r = e.second;
+            rpk.push_back((shots[s].recpos[shots[s].ntr + r] << 16) | (shots[s].recpos[r] & 0xffff));
+            rid.push_back(r);
+        }
+    }
+    rec_off[S] = (int)rec_pt.size();
 
-    /* one int buffer: fgrp_off[S+1] agrp_off[S+1] rec_off[S+1], then four
-     * equally sized sub-arrays grp_pt, grp_beg, src_id, rec_pt */
+    /* one int buffer: fixed tables, then 7 variable sections of capacity cp */
+    const long long F = 3LL * (S + 1) + 3LL * S * (T + 1);
+    const long long maxlen = (long long)std::max({grp_pt.size(), grp_beg.size(), src_id.size(), rec_pt.size(),
+                                                  gpk.size(), rpk.size(), rid.size()}) + 1;
     bool realloc = false;
-    const long long maxlen = (long long)std::max({grp_pt.size(), grp_beg.size(), src_id.size(), rec_pt.size()}) + 1;
-    const long long head = 3LL * (ctx->S + 1);
-    if (head + 4 * maxlen > ctx->geo_cap) {
+    if (F + 7 * maxlen > ctx->geo_cap) {
         cudaFree(ctx->d_geo);
         ctx->d_geo = nullptr;
-        ctx->geo_cap = head + 4 * std::max(maxlen, 2 * ((ctx->geo_cap - head) / 4 + 1));
+        const long long cp_old = ctx->geo_cap > F ? (ctx->geo_cap - F) / 7 : 0;
+        ctx->geo_cap = F + 7 * std::max(maxlen, 2 * cp_old);
         CK(cudaMalloc(&ctx->d_geo, (size_t)ctx->geo_cap * sizeof(int)));
         realloc = true;
     }
-    const long long cp = (ctx->geo_cap - head) / 4;
-    ctx->d_fgrp_off = ctx->d_geo;
-    ctx->d_agrp_off = ctx->d_geo + (ctx->S + 1);
-    ctx->d_rec_off = ctx->d_geo + 2 * (ctx->S + 1);
-    ctx->d_grp_pt = ctx->d_geo + head;
-    ctx->d_grp_beg = ctx->d_grp_pt + cp;
-    ctx->d_src_id = ctx->d_grp_beg + cp;
-    ctx->d_rec_pt = ctx->d_src_id + cp;
-    std::vector<int> hostgeo((size_t)ctx->geo_cap, 0);
-    memcpy(&hostgeo[0], fgrp_off.data(), (ctx->S + 1) * sizeof(int));
-    memcpy(&hostgeo[ctx->S + 1], agrp_off.data(), (ctx->S + 1) * sizeof(int));
-    memcpy(&hostgeo[2 * (ctx->S + 1)], rec_off.data(), (ctx->S + 1) * sizeof(int));
-    if (!grp_pt.empty()) memcpy(&hostgeo[head], grp_pt.data(), grp_pt.size() * sizeof(int));
-    memcpy(&hostgeo[head + cp], grp_beg.data(), grp_beg.size() * sizeof(int));
-    if (!src_id.empty()) memcpy(&hostgeo[head + 2 * cp], src_id.data(), src_id.size() * sizeof(int));
-    if (!rec_pt.empty()) memcpy(&hostgeo[head + 3 * cp], rec_pt.data(), rec_pt.size() * sizeof(int));
-    CK(cudaMemcpyAsync(ctx->d_geo, hostgeo.data(), (size_t)ctx->geo_cap * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
+    const long long cp = (ctx->geo_cap - F) / 7;
+    int *G = ctx->d_geo;
+    ctx->d_fgrp_off = G; ctx->d_agrp_off = G + (S + 1); ctx->d_rec_off = G + 2 * (S + 1);
+    ctx->d_ftile = G + 3 * (S + 1); ctx->d_atile = ctx->d_ftile + S * (T + 1); ctx->d_rtile = ctx->d_atile + S * (T + 1);
+    ctx->d_grp_pt = G + F; ctx->d_grp_beg = ctx->d_grp_pt + cp; ctx->d_src_id = ctx->d_grp_beg + cp;
+    ctx->d_rec_pt = ctx->d_src_id + cp; ctx->d_gpk = ctx->d_rec_pt + cp; ctx->d_rpk = ctx->d_gpk + cp;
+    ctx->d_rid = ctx->d_rpk + cp;
+    ctx->ntiles = T;
+    ctx->fused_inject = fused && getenv("DSH_NO_FUSED_INJECT") == nullptr;
+    std::vector<int> host((size_t)ctx->geo_cap, 0);
+    auto put = [&](long long off, const std::vector<int> &v) { if (!v.empty()) memcpy(&host[off], v.data(), v.size() * sizeof(int)); };
+    put(0, fgrp_off); put(S + 1, agrp_off); put(2 * (S + 1), rec_off);
+    put(3 * (S + 1), ftile); put(3 * (S + 1) + S * (T + 1), atile); put(3 * (S + 1) + 2 * S * (T + 1), rtile);
+    put(F, grp_pt); put(F + cp, grp_beg); put(F + 2 * cp, src_id); put(F + 3 * cp, rec_pt);
+    put(F + 4 * cp, gpk); put(F + 5 * cp, rpk); put(F + 6 * cp, rid);
+    CK(cudaMemcpyAsync(ctx->d_geo, host.data(), (size_t)ctx->geo_cap * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
 
     /* signals */
@@ -627,6 +675,13 @@ static int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float
 
 /* ---------------- passes ---------------- */
 
+/* DH = 2^k: x/DH and x*(1/DH) are the same correctly rounded number */
+static bool dh_pow2(float dh)
+{
+    int e;
+    return dh > 0 && std::frexp(dh, &e) == 0.5f;
+}
+
 static StepArgs step_args(dsh_ctx *ctx, Pass pass)
 {
     const dsh_params &p = ctx->p;
@@ -638,6 +693,7 @@ static StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.fstride = ctx->fstride; a.dstride = ctx->dstride; a.slot_stride = ctx->slot_stride;
     for (int k = 0; k < 7; k++) a.hc[k] = ctx->hc[k];
     a.dt = p.dt; a.dh = p.dh;
+    a.inv_dh = (float)(1.0 / (double)p.dh);
     a.dhi_el = p.dt / p.dh;
     a.dhi_visc = (float)(1.0 / (double)p.dh);
     a.dthalbe = (float)((double)p.dt / 2.0);
@@ -659,6 +715,23 @@ static StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.fwd_slot_stride = ctx->fwd_slot_stride;
     a.fwd_step_stride = ctx->fwd_step_stride;
     a.status = ctx->d_status;
+    /* fused injection / sampling lists */
+    a.tl.on = ctx->fused_inject;
+    a.tl.ntiles = ctx->ntiles;
+    a.tl.gpt = ctx->d_gpk; a.tl.gbeg = ctx->d_grp_beg; a.tl.src_id = ctx->d_src_id;
+    a.tl.roff = ctx->d_rtile; a.tl.rpt = ctx->d_rpk; a.tl.rid = ctx->d_rid; a.tl.rec_off = ctx->d_rec_off;
+    a.tl.seis = ctx->d_seis; a.tl.seis_off = ctx->d_offs + ctx->S;
+    if (pass == P_ADJ) {
+        a.tl.goff = ctx->d_atile;
+        a.tl.sig = ctx->d_res; a.tl.sig_off = ctx->d_offs + ctx->S;
+        a.tl.sig_ss = p.nt; a.tl.sig_ts = 1;
+        a.tl.sample = 0;
+    } else {
+        a.tl.goff = ctx->d_ftile;
+        a.tl.sig = ctx->d_sig; a.tl.sig_off = ctx->d_offs;
+        a.tl.sig_ss = p.nt; a.tl.sig_ts = 1;
+        a.tl.sample = (pass == P_FWD_HESS) ? 0 : 1;
+    }
     switch (pass) {
     case P_FWD_PLAIN:
         break;
@@ -712,7 +785,7 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
     case P_FWD_HESS: vflags = VF_HESS; sflags = SF_HESS; break;
     case P_ADJ: vflags = VF_ADJOINT | VF_CORR; sflags = SF_CORR; break;
     }
-    KFn vk = v_kernel(p.fdorder, vflags), sk = s_kernel(p.fdorder, p.l, sflags);
+    KFn vk = v_kernel(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
     StepArgs sa = step_args(ctx, pass);
     InjectArgs ia = inject_args(ctx, pass);
@@ -722,10 +795,13 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
         int off = k;
         void *args[2] = {&sa, &off};
         CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
-        void *iargs[2] = {&ia, &off};
-        CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
+        if (!sa.tl.on) {
+            void *iargs[2] = {&ia, &off};
+            CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
+            *nlaunch += 1;
+        }
         CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
-        *nlaunch += 3;
+        *nlaunch += 2;
     }
     advance_step<<<1, 1, 0, ctx->st>>>(ctx->d_nt, nsteps_in_chunk);
     *nlaunch += 1;
@@ -737,7 +813,8 @@ static int run_pass(dsh_ctx *ctx, Pass pass, int nb)
 {
     const int NT = ctx->p.nt;
     const int K = std::min(ctx->chunk, NT);
-    const long long key = ((long long)pass << 40) | ((long long)nb << 20) | (long long)ctx->geo_version;
+    const long long key = ((long long)pass << 40) | ((long long)ctx->fused_inject << 39) | ((long long)nb << 20) |
+                          (long long)ctx->geo_version;
     set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
     ctx->launches += 1;
     static const bool use_graphs = getenv("DSH_NO_GRAPHS") == nullptr;
@@ -767,7 +844,7 @@ static int run_pass(dsh_ctx *ctx, Pass pass, int nb)
     } else {
         exec = it->second;
     }
-    per_chunk = 3LL * K + 1;
+    per_chunk = (ctx->fused_inject ? 2LL : 3LL) * K + 1;
     for (int c = 0; c < nchunks; c++) CK(cudaGraphLaunch(exec, ctx->st));
     ctx->launches += per_chunk * nchunks;
     return DSH_OK;
@@ -1101,7 +1178,7 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
     if (pass == P_FWD_STORE) sflags = SF_STRAIN_OUT;
     if (pass == P_FWD_HESS) { vflags = VF_HESS; sflags = SF_HESS; }
     if (pass == P_ADJ) { vflags = VF_ADJOINT | VF_CORR; sflags = SF_CORR; }
-    KFn vk = v_kernel(p.fdorder, vflags), sk = s_kernel(p.fdorder, p.l, sflags);
+    KFn vk = v_kernel(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
     StepArgs sa = step_args(ctx, (Pass)pass);
     InjectArgs ia = inject_args(ctx, (Pass)pass);
@@ -1118,7 +1195,7 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
         CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
         CK(cudaEventRecord(ev[6 * k + 1], ctx->st));
         CK(cudaEventRecord(ev[6 * k + 2], ctx->st));
-        CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
+        if (!sa.tl.on) CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
         CK(cudaEventRecord(ev[6 * k + 3], ctx->st));
         CK(cudaEventRecord(ev[6 * k + 4], ctx->st));
         CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));

@@ -5,17 +5,19 @@
 
 #define DSH_INSTANTIATE_FD(N)                                                                 \
     namespace dsh {                                                                           \
-    KFn v_kernel_fd##N(int flags)                                                             \
+    template <bool P2>                                                                        \
+    static KFn v_pick_##N(int flags)                                                          \
     {                                                                                         \
         switch (flags) {                                                                      \
-        case 0: return v_step<N, 0>;                                                          \
-        case VF_HESS: return v_step<N, VF_HESS>;                                              \
-        case VF_ADJOINT | VF_CORR: return v_step<N, VF_ADJOINT | VF_CORR>;                    \
-        case VF_ACC_OUT: return v_step<N, VF_ACC_OUT>;                                        \
-        case VF_ADJOINT | VF_ACC_OUT: return v_step<N, VF_ADJOINT | VF_ACC_OUT>;              \
+        case 0: return v_step<N, 0, P2>;                                                      \
+        case VF_HESS: return v_step<N, VF_HESS, P2>;                                          \
+        case VF_ADJOINT | VF_CORR: return v_step<N, VF_ADJOINT | VF_CORR, P2>;                \
+        case VF_ACC_OUT: return v_step<N, VF_ACC_OUT, P2>;                                    \
+        case VF_ADJOINT | VF_ACC_OUT: return v_step<N, VF_ADJOINT | VF_ACC_OUT, P2>;          \
         default: return nullptr;                                                              \
         }                                                                                     \
     }                                                                                         \
+    KFn v_kernel_fd##N(int flags, bool p2) { return p2 ? v_pick_##N<true>(flags) : v_pick_##N<false>(flags); } \
     template <int L>                                                                          \
     static KFn s_pick_##N(int flags)                                                          \
     {                                                                                         \

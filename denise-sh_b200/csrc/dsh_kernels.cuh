@@ -42,6 +42,28 @@ struct PmlCoef {                 /* device copies, index 1..2fw */
     const float *K_y, *a_y, *b_y, *K_y_half, *a_y_half, *b_y_half;
 };
 
+/* Source injection and receiver sampling fused into the velocity kernel:
+ * per slot, the groups of sources (one group per grid point, members in the
+ * reference's order) and the receivers are listed per thread block tile. */
+struct TileLists {
+    const int *goff;             /* [slot][ntiles+1] -> group index range of a tile */
+    const int *gpt;              /* packed point (j << 16 | i) of group g */
+    const int *gbeg;             /* members of group g: src_id[gbeg[g] .. gbeg[g+1]) */
+    const int *src_id;
+    const float *sig;            /* signal of source sid at step nt: sig[sig_off[s] + sid*sig_ss + (nt-1)*sig_ts] */
+    const long long *sig_off;
+    long long sig_ss, sig_ts;
+    const int *roff;             /* [slot][ntiles+1] -> receiver entries of a tile */
+    const int *rpt;              /* packed point of receiver entry e */
+    const int *rid;              /* receiver index (within its slot) of entry e */
+    const int *rec_off;          /* [slot+1]: receivers of slot s are rec_off[s] .. rec_off[s+1] */
+    float *seis;                 /* slot s: seis[seis_off[s] + (nt-1)*ntr_s + r] */
+    const long long *seis_off;
+    int ntiles;
+    int on;                      /* fused path active (all positions inside the grid) */
+    int sample;
+};
+
 struct StepArgs {
     int nx, ny, pitch, hy, fw, free_surf, l;
     int fd12_compat;
@@ -52,7 +74,7 @@ struct StepArgs {
     long long dstride;           /* floats per interior field */
     long long slot_stride;       /* floats between consecutive shot slots */
     float hc[7];
-    float dt, dh, dhi_el, dhi_visc, dthalbe;
+    float dt, dh, inv_dh, dhi_el, dhi_visc, dthalbe;
     PmlCoef pml;
     /* per-slot state (slot 0 base; slot s at + s*slot_stride) */
     float *vy, *sxy, *syz, *r, *q, *psi_vxx, *psi_vyy_v, *psi_sxx, *psi_syy;
@@ -64,11 +86,11 @@ struct StepArgs {
        fwd + s*fwd_slot_stride + k*fwd_step_stride (+ 0/1/2 * dstride for acc/uy/uyx) */
     float *fwd;
     long long fwd_slot_stride, fwd_step_stride;
-    int fwd_step_of_nt_sign;     /* +1: store step nt at k=nt-1-k0; -1: read k = ntd - nt */
     int fwd_k0;                  /* forward: k = nt - 1 - fwd_k0; adjoint: k = fwd_k0 - nt */
     /* compat outputs (Layer-1): explicit vyp1/uy/uyx haloed fields */
     float *out_acc, *out_uy, *out_uyx;
     int *status;                 /* device error word (non-finite detection) */
+    TileLists tl;
 };
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
@@ -89,25 +111,39 @@ __device__ __forceinline__ void st4m(float *p, float4 v, int nvalid)
     if (nvalid > 2) p[2] = v.z;
 }
 
+/* lane k of a float4 with a runtime k (rare paths only) */
+__device__ __forceinline__ float lane(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+__device__ __forceinline__ void set_lane(float4 &v, int k, float x)
+{
+    if (k == 0) v.x = x; else if (k == 1) v.y = x; else if (k == 2) v.z = x; else v.w = x;
+}
+
+/* x / DH: when DH is a power of two the product with the exact reciprocal is
+ * the same correctly rounded value, so P2 kernels multiply. */
+template <bool P2>
+__device__ __forceinline__ float div_dh(float x, const StepArgs &a) { return P2 ? x * a.inv_dh : x / a.dh; }
+
 /*
  * Velocity half-step (update_v_PML.c:51-198 for FDORDER = FDO): per point
  *   sxy_x = sum_m hc[m] (sxy[i+m-1] - sxy[i-m]),  syy_y = sum_m hc[m] (syz[j+m-1] - syz[j-m])
  *   CPML strips: psi = b*psi + a*d;  d = d/K + psi   (full-grid profiles)
  *   vy += b*DT*(sxy_x+syy_y)/DH with b = 1/rho
+ * followed, when the tile holds any, by the source injection of this step
+ * (update_v_PML.c:564-583) and the receiver samples (seismo_ssg.c:17-27).
  * Thread = 4 x-consecutive points of one row; block = 128 x 8 points; z = shot slot.
+ * All global loads are issued before any store so their latencies overlap.
  */
-template <int FDO, int FLAGS>
-__global__ void __launch_bounds__(BX *BY) v_step(StepArgs a, int nt_off)
+template <int FDO, int FLAGS, bool P2>
+__global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
 {
     constexpr int H = FDO / 2;
     constexpr int NL = (H + 3) / 4;          /* float4s left of the own vector (needs H)   */
     constexpr int NR = (H - 1 + 3) / 4;      /* float4s right of the own vector (needs H-1) */
     constexpr int NXS = 4 * (NL + 1 + NR);
-    const int nt = *a.nt_base + nt_off;
-    if (nt > a.nt_last) return;
     const int i0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x);
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
     if (i0 > a.nx || j > a.ny) return;
+    const int nt = *a.nt_base + nt_off;
     const int slot = blockIdx.z;
     const long long so = (long long)slot * a.slot_stride;
     const int pitch = a.pitch;
@@ -115,8 +151,8 @@ __global__ void __launch_bounds__(BX *BY) v_step(StepArgs a, int nt_off)
     const long long hrow = (long long)(j - 1 + a.hy) * pitch;
     const long long drow = (long long)(j - 1) * pitch;
 
-    /* x taps of sxy: xs[p] = sxy[i0 - 4*NL + p] */
-    float xs[NXS];
+    /* ---- loads ---- */
+    float xs[NXS];                           /* xs[p] = sxy[i0 - 4*NL + p] */
     {
         const float *row = a.sxy + so + hrow + col0 - 4 * NL;
 #pragma unroll
@@ -125,8 +161,7 @@ __global__ void __launch_bounds__(BX *BY) v_step(StepArgs a, int nt_off)
             xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
         }
     }
-    /* y taps of syz: rows j-H .. j+H-1 */
-    float4 ys[2 * H];
+    float4 ys[2 * H];                        /* syz rows j-H .. j+H-1 */
     {
         const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * pitch + col0;
 #pragma unroll
@@ -134,9 +169,30 @@ __global__ void __launch_bounds__(BX *BY) v_step(StepArgs a, int nt_off)
     }
     const float4 b4 = ldg4(a.brho + drow + col0);
     float4 vy4 = ld4(a.vy + so + hrow + col0);
-    float4 acc4 = make_float4(0.f, 0.f, 0.f, 0.f), old4 = vy4;
-    const int nvalid = min(4, a.nx - i0 + 1);
+    float4 g4, h4;
+    if (FLAGS & VF_CORR) g4 = ld4(a.grho + so + drow + col0);
+    if (FLAGS & VF_HESS) h4 = ld4(a.hrho + so + drow + col0);
+    int tg0 = 0, tg1 = 0, tr0 = 0, tr1 = 0;
+    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+    if (a.tl.on) {
+        const int *go = a.tl.goff + (long long)slot * (a.tl.ntiles + 1) + tile;
+        tg0 = __ldg(go); tg1 = __ldg(go + 1);
+        if (a.tl.sample) {
+            const int *ro = a.tl.roff + (long long)slot * (a.tl.ntiles + 1) + tile;
+            tr0 = __ldg(ro); tr1 = __ldg(ro + 1);
+        }
+    }
+    if (nt > a.nt_last) return;
+    float4 f4;
+    if (FLAGS & VF_CORR) {                   /* stored forward acceleration of step NT-nt+1 */
+        const long long k = (long long)a.fwd_k0 - nt;
+        f4 = ldg4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
+    }
 
+    /* ---- compute ---- */
+    float4 acc4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 old4 = vy4;
+    const int nvalid = min(4, a.nx - i0 + 1);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const int i = i0 + k;
@@ -180,32 +236,48 @@ __global__ void __launch_bounds__(BX *BY) v_step(StepArgs a, int nt_off)
         }
         const float b = get(b4, k);
         const float s = sxy_x + syy_y;
-        if (!(FLAGS & VF_ADJOINT)) set(acc4, k, b * s / a.dh);
-        set(vy4, k, get(vy4, k) + b * a.dt * s / a.dh);
+        if (!(FLAGS & VF_ADJOINT)) set(acc4, k, div_dh<P2>(b * s, a));
+        set(vy4, k, get(vy4, k) + div_dh<P2>(b * a.dt * s, a));
     }
-    st4m(a.vy + so + hrow + col0, vy4, nvalid);
 
+    /* ---- fused injection (sources in order per point) and sampling ---- */
+    for (int g = tg0; g < tg1; g++) {
+        const int pk = __ldg(a.tl.gpt + g);
+        const int gi = pk & 0xffff, gj = pk >> 16;
+        if (gj == j && gi >= i0 && gi < i0 + 4) {
+            float v = lane(vy4, gi - i0);
+            const float *sg = a.tl.sig + a.tl.sig_off[slot] + (long long)(nt - 1) * a.tl.sig_ts;
+            for (int e = __ldg(a.tl.gbeg + g); e < __ldg(a.tl.gbeg + g + 1); e++)
+                v = v + sg[(long long)__ldg(a.tl.src_id + e) * a.tl.sig_ss];
+            set_lane(vy4, gi - i0, v);
+        }
+    }
+    if (tr1 > tr0) {
+        const int r0 = a.tl.rec_off[slot], ntr = a.tl.rec_off[slot + 1] - r0;
+        float *sm = a.tl.seis + a.tl.seis_off[slot] + (long long)(nt - 1) * ntr;
+        for (int e = tr0; e < tr1; e++) {
+            const int pk = __ldg(a.tl.rpt + e);
+            const int ri = pk & 0xffff, rj = pk >> 16;
+            if (rj == j && ri >= i0 && ri < i0 + 4) sm[__ldg(a.tl.rid + e)] = lane(vy4, ri - i0);
+        }
+    }
+
+    /* ---- stores ---- */
+    st4m(a.vy + so + hrow + col0, vy4, nvalid);
     if (FLAGS & VF_ACC_OUT) st4m(a.out_acc + so + hrow + col0, (FLAGS & VF_ADJOINT) ? old4 : acc4, nvalid);
-    if (FLAGS & VF_CORR) {          /* adjoint: g_rho += vyp1 * forward acceleration of step NT-nt+1 */
-        const long long k = (long long)a.fwd_k0 - nt;
-        const float *fa = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
-        const float4 f4 = ldg4(fa);
-        float *g = a.grho + so + drow + col0;
-        float4 g4 = ld4(g);
+    if (FLAGS & VF_CORR) {          /* adjoint: g_rho += vyp1 * forward acceleration (denise.c:1589) */
         g4.x = g4.x + (old4.x * f4.x); g4.y = g4.y + (old4.y * f4.y);
         g4.z = g4.z + (old4.z * f4.z); g4.w = g4.w + (old4.w * f4.w);
-        st4m(g, g4, nvalid);
+        st4m(a.grho + so + drow + col0, g4, nvalid);
     }
     if (!(FLAGS & VF_ADJOINT) && a.fwd && !(FLAGS & VF_CORR)) {   /* forward storage of vyp1 */
         const long long k = (long long)nt - 1 - a.fwd_k0;
         st4m(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4, nvalid);
     }
     if ((FLAGS & VF_HESS) && nt < a.nt_total) {
-        float *h = a.hrho + so + drow + col0;
-        float4 h4 = ld4(h);
         h4.x = h4.x + (acc4.x * acc4.x); h4.y = h4.y + (acc4.y * acc4.y);
         h4.z = h4.z + (acc4.z * acc4.z); h4.w = h4.w + (acc4.w * acc4.w);
-        st4m(h, h4, nvalid);
+        st4m(a.hrho + so + drow + col0, h4, nvalid);
     }
 }
 
@@ -217,19 +289,21 @@ __global__ void __launch_bounds__(BX *BY) v_step(StepArgs a, int nt_off)
  *   elastic: sxy += uip*vyx, syz += ujp*vyy  (dhi = DT/DH)
  *   visc:    sxy += fipjp*vyx + DT/2*sum r;  r_l = bip_l (r_l cip_l - dip_l vyx);
  *            sxy += DT/2*sum r_new (same for syz / q)   (dhi = 1/DH)
+ * All loads (taps, stresses, memory variables, coefficients, accumulators)
+ * are issued before the first store.
  */
 template <int FDO, int L, int FLAGS>
-__global__ void __launch_bounds__(BX *BY) s_step(StepArgs a, int nt_off)
+__global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
 {
     constexpr int H = FDO / 2;
     constexpr int NL = (H - 1 + 3) / 4;      /* needs vy[i0-(H-1)] */
     constexpr int NR = (H + 3) / 4;          /* needs vy[i0+3+H]   */
     constexpr int NXS = 4 * (NL + 1 + NR);
-    const int nt = *a.nt_base + nt_off;
-    if (nt > a.nt_last) return;
+    constexpr int LL = L > 0 ? L : 1;
     const int i0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x);
     const int j = 1 + blockIdx.y * BY + threadIdx.y;
     if (i0 > a.nx || j > a.ny) return;
+    const int nt = *a.nt_base + nt_off;
     const int slot = blockIdx.z;
     const long long so = (long long)slot * a.slot_stride;
     const int pitch = a.pitch;
@@ -238,6 +312,7 @@ __global__ void __launch_bounds__(BX *BY) s_step(StepArgs a, int nt_off)
     const long long drow = (long long)(j - 1) * pitch;
     const int nvalid = min(4, a.nx - i0 + 1);
 
+    /* ---- loads ---- */
     float xs[NXS];
     {
         const float *row = a.vy + so + hrow + col0 - 4 * NL;
@@ -247,13 +322,44 @@ __global__ void __launch_bounds__(BX *BY) s_step(StepArgs a, int nt_off)
             xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
         }
     }
-    /* rows j-H+1 .. j+H: ys[r] = vy row (j - H + 1 + r) */
-    float4 ys[2 * H];
+    float4 ys[2 * H];                        /* vy rows j-H+1 .. j+H */
     {
         const float *col = a.vy + so + (long long)(j - 1 + a.hy - H + 1) * pitch + col0;
 #pragma unroll
         for (int r = 0; r < 2 * H; r++) ys[r] = ldg4(col + (long long)r * pitch);
     }
+    float *sxy_p = a.sxy + so + hrow + col0;
+    float *syz_p = a.syz + so + hrow + col0;
+    float4 sxy4 = ld4(sxy_p), syz4 = ld4(syz_p);
+    float4 c1, c2;                           /* uip/ujp (elastic) or fipjp/f (visc) */
+    float4 rr[LL], qq[LL], dip4[LL], d4[LL];
+    if (L == 0) {
+        c1 = ldg4(a.uip + drow + col0);
+        c2 = ldg4(a.ujp + drow + col0);
+    } else {
+        c1 = ldg4(a.fipjp + drow + col0);
+        c2 = ldg4(a.f + drow + col0);
+#pragma unroll
+        for (int l = 0; l < L; l++) {
+            rr[l] = ld4(a.r + so + l * a.dstride + drow + col0);
+            qq[l] = ld4(a.q + so + l * a.dstride + drow + col0);
+            dip4[l] = ldg4(a.dip + l * a.dstride + drow + col0);
+            d4[l] = ldg4(a.d + l * a.dstride + drow + col0);
+        }
+    }
+    float4 w4, g4, h4, fy, fu;
+    if (a.ws) w4 = ld4(a.ws + so + drow + col0);
+    if (FLAGS & SF_CORR) g4 = ld4(a.gu + so + drow + col0);
+    if (FLAGS & SF_HESS) h4 = ld4(a.hu + so + drow + col0);
+    if (nt > a.nt_last) return;
+    if (FLAGS & SF_CORR) {
+        const long long k = (long long)a.fwd_k0 - nt;
+        const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
+        fy = ldg4(base + a.dstride);
+        fu = ldg4(base + 2 * a.dstride);
+    }
+
+    /* ---- derivatives and CPML ---- */
     const float dhi = (L > 0) ? a.dhi_visc : a.dhi_el;
     float4 vyx4 = make_float4(0.f, 0.f, 0.f, 0.f), vyy4 = vyx4;
 #pragma unroll
@@ -308,24 +414,17 @@ __global__ void __launch_bounds__(BX *BY) s_step(StepArgs a, int nt_off)
         set(vyy4, k, vyy);
     }
 
-    float *sxy_p = a.sxy + so + hrow + col0;
-    float *syz_p = a.syz + so + hrow + col0;
-    float4 sxy4 = ld4(sxy_p), syz4 = ld4(syz_p);
+    /* ---- stress and memory-variable update ---- */
     if (L == 0) {
-        const float4 uip4 = ldg4(a.uip + drow + col0), ujp4 = ldg4(a.ujp + drow + col0);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            set(sxy4, k, get(sxy4, k) + get(uip4, k) * get(vyx4, k));
-            set(syz4, k, get(syz4, k) + get(ujp4, k) * get(vyy4, k));
+            set(sxy4, k, get(sxy4, k) + get(c1, k) * get(vyx4, k));
+            set(syz4, k, get(syz4, k) + get(c2, k) * get(vyy4, k));
         }
     } else {
-        const float4 fipjp4 = ldg4(a.fipjp + drow + col0), f4 = ldg4(a.f + drow + col0);
-        float4 rr[L > 0 ? L : 1], qq[L > 0 ? L : 1];
         float4 sumr4 = make_float4(0.f, 0.f, 0.f, 0.f), sumq4 = sumr4;
 #pragma unroll
         for (int l = 0; l < L; l++) {
-            rr[l] = ld4(a.r + so + l * a.dstride + drow + col0);
-            qq[l] = ld4(a.q + so + l * a.dstride + drow + col0);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 set(sumr4, k, get(sumr4, k) + get(rr[l], k));
@@ -334,26 +433,22 @@ __global__ void __launch_bounds__(BX *BY) s_step(StepArgs a, int nt_off)
         }
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            set(sxy4, k, get(sxy4, k) + ((get(fipjp4, k) * get(vyx4, k)) + (a.dthalbe * get(sumr4, k))));
-            set(syz4, k, get(syz4, k) + ((get(f4, k) * get(vyy4, k)) + (a.dthalbe * get(sumq4, k))));
+            set(sxy4, k, get(sxy4, k) + ((get(c1, k) * get(vyx4, k)) + (a.dthalbe * get(sumr4, k))));
+            set(syz4, k, get(syz4, k) + ((get(c2, k) * get(vyy4, k)) + (a.dthalbe * get(sumq4, k))));
         }
         sumr4 = make_float4(0.f, 0.f, 0.f, 0.f);
         sumq4 = sumr4;
 #pragma unroll
         for (int l = 0; l < L; l++) {
-            const float4 dip4 = ldg4(a.dip + l * a.dstride + drow + col0);
-            const float4 d4 = ldg4(a.d + l * a.dstride + drow + col0);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                float rn = a.bip[l] * (get(rr[l], k) * a.cip[l] - (get(dip4, k) * get(vyx4, k)));
-                float qn = a.bjm[l] * (get(qq[l], k) * a.cjm[l] - (get(d4, k) * get(vyy4, k)));
+                float rn = a.bip[l] * (get(rr[l], k) * a.cip[l] - (get(dip4[l], k) * get(vyx4, k)));
+                float qn = a.bjm[l] * (get(qq[l], k) * a.cjm[l] - (get(d4[l], k) * get(vyy4, k)));
                 set(rr[l], k, rn);
                 set(qq[l], k, qn);
                 set(sumr4, k, get(sumr4, k) + rn);
                 set(sumq4, k, get(sumq4, k) + qn);
             }
-            st4m(a.r + so + l * a.dstride + drow + col0, rr[l], nvalid);
-            st4m(a.q + so + l * a.dstride + drow + col0, qq[l], nvalid);
         }
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -361,12 +456,18 @@ __global__ void __launch_bounds__(BX *BY) s_step(StepArgs a, int nt_off)
             set(syz4, k, get(syz4, k) + (a.dthalbe * get(sumq4, k)));
         }
     }
+
+    /* ---- stores ---- */
     st4m(sxy_p, sxy4, nvalid);
     st4m(syz_p, syz4, nvalid);
+#pragma unroll
+    for (int l = 0; l < L; l++) {
+        st4m(a.r + so + l * a.dstride + drow + col0, rr[l], nvalid);
+        st4m(a.q + so + l * a.dstride + drow + col0, qq[l], nvalid);
+    }
     if (!(isfinite(sxy4.x) && isfinite(sxy4.y) && isfinite(sxy4.z) && isfinite(sxy4.w) && isfinite(syz4.x) &&
           isfinite(syz4.y) && isfinite(syz4.z) && isfinite(syz4.w) && isfinite(xs[4 * NL])))
         atomicOr(a.status, 1);
-
     if (FLAGS & SF_STRAIN_OUT) {
         if (a.out_uy) {               /* compat fields */
             st4m(a.out_uy + so + hrow + col0, vyy4, nvalid);
@@ -378,36 +479,27 @@ __global__ void __launch_bounds__(BX *BY) s_step(StepArgs a, int nt_off)
             st4m(base + 2 * a.dstride, vyx4, nvalid);
         }
     }
-    if (a.ws) {                       /* energy W += vy^2; vy at the point is xs[4NL+k] */
-        float *w = a.ws + so + drow + col0;
-        float4 w4 = ld4(w);
+    if (a.ws) {                       /* energy W += vy^2 (eprecond.c:11); vy at the point is xs[4NL+k] */
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const float v = xs[4 * NL + k];
             set(w4, k, get(w4, k) + v * v);
         }
-        st4m(w, w4, nvalid);
+        st4m(a.ws + so + drow + col0, w4, nvalid);
     }
-    if (FLAGS & SF_CORR) {
-        const long long k = (long long)a.fwd_k0 - nt;
-        const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
-        const float4 fy = ldg4(base + a.dstride), fu = ldg4(base + 2 * a.dstride);
-        float *g = a.gu + so + drow + col0;
-        float4 g4 = ld4(g);
+    if (FLAGS & SF_CORR) {            /* g_u += uyx_fwd*sxy + uy_fwd*syz (denise.c:1609) */
 #pragma unroll
         for (int kk = 0; kk < 4; kk++)
             set(g4, kk, get(g4, kk) + ((get(fu, kk) * get(sxy4, kk)) + (get(fy, kk) * get(syz4, kk))));
-        st4m(g, g4, nvalid);
+        st4m(a.gu + so + drow + col0, g4, nvalid);
     }
     if ((FLAGS & SF_HESS) && nt < a.nt_total) {
-        float *h = a.hu + so + drow + col0;
-        float4 h4 = ld4(h);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const float eyy = get(vyy4, k), eyx = 0.5f * get(vyx4, k);
             set(h4, k, get(h4, k) + ((eyy * eyy) + (eyx * eyx)));
         }
-        st4m(h, h4, nvalid);
+        st4m(a.hu + so + drow + col0, h4, nvalid);
     }
 }
 
