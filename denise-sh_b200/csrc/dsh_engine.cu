@@ -791,16 +791,32 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
     InjectArgs ia = inject_args(ctx, pass);
     dim3 block(BX, BY, 1);
     dim3 grid((unsigned)((p.nx + 4 * BX - 1) / (4 * BX)), (unsigned)((p.ny + BY - 1) / BY), (unsigned)nb);
+    /* velocity and stress kernels overlap their prologues with the
+     * predecessor through programmatic dependent launch; the first velocity
+     * kernel of a chunk follows the step-counter update and is launched plainly */
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = ctx->st;
+    static const bool use_pdl = getenv("DSH_NO_PDL") == nullptr;
     for (int k = 0; k < nsteps_in_chunk; k++) {
         int off = k;
         void *args[2] = {&sa, &off};
-        CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
+        cfg.attrs = (use_pdl && k > 0) ? &attr : nullptr;
+        cfg.numAttrs = (use_pdl && k > 0) ? 1 : 0;
+        CK(cudaLaunchKernelExC(&cfg, (const void *)vk, args));
         if (!sa.tl.on) {
             void *iargs[2] = {&ia, &off};
             CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
             *nlaunch += 1;
         }
-        CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
+        cfg.attrs = use_pdl ? &attr : nullptr;
+        cfg.numAttrs = use_pdl ? 1 : 0;
+        CK(cudaLaunchKernelExC(&cfg, (const void *)sk, args));
         *nlaunch += 2;
     }
     advance_step<<<1, 1, 0, ctx->st>>>(ctx->d_nt, nsteps_in_chunk);
@@ -809,44 +825,54 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
     return DSH_OK;
 }
 
+static int get_graph(dsh_ctx *ctx, Pass pass, int nb, int K, cudaGraphExec_t *out)
+{
+    const long long key = ((long long)pass << 48) | ((long long)ctx->fused_inject << 47) | ((long long)K << 32) |
+                          ((long long)nb << 16) | (long long)(ctx->geo_version & 0xffff);
+    auto it = ctx->graphs.find(key);
+    if (it != ctx->graphs.end()) { *out = it->second; return DSH_OK; }
+    cudaGraph_t g;
+    long long nl = 0;
+    CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
+    int rc = launch_step_chunk(ctx, pass, nb, K, &nl);
+    cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
+    if (rc != DSH_OK) return rc;
+    CK(e);
+    cudaGraphExec_t exec;
+    CK(cudaGraphInstantiate(&exec, g, 0));
+    cudaGraphDestroy(g);
+    ctx->graphs[key] = exec;
+    *out = exec;
+    return DSH_OK;
+}
+
+/* One pass over NT steps: graphs of `chunk` steps replayed NT/chunk times,
+ * then one graph for the remaining NT % chunk steps. */
 static int run_pass(dsh_ctx *ctx, Pass pass, int nb)
 {
     const int NT = ctx->p.nt;
     const int K = std::min(ctx->chunk, NT);
-    const long long key = ((long long)pass << 40) | ((long long)ctx->fused_inject << 39) | ((long long)nb << 20) |
-                          (long long)ctx->geo_version;
+    const int nfull = NT / K, rem = NT % K;
+    const long long per_step = ctx->fused_inject ? 2 : 3;
     set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
     ctx->launches += 1;
     static const bool use_graphs = getenv("DSH_NO_GRAPHS") == nullptr;
-    const int nchunks = (NT + K - 1) / K;
-    long long per_chunk = 0;
     if (!use_graphs) {
-        for (int c = 0; c < nchunks; c++) {
+        for (int c = 0; c < nfull + (rem ? 1 : 0); c++) {
             long long nl = 0;
-            int rc = launch_step_chunk(ctx, pass, nb, K, &nl);
+            int rc = launch_step_chunk(ctx, pass, nb, c < nfull ? K : rem, &nl);
             if (rc != DSH_OK) return rc;
             ctx->launches += nl;
         }
         return DSH_OK;
     }
-    auto it = ctx->graphs.find(key);
-    cudaGraphExec_t exec;
-    if (it == ctx->graphs.end()) {
-        cudaGraph_t g;
-        CK(cudaStreamBeginCapture(ctx->st, cudaStreamCaptureModeThreadLocal));
-        int rc = launch_step_chunk(ctx, pass, nb, K, &per_chunk);
-        cudaError_t e = cudaStreamEndCapture(ctx->st, &g);
-        if (rc != DSH_OK) return rc;
-        CK(e);
-        CK(cudaGraphInstantiate(&exec, g, 0));
-        cudaGraphDestroy(g);
-        ctx->graphs[key] = exec;
-    } else {
-        exec = it->second;
-    }
-    per_chunk = (ctx->fused_inject ? 2LL : 3LL) * K + 1;
-    for (int c = 0; c < nchunks; c++) CK(cudaGraphLaunch(exec, ctx->st));
-    ctx->launches += per_chunk * nchunks;
+    cudaGraphExec_t full, tail = nullptr;
+    int rc = get_graph(ctx, pass, nb, K, &full);
+    if (rc != DSH_OK) return rc;
+    if (rem && (rc = get_graph(ctx, pass, nb, rem, &tail)) != DSH_OK) return rc;
+    for (int c = 0; c < nfull; c++) CK(cudaGraphLaunch(full, ctx->st));
+    if (rem) CK(cudaGraphLaunch(tail, ctx->st));
+    ctx->launches += (per_step * K + 1) * nfull + (rem ? per_step * rem + 1 : 0);
     return DSH_OK;
 }
 

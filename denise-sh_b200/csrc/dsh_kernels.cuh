@@ -111,6 +111,15 @@ __device__ __forceinline__ void st4m(float *p, float4 v, int nvalid)
     if (nvalid > 2) p[2] = v.z;
 }
 
+/* Programmatic dependent launch (PTX griddepcontrol): a kernel launched with
+ * programmatic stream serialization may start while its predecessor drains.
+ * It reads only data its predecessor does not write until pdl_wait() returns
+ * (the predecessor grid has completed and its writes are visible), and calls
+ * pdl_trigger() after its own wait so the next kernel can start prefetching.
+ * Without the launch attribute both are no-ops. */
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
 /* lane k of a float4 with a runtime k (rare paths only) */
 __device__ __forceinline__ float lane(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
 __device__ __forceinline__ void set_lane(float4 &v, int k, float x)
@@ -151,25 +160,10 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
     const long long hrow = (long long)(j - 1 + a.hy) * pitch;
     const long long drow = (long long)(j - 1) * pitch;
 
-    /* ---- loads ---- */
-    float xs[NXS];                           /* xs[p] = sxy[i0 - 4*NL + p] */
-    {
-        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
-#pragma unroll
-        for (int v = 0; v < NL + 1 + NR; v++) {
-            float4 t = ldg4(row + 4 * v);
-            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
-        }
-    }
-    float4 ys[2 * H];                        /* syz rows j-H .. j+H-1 */
-    {
-        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * pitch + col0;
-#pragma unroll
-        for (int r = 0; r < 2 * H; r++) ys[r] = ldg4(col + (long long)r * pitch);
-    }
+    /* ---- loads of data the preceding stress kernel does not write ---- */
     const float4 b4 = ldg4(a.brho + drow + col0);
     float4 vy4 = ld4(a.vy + so + hrow + col0);
-    float4 g4, h4;
+    float4 g4, h4, f4;
     if (FLAGS & VF_CORR) g4 = ld4(a.grho + so + drow + col0);
     if (FLAGS & VF_HESS) h4 = ld4(a.hrho + so + drow + col0);
     int tg0 = 0, tg1 = 0, tr0 = 0, tr1 = 0;
@@ -183,10 +177,28 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
         }
     }
     if (nt > a.nt_last) return;
-    float4 f4;
     if (FLAGS & VF_CORR) {                   /* stored forward acceleration of step NT-nt+1 */
         const long long k = (long long)a.fwd_k0 - nt;
         f4 = ldg4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
+    }
+    pdl_wait();                              /* stresses of the previous step are complete */
+    pdl_trigger();
+
+    /* ---- stress taps ---- */
+    float xs[NXS];                           /* xs[p] = sxy[i0 - 4*NL + p] */
+    {
+        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
+#pragma unroll
+        for (int v = 0; v < NL + 1 + NR; v++) {
+            float4 t = ld4(row + 4 * v);
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+    }
+    float4 ys[2 * H];                        /* syz rows j-H .. j+H-1 */
+    {
+        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * pitch + col0;
+#pragma unroll
+        for (int r = 0; r < 2 * H; r++) ys[r] = ld4(col + (long long)r * pitch);
     }
 
     /* ---- compute ---- */
@@ -312,22 +324,7 @@ __global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
     const long long drow = (long long)(j - 1) * pitch;
     const int nvalid = min(4, a.nx - i0 + 1);
 
-    /* ---- loads ---- */
-    float xs[NXS];
-    {
-        const float *row = a.vy + so + hrow + col0 - 4 * NL;
-#pragma unroll
-        for (int v = 0; v < NL + 1 + NR; v++) {
-            float4 t = ldg4(row + 4 * v);
-            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
-        }
-    }
-    float4 ys[2 * H];                        /* vy rows j-H+1 .. j+H */
-    {
-        const float *col = a.vy + so + (long long)(j - 1 + a.hy - H + 1) * pitch + col0;
-#pragma unroll
-        for (int r = 0; r < 2 * H; r++) ys[r] = ldg4(col + (long long)r * pitch);
-    }
+    /* ---- loads of data the preceding velocity kernel does not write ---- */
     float *sxy_p = a.sxy + so + hrow + col0;
     float *syz_p = a.syz + so + hrow + col0;
     float4 sxy4 = ld4(sxy_p), syz4 = ld4(syz_p);
@@ -357,6 +354,25 @@ __global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
         const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
         fy = ldg4(base + a.dstride);
         fu = ldg4(base + 2 * a.dstride);
+    }
+    pdl_wait();                              /* velocities of this step are complete */
+    pdl_trigger();
+
+    /* ---- velocity taps ---- */
+    float xs[NXS];
+    {
+        const float *row = a.vy + so + hrow + col0 - 4 * NL;
+#pragma unroll
+        for (int v = 0; v < NL + 1 + NR; v++) {
+            float4 t = ld4(row + 4 * v);
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+    }
+    float4 ys[2 * H];                        /* vy rows j-H+1 .. j+H */
+    {
+        const float *col = a.vy + so + (long long)(j - 1 + a.hy - H + 1) * pitch + col0;
+#pragma unroll
+        for (int r = 0; r < 2 * H; r++) ys[r] = ld4(col + (long long)r * pitch);
     }
 
     /* ---- derivatives and CPML ---- */
