@@ -79,6 +79,8 @@ def lib() -> C.CDLL:
         L.dsh_params_default.argtypes = [C.POINTER(Params)]
         L.dsh_set_stream.argtypes = [C.c_void_p, C.c_void_p]
         L.dsh_profile_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
+        L.dsh_residual_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p]
         L.dsh_setup_holberg.argtypes = [C.c_int, C.c_int, C.c_void_p]
         L.dsh_setup_pml.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
                                     C.c_float, C.c_float, C.c_void_p]
@@ -263,6 +265,16 @@ class Engine:
         s = Stats()
         _check(lib().dsh_get_stats(self.h, C.byref(s)), "dsh_get_stats")
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+NOALLOC_MAX_SHOTS = 64
+
+
+def residual_noalloc(nshots: int, ntr: int, nt: int, syn_ptr: int, obs_ptr: int, res_ptr: int, l2_ptr: int,
+                     stream: int | None = None) -> None:
+    """Allocation-free residual + L2 on device pointers (see dsh_residual_noalloc in include/dsh.h)."""
+    _check(lib().dsh_residual_noalloc(nshots, ntr, nt, syn_ptr, obs_ptr, res_ptr, l2_ptr, stream),
+           "dsh_residual_noalloc")
 
 
 def _split(flat, shots, nt):

@@ -142,6 +142,27 @@ int dsh_set_stream(dsh_ctx *ctx, void *stream);
  * dsh_gradient on the same shots; it overwrites the wavefield state. */
 int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
 
+/* Residual and L2 misfit with no device allocation at all.  This entry point
+ * has no counterpart in the reference; it exists for callers that cannot
+ * allocate device memory themselves or let a library do it — for instance an
+ * application whose device memory is entirely owned by its own pool or arena,
+ * or a misfit evaluation inside a loop that must not touch the allocator.
+ * It computes, for nshots gathers of ntr traces x nt samples (device arrays
+ * [nshots][ntr][nt]), the time-reversed residual res (the adjoint source, as
+ * dsh_gradient forms it) and per-shot L2 = sum res^2 (device doubles [nshots]),
+ * on the caller's stream (a cudaStream_t as void*, NULL = default stream) and
+ * the caller's current device.  Its reduction scratch is a fixed array inside
+ * the library (DSH_NOALLOC_MAX_SHOTS shots, 151,552 bytes held by every GPU
+ * that loads the library until the process exits); larger nshots is rejected
+ * with DSH_ERR_PARAM.  The first call on a device looks up that array's device
+ * address (cudaGetSymbolAddress), so make the first call on each device before
+ * any stream capture.  All calls on a device share the array and it keeps the
+ * last call's contents; calls that overlap on the GPU race on it and must be
+ * serialised by the caller. */
+#define DSH_NOALLOC_MAX_SHOTS 64
+int dsh_residual_noalloc(int nshots, int ntr, int nt, const float *syn, const float *obs, float *res, double *l2,
+                         void *stream);
+
 /* Statistics of the last dsh_forward / dsh_gradient call. */
 typedef struct dsh_stats {
     double ms_forward, ms_adjoint, ms_total;   /* device time (CUDA events) */
