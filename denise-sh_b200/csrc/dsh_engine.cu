@@ -30,7 +30,10 @@ using namespace dsh;
 
 namespace {
 
-enum Pass { P_FWD_PLAIN = 0, P_FWD_STORE = 1, P_FWD_HESS = 2, P_ADJ = 3 };
+/* passes: plain forward (modelling), forward storing every step, forward
+ * with Hessian sums, adjoint, forward saving only checkpoints, and the
+ * recomputation of one segment from a checkpoint on the shadow state */
+enum Pass { P_FWD_PLAIN = 0, P_FWD_STORE = 1, P_FWD_HESS = 2, P_ADJ = 3, P_FWD_CKPT = 4, P_RECOMP = 5 };
 
 constexpr int RED_BLOCKS = 296;        /* 2 x 148 SMs for reductions */
 constexpr int RED_THREADS = 256;
@@ -243,6 +246,11 @@ struct dsh_ctx {
     float *fwd = nullptr;
     long long fwd_slot_stride = 0, fwd_step_stride = 0;
     size_t fwd_bytes = 0;
+    int fwd_mod = 0;                      /* stored steps per slot: NT (full storage) or C (checkpointing) */
+    int ckpt_c = 0;                       /* checkpoint interval C; 0 = full storage */
+    float *ckpt = nullptr;                /* checkpoints: [k][slot][state] */
+    size_t ckpt_bytes = 0;
+    float *shadow = nullptr;              /* recomputation state, same slot layout as slab */
     /* geometry */
     int *d_geo = nullptr;
     long long geo_cap = 0;
@@ -407,6 +415,7 @@ extern "C" int dsh_destroy(dsh_ctx *ctx)
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     drop_graphs(ctx);
     cudaFree(ctx->slab); cudaFree(ctx->model); cudaFree(ctx->pml); cudaFree(ctx->sums); cudaFree(ctx->fwd);
+    cudaFree(ctx->ckpt); cudaFree(ctx->shadow);
     cudaFree(ctx->d_geo); cudaFree(ctx->d_offs); cudaFree(ctx->d_sig); cudaFree(ctx->d_seis); cudaFree(ctx->d_res);
     cudaFree(ctx->d_obs); cudaFree(ctx->d_tmp); cudaFree(ctx->d_out); cudaFree(ctx->d_nt); cudaFree(ctx->d_part); cudaFree(ctx->d_l2);
     cudaFree(ctx->d_wemax);
@@ -703,7 +712,7 @@ static StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.pml.K_x_half = pm + 3 * vlen; a.pml.a_x_half = pm + 4 * vlen; a.pml.b_x_half = pm + 5 * vlen;
     a.pml.K_y = pm + 6 * vlen; a.pml.a_y = pm + 7 * vlen; a.pml.b_y = pm + 8 * vlen;
     a.pml.K_y_half = pm + 9 * vlen; a.pml.a_y_half = pm + 10 * vlen; a.pml.b_y_half = pm + 11 * vlen;
-    float *sl = ctx->slab;
+    float *sl = (pass == P_RECOMP) ? ctx->shadow : ctx->slab;
     a.vy = sl + ctx->o_vy; a.sxy = sl + ctx->o_sxy; a.syz = sl + ctx->o_syz;
     a.r = sl + ctx->o_r; a.q = sl + ctx->o_q;
     a.psi_vxx = sl + ctx->o_pvxx; a.psi_sxx = sl + ctx->o_psxx;
@@ -713,6 +722,7 @@ static StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.dip = ctx->m_dip; a.d = ctx->m_d;
     for (int l = 0; l < 4; l++) { a.bip[l] = ctx->bip[l]; a.bjm[l] = ctx->bjm[l]; a.cip[l] = ctx->cip[l]; a.cjm[l] = ctx->cjm[l]; }
     a.fwd_slot_stride = ctx->fwd_slot_stride;
+    a.fwd_mod = ctx->fwd_mod > 0 ? ctx->fwd_mod : p.nt;
     a.fwd_step_stride = ctx->fwd_step_stride;
     a.status = ctx->d_status;
     /* fused injection / sampling lists */
@@ -730,19 +740,25 @@ static StepArgs step_args(dsh_ctx *ctx, Pass pass)
         a.tl.goff = ctx->d_ftile;
         a.tl.sig = ctx->d_sig; a.tl.sig_off = ctx->d_offs;
         a.tl.sig_ss = p.nt; a.tl.sig_ts = 1;
-        a.tl.sample = (pass == P_FWD_HESS) ? 0 : 1;
+        a.tl.sample = (pass == P_FWD_HESS || pass == P_RECOMP) ? 0 : 1;
     }
     switch (pass) {
     case P_FWD_PLAIN:
         break;
     case P_FWD_STORE:
-        a.fwd = ctx->fwd; a.fwd_k0 = 0;
+        a.fwd = ctx->fwd;
         if (p.eprecond == 1 || p.eprecond == 3) a.ws = sl + ctx->o_ws;
+        break;
+    case P_FWD_CKPT:
+        if (p.eprecond == 1 || p.eprecond == 3) a.ws = sl + ctx->o_ws;
+        break;
+    case P_RECOMP:
+        a.fwd = ctx->fwd;
         break;
     case P_FWD_HESS:
         break;
     case P_ADJ:
-        a.fwd = ctx->fwd; a.fwd_k0 = p.nt;
+        a.fwd = ctx->fwd;
         if (p.eprecond == 1) a.ws = sl + ctx->o_wr;
         break;
     }
@@ -757,7 +773,7 @@ static InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
     a.nt_last = ctx->p.nt;
     a.nt_total = ctx->p.nt;
     a.slot_stride = ctx->slot_stride;
-    a.vy = ctx->slab + ctx->o_vy;
+    a.vy = (pass == P_RECOMP ? ctx->shadow : ctx->slab) + ctx->o_vy;
     a.grp_pt = ctx->d_grp_pt; a.grp_beg = ctx->d_grp_beg; a.src_id = ctx->d_src_id;
     a.rec_off = ctx->d_rec_off; a.rec_pt = ctx->d_rec_pt;
     a.seis = ctx->d_seis; a.seis_off = ctx->d_offs + ctx->S;
@@ -770,7 +786,7 @@ static InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
         a.grp_off = ctx->d_fgrp_off;
         a.sig = ctx->d_sig; a.sig_off = ctx->d_offs;
         a.sig_ss = ctx->p.nt; a.sig_ts = 1;
-        a.sample = (pass == P_FWD_HESS) ? 0 : 1;
+        a.sample = (pass == P_FWD_HESS || pass == P_RECOMP) ? 0 : 1;
     }
     return a;
 }
@@ -784,6 +800,8 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
     case P_FWD_STORE: sflags = SF_STRAIN_OUT; break;
     case P_FWD_HESS: vflags = VF_HESS; sflags = SF_HESS; break;
     case P_ADJ: vflags = VF_ADJOINT | VF_CORR; sflags = SF_CORR; break;
+    case P_FWD_CKPT: break;
+    case P_RECOMP: sflags = SF_STRAIN_OUT; break;
     }
     KFn vk = v_kernel(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
@@ -846,15 +864,15 @@ static int get_graph(dsh_ctx *ctx, Pass pass, int nb, int K, cudaGraphExec_t *ou
     return DSH_OK;
 }
 
-/* One pass over NT steps: graphs of `chunk` steps replayed NT/chunk times,
- * then one graph for the remaining NT % chunk steps. */
-static int run_pass(dsh_ctx *ctx, Pass pass, int nb)
+/* Steps n0 .. n0+count-1 of a pass: graphs of `chunk` steps replayed
+ * count/chunk times, then one graph for the remaining steps. */
+static int run_steps(dsh_ctx *ctx, Pass pass, int nb, int n0, int count)
 {
-    const int NT = ctx->p.nt;
-    const int K = std::min(ctx->chunk, NT);
-    const int nfull = NT / K, rem = NT % K;
+    if (count <= 0) return DSH_OK;
+    const int K = std::min(ctx->chunk, count);
+    const int nfull = count / K, rem = count % K;
     const long long per_step = ctx->fused_inject ? 2 : 3;
-    set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
+    set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, n0);
     ctx->launches += 1;
     static const bool use_graphs = getenv("DSH_NO_GRAPHS") == nullptr;
     if (!use_graphs) {
@@ -873,6 +891,61 @@ static int run_pass(dsh_ctx *ctx, Pass pass, int nb)
     for (int c = 0; c < nfull; c++) CK(cudaGraphLaunch(full, ctx->st));
     if (rem) CK(cudaGraphLaunch(tail, ctx->st));
     ctx->launches += (per_step * K + 1) * nfull + (rem ? per_step * rem + 1 : 0);
+    return DSH_OK;
+}
+
+static int run_pass(dsh_ctx *ctx, Pass pass, int nb) { return run_steps(ctx, pass, nb, 1, ctx->p.nt); }
+
+/* state (wavefields, memory variables, CPML memory) of slots [0, nb):
+ * copy between a slab and checkpoint k */
+static int copy_state(dsh_ctx *ctx, int nb, float *dst, size_t dpitch, const float *src, size_t spitch)
+{
+    CK(cudaMemcpy2DAsync(dst, dpitch * sizeof(float), src, spitch * sizeof(float),
+                         (size_t)ctx->o_state_end * sizeof(float), nb, cudaMemcpyDeviceToDevice, ctx->st));
+    return DSH_OK;
+}
+
+/* Forward pass of a gradient: every step stored (full storage), or the state
+ * saved after every C steps (checkpoint k = state after step (k+1)*C). */
+static int forward_for_gradient(dsh_ctx *ctx, int nb)
+{
+    const int NT = ctx->p.nt;
+    if (!ctx->ckpt_c) return run_pass(ctx, P_FWD_STORE, nb);
+    const int C = ctx->ckpt_c, nseg = (NT + C - 1) / C;
+    for (int k = 0; k < nseg; k++) {
+        const int a = k * C, len = std::min(C, NT - a);
+        int rc = run_steps(ctx, P_FWD_CKPT, nb, a + 1, len);
+        if (rc != DSH_OK) return rc;
+        if (k < nseg - 1) {
+            float *dst = ctx->ckpt + (size_t)k * ctx->S * ctx->o_state_end;
+            if ((rc = copy_state(ctx, nb, dst, ctx->o_state_end, ctx->slab, ctx->slot_stride)) != DSH_OK) return rc;
+        }
+    }
+    return DSH_OK;
+}
+
+/* Adjoint pass: with checkpoints, segments are processed last to first:
+ * restore the checkpoint into the shadow state, recompute the segment's
+ * forward steps into the C-step buffer, then run the adjoint steps that
+ * correlate with them (adjoint step nt uses forward step NT-nt+1). */
+static int adjoint_for_gradient(dsh_ctx *ctx, int nb)
+{
+    const int NT = ctx->p.nt;
+    if (!ctx->ckpt_c) return run_pass(ctx, P_ADJ, nb);
+    const int C = ctx->ckpt_c, nseg = (NT + C - 1) / C;
+    for (int k = nseg - 1; k >= 0; k--) {
+        const int a = k * C, b = std::min(a + C, NT);
+        int rc;
+        if (k == 0) {
+            CK(cudaMemset2DAsync(ctx->shadow, (size_t)ctx->slot_stride * sizeof(float), 0,
+                                 (size_t)ctx->o_state_end * sizeof(float), nb, ctx->st));
+        } else {
+            const float *src = ctx->ckpt + (size_t)(k - 1) * ctx->S * ctx->o_state_end;
+            if ((rc = copy_state(ctx, nb, ctx->shadow, ctx->slot_stride, src, ctx->o_state_end)) != DSH_OK) return rc;
+        }
+        if ((rc = run_steps(ctx, P_RECOMP, nb, a + 1, b - a)) != DSH_OK) return rc;
+        if ((rc = run_steps(ctx, P_ADJ, nb, NT - b + 1, b - a)) != DSH_OK) return rc;
+    }
     return DSH_OK;
 }
 
@@ -898,21 +971,55 @@ static int check_status(dsh_ctx *ctx)
     return DSH_OK;
 }
 
+/* Storage for the adjoint's forward wavefields.  Full storage (3 fields per
+ * step and shot) when it fits the budget (mem_budget, or the free device
+ * memory less a 2 GiB reserve when mem_budget is 0); otherwise checkpoints
+ * every C steps, C = sqrt(NT*(3+2L)/3) (minimises checkpoints + C-step buffer),
+ * with one recomputed forward pass. */
 static int ensure_storage(dsh_ctx *ctx)
 {
     const dsh_params &p = ctx->p;
-    ctx->fwd_step_stride = 3 * ctx->dstride;
-    ctx->fwd_slot_stride = (long long)p.nt * ctx->fwd_step_stride;
-    const size_t need = (size_t)ctx->S * ctx->fwd_slot_stride * sizeof(float);
-    if (p.mem_budget > 0 && (long long)need > p.mem_budget) return DSH_ERR_OOM;
-    if (ctx->fwd && ctx->fwd_bytes >= need) return DSH_OK;
-    cudaFree(ctx->fwd);
-    ctx->fwd = nullptr;
-    ctx->fwd_bytes = 0;
-    if (cudaMalloc(&ctx->fwd, need) != cudaSuccess) { cudaGetLastError(); return DSH_ERR_OOM; }
-    ctx->fwd_bytes = need;
+    const size_t S = ctx->S, D = ctx->dstride, st = ctx->o_state_end;
+    const size_t full = S * (size_t)p.nt * 3 * D * sizeof(float);
+    int C = (int)std::lround(std::sqrt((double)p.nt * (3.0 + 2.0 * p.l) / 3.0));
+    C = std::max(1, std::min(C, p.nt));
+    const int nck = (p.nt + C - 1) / C - 1;
+    const size_t ckpt_need = S * (size_t)C * 3 * D * sizeof(float) + (size_t)nck * S * st * sizeof(float) +
+                             S * (size_t)ctx->slot_stride * sizeof(float);
+    if (ctx->fwd && ((ctx->ckpt_c == 0 && ctx->fwd_bytes >= full) || (ctx->ckpt_c == C && ctx->ckpt))) return DSH_OK;
+    cudaFree(ctx->fwd); cudaFree(ctx->ckpt); cudaFree(ctx->shadow);
+    ctx->fwd = ctx->ckpt = ctx->shadow = nullptr;
+    ctx->fwd_bytes = ctx->ckpt_bytes = 0;
     drop_graphs(ctx);
     ctx->geo_version++;
+    long long budget = p.mem_budget;
+    if (budget <= 0) {
+        size_t fr = 0, tot = 0;
+        CK(cudaMemGetInfo(&fr, &tot));
+        budget = (long long)fr - (2LL << 30);
+    }
+    ctx->fwd_step_stride = 3 * D;
+    if ((long long)full <= budget) {
+        if (cudaMalloc(&ctx->fwd, full) != cudaSuccess) { cudaGetLastError(); return DSH_ERR_OOM; }
+        ctx->fwd_bytes = full;
+        ctx->fwd_mod = p.nt;
+        ctx->ckpt_c = 0;
+    } else {
+        if ((long long)ckpt_need > budget) return DSH_ERR_OOM;
+        const size_t seg = S * (size_t)C * 3 * D * sizeof(float);
+        if (cudaMalloc(&ctx->fwd, seg) != cudaSuccess) { cudaGetLastError(); return DSH_ERR_OOM; }
+        if (nck > 0 && cudaMalloc(&ctx->ckpt, (size_t)nck * S * st * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError(); return DSH_ERR_OOM;
+        }
+        if (cudaMalloc(&ctx->shadow, S * (size_t)ctx->slot_stride * sizeof(float)) != cudaSuccess) {
+            cudaGetLastError(); return DSH_ERR_OOM;
+        }
+        ctx->fwd_bytes = seg;
+        ctx->ckpt_bytes = (size_t)nck * S * st * sizeof(float) + S * (size_t)ctx->slot_stride * sizeof(float);
+        ctx->fwd_mod = C;
+        ctx->ckpt_c = C;
+    }
+    ctx->fwd_slot_stride = (long long)ctx->fwd_mod * ctx->fwd_step_stride;
     return DSH_OK;
 }
 
@@ -1011,7 +1118,7 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
         cudaEvent_t e0, e1, e2;
         cudaEventCreate(&e0); cudaEventCreate(&e1); cudaEventCreate(&e2);
         cudaEventRecord(e0, ctx->st);
-        if ((rc = run_pass(ctx, P_FWD_STORE, nb)) != DSH_OK) return rc;
+        if ((rc = forward_for_gradient(ctx, nb)) != DSH_OK) return rc;
         cudaEventRecord(e1, ctx->st);
         /* residual + L2 */
         residual_kernel<<<dim3(RED_BLOCKS, nb), RED_THREADS, 0, ctx->st>>>(p.nt, ctx->d_rec_off, ctx->d_seis,
@@ -1024,7 +1131,7 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
             if ((rc = copy_seis_out(ctx, nb, seis_host + out, nullptr)) != DSH_OK) return rc;
         }
         if ((rc = zero_slots(ctx, nb, false)) != DSH_OK) return rc;
-        if ((rc = run_pass(ctx, P_ADJ, nb)) != DSH_OK) return rc;
+        if ((rc = adjoint_for_gradient(ctx, nb)) != DSH_OK) return rc;
         cudaEventRecord(e2, ctx->st);
         if (ws_host || wr_host) {
             for (int s = 0; s < nb; s++) {
@@ -1083,8 +1190,8 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
     ctx->stats.ms_forward = ms_f; ctx->stats.ms_adjoint = ms_a; ctx->stats.ms_total = ms;
     ctx->stats.kernel_launches = ctx->launches;
     ctx->stats.point_updates = 2LL * p.nx * p.ny * p.nt * nshots;
-    ctx->stats.storage_bytes = (long long)ctx->fwd_bytes;
-    ctx->stats.checkpoint_interval = 0;
+    ctx->stats.storage_bytes = (long long)(ctx->fwd_bytes + ctx->ckpt_bytes);
+    ctx->stats.checkpoint_interval = ctx->ckpt_c;
     if (l2) *l2 = l2_total;
     return check_status(ctx);
 }
@@ -1196,6 +1303,7 @@ extern "C" int dsh_set_stream(dsh_ctx *ctx, void *stream)
 extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3)
 {
     if (!ctx || !out_ms3 || pass < 0 || pass > 3 || nsteps < 1 || nsteps > ctx->p.nt) return DSH_ERR_PARAM;
+    if (ctx->ckpt_c && (pass == P_FWD_STORE || pass == P_ADJ) && nsteps > ctx->ckpt_c) nsteps = ctx->ckpt_c;
     if (!ctx->model_set || ctx->ntr_b.empty() || ((pass == P_FWD_STORE || pass == P_ADJ) && !ctx->fwd)) return DSH_ERR_STATE;
     CK(cudaSetDevice(ctx->dev));
     const dsh_params &p = ctx->p;

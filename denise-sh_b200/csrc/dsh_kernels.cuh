@@ -86,7 +86,8 @@ struct StepArgs {
        fwd + s*fwd_slot_stride + k*fwd_step_stride (+ 0/1/2 * dstride for acc/uy/uyx) */
     float *fwd;
     long long fwd_slot_stride, fwd_step_stride;
-    int fwd_k0;                  /* forward: k = nt - 1 - fwd_k0; adjoint: k = fwd_k0 - nt */
+    int fwd_mod;                 /* stored-step index: forward (nt-1) % fwd_mod, adjoint (NT-nt) % fwd_mod
+                                    (fwd_mod = NT: full storage; = C: a C-step segment buffer) */
     /* compat outputs (Layer-1): explicit vyp1/uy/uyx haloed fields */
     float *out_acc, *out_uy, *out_uyx;
     int *status;                 /* device error word (non-finite detection) */
@@ -178,7 +179,7 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
     }
     if (nt > a.nt_last) return;
     if (FLAGS & VF_CORR) {                   /* stored forward acceleration of step NT-nt+1 */
-        const long long k = (long long)a.fwd_k0 - nt;
+        const long long k = (a.nt_total - nt) % a.fwd_mod;
         f4 = ldg4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
     }
     pdl_wait();                              /* stresses of the previous step are complete */
@@ -283,7 +284,7 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
         st4m(a.grho + so + drow + col0, g4, nvalid);
     }
     if (!(FLAGS & VF_ADJOINT) && a.fwd && !(FLAGS & VF_CORR)) {   /* forward storage of vyp1 */
-        const long long k = (long long)nt - 1 - a.fwd_k0;
+        const long long k = (nt - 1) % a.fwd_mod;
         st4m(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4, nvalid);
     }
     if ((FLAGS & VF_HESS) && nt < a.nt_total) {
@@ -350,7 +351,7 @@ __global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
     if (FLAGS & SF_HESS) h4 = ld4(a.hu + so + drow + col0);
     if (nt > a.nt_last) return;
     if (FLAGS & SF_CORR) {
-        const long long k = (long long)a.fwd_k0 - nt;
+        const long long k = (a.nt_total - nt) % a.fwd_mod;
         const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
         fy = ldg4(base + a.dstride);
         fu = ldg4(base + 2 * a.dstride);
@@ -489,7 +490,7 @@ __global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
             st4m(a.out_uy + so + hrow + col0, vyy4, nvalid);
             st4m(a.out_uyx + so + hrow + col0, vyx4, nvalid);
         } else {                      /* forward storage: uy at +dstride, uyx at +2*dstride */
-            const long long k = (long long)nt - 1 - a.fwd_k0;
+            const long long k = (nt - 1) % a.fwd_mod;
             float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
             st4m(base + a.dstride, vyy4, nvalid);
             st4m(base + 2 * a.dstride, vyx4, nvalid);
