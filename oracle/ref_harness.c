@@ -39,6 +39,41 @@ typedef struct {
     float fl[8];
 } refh_params;
 
+/* Implementation switch (tests of a reference-signature replacement):
+ * the loops below call these pointers; NULL restores the reference's own. */
+typedef void (*fn_v_t)(int, int, int, int, int, float **, float **, float **, float **, float **, float **, float **,
+                       float **, float **, int, float **, float *, int, int, float *, float *, float *, float *,
+                       float *, float *, float *, float *, float *, float *, float *, float *, float **, float **);
+typedef void (*fn_se_t)(int, int, int, int, float **, float **, float **, float **, float **, float **, float **,
+                        float **, float **, float **, float *, int, float *, float *, float *, float *, float *,
+                        float *, float *, float *, float *, float *, float *, float *, float **, float **);
+typedef void (*fn_sv_t)(int, int, int, int, float **, float **, float **, float **, float **, float **, float **,
+                        float **, float *, int, float ***, float ***, float ***, float **, float **, float **,
+                        float *, float *, float *, float *, float ***, float ***, float ***, float *, float *,
+                        float *, float *, float *, float *, float *, float *, float *, float *, float *, float *,
+                        float **, float **);
+typedef void (*fn_ep_t)(float **, float **);
+typedef void (*fn_ep1_t)(float **, float **, float **);
+static fn_v_t impl_v = NULL;
+static fn_se_t impl_se = NULL;
+static fn_sv_t impl_sv = NULL;
+static fn_ep_t impl_ep = NULL;
+static fn_ep1_t impl_ep1 = NULL;
+
+void refh_set_impl(void *v, void *s_el, void *s_visc, void *ep, void *ep1)
+{
+    impl_v = (fn_v_t)v;
+    impl_se = (fn_se_t)s_el;
+    impl_sv = (fn_sv_t)s_visc;
+    impl_ep = (fn_ep_t)ep;
+    impl_ep1 = (fn_ep1_t)ep1;
+}
+#define CALL_V (impl_v ? impl_v : update_v_PML)
+#define CALL_SE (impl_se ? impl_se : update_s_elastic_PML)
+#define CALL_SV (impl_sv ? impl_sv : update_s_visc_PML)
+#define CALL_EP (impl_ep ? impl_ep : eprecond)
+#define CALL_EP1 (impl_ep1 ? impl_ep1 : eprecond1)
+
 static int nd;
 static float **pvy, **psxy, **psyz, **pvyp1, **pvym1, **uy, **uyx, **utty;
 static float **prho, **pu, **puip, **pujp, **absorb_coeff;
@@ -358,12 +393,12 @@ static void zero_state(void)
 static void step_stress(void)
 {
     if (L)
-        update_s_visc_PML(1, NX, 1, NY, pvy, uy, uyx, psyz, psxy, pujp, puip, prho, hc, 0,
+        CALL_SV(1, NX, 1, NY, pvy, uy, uyx, psyz, psxy, pujp, puip, prho, hc, 0,
                           pr, pp, pq, fipjp, f, g, bip, bjm, cip, cjm, d, e, dip,
                           K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half,
                           psi_vyy, psi_vyx);
     else
-        update_s_elastic_PML(1, NX, 1, NY, pvy, uy, uyx, psyz, psxy, pu, puip, pujp, absorb_coeff, prho, hc, 0,
+        CALL_SE(1, NX, 1, NY, pvy, uy, uyx, psyz, psxy, pu, puip, pujp, absorb_coeff, prho, hc, 0,
                              K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half, b_y_half,
                              psi_vyy, psi_vyx);
 }
@@ -424,7 +459,7 @@ int refh_forward(int nsrc, const float *srcpos8, const float *signals_in, int nt
     }
     hin = 1; hin1 = 1; imat = 1; imat1 = 1; imat2 = 1;
     for (nt = 1; nt <= nsteps; nt++) {
-        update_v_PML(1, NX, 1, NY, nt, pvy, pvyp1, pvym1, utty, psyz, psxy, prho, sp, signals, nsrc, absorb_coeff,
+        CALL_V(1, NX, 1, NY, nt, pvy, pvyp1, pvym1, utty, psyz, psxy, prho, sp, signals, nsrc, absorb_coeff,
                      hc, 0, 0, K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half,
                      b_y_half, psi_syz_y, psi_sxy_x);
         step_stress();
@@ -436,7 +471,7 @@ int refh_forward(int nsrc, const float *srcpos8, const float *signals_in, int nt
                 for (i = 1; i <= NX; i++) for (j = 1; j <= NY; j++) fwd_u[imat2++] = uyx[j][i];
             }
             if (hessian_on) hess_save(hin, uy, uyx, pvyp1, hess_eyy, hess_eyx, hess_utty);
-            if ((EPRECOND == 1) || (EPRECOND == 3)) eprecond(Ws, pvy);
+            if ((EPRECOND == 1) || (EPRECOND == 3)) CALL_EP(Ws, pvy);
             hin++;
             hin1 = hin1 + DTINV;
         }
@@ -492,7 +527,7 @@ int refh_adjoint(const float *adj, int nsteps)
     zero_state();
     hin = 1;
     for (nt = 1; nt <= nsteps; nt++) {
-        update_v_PML(1, NX, 1, NY, nt, pvy, pvyp1, pvym1, utty, psyz, psxy, prho, srcpos_loc_back, sig, ntr,
+        CALL_V(1, NX, 1, NY, nt, pvy, pvyp1, pvym1, utty, psyz, psxy, prho, srcpos_loc_back, sig, ntr,
                      absorb_coeff, hc, 0, 1, K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half,
                      a_y_half, b_y_half, psi_syz_y, psi_sxy_x);
         step_stress();
@@ -504,7 +539,7 @@ int refh_adjoint(const float *adj, int nsteps)
                 g_u_shot[j][i] += (fwd_u[imat] * psxy[j][i]) + (fwd_y[imat] * psyz[j][i]);
                 imat++;
             }
-        if (EPRECOND == 1) eprecond(Wr, pvy);
+        if (EPRECOND == 1) CALL_EP(Wr, pvy);
         hin++;
     }
     free_matrix(sig, 1, ntr, 1, NT);
@@ -517,7 +552,7 @@ int refh_eprecond_scale(void)
 {
     int i, j;
     if ((EPRECOND == 1) || (EPRECOND == 3)) {
-        eprecond1(We, Ws, Wr);
+        CALL_EP1(We, Ws, Wr);
         for (i = 1; i <= NX; i = i + IDX)
             for (j = 1; j <= NY; j = j + IDY) {
                 g_u_shot[j][i] = g_u_shot[j][i] / (We[j][i] * C_vs * C_vs);

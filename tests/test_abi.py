@@ -13,16 +13,29 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
 def declared(header):
+    """Function names declared in an include/ header."""
     src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(dsh_[a-z0-9_]+)\s*\(", src)))
+    src = re.sub(r"#define[^\n]*", "", src)
+    return sorted(set(re.findall(r"\b(?:void|int|float|double|dsh_ctx \*|const char \*)\s*\**\s*([A-Za-z_][A-Za-z0-9_]*)\s*\(", src)))
+
+
+def _library_for(header):
+    if header == "dsh_compat.h":
+        import oracle as O
+
+        if not O.available("ref"):
+            pytest.skip("the compat layer resolves the reference's globals from the program that loads it")
+        C.CDLL(os.path.join(O.REF_DIR, "libdenise_ref.so"), mode=C.RTLD_GLOBAL)
+        return C.CDLL(os.path.join(ROOT, "denise-sh_b200", "libdsh_compat.so"))
+    return dsh.lib()
 
 
 @pytest.mark.parametrize("header", sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h")))
 def test_every_declared_symbol_is_exported(header):
-    lib = dsh.lib()
+    lib = _library_for(header)
     names = declared(header)
-    assert names, header
+    assert len(names) >= 10, (header, names)
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
 

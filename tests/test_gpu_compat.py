@@ -1,0 +1,57 @@
+"""The reference-signature layer (libdsh_compat.so) is a drop-in for the
+reference's own functions: the reference's per-shot loops (forward with
+storage, residual, adjoint with correlation, eprecond) run once with the
+reference's update_v_PML / update_s_*_PML / eprecond / eprecond1 and once
+with the library's, on the same Numerical-Recipes arrays and globals; every
+output must be bit-identical (and equal to the golden fixtures)."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from conftest import golden, oracle_model
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _libs():
+    ref = C.CDLL(os.path.join(O.REF_DIR, "libdenise_ref.so"), mode=C.RTLD_GLOBAL)   # defines the globals
+    comp = C.CDLL(os.path.join(ROOT, "denise-sh_b200", "libdsh_compat.so"))
+    return ref, comp
+
+
+def _run(d):
+    m = oracle_model(d)
+    o = O.Oracle(m, "ref")
+    g = o.shot_gradient(d["srcpos"], d["recpos"], d["obs"])
+    out = {k: g[k] for k in ("seis", "res", "Ws", "Wr", "We", "g_u", "g_rho")}
+    out["l2"] = g["l2"]
+    for k in ("vy", "sxy", "syz", "uy", "uyx", "vyp1"):
+        out["end_" + k] = o.field(k)
+    o.close()
+    return out
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference not compiled here")
+@pytest.mark.parametrize("name", ["elastic_fd4_fs", "elastic_fd2_pml", "visc_fd8_L2", "visc_fd6_L3_pml",
+                                  "elastic_fd12_fs"])
+def test_compat_layer_is_drop_in(name):
+    ref, comp = _libs()
+    d = golden(name)
+    ref.refh_set_impl(None, None, None, None, None)
+    base = _run(d)
+    ptr = lambda f: C.cast(getattr(comp, f), C.c_void_p).value
+    ref.refh_set_impl(C.c_void_p(ptr("update_v_PML")), C.c_void_p(ptr("update_s_elastic_PML")),
+                      C.c_void_p(ptr("update_s_visc_PML")), C.c_void_p(ptr("eprecond")), C.c_void_p(ptr("eprecond1")))
+    try:
+        gpu = _run(d)
+    finally:
+        ref.refh_set_impl(None, None, None, None, None)
+    for k in base:
+        assert np.array_equal(np.asarray(gpu[k]), np.asarray(base[k])), k
+    assert np.array_equal(gpu["seis"], d["seis"])
+    assert np.array_equal(gpu["g_u"], d["g_u"])
