@@ -614,3 +614,85 @@ int refh_psource(int nt, float *sxx, float *syy, int nsrc, const float *srcpos8,
     free_matrix(sp, 1, 8, 1, nsrc); free_matrix(sig, 1, nsrc, 1, NT);
     return 0;
 }
+
+/* ---------------- the reference's file readers / writers ---------------- */
+extern char SOURCE_FILE[], REC_FILE[], MFILE[], SEIS_FILE_VY[], DATA_DIR[], SIGNAL_FILE[];
+extern int NPROCX, NPROCY, MAXRELERROR, QUELLTYP, SRCREC, RUN_MULTIPLE_SHOTS, READMOD, READREC, SEIS_FORMAT;
+extern int HESSIAN, GRAD_METHOD, LNORM, DTINV, INVMAT1, INVMAT;
+extern float TAU, FC_HESSIAN, REFREC[4];
+extern int IENDX, IENDY;
+
+/* read_par() on a .inp file; numeric results in a fixed order, strings
+ * concatenated with '\n' separators into strs (6 names). */
+int refh_read_par(const char *path, double *v, char *strs, int nstr)
+{
+    FILE *fp = fopen(path, "r");
+    int k = 0, l;
+    if (!fp) return -1;
+    FP = stderr;
+    MYID = 0;
+    read_par(fp);   /* closes fp */
+    v[k++] = NPROCX; v[k++] = NPROCY; v[k++] = FDORDER; v[k++] = MAXRELERROR; v[k++] = NX; v[k++] = NY;
+    v[k++] = DH; v[k++] = TIME; v[k++] = DT; v[k++] = QUELLART; v[k++] = QUELLTYP; v[k++] = SRCREC;
+    v[k++] = RUN_MULTIPLE_SHOTS; v[k++] = READMOD; v[k++] = L;
+    for (l = 1; l <= 8; l++) v[k++] = (l <= L) ? FL[l] : 0.0;
+    v[k++] = TAU; v[k++] = FREE_SURF; v[k++] = FW; v[k++] = DAMPING; v[k++] = FPML; v[k++] = BOUNDARY;
+    v[k++] = SEISMO; v[k++] = READREC; v[k++] = REFREC[1]; v[k++] = REFREC[2]; v[k++] = NDT; v[k++] = SEIS_FORMAT;
+    v[k++] = INVMAT1; v[k++] = INVMAT; v[k++] = QUELLTYPB; v[k++] = npower; v[k++] = k_max_PML; v[k++] = HESSIAN;
+    v[k++] = FC_HESSIAN; v[k++] = GRAD_METHOD; v[k++] = LNORM; v[k++] = DTINV;
+    snprintf(strs, nstr, "%s\n%s\n%s\n%s\n%s\n%s", SIGNAL_FILE, SOURCE_FILE, MFILE, REC_FILE, SEIS_FILE_VY, DATA_DIR);
+    return k;
+}
+
+/* sources() + splitsrc() for one rank: srcpos_m [8][max] (metres), srcpos_loc [8][max] (grid) */
+int refh_sources(const char *path, float dh, int nx, int ny, int max, float *srcpos_m, float *srcpos_loc, int *nloc)
+{
+    float **sp, **spl;
+    int nsrc = 0, n, r, k;
+    FP = stderr; MYID = 0; SRCREC = 1; DH = dh; NX = NXG = nx; NY = NYG = ny; IENDX = nx; IENDY = ny;
+    POS[1] = POS[2] = 0;
+    strncpy(SOURCE_FILE, path, 73); SOURCE_FILE[73] = 0;
+    sp = sources(&nsrc);
+    if (nsrc > max) return -1;
+    for (r = 1; r <= 8; r++) for (k = 1; k <= nsrc; k++) srcpos_m[(r - 1) * max + k - 1] = sp[r][k];
+    spl = splitsrc(sp, &n, nsrc);
+    for (r = 1; r <= 8; r++) for (k = 1; k <= n; k++) srcpos_loc[(r - 1) * max + k - 1] = spl[r][k];
+    *nloc = n;
+    return nsrc;
+}
+
+/* receiver() with READREC=1: recpos [3][max] */
+int refh_receivers(const char *path, float dh, float refx, float refy, int max, int *recpos)
+{
+    int ntr = 0, r, k;
+    int **rp;
+    FP = stderr; MYID = 0; READREC = 1; DH = dh; REFREC[1] = refx; REFREC[2] = refy; REFREC[3] = 0.0;
+    strncpy(REC_FILE, path, 73); REC_FILE[73] = 0;
+    rp = receiver(stderr, &ntr);
+    if (ntr > max) return -1;
+    for (r = 1; r <= 3; r++) for (k = 1; k <= ntr; k++) recpos[(r - 1) * max + k - 1] = rp[r][k];
+    return ntr;
+}
+
+/* outseis_glob() in SU format for one shot: section [ntr][ns], recpos [3][ntr],
+ * source (xs, ys) in metres */
+int refh_write_su(const char *path, int ntr, int ns, const float *section, const int *recpos, float xs, float ys,
+                  float dh, float dt, float refx, float refy)
+{
+    float **sec = matrix(1, ntr, 1, ns), **sp = matrix(1, 8, 1, 1);
+    int **rp = imatrix(1, 3, 1, ntr);
+    int k, s;
+    FILE *fp = fopen(path, "wb");
+    if (!fp) return -1;
+    FP = stderr; DH = dh; DT = dt; NDT = 1; TIME = ns * dt; REFREC[1] = refx; REFREC[2] = refy;
+    for (k = 1; k <= ntr; k++) {
+        for (s = 1; s <= ns; s++) sec[k][s] = section[(k - 1) * ns + s - 1];
+        rp[1][k] = recpos[k - 1]; rp[2][k] = recpos[ntr + k - 1]; rp[3][k] = recpos[2 * ntr + k - 1];
+    }
+    sp[1][1] = xs; sp[2][1] = ys;
+    outseis_glob(stderr, fp, 0, sec, rp, rp, ntr, sp, 1, ns, 1, 1, 0);   /* closes fp */
+    free_matrix(sec, 1, ntr, 1, ns);
+    free_matrix(sp, 1, 8, 1, 1);
+    free_imatrix(rp, 1, 3, 1, ntr);
+    return 0;
+}
