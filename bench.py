@@ -64,22 +64,26 @@ def peaks():
 
 def bytes_per_point(l, nx, ny, fw, free_surf):
     """Algorithmic bytes per grid-point time step (each array touched once):
-    forward with storage = state (3+2L) R/W + parameters (3+2L) R + stored
-    acceleration/strains 12 B W + Ws R/W; adjoint = state + parameters +
-    stored wavefield 12 B R + g_u, g_rho, Wr R/W; plus CPML memory R/W on the
-    strip points (2 psi arrays per strip per half-step pair)."""
-    core = 12 * (3 + 2 * l)
+    state vy, sxy, syz and the 2L memory variables read and written; model
+    parameters read once (elastic: 1/rho, uip, ujp; viscoelastic: 1/rho and
+    the four factors muip, mujp, tausipjp, taus that every viscoelastic
+    coefficient is a product of); forward pass: stored acceleration and
+    strains written (12 B) and Ws R/W; adjoint: stored wavefield read (12 B)
+    and g_u, g_rho, Wr R/W; plus CPML memory R/W on the strip points."""
+    state = 8 * (3 + 2 * l)
+    params = 12 if l == 0 else 20
     strips = 2 * fw * ny + (1 if free_surf else 2) * fw * nx
     cpml = 16.0 * strips / (nx * ny)
-    fwd = core + 12 + 8 + cpml
-    adj = core + 12 + 24 + cpml
+    fwd = state + params + 12 + 8 + cpml
+    adj = state + params + 12 + 24 + cpml
     return fwd, adj
 
 
 def kernel_bytes(l):
     """Per-point bytes a single launch must move (forward pass with storage)."""
     v = 8 + 8 + 4 + 4                      # vy R/W, sxy+syz R, 1/rho R, stored acceleration W
-    s = 16 + 16 * l + 4 + (2 + 2 * l) * 4 + 8 + 8   # sxy/syz R/W, r/q R/W, vy R, params, strains W, Ws R/W
+    params = 8 if l == 0 else 16           # uip, ujp | muip, mujp, tausipjp, taus
+    s = 16 + 16 * l + 4 + params + 8 + 8   # sxy/syz R/W, r/q R/W, vy R, params, strains W, Ws R/W
     return v, s
 
 
@@ -329,7 +333,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_e2e = float(t.item())
     e2e_value = pts_step * a.steps / (ms_e2e / 1e3) / 1e9
-    h2d = (7 + 2 * L) * n * 4 + ntr * nt * 4 + 8 * 4 + 2 * ntr * 4
+    h2d = (9 if L else 5) * n * 4 + ntr * nt * 4 + 8 * 4 + 2 * ntr * 4   # model fields, observed data, geometry
     d2h = 2 * n * 4 + 8
 
     # --- roofline: whole step (both passes) and the dominant kernel

@@ -370,7 +370,7 @@ static void stress_common(const char *name, int nx1, int nx2, int ny1, int ny2, 
     put_psi_x(G.psx, psi_vyx);
     put_psi_y(G.psy, psi_vyy);
     put_pml(pml);
-    KFn fn = s_kernel(FDORDER, l, SF_STRAIN_OUT);
+    KFn fn = s_kernel(FDORDER, l, SF_STRAIN_OUT | SF_PARAMS);
     StepArgs a = base_args(hc);
     for (int k = 0; k < l; k++) { a.bip[k] = bip[k + 1]; a.bjm[k] = bjm[k + 1]; a.cip[k] = cip[k + 1]; a.cjm[k] = cjm[k + 1]; }
     a.out_uy = G.uy;

@@ -237,8 +237,9 @@ struct dsh_ctx {
     long long o_vy, o_sxy, o_syz, o_r, o_q, o_pvxx, o_psxx, o_pvyy, o_psyy, o_state_end;
     long long o_ws, o_wr, o_we, o_gu, o_grho, o_hu, o_hrho;
     float *slab = nullptr;
-    float *model = nullptr;               /* brho uip ujp fipjp f dip[L] d[L] vs rho */
-    float *m_brho, *m_uip, *m_ujp, *m_fipjp, *m_f, *m_dip, *m_d, *m_vs, *m_rho;
+    float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho */
+    float *m_brho, *m_uip, *m_ujp, *m_muip, *m_mujp, *m_tip, *m_taus, *m_vs, *m_rho;
+    float eta[4] = {0};
     float *pml = nullptr;
     float *sums = nullptr;                /* sum_u, sum_rho, out_a, out_b (dense pitched) */
     float hc[7] = {0}, bip[4] = {0}, bjm[4] = {0}, cip[4] = {0}, cjm[4] = {0}, cnorm[2] = {0};
@@ -373,17 +374,17 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     ctx->o_hrho = o; o += ctx->dstride;
     ctx->slot_stride = o;
     if (cudaMalloc(&ctx->slab, (size_t)ctx->S * ctx->slot_stride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
-    const long long nmodel = (long long)(7 + 2 * L) * ctx->dstride;
+    const long long nmodel = 9LL * ctx->dstride;
     if (cudaMalloc(&ctx->model, (size_t)nmodel * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     cudaMemset(ctx->model, 0, (size_t)nmodel * sizeof(float));
     float *m = ctx->model;
     ctx->m_brho = m; m += ctx->dstride;
     ctx->m_uip = m; m += ctx->dstride;
     ctx->m_ujp = m; m += ctx->dstride;
-    ctx->m_fipjp = m; m += ctx->dstride;
-    ctx->m_f = m; m += ctx->dstride;
-    ctx->m_dip = m; m += (long long)L * ctx->dstride;
-    ctx->m_d = m; m += (long long)L * ctx->dstride;
+    ctx->m_muip = m; m += ctx->dstride;
+    ctx->m_mujp = m; m += ctx->dstride;
+    ctx->m_tip = m; m += ctx->dstride;
+    ctx->m_taus = m; m += ctx->dstride;
     ctx->m_vs = m; m += ctx->dstride;
     ctx->m_rho = m;
     if (cudaMalloc(&ctx->pml, 12 * (size_t)(2 * DSH_MAX_FW + 1) * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
@@ -443,11 +444,13 @@ extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, co
         if (!std::isfinite(vs[k]) || !std::isfinite(rho[k]) || vs[k] < 0 || rho[k] < 0) return DSH_ERR_PARAM;
         if (L > 0 && !(qs[k] > 0)) return DSH_ERR_PARAM;
     }
-    std::vector<float> brho(n), uip(n), ujp(n), fipjp(L ? n : 1), f(L ? n : 1), dip(L ? n * L : 1), d(L ? n * L : 1);
+    std::vector<float> brho(n), uip(n), ujp(n), muip(L ? n : 1), mujp(L ? n : 1), tip(L ? n : 1), taus(L ? n : 1);
     if (dsh_setup_holberg(p.fdorder, p.maxrelerror, ctx->hc) != 0) return DSH_ERR_PARAM;
-    if (dsh_setup_model(p.nx, p.ny, L, p.fl, p.dt, vs, rho, qs, brho.data(), uip.data(), ujp.data(),
-                        L ? fipjp.data() : nullptr, L ? f.data() : nullptr, L ? dip.data() : nullptr,
-                        L ? d.data() : nullptr, ctx->bip, ctx->bjm, ctx->cip, ctx->cjm, ctx->cnorm) != 0)
+    if (dsh_setup_model(p.nx, p.ny, L, p.fl, p.dt, vs, rho, qs, brho.data(), uip.data(), ujp.data(), nullptr, nullptr,
+                        nullptr, nullptr, ctx->bip, ctx->bjm, ctx->cip, ctx->cjm, ctx->cnorm) != 0)
+        return DSH_ERR_PARAM;
+    if (L > 0 && dsh_setup_visc_base(p.nx, p.ny, L, p.fl, p.dt, vs, rho, qs, muip.data(), mujp.data(), tip.data(),
+                                     taus.data(), ctx->eta) != 0)
         return DSH_ERR_PARAM;
     dsh_pml pml;
     float damping = p.damping;
@@ -466,12 +469,10 @@ extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, co
     if ((rc = upload_field(ctx, ctx->m_vs, vs)) != DSH_OK) return rc;
     if ((rc = upload_field(ctx, ctx->m_rho, rho)) != DSH_OK) return rc;
     if (L > 0) {
-        if ((rc = upload_field(ctx, ctx->m_fipjp, fipjp.data())) != DSH_OK) return rc;
-        if ((rc = upload_field(ctx, ctx->m_f, f.data())) != DSH_OK) return rc;
-        for (int l = 0; l < L; l++) {
-            if ((rc = upload_field(ctx, ctx->m_dip + (long long)l * ctx->dstride, dip.data() + l * n)) != DSH_OK) return rc;
-            if ((rc = upload_field(ctx, ctx->m_d + (long long)l * ctx->dstride, d.data() + l * n)) != DSH_OK) return rc;
-        }
+        if ((rc = upload_field(ctx, ctx->m_muip, muip.data())) != DSH_OK) return rc;
+        if ((rc = upload_field(ctx, ctx->m_mujp, mujp.data())) != DSH_OK) return rc;
+        if ((rc = upload_field(ctx, ctx->m_tip, tip.data())) != DSH_OK) return rc;
+        if ((rc = upload_field(ctx, ctx->m_taus, taus.data())) != DSH_OK) return rc;
     }
     CK(cudaStreamSynchronize(ctx->st));   /* host staging vectors go out of scope */
     ctx->model_set = 1;
@@ -718,8 +719,10 @@ static StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.psi_vxx = sl + ctx->o_pvxx; a.psi_sxx = sl + ctx->o_psxx;
     a.psi_vyy_v = sl + ctx->o_pvyy; a.psi_syy = sl + ctx->o_psyy;
     a.gu = sl + ctx->o_gu; a.grho = sl + ctx->o_grho; a.hu = sl + ctx->o_hu; a.hrho = sl + ctx->o_hrho;
-    a.brho = ctx->m_brho; a.uip = ctx->m_uip; a.ujp = ctx->m_ujp; a.fipjp = ctx->m_fipjp; a.f = ctx->m_f;
-    a.dip = ctx->m_dip; a.d = ctx->m_d;
+    a.brho = ctx->m_brho; a.uip = ctx->m_uip; a.ujp = ctx->m_ujp;
+    a.muip = ctx->m_muip; a.mujp = ctx->m_mujp; a.tausipjp = ctx->m_tip; a.taus = ctx->m_taus;
+    for (int l = 0; l < 4; l++) a.eta[l] = ctx->eta[l];
+    a.lf = (float)p.l;
     for (int l = 0; l < 4; l++) { a.bip[l] = ctx->bip[l]; a.bjm[l] = ctx->bjm[l]; a.cip[l] = ctx->cip[l]; a.cjm[l] = ctx->cjm[l]; }
     a.fwd_slot_stride = ctx->fwd_slot_stride;
     a.fwd_mod = ctx->fwd_mod > 0 ? ctx->fwd_mod : p.nt;
@@ -1318,32 +1321,31 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
     InjectArgs ia = inject_args(ctx, (Pass)pass);
     dim3 block(BX, BY, 1);
     dim3 grid((unsigned)((p.nx + 4 * BX - 1) / (4 * BX)), (unsigned)((p.ny + BY - 1) / BY), (unsigned)nb);
-    std::vector<cudaEvent_t> ev(6 * nsteps);
+    /* each kernel launched nsteps times back to back between one event pair */
+    cudaEvent_t ev[6];
     for (auto &e : ev) CK(cudaEventCreate(&e));
     set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
-    for (int k = 0; k < nsteps; k++) {
-        int off = k;
-        void *args[2] = {&sa, &off};
-        void *iargs[2] = {&ia, &off};
-        CK(cudaEventRecord(ev[6 * k + 0], ctx->st));
-        CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
-        CK(cudaEventRecord(ev[6 * k + 1], ctx->st));
-        CK(cudaEventRecord(ev[6 * k + 2], ctx->st));
-        if (!sa.tl.on) CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
-        CK(cudaEventRecord(ev[6 * k + 3], ctx->st));
-        CK(cudaEventRecord(ev[6 * k + 4], ctx->st));
-        CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
-        CK(cudaEventRecord(ev[6 * k + 5], ctx->st));
+    for (int q = 0; q < 3; q++) {
+        CK(cudaEventRecord(ev[2 * q], ctx->st));
+        for (int k = 0; k < nsteps; k++) {
+            int off = k;
+            void *args[2] = {&sa, &off};
+            void *iargs[2] = {&ia, &off};
+            if (q == 0) CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
+            if (q == 1 && !sa.tl.on) CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
+            if (q == 2) CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
+        }
+        CK(cudaEventRecord(ev[2 * q + 1], ctx->st));
     }
     CK(cudaStreamSynchronize(ctx->st));
     double acc[3] = {0, 0, 0};
-    for (int k = 0; k < nsteps; k++)
-        for (int q = 0; q < 3; q++) {
-            float ms = 0;
-            cudaEventElapsedTime(&ms, ev[6 * k + 2 * q], ev[6 * k + 2 * q + 1]);
-            acc[q] += ms;
-        }
+    for (int q = 0; q < 3; q++) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, ev[2 * q], ev[2 * q + 1]);
+        acc[q] = ms;
+    }
     for (auto &e : ev) cudaEventDestroy(e);
     for (int q = 0; q < 3; q++) out_ms3[q] = (float)(acc[q] / nsteps);
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->st);   /* repeated steps of one kernel may overflow */
     return check_status(ctx);
 }

@@ -26,6 +26,7 @@
         case SF_STRAIN_OUT: return s_step<N, L, SF_STRAIN_OUT>;                               \
         case SF_HESS: return s_step<N, L, SF_HESS>;                                           \
         case SF_CORR: return s_step<N, L, SF_CORR>;                                           \
+        case SF_STRAIN_OUT | SF_PARAMS: return s_step<N, L, SF_STRAIN_OUT | SF_PARAMS>;       \
         default: return nullptr;                                                              \
         }                                                                                     \
     }                                                                                         \

@@ -36,6 +36,8 @@ constexpr int SF_STRAIN_OUT = 1; /* write uy = vyy, uyx = vyx (GRAD_FORM=2) */
 constexpr int SF_ENERGY = 2;     /* unused: the energy W += vy^2 (eprecond.c:11) runs when ws != nullptr */
 constexpr int SF_CORR = 4;       /* g_u += uyx_fwd*sxy + uy_fwd*syz (denise.c:1609) */
 constexpr int SF_HESS = 8;       /* H_u += uy^2 + (0.5 uyx)^2 (hessian.c:92) */
+constexpr int SF_PARAMS = 16;    /* viscoelastic: read precomputed fipjp, f, dip_l, d_l (the compat layer)
+                                    instead of forming them from muip, mujp, tausipjp, taus */
 
 struct PmlCoef {                 /* device copies, index 1..2fw */
     const float *K_x, *a_x, *b_x, *K_x_half, *a_x_half, *b_x_half;
@@ -81,6 +83,9 @@ struct StepArgs {
     float *ws, *gu, *grho, *hu, *hrho;
     /* model (shared by all slots) */
     const float *brho, *uip, *ujp, *fipjp, *f, *dip, *d;
+    const float *muip, *mujp, *tausipjp, *taus;   /* viscoelastic base factors */
+    float eta[4];                /* DT / tau_l */
+    float lf;                    /* L as a float */
     float bip[4], bjm[4], cip[4], cjm[4];
     /* stored forward wavefields: slot s, stored step k (0-based) at
        fwd + s*fwd_slot_stride + k*fwd_step_stride (+ 0/1/2 * dstride for acc/uy/uyx) */
@@ -331,18 +336,29 @@ __global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
     float4 sxy4 = ld4(sxy_p), syz4 = ld4(syz_p);
     float4 c1, c2;                           /* uip/ujp (elastic) or fipjp/f (visc) */
     float4 rr[LL], qq[LL], dip4[LL], d4[LL];
+    float4 mi4, mj4, ti4, tj4;               /* muip, mujp, tausipjp, taus */
     if (L == 0) {
         c1 = ldg4(a.uip + drow + col0);
         c2 = ldg4(a.ujp + drow + col0);
     } else {
-        c1 = ldg4(a.fipjp + drow + col0);
-        c2 = ldg4(a.f + drow + col0);
 #pragma unroll
         for (int l = 0; l < L; l++) {
             rr[l] = ld4(a.r + so + l * a.dstride + drow + col0);
             qq[l] = ld4(a.q + so + l * a.dstride + drow + col0);
-            dip4[l] = ldg4(a.dip + l * a.dstride + drow + col0);
-            d4[l] = ldg4(a.d + l * a.dstride + drow + col0);
+        }
+        if (FLAGS & SF_PARAMS) {
+            c1 = ldg4(a.fipjp + drow + col0);
+            c2 = ldg4(a.f + drow + col0);
+#pragma unroll
+            for (int l = 0; l < L; l++) {
+                dip4[l] = ldg4(a.dip + l * a.dstride + drow + col0);
+                d4[l] = ldg4(a.d + l * a.dstride + drow + col0);
+            }
+        } else {
+            mi4 = ldg4(a.muip + drow + col0);
+            mj4 = ldg4(a.mujp + drow + col0);
+            ti4 = ldg4(a.tausipjp + drow + col0);
+            tj4 = ldg4(a.taus + drow + col0);
         }
     }
     float4 w4, g4, h4, fy, fu;
@@ -439,6 +455,15 @@ __global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
             set(syz4, k, get(syz4, k) + get(c2, k) * get(vyy4, k));
         }
     } else {
+        if (!(FLAGS & SF_PARAMS)) {
+            /* fipjp = muip*DT*(1+L*tausipjp), f = mujp*DT*(1+L*taus) with the
+               reference's float/double mix (prepare_update_s.c:46-47) */
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                set(c1, k, (float)((double)(get(mi4, k) * a.dt) * (1.0 + (double)(a.lf * get(ti4, k)))));
+                set(c2, k, (float)((double)(get(mj4, k) * a.dt) * (1.0 + (double)(a.lf * get(tj4, k)))));
+            }
+        }
         float4 sumr4 = make_float4(0.f, 0.f, 0.f, 0.f), sumq4 = sumr4;
 #pragma unroll
         for (int l = 0; l < L; l++) {
@@ -459,8 +484,11 @@ __global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
         for (int l = 0; l < L; l++) {
 #pragma unroll
             for (int k = 0; k < 4; k++) {
-                float rn = a.bip[l] * (get(rr[l], k) * a.cip[l] - (get(dip4[l], k) * get(vyx4, k)));
-                float qn = a.bjm[l] * (get(qq[l], k) * a.cjm[l] - (get(d4[l], k) * get(vyy4, k)));
+                /* dip_l = muip*eta_l*tausipjp, d_l = mujp*eta_l*taus (prepare_update_s.c:54-55) */
+                const float dipv = (FLAGS & SF_PARAMS) ? get(dip4[l], k) : (get(mi4, k) * a.eta[l]) * get(ti4, k);
+                const float dv = (FLAGS & SF_PARAMS) ? get(d4[l], k) : (get(mj4, k) * a.eta[l]) * get(tj4, k);
+                float rn = a.bip[l] * (get(rr[l], k) * a.cip[l] - (dipv * get(vyx4, k)));
+                float qn = a.bjm[l] * (get(qq[l], k) * a.cjm[l] - (dv * get(vyy4, k)));
                 set(rr[l], k, rn);
                 set(qq[l], k, qn);
                 set(sumr4, k, get(sumr4, k) + rn);

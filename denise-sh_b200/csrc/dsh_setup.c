@@ -245,6 +245,38 @@ int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const floa
     return 0;
 }
 
+int dsh_setup_visc_base(int nx, int ny, int l, const float *fl, float dt, const float *vs, const float *rho,
+                        const float *qs, float *muip, float *mujp, float *tausipjp, float *taus, float *eta)
+{
+    const size_t n = (size_t)nx * ny;
+    float tau_sls[DSH_MAX_L], omega, sumu = 0.0;
+    size_t k;
+    int i, j, m;
+    if (nx < 1 || ny < 1 || l < 1 || l > DSH_MAX_L) return -1;
+    if (dsh_setup_model(nx, ny, 0, fl, dt, vs, rho, qs, NULL, muip, mujp, NULL, NULL, NULL, NULL, NULL, NULL, NULL,
+                        NULL, NULL) != 0)
+        return -1;                          /* harmonic means uip, ujp into muip, mujp */
+    for (m = 0; m < l; m++) {
+        tau_sls[m] = 1.0 / (2.0 * DSH_PI * fl[m]);
+        eta[m] = dt / tau_sls[m];
+    }
+    for (k = 0; k < n; k++) taus[k] = 2.0 / qs[k];
+    for (j = 1; j <= ny; j++)
+        for (i = 1; i <= nx; i++)
+            tausipjp[nb(nx, ny, i, j)] = 0.25 * (taus[nb(nx, ny, i, j)] + taus[nb(nx, ny, i + 1, j)] +
+                                                 taus[nb(nx, ny, i, j + 1)] + taus[nb(nx, ny, i + 1, j + 1)]);
+    omega = 2.0 * DSH_PI * fl[0];
+    for (m = 0; m < l; m++)
+        sumu = sumu + ((omega * omega * tau_sls[m] * tau_sls[m]) / (1.0 + omega * omega * tau_sls[m] * tau_sls[m]));
+    for (k = 0; k < n; k++) {
+        float u_jp = mujp[k] / (1.0 + sumu * taus[k]);
+        float u_ip = muip[k] / (1.0 + sumu * tausipjp[k]);
+        mujp[k] = u_jp;
+        muip[k] = u_ip;
+    }
+    return 0;
+}
+
 int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *srcpos8, float *out)
 {
     int it, s;

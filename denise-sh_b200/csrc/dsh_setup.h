@@ -41,6 +41,14 @@ int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const floa
                     const float *qs, float *brho, float *uip, float *ujp, float *fipjp, float *f, float *dip,
                     float *d, float *bip, float *bjm, float *cip, float *cjm, float *cnorm);
 
+/* The per-point factors from which every viscoelastic coefficient is a
+ * product (src/prepare_update_s.c:43-57): relaxed moduli muip/mujp at the
+ * two stress positions, tau at (i+1/2, j+1/2) and (i, j+1/2) (av_tau), and
+ * eta_l = DT/tau_l.  fipjp = muip*DT*(1+L*tausipjp), f = mujp*DT*(1+L*taus),
+ * dip_l = muip*eta_l*tausipjp, d_l = mujp*eta_l*taus are formed from them. */
+int dsh_setup_visc_base(int nx, int ny, int l, const float *fl, float dt, const float *vs, const float *rho,
+                        const float *qs, float *muip, float *mujp, float *tausipjp, float *taus, float *eta);
+
 /* Source time functions (src/wavelet.c:26-84): out [nsrc][nt]. */
 int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *srcpos8, float *out);
 

@@ -134,12 +134,13 @@ int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out);
  * with their own work and time it with events on that stream. */
 int dsh_set_stream(dsh_ctx *ctx, void *stream);
 
-/* Per-kernel timing: re-runs `nsteps` steps of pass `pass` (0 forward,
- * 1 forward with storage, 2 forward with Hessian sums, 3 adjoint) of the
- * last batch with a CUDA event pair around every kernel (no graph) and
+/* Per-kernel timing: launches each kernel of pass `pass` (0 forward,
+ * 1 forward with storage, 2 forward with Hessian sums, 3 adjoint) `nsteps`
+ * times back to back on the last batch between one CUDA event pair and
  * returns the mean device time per launch in ms: out[0] velocity step,
- * out[1] injection/sampling, out[2] stress step.  Call it after a
- * dsh_gradient on the same shots; it overwrites the wavefield state. */
+ * out[1] separate injection/sampling (0 when fused), out[2] stress step.
+ * Call it after a dsh_gradient on the same shots; it overwrites the
+ * wavefield state, which is rebuilt by the next call. */
 int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
 
 /* Residual and L2 misfit with no device allocation at all.  This entry point
