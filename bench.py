@@ -2,10 +2,17 @@
 """Throughput of the SH FWI gradient (forward + residual + adjoint with
 correlation + energy preconditioning + conversion) on B200.
 
-Workload: the viscoelastic forward + adjoint gradient configuration —
-NX=2000, NY=800, DH=0.25 m, FDORDER=8, L=3, NT=6000, one 40 Hz shot, 200
-receivers; seeded synthetic model (no dataset exists for this path).  One
-step = one full gradient evaluation (2 x NX x NY x NT grid-point updates).
+Workloads (--config; seeded synthetic models, no dataset exists for this path):
+  c2 (default)  viscoelastic forward + adjoint gradient: NX=2000, NY=800,
+                DH=0.25 m, FDORDER=8, L=3, NT=6000, one 40 Hz shot, 200
+                receivers.  One step = one gradient (2 x NX x NY x NT updates).
+  c1            elastic forward modelling: NX=500, NY=200, FDORDER=4, NT=2000,
+                one 30 Hz shot, 96 receivers.  One step = NX x NY x NT updates.
+  c3            batched gradient of 64 shots in one launch per half-step:
+                NX=1000, NY=300, FDORDER=8, L=2, NT=4000, 192 receivers, forward
+                wavefield checkpointed with recompute (full storage would need
+                0.92 TB).  One step = 2 x NX x NY x NT x 64 updates; the
+                recompute pass is extra work that is not counted.
 
   value  device-resident inputs (model and observed data already in HBM),
          through dsh_gradient_device; CUDA events on the launching stream
@@ -45,9 +52,11 @@ def args_parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dsh", choices=["dsh", "reference"])
-    ap.add_argument("--nt", type=int, default=6000)
-    ap.add_argument("--nx", type=int, default=2000)
-    ap.add_argument("--ny", type=int, default=800)
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--nt", type=int, default=None, help="time steps (default: the workload's NT)")
+    ap.add_argument("--nx", type=int, default=2000, help="c2 only")
+    ap.add_argument("--ny", type=int, default=800, help="c2 only")
+    ap.add_argument("--shots", type=int, default=64, help="c3 only: shots per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=24, help="time steps per pass in the CPU sample")
     ap.add_argument("--profile-steps", type=int, default=20)
@@ -79,12 +88,27 @@ def bytes_per_point(l, nx, ny, fw, free_surf):
     return fwd, adj
 
 
-def kernel_bytes(l):
-    """Per-point bytes a single launch must move (forward pass with storage)."""
-    v = 8 + 8 + 4 + 4                      # vy R/W, sxy+syz R, 1/rho R, stored acceleration W
+def kernel_bytes(l, store=True):
+    """Per-point bytes a single launch must move (forward pass, with or
+    without storage of acceleration, strains and the energy Ws)."""
+    v = 8 + 8 + 4 + (4 if store else 0)    # vy R/W, sxy+syz R, 1/rho R, stored acceleration W
     params = 8 if l == 0 else 16           # uip, ujp | muip, mujp, tausipjp, taus
-    s = 16 + 16 * l + 4 + params + 8 + 8   # sxy/syz R/W, r/q R/W, vy R, params, strains W, Ws R/W
+    s = 16 + 16 * l + 4 + params + (16 if store else 0)   # sxy/syz R/W, r/q R/W, vy R, params, strains W, Ws R/W
     return v, s
+
+
+def workload(name, nt=None, nx=2000, ny=800, shots=64):
+    """(cfg, kind, label, fdorder) of a named workload."""
+    from dsh import configs
+
+    if name == "c1":
+        cfg = configs.config1(**({"nt": nt} if nt else {}))
+        return cfg, "forward", f"elastic-forward-500x200-fd4", 4
+    if name == "c3":
+        cfg = configs.config3(nshots=shots, **({"nt": nt} if nt else {}))
+        return cfg, "gradient", f"batched-gradient-1000x300-fd8-L2-{shots}shots", 8
+    cfg = configs.config2(nx=nx, ny=ny, **({"nt": nt} if nt else {}))
+    return cfg, "gradient", f"visc-gradient-{nx}x{ny}-fd8-L3", 8
 
 
 class Clocks:
@@ -144,47 +168,47 @@ def _cpu_sample(payload):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    cfg, steps, kind = payload
+    cfg, steps, kind, gradient = payload
     devnull = os.open(os.devnull, os.O_WRONLY)      # the reference logs to stdout/stderr
     os.dup2(devnull, 1)
     os.dup2(devnull, 2)
     p = dict(cfg["params"])
     m = O.Model(nx=p["nx"], ny=p["ny"], nt=steps, dh=p["dh"], dt=p["dt"], vs=cfg["vs"], rho=cfg["rho"],
-                qs=cfg["qs"], fdorder=p["fdorder"], fw=p["fw"], free_surf=p["free_surf"], l=p["l"], fl=p["fl"],
-                fpml=p["fpml"], damping=p["damping"])
+                qs=cfg["qs"], fdorder=p["fdorder"], fw=p["fw"], free_surf=p["free_surf"], l=p["l"],
+                fl=p.get("fl", ()), fpml=p["fpml"], damping=p["damping"])
     o = O.Oracle(m, kind)
     sh = cfg["shots"][0]
     t0 = time.perf_counter()
-    seis = o.forward(sh.srcpos, sh.recpos, store=True)
-    o.residual(seis * np.float32(0.9))
-    o.adjoint()
-    o.eprecond_scale()
+    seis = o.forward(sh.srcpos, sh.recpos, store=gradient)
+    if gradient:
+        o.residual(seis * np.float32(0.9))
+        o.adjoint()
+        o.eprecond_scale()
     dt = time.perf_counter() - t0
     o.close()
     return dt
 
 
-def cpu_workload(nx, ny):
-    from dsh import configs
-
-    cfg = configs.config2(nt=16, nx=nx, ny=ny)
+def cpu_workload(a):
+    cfg, kind, label, fdo = workload(a.config, 16, a.nx, a.ny, 1)
     cfg.pop("true", None)
-    return cfg
+    cfg["shots"] = cfg["shots"][:1]
+    return cfg, kind == "gradient"
 
 
-def run_cpu(nprocs, steps, nx, ny, repeats=1):
+def run_cpu(nprocs, steps, a, repeats=1):
     """Times `repeats` rounds of nprocs concurrent samples; returns per-round seconds (max over processes)."""
     import multiprocessing as mp
 
     import oracle as O
 
     kind = "ref_fast" if O.available("ref_fast") else "port"
-    cfg = cpu_workload(nx, ny)
+    cfg, gradient = cpu_workload(a)
     ctx = mp.get_context("spawn")
     times = []
     with ctx.Pool(nprocs) as pool:
         for _ in range(repeats):
-            t = pool.map(_cpu_sample, [(cfg, steps, kind)] * nprocs)
+            t = pool.map(_cpu_sample, [(cfg, steps, kind, gradient)] * nprocs)
             times.append(max(t))
     return times, ("reference" if kind == "ref_fast" else "port")
 
@@ -194,20 +218,24 @@ def reference_arm(a, rank, world):
         return
     ncpu = os.cpu_count() or 1
     nprocs = max(1, min(ncpu, 32))
-    steps = 12
-    nx, ny = a.nx, a.ny
-    times, kind = run_cpu(nprocs, steps, nx, ny, repeats=a.warmup + a.steps)
+    cfg, wkind, label, fdo = workload(a.config, a.nt, a.nx, a.ny, a.shots)
+    steps = 12 if wkind == "gradient" else 200
+    p = cfg["params"]
+    nx, ny, L = p["nx"], p["ny"], p["l"]
+    passes = 2 if wkind == "gradient" else 1
+    times, kind = run_cpu(nprocs, steps, a, repeats=a.warmup + a.steps)
     timed = times[a.warmup:]
-    pts = 2.0 * nx * ny * steps * nprocs
+    pts = passes * nx * ny * steps * nprocs
     val = pts * len(timed) / sum(timed) / 1e9
+    what = f"{steps} forward (with storage) + {steps} adjoint steps" if passes == 2 else f"{steps} forward steps"
     line = {"impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": 1000 * sum(timed) / len(timed), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"visc-gradient-{nx}x{ny}-fd8-L3", "nx": nx, "ny": ny, "fdorder": 8, "l": 3,
+            "config": {"workload": label, "nx": nx, "ny": ny, "fdorder": fdo, "l": L,
                        "nt_sample": steps, "shots": nprocs},
             "cpu_baseline": {"value": val, "unit": UNIT, "cores": nprocs, "kind": kind,
-                             "sample": f"{steps} forward (with storage) + {steps} adjoint steps of the {nx}x{ny} "
-                                       f"FD8 L=3 gradient per process, {nprocs} independent single-rank processes"},
+                             "sample": f"{what} of the {nx}x{ny} FD{fdo} L={L} {wkind} per process, "
+                                       f"{nprocs} independent single-rank processes (one shot each)"},
             "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -223,43 +251,50 @@ def main():
         reference_arm(a, rank, world)
         return
 
+    import ctypes as C
+
     import numpy as np
     import torch
     import torch.distributed as dist
 
     import dsh
-    from dsh import configs
 
     torch.cuda.set_device(local)
     if world > 1:
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    cfg = configs.config2(nt=a.nt, nx=a.nx, ny=a.ny)
+    cfg, wkind, label, fdo = workload(a.config, a.nt, a.nx, a.ny, a.shots)
+    gradient = wkind == "gradient"
     p = cfg["params"]
     shots = cfg["shots"]
-    if world > 1:   # one distinct shot per rank (weak scaling)
-        sp = shots[0].srcpos.copy()
-        sp[0, 0] = 1 + (int(sp[0, 0]) - 1 + rank * (p["nx"] // (world + 1))) % p["nx"]
-        shots = [dsh.Shot(sp, shots[0].recpos)]
     nx, ny, nt, L = p["nx"], p["ny"], p["nt"], p["l"]
+    if world > 1:   # distinct shots per rank (weak scaling): sources shifted along x
+        moved = []
+        for sh in shots:
+            sp = sh.srcpos.copy()
+            sp[0, 0] = 1 + (int(sp[0, 0]) - 1 + rank * (nx // (world + 1))) % nx
+            moved.append(dsh.Shot(sp, sh.recpos))
+        shots = moved
+    nsh = len(shots)
     n = nx * ny
-    ntr = shots[0].ntr
-    params = dsh.make_params(**p, max_shots=1)
+    ntr_all = sum(s.ntr for s in shots)
+    params = dsh.make_params(**p, max_shots=nsh)
     eng = dsh.Engine(params, device=local)
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
 
-    # observed data: synthesised by the engine on the true model, kept in HBM
-    obs = torch.empty(ntr * nt, device="cuda", dtype=torch.float32)
-    eng.set_model(cfg["true"], cfg["rho"], cfg["qs"])
-    eng.forward_device(shots, obs.data_ptr())
+    seis = torch.empty(ntr_all * nt, device="cuda", dtype=torch.float32)
+    if gradient:
+        # observed data: synthesised by the engine on the true model, kept in HBM
+        eng.set_model(cfg["true"], cfg["rho"], cfg["qs"])
+        eng.forward_device(shots, seis.data_ptr())
     eng.set_model(cfg["vs"], cfg["rho"], cfg["qs"])
     gv = torch.empty(n, device="cuda", dtype=torch.float32)
     gr = torch.empty(n, device="cuda", dtype=torch.float32)
 
     def allreduce():
-        if world > 1:
+        if world > 1 and gradient:
             with torch.cuda.stream(stream):
                 dist.all_reduce(gv)
                 dist.all_reduce(gr)
@@ -268,55 +303,68 @@ def main():
         if world > 1:
             dist.barrier()
 
-    for _ in range(a.warmup):
-        eng.gradient_device(shots, obs.data_ptr(), gv.data_ptr(), gr.data_ptr())
+    def device_step():
+        if gradient:
+            l2 = eng.gradient_device(shots, seis.data_ptr(), gv.data_ptr(), gr.data_ptr())
+        else:
+            eng.forward_device(shots, seis.data_ptr())
+            l2 = None
         allreduce()
+        return l2
+
+    for _ in range(a.warmup):
+        device_step()
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local)
     clocks.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    launches, ms_f, ms_a = 0, 0.0, 0.0
+    launches, ms_f, ms_a, l2 = 0, 0.0, 0.0, None
+    ckpt = 0
     e0.record(stream)
     for _ in range(a.steps):
-        l2 = eng.gradient_device(shots, obs.data_ptr(), gv.data_ptr(), gr.data_ptr())
+        l2 = device_step()
         st = eng.stats()
         launches += st["kernel_launches"]
         ms_f += st["ms_forward"]
         ms_a += st["ms_adjoint"]
-        allreduce()
+        ckpt = st["checkpoint_interval"]
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
     torch.cuda.synchronize()
     clk = clocks.stop()
+    storage = eng.stats()["storage_bytes"]
     ms = e0.elapsed_time(e1)
     t = torch.tensor([ms], device="cuda", dtype=torch.float64)
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms = float(t.item())
-    pts_step = 2.0 * n * nt * world
+    passes = 2 if gradient else 1
+    pts_step = float(passes) * n * nt * nsh * world
     value = pts_step * a.steps / (ms / 1e3) / 1e9
 
-    # --- e2e through the host API: model + observed data in, gradients out, every step
-    obs_h = obs.cpu().numpy().reshape(ntr, nt).copy()
+    # --- e2e through the host API, every step: model (and observed data) in, gradients (or seismograms) out
     pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy()
-    vs_h, rho_h, qs_h, obs_p = pin(cfg["vs"]), pin(cfg["rho"]), pin(cfg["qs"]), pin(obs_h)
+    vs_h, rho_h = pin(cfg["vs"]), pin(cfg["rho"])
+    qs_h = pin(cfg["qs"]) if L else None
+    obs_p = pin(seis.cpu().numpy()) if gradient else None
+    seis_h = torch.empty(ntr_all * nt, dtype=torch.float32).pin_memory()
     gvs_h = torch.empty((ny, nx), dtype=torch.float32).pin_memory()
     grh_h = torch.empty((ny, nx), dtype=torch.float32).pin_memory()
-    L2v = []
-    import ctypes as C
+    arr = dsh._shots_c(shots)
 
     def host_step():
         eng.set_model(vs_h, rho_h, qs_h)
-        arr = dsh._shots_c(shots)
-        l2c = C.c_double(0)
-        rc = dsh.lib().dsh_gradient(eng.h, arr, 1, obs_p.ctypes.data, gvs_h.data_ptr(), grh_h.data_ptr(),
-                                    C.byref(l2c), None, None, None)
+        if gradient:
+            l2c = C.c_double(0)
+            rc = dsh.lib().dsh_gradient(eng.h, arr, nsh, obs_p.ctypes.data, gvs_h.data_ptr(), grh_h.data_ptr(),
+                                        C.byref(l2c), None, None, None)
+        else:
+            rc = dsh.lib().dsh_forward(eng.h, arr, nsh, seis_h.data_ptr())
         if rc != 0:
-            raise dsh.DshError(rc, "dsh_gradient")
-        L2v.append(l2c.value)
+            raise dsh.DshError(rc, "dsh_gradient" if gradient else "dsh_forward")
 
     host_step()
     torch.cuda.synchronize()
@@ -333,19 +381,27 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     ms_e2e = float(t.item())
     e2e_value = pts_step * a.steps / (ms_e2e / 1e3) / 1e9
-    h2d = (9 if L else 5) * n * 4 + ntr * nt * 4 + 8 * 4 + 2 * ntr * 4   # model fields, observed data, geometry
-    d2h = 2 * n * 4 + 8
+    nsrc_all = sum(s.srcpos.shape[1] for s in shots)
+    h2d = (5 if L else 2) * n * 4 + 8 * 4 * nsrc_all + 2 * 4 * ntr_all   # model fields, geometry
+    if gradient:
+        h2d += ntr_all * nt * 4                                          # observed data
+        d2h = 2 * n * 4 + 8
+    else:
+        d2h = ntr_all * nt * 4
 
-    # --- roofline: whole step (both passes) and the dominant kernel
+    # --- roofline: whole step and the dominant kernel
     hbm, peak_kind = peaks()
     bf, ba = bytes_per_point(L, nx, ny, p["fw"], p["free_surf"])
-    step_gbs = n * nt * (bf + ba) * a.steps / ((ms_f + ms_a) / 1e3) / 1e9
-    prof = eng.profile_step("forward_store", a.profile_steps)
-    kv, ks = kernel_bytes(L)
-    s_gbs = ks * n / (prof["s_step"] / 1e3) / 1e9
+    if not gradient:
+        bf -= 12 + 8                       # no storage, no energy in plain forward modelling
+    step_bytes = n * nt * nsh * (bf + (ba if gradient else 0)) * a.steps
+    step_gbs = step_bytes / ((ms_f + ms_a) / 1e3) / 1e9
+    prof = eng.profile_step("forward_store" if gradient else "forward", a.profile_steps)
+    kv, ks = kernel_bytes(L, store=gradient)
+    s_gbs = ks * n * nsh / (prof["s_step"] / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and a.config == "c2":
         try:
             traffic = json.load(open(tpath)).get("s_step_forward_store_bytes_per_launch")
         except Exception:
@@ -354,28 +410,36 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         steps = a.cpu_steps
-        times, kind = run_cpu(1, steps, nx, ny, repeats=1)
-        cpu = {"value": 2.0 * nx * ny * steps / times[0] / 1e9, "unit": UNIT, "cores": 1, "kind": kind,
-               "sample": f"{steps} forward (with storage) + {steps} adjoint steps of the same {nx}x{ny} FD8 L=3 "
-                         f"gradient, one core"}
+        times, kind = run_cpu(1, steps, a, repeats=1)
+        what = f"{steps} forward (with storage) + {steps} adjoint steps" if gradient else f"{steps} forward steps"
+        cpu = {"value": passes * nx * ny * steps / times[0] / 1e9, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"{what} of one shot of the same {nx}x{ny} FD{fdo} L={L} {wkind}, one core"}
 
     if rank == 0:
+        state_mb = (3 + 2 * L) * n * 4 * nsh / 1e6
+        if gradient and not ckpt:
+            l2note = f"inputs larger than L2 (stored forward wavefield {3 * n * nt * 4 * nsh / 1e9:.0f} GB)"
+        elif gradient:
+            l2note = (f"inputs larger than L2 (wavefield state {state_mb:.0f} MB, checkpoints + recompute "
+                      f"buffer {storage / 1e9:.1f} GB)")
+        else:
+            l2note = (f"state {state_mb:.1f} MB fits in L2: no flush between steps, "
+                      f"bytes counted algorithmically")
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
             "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"visc-gradient-{nx}x{ny}-fd8-L3-nt{nt}", "nx": nx, "ny": ny, "nt": nt,
-                       "fdorder": 8, "l": 3, "shots_per_gpu": 1, "receivers": ntr, "parallelism": f"shots{world}",
-                       "l2": "inputs larger than L2 (stored forward wavefield " +
-                             f"{3 * n * nt * 4 / 1e9:.0f} GB per shot)"},
-            "gradients_per_s": world * a.steps / (ms / 1e3),
-            "l2_misfit": l2,
+            "config": {"workload": f"{label}-nt{nt}", "nx": nx, "ny": ny, "nt": nt, "fdorder": fdo, "l": L,
+                       "shots_per_gpu": nsh, "receivers": shots[0].ntr, "parallelism": f"shots{world}",
+                       "checkpoint_interval": ckpt, "storage_gb": storage / 1e9, "l2": l2note},
             "roofline": {"bound": "hbm", "achieved": s_gbs, "peak": hbm, "unit": "GB/s", "frac": s_gbs / hbm,
-                         "traffic": traffic, "kernel": "s_step<8,3> (forward pass with storage)",
+                         "traffic": traffic,
+                         "kernel": f"s_step<{fdo},{L}> (forward pass{' with storage' if gradient else ''})",
                          "bytes_per_point": ks, "ms_per_launch": prof["s_step"], "peak_source": peak_kind},
             "step_roofline": {"achieved": step_gbs, "frac": step_gbs / hbm, "bytes_per_point_fwd": bf,
-                              "bytes_per_point_adj": ba, "ms_forward_pass": ms_f / a.steps,
-                              "ms_adjoint_pass": ms_a / a.steps},
+                              "bytes_per_point_adj": ba if gradient else None,
+                              "ms_forward_pass": ms_f / a.steps,
+                              "ms_adjoint_pass": ms_a / a.steps if gradient else None},
             "kernels_ms": prof,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "ms_per_step": ms_e2e / a.steps},
@@ -383,6 +447,9 @@ def main():
             "clocks": clk,
             "cpu_baseline": cpu,
         }
+        if gradient:
+            line["gradients_per_s"] = world * nsh * a.steps / (ms / 1e3)
+            line["l2_misfit"] = l2
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:

@@ -60,9 +60,11 @@ typedef struct dsh_params {
     int max_shots;            /* shots advanced together in one launch (>= 1) */
     int compat_fd12;          /* 1: reuse hc[5] in the 6th y term of the FDORDER=12 velocity
                                  operator, as src/update_v_PML.c:469 does */
-    long long mem_budget;     /* device bytes for stored forward wavefields; 0 = as
-                                 needed (full storage); smaller budgets select
-                                 checkpoint-and-recompute */
+    long long mem_budget;     /* device bytes for the adjoint's stored forward wavefields;
+                                 0 = the free device memory less 2 GiB.  Full storage
+                                 when it fits, else checkpoints every
+                                 C = sqrt(NT*(3+2L)/3) steps and one recomputed
+                                 forward pass (DSH_ERR_OOM if even that does not fit) */
 } dsh_params;
 
 /* One shot (one source gather). */

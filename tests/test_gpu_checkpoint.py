@@ -49,3 +49,29 @@ def test_budget_too_small_is_reported():
         with pytest.raises(dsh.DshError) as ei:
             e.gradient(shots, [np.zeros((shots[0].ntr, 60), np.float32)])
         assert ei.value.code == -3
+
+
+def test_64_shots_one_launch_checkpointed():
+    """The batched-gradient layout: 64 shots advance in one launch per
+    half-step (grid z = shot) with checkpoints; the shot sum is bit-identical
+    to the reference's shot loop."""
+    nt = 130
+    d, shots = _case(964, nx=72, ny=40, nt=nt, fdo=8, L=2, fs=1, fw=8, nshots=64)
+    m = oracle_model(d)
+    obs = []
+    for sh in shots:
+        o = O.Oracle(m, "port")
+        obs.append((o.forward(sh.srcpos, sh.recpos) * np.float32(0.9)).astype(np.float32))
+        o.close()
+    with engine_from(d, max_shots=64) as e:
+        full = e.gradient(shots, obs)
+        st_full = e.stats()
+    with engine_from(d, max_shots=64, mem_budget=st_full["storage_bytes"] // 3) as e:
+        ck = e.gradient(shots, obs)
+        st = e.stats()
+    assert st["checkpoint_interval"] > 0
+    gv, gr, l2, _ = _oracle_gradient(d, shots, obs)
+    for out in (full, ck):
+        assert np.array_equal(out["g_vs"], gv)
+        assert np.array_equal(out["g_rho"], gr)
+        assert abs(out["l2"] - l2) <= l2_tol(sum(o.size for o in obs)) * abs(l2)
