@@ -8,6 +8,12 @@ Workloads (--config; seeded synthetic models, no dataset exists for this path):
                 receivers.  One step = one gradient (2 x NX x NY x NT updates).
   c1            elastic forward modelling: NX=500, NY=200, FDORDER=4, NT=2000,
                 one 30 Hz shot, 96 receivers.  One step = NX x NY x NT updates.
+  c4            uneven batch of 32 models (NX 256-2048, NY 128-512, FDORDER
+                4/6/8, elastic / L=2, 8-32 shots each) in one velocity and one
+                stress launch per step, tile shape picked by the autotuner;
+                forward modelling; NT per model = 1.5 x diagonal traveltime
+                (--nt-scale shortens all NTs alike).  Per-model throughput is
+                reported beside the aggregate.
   c3            batched gradient of 64 shots in one launch per half-step:
                 NX=1000, NY=300, FDORDER=8, L=2, NT=4000, 192 receivers, forward
                 wavefield checkpointed with recompute (full storage would need
@@ -52,7 +58,8 @@ def args_parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dsh", choices=["dsh", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--nt-scale", type=float, default=1.0, help="c4 only: factor on every model's NT")
     ap.add_argument("--nt", type=int, default=None, help="time steps (default: the workload's NT)")
     ap.add_argument("--nx", type=int, default=2000, help="c2 only")
     ap.add_argument("--ny", type=int, default=800, help="c2 only")
@@ -101,6 +108,13 @@ def workload(name, nt=None, nx=2000, ny=800, shots=64):
     """(cfg, kind, label, fdorder) of a named workload."""
     from dsh import configs
 
+    if name == "c4":   # the CPU sample of the uneven batch: its largest model, one shot
+        ms = configs.config4()
+        m = max(ms, key=lambda m: m["params"]["nx"] * m["params"]["ny"])
+        m["params"].pop("max_shots")
+        if nt:
+            m["params"]["nt"] = nt
+        return m, "forward", "uneven-batch-32-models", m["params"]["fdorder"]
     if name == "c1":
         cfg = configs.config1(**({"nt": nt} if nt else {}))
         return cfg, "forward", f"elastic-forward-500x200-fd4", 4
@@ -191,6 +205,7 @@ def _cpu_sample(payload):
 
 def cpu_workload(a):
     cfg, kind, label, fdo = workload(a.config, 16, a.nx, a.ny, 1)
+    cfg = dict(cfg)
     cfg.pop("true", None)
     cfg["shots"] = cfg["shots"][:1]
     return cfg, kind == "gradient"
@@ -264,6 +279,8 @@ def main():
         import datetime
 
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    if a.config == "c4":
+        return bench_batch(a, rank, world, local)
     cfg, wkind, label, fdo = workload(a.config, a.nt, a.nx, a.ny, a.shots)
     gradient = wkind == "gradient"
     p = cfg["params"]
@@ -452,6 +469,154 @@ def main():
             line["l2_misfit"] = l2
         print(json.dumps(line), flush=True)
     eng.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def bench_batch(a, rank, world, local):
+    """The uneven multi-model batch through dsh_batch (one launch per half-step)."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import dsh
+    from dsh import configs
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    models = configs.config4(nt_scale=a.nt_scale)
+    if world > 1:   # weak scaling: every rank its own copy of the batch, sources shifted
+        for m in models:
+            nx = m["params"]["nx"]
+            for sh in m["shots"]:
+                sh.srcpos[0, 0] = 1 + (int(sh.srcpos[0, 0]) - 1 + rank * (nx // (world + 1))) % nx
+    plist = [dsh.make_params(**m["params"]) for m in models]
+    b = dsh.Batch(plist, device=local)
+    stream = torch.cuda.Stream()
+    b.set_stream(stream.cuda_stream)
+    for k, m in enumerate(models):
+        b.set_model(k, m["vs"], m["rho"], m["qs"])
+    shots = [m["shots"] for m in models]
+    nseis = sum(sh.ntr * m["params"]["nt"] for m in models for sh in m["shots"])
+    seis = torch.empty(max(nseis, 1), device="cuda", dtype=torch.float32)
+    pts_model = [m["params"]["nx"] * m["params"]["ny"] * m["params"]["nt"] * len(m["shots"]) for m in models]
+    pts = float(sum(pts_model))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(a.warmup):
+        b.forward_device(shots, seis.data_ptr())
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    model_ms = np.zeros(len(models))
+    e0.record(stream)
+    for _ in range(a.steps):
+        b.forward_device(shots, seis.data_ptr())
+        st = b.stats()
+        launches += st["kernel_launches"]
+        model_ms += st["model_ms"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    value = pts * world * a.steps / (ms / 1e3) / 1e9
+
+    # e2e: models in, seismograms out, through the host API every step
+    import ctypes as C
+
+    pin = lambda x: torch.from_numpy(np.ascontiguousarray(x)).pin_memory().numpy() if x is not None else None
+    host_models = [(pin(m["vs"]), pin(m["rho"]), pin(m["qs"])) for m in models]
+    seis_h = torch.empty(max(nseis, 1), dtype=torch.float32).pin_memory()
+    flat = [sh for g in shots for sh in g]
+    arr = dsh._shots_c(flat)
+    nsh = np.array([len(g) for g in shots], np.int32)
+
+    def host_step():
+        for k, (vs, rho, qs) in enumerate(host_models):
+            b.set_model(k, vs, rho, qs)
+        rc = dsh.lib().dsh_batch_forward(b.h, arr, nsh.ctypes.data, seis_h.data_ptr())
+        if rc != 0:
+            raise dsh.DshError(rc, "dsh_batch_forward")
+
+    host_step()
+    torch.cuda.synchronize()
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(a.steps):
+        host_step()
+    f1.record(stream)
+    torch.cuda.synchronize()
+    ms_e2e = f0.elapsed_time(f1)
+    t = torch.tensor([ms_e2e], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_e2e = float(t.item())
+    e2e_value = pts * world * a.steps / (ms_e2e / 1e3) / 1e9
+    h2d = sum((3 if m["qs"] is not None else 2) * m["params"]["nx"] * m["params"]["ny"] * 4 for m in models)
+    h2d += sum(8 * 4 + 2 * 4 * sh.ntr for sh in flat)
+    d2h = nseis * 4
+
+    # roofline of the stress launch: algorithmic bytes of every model's points / autotuned launch time
+    st = b.stats()
+    hbm, peak_kind = peaks()
+    sbytes = sum(kernel_bytes(m["params"]["l"], store=False)[1] * m["params"]["nx"] * m["params"]["ny"] *
+                 len(m["shots"]) for m in models)
+    s_ms = st["s_ms"][st["s_variant"]]
+    s_gbs = sbytes / (s_ms / 1e3) / 1e9
+    per_model = [{"model": m["name"], "nt": m["params"]["nt"], "shots": len(m["shots"]),
+                  "gpt_s": pts_model[k] / (model_ms[k] / a.steps / 1e3) / 1e9,
+                  "ms_done": model_ms[k] / a.steps} for k, m in enumerate(models)]
+    cpu = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        steps = max(a.cpu_steps, 48)
+        times, kind = run_cpu(1, steps, a, repeats=1)
+        cfg, _, _, fdo = workload("c4", 16)
+        q = cfg["params"]
+        cpu = {"value": q["nx"] * q["ny"] * steps / times[0] / 1e9, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"{steps} forward steps of one shot of the batch's largest model "
+                         f"({q['nx']}x{q['ny']} FD{fdo} L={q['l']}), one core"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+            "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "uneven-batch-32-models-forward", "models": len(models),
+                       "shots": int(nsh.sum()), "nt_scale": a.nt_scale, "phases": st["phases"],
+                       "tile_variant": {"v": dsh.Batch.VARIANTS[st["v_variant"]],
+                                        "s": dsh.Batch.VARIANTS[st["s_variant"]]},
+                       "autotune_ms": {"v": st["v_ms"], "s": st["s_ms"]},
+                       "l2": f"wavefield state {sum((3 + 2 * m['params']['l']) * m['params']['nx'] * m['params']['ny'] * len(m['shots']) for m in models) * 4 / 1e9:.1f} GB, larger than L2",
+                       "parallelism": f"models{world}"},
+            "roofline": {"bound": "hbm", "achieved": s_gbs, "peak": hbm, "unit": "GB/s", "frac": s_gbs / hbm,
+                         "traffic": None, "kernel": "s_multi (all 32 models, one launch)",
+                         "bytes": sbytes, "ms_per_launch": s_ms, "peak_source": peak_kind},
+            "per_model": per_model,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "ms_per_step": ms_e2e / a.steps},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    b.close()
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -15,7 +15,7 @@
  * conversion :1743-1813, Hessian hessian.c:91-94 + hessian_out.c:20-31.
  */
 #include "dsh.h"
-#include "dsh_dispatch.h"
+#include "dsh_engine_int.h"
 #include "dsh_setup.h"
 
 #include <algorithm>
@@ -27,13 +27,10 @@
 #include <vector>
 
 using namespace dsh;
+using namespace dsh::eng;
 
 namespace {
 
-/* passes: plain forward (modelling), forward storing every step, forward
- * with Hessian sums, adjoint, forward saving only checkpoints, and the
- * recomputation of one segment from a checkpoint on the shadow state */
-enum Pass { P_FWD_PLAIN = 0, P_FWD_STORE = 1, P_FWD_HESS = 2, P_ADJ = 3, P_FWD_CKPT = 4, P_RECOMP = 5 };
 
 constexpr int RED_BLOCKS = 296;        /* 2 x 148 SMs for reductions */
 constexpr int RED_THREADS = 256;
@@ -225,54 +222,7 @@ __global__ void set_int_kernel(int *p, int v) { *p = v; }
 
 }  // namespace
 
-/* ======================= context ======================= */
-
-struct dsh_ctx {
-    dsh_params p;
-    int dev = 0;
-    cudaStream_t st = nullptr;
-    cudaStream_t own_st = nullptr;
-    int H = 0, hy = 0, pitch = 0, S = 1, chunk = 32;
-    long long fstride = 0, dstride = 0, slot_stride = 0;
-    long long o_vy, o_sxy, o_syz, o_r, o_q, o_pvxx, o_psxx, o_pvyy, o_psyy, o_state_end;
-    long long o_ws, o_wr, o_we, o_gu, o_grho, o_hu, o_hrho;
-    float *slab = nullptr;
-    float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho */
-    float *m_brho, *m_uip, *m_ujp, *m_muip, *m_mujp, *m_tip, *m_taus, *m_vs, *m_rho;
-    float eta[4] = {0};
-    float *pml = nullptr;
-    float *sums = nullptr;                /* sum_u, sum_rho, out_a, out_b (dense pitched) */
-    float hc[7] = {0}, bip[4] = {0}, bjm[4] = {0}, cip[4] = {0}, cjm[4] = {0}, cnorm[2] = {0};
-    int model_set = 0;
-    float *fwd = nullptr;
-    long long fwd_slot_stride = 0, fwd_step_stride = 0;
-    size_t fwd_bytes = 0;
-    int fwd_mod = 0;                      /* stored steps per slot: NT (full storage) or C (checkpointing) */
-    int ckpt_c = 0;                       /* checkpoint interval C; 0 = full storage */
-    float *ckpt = nullptr;                /* checkpoints: [k][slot][state] */
-    size_t ckpt_bytes = 0;
-    float *shadow = nullptr;              /* recomputation state, same slot layout as slab */
-    /* geometry */
-    int *d_geo = nullptr;
-    long long geo_cap = 0;
-    int *d_fgrp_off, *d_agrp_off, *d_grp_pt, *d_grp_beg, *d_src_id, *d_rec_off, *d_rec_pt;
-    int *d_ftile, *d_atile, *d_rtile, *d_gpk, *d_rpk, *d_rid;
-    int ntiles = 0, fused_inject = 0;
-    long long *d_offs = nullptr;          /* sig_off[S], seis_off[S], obs_off[S], out_off[S] */
-    float *d_sig = nullptr, *d_seis = nullptr, *d_res = nullptr, *d_obs = nullptr, *d_tmp = nullptr;
-    float *d_out = nullptr;               /* 2 x [ny][nx] dense outputs */
-    long long cap_sig = 0, cap_seis = 0, cap_obs = 0;
-    int geo_version = 0;
-    int *d_nt = nullptr, *d_status = nullptr;
-    double *d_part = nullptr, *d_l2 = nullptr;
-    unsigned *d_wemax = nullptr;
-    std::vector<int> ntr_b;
-    std::map<long long, cudaGraphExec_t> graphs;
-    cudaEvent_t ev[4];
-    dsh_stats stats;
-    long long launches = 0;
-    int last_cuda = 0;
-};
+/* ======================= context (struct dsh_ctx: dsh_engine_int.h) ======================= */
 
 static int fail_cuda(dsh_ctx *c, cudaError_t e)
 {
@@ -403,11 +353,13 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     return ctx;
 }
 
-static void drop_graphs(dsh_ctx *ctx)
+namespace dsh::eng {
+void drop_graphs(dsh_ctx *ctx)
 {
     for (auto &kv : ctx->graphs) cudaGraphExecDestroy(kv.second);
     ctx->graphs.clear();
 }
+}  // namespace dsh::eng
 
 extern "C" int dsh_destroy(dsh_ctx *ctx)
 {
@@ -487,8 +439,9 @@ static bool in_grid(const dsh_params &p, int i, int j) { return i >= 0 && i <= p
  * of shots[0..nb) into slots 0..nb).  Sources at one grid point form a group
  * (members in source order); groups and receivers are also listed per thread
  * block tile for the fused injection/sampling of the velocity kernel. */
-static int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_host, const float *obs_dev,
-                        long long obs_dev_off)
+namespace dsh::eng {
+int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_host, const float *obs_dev,
+                 long long obs_dev_off)
 {
     const dsh_params &p = ctx->p;
     const int NT = p.nt, S = ctx->S;
@@ -682,23 +635,28 @@ static int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float
     if (realloc) { drop_graphs(ctx); ctx->geo_version++; }
     return DSH_OK;
 }
+}  // namespace dsh::eng
 
 /* ---------------- passes ---------------- */
 
 /* DH = 2^k: x/DH and x*(1/DH) are the same correctly rounded number */
-static bool dh_pow2(float dh)
+namespace dsh::eng {
+bool dh_pow2(float dh)
 {
     int e;
     return dh > 0 && std::frexp(dh, &e) == 0.5f;
 }
+}  // namespace dsh::eng
 
-static StepArgs step_args(dsh_ctx *ctx, Pass pass)
+namespace dsh::eng {
+StepArgs step_args(dsh_ctx *ctx, Pass pass)
 {
     const dsh_params &p = ctx->p;
     StepArgs a;
     memset(&a, 0, sizeof(a));
     a.nx = p.nx; a.ny = p.ny; a.pitch = ctx->pitch; a.hy = ctx->hy; a.fw = p.fw; a.free_surf = p.free_surf;
     a.l = p.l; a.fd12_compat = p.compat_fd12;
+    a.fdo = p.fdorder; a.p2 = dh_pow2(p.dh) ? 1 : 0; a.nslots = ctx->S;
     a.nt_last = p.nt; a.nt_total = p.nt; a.nt_base = ctx->d_nt;
     a.fstride = ctx->fstride; a.dstride = ctx->dstride; a.slot_stride = ctx->slot_stride;
     for (int k = 0; k < 7; k++) a.hc[k] = ctx->hc[k];
@@ -731,6 +689,7 @@ static StepArgs step_args(dsh_ctx *ctx, Pass pass)
     /* fused injection / sampling lists */
     a.tl.on = ctx->fused_inject;
     a.tl.ntiles = ctx->ntiles;
+    a.tl.ntx = (p.nx + 4 * BX - 1) / (4 * BX);
     a.tl.gpt = ctx->d_gpk; a.tl.gbeg = ctx->d_grp_beg; a.tl.src_id = ctx->d_src_id;
     a.tl.roff = ctx->d_rtile; a.tl.rpt = ctx->d_rpk; a.tl.rid = ctx->d_rid; a.tl.rec_off = ctx->d_rec_off;
     a.tl.seis = ctx->d_seis; a.tl.seis_off = ctx->d_offs + ctx->S;
@@ -767,8 +726,10 @@ static StepArgs step_args(dsh_ctx *ctx, Pass pass)
     }
     return a;
 }
+}  // namespace dsh::eng
 
-static InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
+namespace dsh::eng {
+InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
 {
     InjectArgs a;
     memset(&a, 0, sizeof(a));
@@ -793,6 +754,7 @@ static InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
     }
     return a;
 }
+}  // namespace dsh::eng
 
 static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chunk, long long *nlaunch)
 {
@@ -954,14 +916,17 @@ static int adjoint_for_gradient(dsh_ctx *ctx, int nb)
 
 /* zero the wavefield state of slots [0, nb) (zero_fdveps(_visc)); with
  * accumulators also the per-shot energies, gradients and Hessian sums */
-static int zero_slots(dsh_ctx *ctx, int nb, bool accumulators)
+namespace dsh::eng {
+int zero_slots(dsh_ctx *ctx, int nb, bool accumulators)
 {
     const size_t w = (size_t)(accumulators ? ctx->slot_stride : ctx->o_state_end) * sizeof(float);
     CK(cudaMemset2DAsync(ctx->slab, (size_t)ctx->slot_stride * sizeof(float), 0, w, nb, ctx->st));
     return DSH_OK;
 }
+}  // namespace dsh::eng
 
-static int check_status(dsh_ctx *ctx)
+namespace dsh::eng {
+int check_status(dsh_ctx *ctx)
 {
     int h = 0;
     CK(cudaMemcpyAsync(&h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
@@ -973,6 +938,7 @@ static int check_status(dsh_ctx *ctx)
     }
     return DSH_OK;
 }
+}  // namespace dsh::eng
 
 /* Storage for the adjoint's forward wavefields.  Full storage (3 fields per
  * step and shot) when it fits the budget (mem_budget, or the free device
@@ -1032,7 +998,8 @@ static dim3 epi_grid(dsh_ctx *ctx, int nb)
     return dim3((unsigned)std::min<long long>((n + 255) / 256, 4 * 148), (unsigned)nb, 1);
 }
 
-static int copy_seis_out(dsh_ctx *ctx, int nb, float *host_out, float *dev_out)
+namespace dsh::eng {
+int copy_seis_out(dsh_ctx *ctx, int nb, float *host_out, float *dev_out)
 {
     long long tot = 0;
     for (int s = 0; s < nb; s++) tot += (long long)ctx->ntr_b[s] * ctx->p.nt;
@@ -1045,13 +1012,16 @@ static int copy_seis_out(dsh_ctx *ctx, int nb, float *host_out, float *dev_out)
     if (host_out) CK(cudaMemcpyAsync(host_out, ctx->d_tmp, (size_t)tot * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
     return DSH_OK;
 }
+}  // namespace dsh::eng
 
-static long long batch_seis_len(dsh_ctx *ctx, const dsh_shot *shots, int nb)
+namespace dsh::eng {
+long long batch_seis_len(dsh_ctx *ctx, const dsh_shot *shots, int nb)
 {
     long long t = 0;
     for (int s = 0; s < nb; s++) t += (long long)shots[s].ntr * ctx->p.nt;
     return t;
 }
+}  // namespace dsh::eng
 
 static int forward_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *seis_host, float *seis_dev)
 {

@@ -1,0 +1,77 @@
+/* dsh_engine_int.h — engine internals shared by the single-model engine
+ * (dsh_engine.cu) and the multi-model batch (dsh_batch.cu). */
+#pragma once
+#include "dsh.h"
+#include "dsh_dispatch.h"
+#include "dsh_setup.h"
+
+#include <map>
+#include <vector>
+
+namespace dsh {
+/* passes: plain forward (modelling), forward storing every step, forward
+ * with Hessian sums, adjoint, forward saving only checkpoints, and the
+ * recomputation of one segment from a checkpoint on the shadow state */
+enum Pass { P_FWD_PLAIN = 0, P_FWD_STORE = 1, P_FWD_HESS = 2, P_ADJ = 3, P_FWD_CKPT = 4, P_RECOMP = 5 };
+}  // namespace dsh
+
+struct dsh_ctx {
+    dsh_params p;
+    int dev = 0;
+    cudaStream_t st = nullptr;
+    cudaStream_t own_st = nullptr;
+    int H = 0, hy = 0, pitch = 0, S = 1, chunk = 32;
+    long long fstride = 0, dstride = 0, slot_stride = 0;
+    long long o_vy, o_sxy, o_syz, o_r, o_q, o_pvxx, o_psxx, o_pvyy, o_psyy, o_state_end;
+    long long o_ws, o_wr, o_we, o_gu, o_grho, o_hu, o_hrho;
+    float *slab = nullptr;
+    float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho */
+    float *m_brho, *m_uip, *m_ujp, *m_muip, *m_mujp, *m_tip, *m_taus, *m_vs, *m_rho;
+    float eta[4] = {0};
+    float *pml = nullptr;
+    float *sums = nullptr;                /* sum_u, sum_rho, out_a, out_b (dense pitched) */
+    float hc[7] = {0}, bip[4] = {0}, bjm[4] = {0}, cip[4] = {0}, cjm[4] = {0}, cnorm[2] = {0};
+    int model_set = 0;
+    float *fwd = nullptr;
+    long long fwd_slot_stride = 0, fwd_step_stride = 0;
+    size_t fwd_bytes = 0;
+    int fwd_mod = 0;                      /* stored steps per slot: NT (full storage) or C (checkpointing) */
+    int ckpt_c = 0;                       /* checkpoint interval C; 0 = full storage */
+    float *ckpt = nullptr;                /* checkpoints: [k][slot][state] */
+    size_t ckpt_bytes = 0;
+    float *shadow = nullptr;              /* recomputation state, same slot layout as slab */
+    /* geometry */
+    int *d_geo = nullptr;
+    long long geo_cap = 0;
+    int *d_fgrp_off, *d_agrp_off, *d_grp_pt, *d_grp_beg, *d_src_id, *d_rec_off, *d_rec_pt;
+    int *d_ftile, *d_atile, *d_rtile, *d_gpk, *d_rpk, *d_rid;
+    int ntiles = 0, fused_inject = 0;
+    long long *d_offs = nullptr;          /* sig_off[S], seis_off[S], obs_off[S], out_off[S] */
+    float *d_sig = nullptr, *d_seis = nullptr, *d_res = nullptr, *d_obs = nullptr, *d_tmp = nullptr;
+    float *d_out = nullptr;               /* 2 x [ny][nx] dense outputs */
+    long long cap_sig = 0, cap_seis = 0, cap_obs = 0;
+    int geo_version = 0;
+    int *d_nt = nullptr, *d_status = nullptr;
+    double *d_part = nullptr, *d_l2 = nullptr;
+    unsigned *d_wemax = nullptr;
+    std::vector<int> ntr_b;
+    std::map<long long, cudaGraphExec_t> graphs;
+    cudaEvent_t ev[4];
+    dsh_stats stats;
+    long long launches = 0;
+    int last_cuda = 0;
+};
+
+namespace dsh::eng {
+/* shots[0..nb) -> slots: sources, receivers, signals, optional observed data */
+int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_host, const float *obs_dev,
+                 long long obs_dev_off);
+StepArgs step_args(dsh_ctx *ctx, Pass pass);
+InjectArgs inject_args(dsh_ctx *ctx, Pass pass);
+int zero_slots(dsh_ctx *ctx, int nb, bool accumulators);
+int copy_seis_out(dsh_ctx *ctx, int nb, float *host_out, float *dev_out);
+int check_status(dsh_ctx *ctx);
+bool dh_pow2(float dh);
+long long batch_seis_len(dsh_ctx *ctx, const dsh_shot *shots, int nb);
+void drop_graphs(dsh_ctx *ctx);
+}  // namespace dsh::eng

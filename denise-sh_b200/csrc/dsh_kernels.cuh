@@ -62,6 +62,7 @@ struct TileLists {
     float *seis;                 /* slot s: seis[seis_off[s] + (nt-1)*ntr_s + r] */
     const long long *seis_off;
     int ntiles;
+    int ntx;                     /* list tiles along x: ceil(nx / 128); tile of (i, j) = ((j-1)/8)*ntx + (i-1)/128 */
     int on;                      /* fused path active (all positions inside the grid) */
     int sample;
 };
@@ -69,6 +70,8 @@ struct TileLists {
 struct StepArgs {
     int nx, ny, pitch, hy, fw, free_surf, l;
     int fd12_compat;
+    int fdo, p2;                 /* FDORDER; DH a power of two (multi-model launches pick the body from these) */
+    int nslots;                  /* shot slots allocated (multi-model launches skip slots >= nslots) */
     int nt_last;                 /* last valid step of this pass (1-based) */
     int nt_total;                /* NT of the pass (for the Hessian's nt < NTDTINV) */
     const int *nt_base;          /* device step counter; step = *nt_base + nt_off */
@@ -145,21 +148,20 @@ __device__ __forceinline__ float div_dh(float x, const StepArgs &a) { return P2 
  *   vy += b*DT*(sxy_x+syy_y)/DH with b = 1/rho
  * followed, when the tile holds any, by the source injection of this step
  * (update_v_PML.c:564-583) and the receiver samples (seismo_ssg.c:17-27).
- * Thread = 4 x-consecutive points of one row; block = 128 x 8 points; z = shot slot.
+ * Thread = 4 x-consecutive points (i0 .. i0+3) of row j of shot slot `slot`;
+ * `tile` = the 128 x 8-point tile of the injection / sampling lists holding
+ * them, ((j-1)/8) * ceil(nx/128) + (i0-1)/128.
  * All global loads are issued before any store so their latencies overlap.
  */
 template <int FDO, int FLAGS, bool P2>
-__global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
+__device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, int j, int slot, int tile)
 {
     constexpr int H = FDO / 2;
     constexpr int NL = (H + 3) / 4;          /* float4s left of the own vector (needs H)   */
     constexpr int NR = (H - 1 + 3) / 4;      /* float4s right of the own vector (needs H-1) */
     constexpr int NXS = 4 * (NL + 1 + NR);
-    const int i0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x);
-    const int j = 1 + blockIdx.y * BY + threadIdx.y;
     if (i0 > a.nx || j > a.ny) return;
     const int nt = *a.nt_base + nt_off;
-    const int slot = blockIdx.z;
     const long long so = (long long)slot * a.slot_stride;
     const int pitch = a.pitch;
     const int col0 = i0 - 1 + HX;
@@ -173,7 +175,6 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
     if (FLAGS & VF_CORR) g4 = ld4(a.grho + so + drow + col0);
     if (FLAGS & VF_HESS) h4 = ld4(a.hrho + so + drow + col0);
     int tg0 = 0, tg1 = 0, tr0 = 0, tr1 = 0;
-    const int tile = blockIdx.y * gridDim.x + blockIdx.x;
     if (a.tl.on) {
         const int *go = a.tl.goff + (long long)slot * (a.tl.ntiles + 1) + tile;
         tg0 = __ldg(go); tg1 = __ldg(go + 1);
@@ -299,6 +300,14 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
     }
 }
 
+/* one thread block = 128 x 8 points of one shot slot (grid z) */
+template <int FDO, int FLAGS, bool P2>
+__global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
+{
+    v_body<FDO, FLAGS, P2>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
+                           blockIdx.z, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
 /*
  * Stress half-step with CPML and, for L > 0, L standard-linear-solid memory
  * variables (update_s_elastic_PML.c:104-158, update_s_visc_PML.c:131-209):
@@ -311,18 +320,15 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
  * are issued before the first store.
  */
 template <int FDO, int L, int FLAGS>
-__global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
+__device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, int j, int slot)
 {
     constexpr int H = FDO / 2;
     constexpr int NL = (H - 1 + 3) / 4;      /* needs vy[i0-(H-1)] */
     constexpr int NR = (H + 3) / 4;          /* needs vy[i0+3+H]   */
     constexpr int NXS = 4 * (NL + 1 + NR);
     constexpr int LL = L > 0 ? L : 1;
-    const int i0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x);
-    const int j = 1 + blockIdx.y * BY + threadIdx.y;
     if (i0 > a.nx || j > a.ny) return;
     const int nt = *a.nt_base + nt_off;
-    const int slot = blockIdx.z;
     const long long so = (long long)slot * a.slot_stride;
     const int pitch = a.pitch;
     const int col0 = i0 - 1 + HX;
@@ -546,6 +552,14 @@ __global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
         }
         st4m(a.hu + so + drow + col0, h4, nvalid);
     }
+}
+
+/* one thread block = 128 x 8 points of one shot slot (grid z) */
+template <int FDO, int L, int FLAGS>
+__global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
+{
+    s_body<FDO, L, FLAGS>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
+                          blockIdx.z);
 }
 
 /* Source injection then receiver sampling for one step, one block per slot

@@ -1,0 +1,99 @@
+/*
+ * dsh_multi.cuh — step kernels for uneven batches of models.
+ *
+ * One launch advances every shot of every model of a batch by one half-step.
+ * Each thread block reads one entry of a block map — (model, x tile, y tile,
+ * slot group) — copies that model's StepArgs into shared memory and runs the
+ * same per-point body as the single-model kernels, picked at run time from
+ * the model's FDORDER and L (uniform across the block, so no divergence).
+ * Results are therefore bit-identical to the single-model kernels.
+ *
+ * Tile-shape variants: a block is always 256 threads, 32 along x (4 points
+ * each, 128 points), ROWS rows and SPB shot slots of the same model
+ * (ROWS * SPB = 8).  Blocks that share a model's coefficients across SPB shots
+ * read them once from L2 per block instead of once per shot; the batch
+ * autotuner times the variants on the actual batch and keeps the fastest.
+ *
+ * Bodies compiled in: FDORDER 4, 6, 8 and L 0 (elastic), 2 (viscoelastic),
+ * the operator and relaxation counts of uneven survey batches; the batch
+ * rejects other combinations (they run through single-model contexts).
+ */
+#pragma once
+#include "dsh_kernels.cuh"
+
+namespace dsh {
+
+constexpr int MULTI_NVAR = 3;
+constexpr int MULTI_ROWS[MULTI_NVAR] = {8, 4, 2};
+constexpr int MULTI_SPB[MULTI_NVAR] = {1, 2, 4};
+
+__host__ __device__ constexpr bool multi_supported(int fdo, int l)
+{
+    return (fdo == 4 || fdo == 6 || fdo == 8) && (l == 0 || l == 2);
+}
+
+/* Block prologue: the model's StepArgs into shared memory, then this
+ * thread's point vector, row, slot and injection/sampling list tile.
+ * Returns false for threads on slots the model does not use this run. */
+template <int ROWS, int SPB>
+__device__ __forceinline__ bool multi_setup(StepArgs &sa, const StepArgs *__restrict__ args,
+                                            const int4 *__restrict__ map, int &i0, int &j, int &slot, int &tile)
+{
+    static_assert(ROWS * SPB == BY, "256-thread blocks");
+    static_assert(sizeof(StepArgs) % 4 == 0, "word copy");
+    const int4 m = map[blockIdx.x];
+    const int tid = threadIdx.x + BX * (threadIdx.y + ROWS * threadIdx.z);
+    const int *src = reinterpret_cast<const int *>(args + m.x);
+    int *dst = reinterpret_cast<int *>(&sa);
+    for (int k = tid; k < (int)(sizeof(StepArgs) / 4); k += BX * BY) dst[k] = __ldg(src + k);
+    __syncthreads();
+    i0 = 1 + 4 * (m.y * BX + threadIdx.x);
+    j = 1 + m.z * ROWS + threadIdx.y;
+    slot = m.w * SPB + threadIdx.z;
+    tile = ((j - 1) / BY) * sa.tl.ntx + (i0 - 1) / (4 * BX);
+    return slot < sa.nslots;
+}
+
+/* velocity half-step of plain forward modelling (flags 0) for all models */
+template <int ROWS, int SPB>
+__global__ void __launch_bounds__(BX *BY, 3) v_multi(const StepArgs *__restrict__ args, const int4 *__restrict__ map,
+                                                     int nt_off)
+{
+    __shared__ StepArgs sa;
+    int i0, j, slot, tile;
+    if (!multi_setup<ROWS, SPB>(sa, args, map, i0, j, slot, tile)) return;
+    switch (sa.fdo * 2 + sa.p2) {
+    case 8: v_body<4, 0, false>(sa, nt_off, i0, j, slot, tile); break;
+    case 9: v_body<4, 0, true>(sa, nt_off, i0, j, slot, tile); break;
+    case 12: v_body<6, 0, false>(sa, nt_off, i0, j, slot, tile); break;
+    case 13: v_body<6, 0, true>(sa, nt_off, i0, j, slot, tile); break;
+    case 16: v_body<8, 0, false>(sa, nt_off, i0, j, slot, tile); break;
+    case 17: v_body<8, 0, true>(sa, nt_off, i0, j, slot, tile); break;
+    default: break;
+    }
+}
+
+/* stress half-step of plain forward modelling (flags 0) for all models */
+template <int ROWS, int SPB>
+__global__ void __launch_bounds__(BX *BY, 2) s_multi(const StepArgs *__restrict__ args, const int4 *__restrict__ map,
+                                                     int nt_off)
+{
+    __shared__ StepArgs sa;
+    int i0, j, slot, tile;
+    if (!multi_setup<ROWS, SPB>(sa, args, map, i0, j, slot, tile)) return;
+    switch (sa.fdo * 8 + sa.l) {
+    case 32: s_body<4, 0, 0>(sa, nt_off, i0, j, slot); break;
+    case 34: s_body<4, 2, 0>(sa, nt_off, i0, j, slot); break;
+    case 48: s_body<6, 0, 0>(sa, nt_off, i0, j, slot); break;
+    case 50: s_body<6, 2, 0>(sa, nt_off, i0, j, slot); break;
+    case 64: s_body<8, 0, 0>(sa, nt_off, i0, j, slot); break;
+    case 66: s_body<8, 2, 0>(sa, nt_off, i0, j, slot); break;
+    default: break;
+    }
+}
+
+using MultiFn = void (*)(const StepArgs *, const int4 *, int);
+MultiFn v_multi_kernel(int variant);
+MultiFn s_multi_kernel(int variant);
+
+}  // namespace dsh

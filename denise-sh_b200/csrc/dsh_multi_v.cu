@@ -1,0 +1,14 @@
+/* velocity kernels of uneven multi-model batches, one per tile-shape variant */
+#include "dsh_multi.cuh"
+
+namespace dsh {
+MultiFn v_multi_kernel(int variant)
+{
+    switch (variant) {
+    case 0: return v_multi<8, 1>;
+    case 1: return v_multi<4, 2>;
+    case 2: return v_multi<2, 4>;
+    default: return nullptr;
+    }
+}
+}  // namespace dsh

@@ -52,6 +52,12 @@ class Stats(C.Structure):
                 ("storage_bytes", C.c_longlong), ("checkpoint_interval", C.c_int)]
 
 
+class BatchStats(C.Structure):
+    _fields_ = [("ms_total", C.c_double), ("kernel_launches", C.c_longlong), ("point_updates", C.c_longlong),
+                ("v_variant", C.c_int), ("s_variant", C.c_int), ("phases", C.c_int), ("v_ms", C.c_float * 4),
+                ("s_ms", C.c_float * 4)]
+
+
 _lib = None
 
 
@@ -81,6 +87,15 @@ def lib() -> C.CDLL:
         L.dsh_profile_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_residual_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]
+        L.dsh_batch_create.restype = C.c_void_p
+        L.dsh_batch_create.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
+        L.dsh_batch_destroy.argtypes = [C.c_void_p]
+        L.dsh_batch_set_model.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_batch_forward.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_void_p, C.c_void_p]
+        L.dsh_batch_forward_device.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_void_p, C.c_void_p]
+        L.dsh_batch_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+        L.dsh_batch_set_variant.argtypes = [C.c_void_p, C.c_int, C.c_int]
+        L.dsh_batch_get_stats.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(BatchStats)]
         L.dsh_setup_holberg.argtypes = [C.c_int, C.c_int, C.c_void_p]
         L.dsh_setup_pml.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
                                     C.c_float, C.c_float, C.c_void_p]
@@ -265,6 +280,83 @@ class Engine:
         s = Stats()
         _check(lib().dsh_get_stats(self.h, C.byref(s)), "dsh_get_stats")
         return {k: getattr(s, k) for k, _ in Stats._fields_}
+
+
+class Batch:
+    """An uneven batch of models advanced together (``dsh_batch``): one
+    velocity and one stress launch per time step for every shot of every
+    model; the block shape is chosen by the batch's autotuner."""
+
+    VARIANTS = ("128x8 points x 1 shot", "128x4 points x 2 shots", "128x2 points x 4 shots")
+
+    def __init__(self, params_list, device: int = 0):
+        self.params = list(params_list)
+        arr = (Params * len(self.params))(*self.params)
+        st = C.c_int(0)
+        self.h = lib().dsh_batch_create(arr, len(self.params), device, C.byref(st))
+        if not self.h:
+            raise DshError(st.value, "dsh_batch_create")
+        self._keep = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dsh_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_model(self, k, vs, rho, qs=None):
+        arrs = [np.ascontiguousarray(x, np.float32) if x is not None else None for x in (vs, rho, qs)]
+        self._keep[k] = arrs
+        _check(lib().dsh_batch_set_model(self.h, k, *[a.ctypes.data if a is not None else None for a in arrs]),
+               "dsh_batch_set_model")
+
+    def set_variant(self, v=-1, s=-1):
+        _check(lib().dsh_batch_set_variant(self.h, v, s), "dsh_batch_set_variant")
+
+    def set_stream(self, stream_handle):
+        _check(lib().dsh_batch_set_stream(self.h, stream_handle), "dsh_batch_set_stream")
+
+    def _flat(self, shots_per_model):
+        flat = [s for group in shots_per_model for s in group]
+        n = np.array([len(g) for g in shots_per_model], np.int32)
+        return flat, n
+
+    def forward(self, shots_per_model):
+        """shots_per_model[k]: list of Shot for model k -> [[seis [ntr, nt_k] per shot] per model]."""
+        flat, n = self._flat(shots_per_model)
+        total = sum(s.ntr * p.nt for g, p in zip(shots_per_model, self.params) for s in g)
+        out = np.zeros(max(total, 1), np.float32)
+        _check(lib().dsh_batch_forward(self.h, _shots_c(flat), n.ctypes.data, out.ctypes.data), "dsh_batch_forward")
+        res, o = [], 0
+        for g, p in zip(shots_per_model, self.params):
+            m = sum(s.ntr for s in g) * p.nt
+            res.append(_split(out[o:o + m], g, p.nt))
+            o += m
+        return res
+
+    def forward_device(self, shots_per_model, seis_dev_ptr: int):
+        flat, n = self._flat(shots_per_model)
+        _check(lib().dsh_batch_forward_device(self.h, _shots_c(flat), n.ctypes.data, seis_dev_ptr),
+               "dsh_batch_forward_device")
+
+    def stats(self) -> dict:
+        ms = np.zeros(len(self.params), np.float64)
+        s = BatchStats()
+        _check(lib().dsh_batch_get_stats(self.h, ms.ctypes.data, C.byref(s)), "dsh_batch_get_stats")
+        return {"ms_total": s.ms_total, "kernel_launches": s.kernel_launches, "point_updates": s.point_updates,
+                "v_variant": s.v_variant, "s_variant": s.s_variant, "phases": s.phases,
+                "v_ms": list(s.v_ms)[:3], "s_ms": list(s.s_ms)[:3], "model_ms": ms}
 
 
 NOALLOC_MAX_SHOTS = 64

@@ -123,3 +123,41 @@ def small_case(nx=64, ny=48, nt=150, fdorder=4, l=0, free_surf=1, fw=10, seed=0,
     params = dict(nx=nx, ny=ny, nt=nt, dh=dh, dt=dt, fdorder=fdorder, maxrelerror=1, fw=fw, free_surf=free_surf,
                   l=l, fl=(7.5, 30.0, 120.0, 240.0)[:l], damping=float(vs.max()), fpml=fc, eprecond=1)
     return dict(name="small", params=params, vs=vs, rho=rho, qs=qs, shots=shots)
+
+
+def config4(seed=5, nmodels=32, nt_scale=1.0):
+    """Uneven batch of independent models: NX ~ U[256, 2048], NY ~ U[128, 512], DH = 0.5 m,
+    FDORDER from {4, 6, 8}, elastic / viscoelastic (L=2, Qs 40) half each, 8-32 shots per model
+    with Ricker fc ~ U[20, 60] Hz, C1-style layered model with seeded +-5% vs perturbations.
+    DT = 0.8 x the stability limit (dt_limit), NT = ceil(1.5 t_max / DT) with t_max the diagonal
+    traveltime at the slowest velocity; ``nt_scale`` shortens every NT by the same factor.
+    Returns a list of per-model dicts like the other builders."""
+    from . import dt_limit
+
+    rng = np.random.default_rng(seed)
+    dh = 0.5
+    models = []
+    for k in range(nmodels):
+        nx = int(rng.integers(256, 2049))
+        ny = int(rng.integers(128, 513))
+        fdo = int(rng.choice([4, 6, 8]))
+        visc = k % 2 == 1
+        nsh = int(rng.integers(8, 33))
+        fc = float(rng.uniform(20.0, 60.0))
+        vs, rho = _layered(nx, ny, dh)
+        vs = (vs * (1.0 + _noise(rng, (ny, nx), 2.0 / dh, 0.05))).astype(np.float32)
+        vmax, vmin = float(vs.max()), float(vs.min())
+        dt = float(np.float32(0.8 * dt_limit(fdo, 1, dh, vmax)))
+        tmax = math.hypot(nx * dh, ny * dh) / vmin
+        nt = max(2, int(math.ceil(1.5 * tmax / dt * nt_scale)))
+        l = 2 if visc else 0
+        qs = np.full((ny, nx), 40.0, np.float32) if visc else None
+        ntr = 48
+        rec = receivers_line(nx * dh * 0.05, nx * dh * 0.9 / ntr, ntr, dh, dh)
+        xs = np.linspace(0.1, 0.9, nsh) * nx * dh
+        shots = [Shot(point_source(iround(x / dh), iround(1.0 / dh), fc), rec) for x in xs]
+        params = dict(nx=nx, ny=ny, nt=nt, dh=dh, dt=dt, fdorder=fdo, maxrelerror=1, fw=20, free_surf=1, l=l,
+                      fl=(fc / 4, 2 * fc)[:l], damping=vmax, fpml=fc, eprecond=1, max_shots=nsh)
+        models.append(dict(name=f"m{k}-{nx}x{ny}-fd{fdo}-L{l}", params=params, vs=vs, rho=rho, qs=qs,
+                           shots=shots))
+    return models

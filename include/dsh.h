@@ -166,6 +166,45 @@ int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
 int dsh_residual_noalloc(int nshots, int ntr, int nt, const float *syn, const float *obs, float *res, double *l2,
                          void *stream);
 
+/* ---- Uneven batches: many models in one launch per half-step ----
+ * A batch holds nmodels independent models, each with its own dsh_params
+ * (grid, FDORDER, L, DT, NT, max_shots, ...).  dsh_batch_forward advances all
+ * their shots together: one velocity and one stress kernel launch per time
+ * step for the whole batch, each thread block working on one 128-point tile
+ * of one model; models leave the launches once their NT is reached.  Results
+ * are bit-identical to running each model through its own context (and so
+ * to the reference's forward loop, src/denise.c:1179-1346); the reference
+ * runs one model per program.  Supported per model: FDORDER 4, 6, 8 and
+ * L 0 or 2 (other combinations: DSH_ERR_PARAM at creation).
+ * Tile shape: each launch uses one of three block shapes (128 x 8 points x 1
+ * shot, 128 x 4 x 2 shots, 128 x 2 x 4 shots); the first run of a batch times
+ * them on the batch itself and keeps the fastest (dsh_batch_set_variant
+ * fixes them instead). */
+typedef struct dsh_batch dsh_batch;
+dsh_batch *dsh_batch_create(const dsh_params *p, int nmodels, int device, int *status);
+int dsh_batch_destroy(dsh_batch *b);
+/* model k's vs, rho, qs as dsh_set_model takes them */
+int dsh_batch_set_model(dsh_batch *b, int model, const float *vs, const float *rho, const float *qs);
+/* Forward modelling of every model: shots holds nshots[0] shots of model 0,
+ * then nshots[1] of model 1, ... (nshots[k] <= max_shots of model k, 0 skips
+ * a model); seis_out receives, in the same order, per shot [ntr][nt_k]. */
+int dsh_batch_forward(dsh_batch *b, const dsh_shot *shots, const int *nshots, float *seis_out);
+int dsh_batch_forward_device(dsh_batch *b, const dsh_shot *shots, const int *nshots, float *seis_dev);
+int dsh_batch_set_stream(dsh_batch *b, void *stream);
+/* tile-shape variants 0..2 for the velocity and stress launches; -1 = autotune */
+int dsh_batch_set_variant(dsh_batch *b, int v_variant, int s_variant);
+typedef struct dsh_batch_stats {
+    double ms_total;                 /* device time of the last run (CUDA events) */
+    long long kernel_launches;
+    long long point_updates;         /* sum over models of nx*ny*nt*shots */
+    int v_variant, s_variant;        /* tile shapes in use */
+    int phases;                      /* distinct NT values (launch grids shrink at each) */
+    float v_ms[4], s_ms[4];          /* autotuner: mean ms per launch of each variant (0 = not timed) */
+} dsh_batch_stats;
+/* model_ms[k] (optional, nmodels doubles): device time from the start of
+ * the last run until model k's last step completed */
+int dsh_batch_get_stats(dsh_batch *b, double *model_ms, dsh_batch_stats *out);
+
 /* Statistics of the last dsh_forward / dsh_gradient call. */
 typedef struct dsh_stats {
     double ms_forward, ms_adjoint, ms_total;   /* device time (CUDA events) */

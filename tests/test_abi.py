@@ -68,3 +68,21 @@ def test_error_strings():
     lib = dsh.lib()
     for code in (0, -1, -2, -3, -4, -5, -6):
         assert lib.dsh_error_string(code)
+
+
+def test_batch_rejects_unsupported_models_without_gpu():
+    """Parameter checks of dsh_batch_create run before any CUDA call."""
+    import ctypes as C
+
+    import dsh
+
+    ok = dsh.make_params(64, 48, 100, 0.5, 1e-4, fdorder=4)
+    for bad in (dict(fdorder=10), dict(fdorder=8, l=3), dict(fdorder=2)):
+        p = dsh.make_params(64, 48, 100, 0.5, 1e-4, **bad)
+        arr = (dsh.Params * 2)(ok, p)
+        st = C.c_int(0)
+        assert not dsh.lib().dsh_batch_create(arr, 2, 0, C.byref(st))
+        assert st.value == -1
+    st = C.c_int(0)
+    assert not dsh.lib().dsh_batch_create(None, 0, 0, C.byref(st))
+    assert st.value == -1

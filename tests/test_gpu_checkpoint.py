@@ -56,7 +56,12 @@ def test_64_shots_one_launch_checkpointed():
     half-step (grid z = shot) with checkpoints; the shot sum is bit-identical
     to the reference's shot loop."""
     nt = 130
-    d, shots = _case(964, nx=72, ny=40, nt=nt, fdo=8, L=2, fs=1, fw=8, nshots=64)
+    d, _ = _case(964, nx=72, ny=40, nt=nt, fdo=8, L=2, fs=1, fw=8, nshots=1)
+    shots = []
+    for k in range(64):           # 64 sources along the surface, receivers within a few points of each
+        sp = np.array([[4 + k], [2], [0], [-0.01], [60.0], [1.0], [0], [3]], np.float32)
+        xi = np.clip(4 + k + np.array([-3, -1, 1, 2, 4]), 1, 72)
+        shots.append(dsh.Shot(sp, np.array([xi, [1, 1, 2, 3, 1]], np.int32)))
     m = oracle_model(d)
     obs = []
     for sh in shots:
