@@ -17,7 +17,7 @@ def declared(header):
     src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     src = re.sub(r"#define[^\n]*", "", src)
-    return sorted(set(re.findall(r"\b(?:void|int|float|double|dsh_ctx \*|const char \*)\s*\**\s*([A-Za-z_][A-Za-z0-9_]*)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(?:void|int|float|double|dsh_ctx \*|dsh_batch \*|const char \*)\s*\**\s*([A-Za-z_][A-Za-z0-9_]*)\s*\(", src)))
 
 
 def _library_for(header):
@@ -28,6 +28,8 @@ def _library_for(header):
             pytest.skip("the compat layer resolves the reference's globals from the program that loads it")
         C.CDLL(os.path.join(O.REF_DIR, "libdenise_ref.so"), mode=C.RTLD_GLOBAL)
         return C.CDLL(os.path.join(ROOT, "denise-sh_b200", "libdsh_compat.so"))
+    if header == "dsh_nn.h":
+        return C.CDLL(os.path.join(ROOT, "denise-sh_b200", "libdsh_nn.so"))
     return dsh.lib()
 
 

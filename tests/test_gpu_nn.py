@@ -1,0 +1,123 @@
+"""Learned pseudo-Hessian preconditioner kernels on the GPU: the tcgen05/TMA
+BF16 GEMM against a float matmul of the same BF16 operands, the U-Net's
+forward pass and hand-written backward pass against the CPU checker
+(oracle/unet_ref.py, PyTorch CPU autograd in FP32 with the same BF16
+rounding points), and a training loop that lowers the loss."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _bf(a):
+    return torch.tensor(a, dtype=torch.float32).to(torch.bfloat16)
+
+
+@pytest.mark.parametrize("M,N,K,splits,bias,relu,out16", [
+    (128, 32, 64, 1, False, False, False),
+    (200, 48, 72, 1, True, True, False),
+    (1000, 256, 576, 1, True, True, True),
+    (300, 288, 128, 1, False, False, False),
+    (130, 64, 1000, 1, False, False, True),
+    (288, 64, 5000, 8, False, False, False),
+])
+def test_gemm_matches_float_matmul(M, N, K, splits, bias, relu, out16):
+    from dsh import nn
+
+    rng = np.random.default_rng(M + N + K)
+    ldk = (K + 7) // 8 * 8
+    A = torch.zeros(M, ldk, dtype=torch.bfloat16)
+    B = torch.zeros(N, ldk, dtype=torch.bfloat16)
+    A[:, :K] = _bf(rng.standard_normal((M, K)))
+    B[:, :K] = _bf(rng.standard_normal((N, K)))
+    A, B = A.cuda(), B.cuda()
+    b = torch.tensor(rng.standard_normal(N), dtype=torch.float32).cuda() if bias else None
+    ctx = nn.Ctx(torch)
+    c32 = torch.full((M, N), 7.0, device="cuda")
+    c16 = torch.zeros(M, N, dtype=torch.bfloat16, device="cuda") if out16 else None
+    ctx.gemm(M, N, K, A, ldk, B, ldk, c32=None if out16 else c32, c16=c16, bias=b, relu=relu, splits=splits)
+    ctx.check()
+    ref = A[:, :K].float() @ B[:, :K].float().t()
+    if bias:
+        ref = ref + b
+    if relu:
+        ref = torch.relu(ref)
+    got = c16.float() if out16 else c32
+    tol = (8e-3 if out16 else 1e-5) * float(ref.abs().max())
+    assert float((got - ref).abs().max()) <= tol
+
+
+def test_gemm_accumulates():
+    from dsh import nn
+
+    rng = np.random.default_rng(5)
+    M, N, K = 96, 40, 4096
+    A = _bf(rng.standard_normal((M, K))).cuda()
+    B = _bf(rng.standard_normal((N, K))).cuda()
+    c = torch.tensor(rng.standard_normal((M, N)), dtype=torch.float32).cuda()
+    c0 = c.clone()
+    ctx = nn.Ctx(torch)
+    ctx.gemm(M, N, K, A, K, B, K, c32=c, splits=4, accumulate=True)
+    ctx.check()
+    ref = c0 + A.float() @ B.float().t()
+    assert float((c - ref).abs().max()) <= 1e-5 * float(ref.abs().max())
+
+
+def _inputs(B, H, W, seed):
+    from dsh import nn
+
+    rng = np.random.default_rng(seed)
+    g = rng.standard_normal((B, H, W)).astype(np.float32)
+    ws = np.exp(rng.standard_normal((B, H, W))).astype(np.float32)
+    wr = np.exp(rng.standard_normal((B, H, W))).astype(np.float32)
+    vs = (300 + 50 * rng.standard_normal((B, H, W))).astype(np.float32)
+    return nn.pack_inputs(torch, g, ws, wr, vs)
+
+
+def test_unet_forward_backward_match_cpu_checker():
+    import unet_ref
+
+    from dsh import nn
+
+    B, H, W = 2, 16, 24
+    net = nn.UNet(torch, seed=3)
+    x = _inputs(B, H, W, 1)
+    out = net.forward(x, B, H, W).clone()
+    dout = torch.tensor(np.random.default_rng(2).standard_normal(B * H * W), dtype=torch.float32).cuda()
+    net.zero_grad()
+    net.backward(dout)
+    net.ctx.check()
+    ref_out, ref_g = unet_ref.gradients(net.state(), x.float().cpu().numpy(), B, H, W, dout.cpu().numpy())
+    got = out.cpu().numpy()
+    assert np.abs(got - ref_out).max() <= 2e-2 * np.abs(ref_out).max()
+    g = net.grads()
+    for k, r in ref_g.items():
+        a = g[k].ravel().astype(np.float64)
+        b = r.ravel().astype(np.float64)
+        if np.abs(b).max() == 0:
+            continue
+        cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        assert cos > 0.999 and rel < 5e-2, (k, cos, rel)
+
+
+def test_unet_training_lowers_loss():
+    from dsh import nn
+
+    B, H, W = 2, 32, 48
+    net = nn.UNet(torch, seed=4)
+    x = _inputs(B, H, W, 7)
+    # a smooth target that depends on the inputs: blurred energy channel
+    t = x.float().view(B, H, W, -1)[..., 1].contiguous().view(-1)
+    losses = []
+    for _ in range(60):
+        net.forward(x, B, H, W)
+        loss, grad = net.loss_grad(t)
+        net.zero_grad()
+        net.backward(grad)
+        net.adam_step(lr=2e-3)
+        losses.append(float(loss.item()))
+    net.ctx.check()
+    assert losses[-1] < 0.2 * losses[0], losses[::10]
