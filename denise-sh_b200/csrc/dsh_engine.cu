@@ -276,7 +276,8 @@ static int check_params(const dsh_params *p)
     if (!(p->dh > 0) || !(p->dt > 0)) return DSH_ERR_PARAM;
     for (int l = 0; l < p->l; l++)
         if (!(p->fl[l] > 0)) return DSH_ERR_PARAM;
-    if (p->eprecond != 0 && p->eprecond != 1 && p->eprecond != 3) return DSH_ERR_PARAM;
+    if (p->eprecond != 0 && p->eprecond != 1 && p->eprecond != 3 && p->eprecond != DSH_EPRECOND_ENERGY_ONLY)
+        return DSH_ERR_PARAM;
     if (p->max_shots < 1 || p->max_shots > 65535) return DSH_ERR_PARAM;
     if (p->nx > 65000 || p->ny > 65000) return DSH_ERR_PARAM;
     if (p->quellart != 1 && p->quellart != 2 && p->quellart != 3 && p->quellart != 4 && p->quellart != 5 &&
@@ -709,10 +710,10 @@ StepArgs step_args(dsh_ctx *ctx, Pass pass)
         break;
     case P_FWD_STORE:
         a.fwd = ctx->fwd;
-        if (p.eprecond == 1 || p.eprecond == 3) a.ws = sl + ctx->o_ws;
+        if (p.eprecond == 1 || p.eprecond == 3 || p.eprecond == DSH_EPRECOND_ENERGY_ONLY) a.ws = sl + ctx->o_ws;
         break;
     case P_FWD_CKPT:
-        if (p.eprecond == 1 || p.eprecond == 3) a.ws = sl + ctx->o_ws;
+        if (p.eprecond == 1 || p.eprecond == 3 || p.eprecond == DSH_EPRECOND_ENERGY_ONLY) a.ws = sl + ctx->o_ws;
         break;
     case P_RECOMP:
         a.fwd = ctx->fwd;
@@ -721,7 +722,7 @@ StepArgs step_args(dsh_ctx *ctx, Pass pass)
         break;
     case P_ADJ:
         a.fwd = ctx->fwd;
-        if (p.eprecond == 1) a.ws = sl + ctx->o_wr;
+        if (p.eprecond == 1 || p.eprecond == DSH_EPRECOND_ENERGY_ONLY) a.ws = sl + ctx->o_wr;
         break;
     }
     return a;

@@ -1,0 +1,138 @@
+/*
+ * dsh_fwi.c — L-BFGS direction, parabolic step length and the bracketing
+ * line search of the FWI loop (host C; see include/dsh_fwi.h).
+ */
+#include "dsh_fwi.h"
+
+#include <math.h>
+#include <stddef.h>
+
+static double dot(long long n, const float *a, const float *b)
+{
+    double s = 0.0;
+    for (long long i = 0; i < n; i++) s += (double)a[i] * (double)b[i];
+    return s;
+}
+
+int dsh_lbfgs_direction(long long n, int count, const float *S, const float *Y, const float *q, float *r)
+{
+    if (n <= 0 || count < 0 || !q || !r || (count > 0 && (!S || !Y)) || count > 64) return -1;
+    double alpha[64], rho[64];
+    double *w = NULL;
+    for (long long i = 0; i < n; i++) r[i] = q[i];
+    if (count == 0) return 0;
+    (void)w;
+    for (int k = 0; k < count; k++) {
+        const double ys = dot(n, Y + (long long)k * n, S + (long long)k * n);
+        rho[k] = fabs(ys) > 0.0 ? 1.0 / ys : 0.0;
+    }
+    /* first loop: newest to oldest (src/LBFGS.c:56-70) */
+    for (int k = count - 1; k >= 0; k--) {
+        const float *s = S + (long long)k * n, *y = Y + (long long)k * n;
+        alpha[k] = rho[k] * dot(n, s, r);
+        for (long long i = 0; i < n; i++) r[i] = (float)((double)r[i] - alpha[k] * (double)y[i]);
+    }
+    /* initial inverse Hessian gamma I from the newest pair (src/LBFGS.c:30-38) */
+    const float *sn = S + (long long)(count - 1) * n, *yn = Y + (long long)(count - 1) * n;
+    const double yy = dot(n, yn, yn);
+    const double gamma = yy > 0.0 ? dot(n, yn, sn) / yy : 1.0;
+    for (long long i = 0; i < n; i++) r[i] = (float)(gamma * (double)r[i]);
+    /* second loop: oldest to newest (src/LBFGS.c:78-92) */
+    for (int k = 0; k < count; k++) {
+        const float *s = S + (long long)k * n, *y = Y + (long long)k * n;
+        const double beta = rho[k] * dot(n, y, r);
+        for (long long i = 0; i < n; i++) r[i] = (float)((double)r[i] + (double)s[i] * (alpha[k] - beta));
+    }
+    return 0;
+}
+
+/* 3x3 solve by Gaussian elimination with partial pivoting (double) */
+static int solve3(double A[3][3], double b[3], double x[3])
+{
+    for (int c = 0; c < 3; c++) {
+        int p = c;
+        for (int r = c + 1; r < 3; r++)
+            if (fabs(A[r][c]) > fabs(A[p][c])) p = r;
+        if (A[p][c] == 0.0) return -1;
+        for (int k = 0; k < 3; k++) { double t = A[c][k]; A[c][k] = A[p][k]; A[p][k] = t; }
+        { double t = b[c]; b[c] = b[p]; b[p] = t; }
+        for (int r = c + 1; r < 3; r++) {
+            const double f = A[r][c] / A[c][c];
+            for (int k = c; k < 3; k++) A[r][k] -= f * A[c][k];
+            b[r] -= f * b[c];
+        }
+    }
+    for (int r = 2; r >= 0; r--) {
+        double s = b[r];
+        for (int k = r + 1; k < 3; k++) s -= A[r][k] * x[k];
+        x[r] = s / A[r][r];
+    }
+    return 0;
+}
+
+float dsh_opt_step(const float L2t[3], const float epst[3])
+{
+    double A[3][3], b[3], x[3];
+    for (int i = 0; i < 3; i++) {
+        A[i][0] = 1.0;
+        A[i][1] = epst[i];
+        A[i][2] = (double)epst[i] * epst[i];
+        b[i] = L2t[i];
+    }
+    if (solve3(A, b, x) != 0) return epst[0] > 0 ? epst[0] : epst[1];
+    float opteps = (float)(-x[1] / (2.0 * x[2]));
+    if (2.0 * x[2] < 0.0 && L2t[1] > L2t[2]) opteps = epst[2];   /* misfit still falling at the 3rd step */
+    if (opteps > epst[2]) opteps = epst[2];
+    if (opteps < 0.0f) opteps = epst[0];
+    return opteps;
+}
+
+void dsh_line_search_init(dsh_line_search *ls, float L2_now, float eps_scale, float scalefac, int stepmax)
+{
+    ls->epst[0] = 0.0f; ls->epst[1] = ls->epst[2] = 0.0f;
+    ls->L2t[0] = L2_now; ls->L2t[1] = ls->L2t[2] = 0.0f;
+    ls->eps_scale = eps_scale;
+    ls->scalefac = scalefac;
+    ls->step1 = ls->step2 = ls->countstep = 0;
+    ls->stepmax = stepmax;
+    ls->slot = 1;
+}
+
+int dsh_line_search_next(dsh_line_search *ls, float L2_test, float *eps_scale, int *slot)
+{
+    /* the misfit of the step just tested goes into its slot (epst1/L2t[itest]) */
+    ls->L2t[ls->slot] = L2_test;
+    ls->epst[ls->slot] = ls->eps_scale;
+    if (ls->step1 == 0 && ls->L2t[0] <= ls->L2t[1]) {          /* no reduction yet: shorter step */
+        ls->eps_scale = ls->eps_scale / ls->scalefac;
+        ls->countstep++;
+    }
+    if (ls->step1 == 1 && ls->L2t[1] < ls->L2t[2]) {           /* bracketed */
+        ls->epst[2] = ls->eps_scale;
+        ls->step2 = 1;
+    }
+    if (ls->step1 == 1 && ls->L2t[1] >= ls->L2t[2]) {          /* still falling: longer third step */
+        ls->epst[2] = ls->eps_scale;
+        ls->eps_scale = ls->eps_scale + ls->eps_scale / ls->scalefac;
+        ls->countstep++;
+    }
+    if (ls->step1 == 0 && ls->L2t[0] > ls->L2t[1]) {           /* first reducing step found */
+        ls->epst[1] = ls->eps_scale;
+        ls->step1 = 1;
+        ls->slot = 2;
+        ls->countstep = 0;
+        ls->eps_scale = ls->eps_scale + ls->eps_scale / ls->scalefac;
+    }
+    if (ls->step1 == 0 && ls->countstep > ls->stepmax) {
+        *eps_scale = 0.0f;
+        return -1;
+    }
+    if (ls->step1 == 1 && ls->countstep > ls->stepmax) ls->step2 = 1;
+    if (ls->step1 == 1 && ls->step2 == 1) {
+        *eps_scale = dsh_opt_step(ls->L2t, ls->epst);
+        return 0;
+    }
+    *eps_scale = ls->eps_scale;
+    *slot = ls->slot;
+    return 1;
+}

@@ -19,6 +19,7 @@ PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 LIB_PATH = os.path.join(PKG_DIR, "libdsh.so")
 
 DSH_OK = 0
+EPRECOND_ENERGY_ONLY = 10      # dsh_params.eprecond: raw gradient plus the energies Ws, Wr
 ERRORS = {-1: "invalid parameter", -2: "CUDA error", -3: "out of device memory or budget",
           -4: "simulation is unstable (non-finite wavefield)", -5: "call out of order", -6: "device wait timed out"}
 

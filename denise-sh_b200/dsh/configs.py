@@ -161,3 +161,47 @@ def config4(seed=5, nmodels=32, nt_scale=1.0):
         models.append(dict(name=f"m{k}-{nx}x{ny}-fd{fdo}-L{l}", params=params, vs=vs, rho=rho, qs=qs,
                            shots=shots))
     return models
+
+
+def _anomaly_model(rng, nx, ny, dh):
+    """Layered C1-style background plus 5-15 elliptical +-20% vs anomalies."""
+    vs, rho = _layered(nx, ny, dh)
+    yy, xx = np.mgrid[1:ny + 1, 1:nx + 1] * dh
+    true = vs.copy()
+    for _ in range(int(rng.integers(5, 16))):
+        cx, cy = rng.uniform(0, nx * dh), rng.uniform(5, ny * dh)
+        a, b = rng.uniform(5, 30), rng.uniform(5, 30)
+        s = rng.choice([-0.2, 0.2])
+        inside = ((xx - cx) / a) ** 2 + ((yy - cy) / b) ** 2 <= 1.0
+        true = np.where(inside, true * (1 + s), true)
+    return true.astype(np.float32), rho
+
+
+def config5(seed=6, nx=1200, ny=400, nt=3000, nshots=32, ntr=240):
+    """Learned-preconditioner FWI problem: NX=1200, NY=400, DH=0.5, L=3, FDORDER=8, DT=2e-4,
+    NT=3000, 30 Hz Ricker; true model = layered background + elliptical anomalies, start model =
+    true smoothed with a 10 m Gaussian; 32 shots along the surface, 240 receivers 2.5 m apart."""
+    dh = 0.5
+    rng = np.random.default_rng(seed)
+    true, rho = _anomaly_model(rng, nx, ny, dh)
+    start = gaussian_filter(true, 10.0 / dh).astype(np.float32)
+    qs = np.full((ny, nx), 40.0, np.float32)
+    fc = 30.0
+    rec = receivers_line(nx * dh * 0.5 - (ntr - 1) * 1.25, 2.5, ntr, 0.5, dh) if ntr * 2.5 < nx * dh else \
+        receivers_line(dh, nx * dh / ntr, ntr, 0.5, dh)
+    xs = np.linspace(0.05, 0.95, nshots) * nx * dh
+    shots = [Shot(point_source(iround(x / dh), iround(1.0 / dh), fc), rec) for x in xs]
+    params = dict(nx=nx, ny=ny, nt=nt, dh=dh, dt=2e-4, fdorder=8, maxrelerror=1, fw=20, free_surf=1, l=3,
+                  fl=(fc / 4, fc, 4 * fc), damping=float(true.max()), fpml=fc, eprecond=1, max_shots=nshots)
+    return dict(name=f"learned-fwi-{nx}x{ny}-fd8-L3", params=params, vs=start, rho=rho, qs=qs, true=true,
+                shots=shots)
+
+
+def training_models(count=200, first_seed=100, nx=1200, ny=400):
+    """Seeded random models of the batched-gradient generator (seeds first_seed ..) at the learned-FWI
+    grid: (true, start) pairs, start = true smoothed with a 10 m Gaussian."""
+    dh = 0.5
+    for seed in range(first_seed, first_seed + count):
+        rng = np.random.default_rng(seed)
+        true, rho = _anomaly_model(rng, nx, ny, dh)
+        yield seed, true, gaussian_filter(true, 10.0 / dh).astype(np.float32), rho

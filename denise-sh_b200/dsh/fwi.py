@@ -1,0 +1,290 @@
+"""FWI loop on the GPU engine: L-BFGS (src/LBFGS.c) with the reference's
+bracketing parabolic line search (src/line_search.c, src/calc_opt_step.c),
+preconditioned either by the energy preconditioner EPRECOND=1 (the plain
+method) or by the learned pseudo-Hessian U-Net (dsh.nn), plus generation of
+the network's training pairs by the solver itself and its training.
+
+Only vs is inverted (rho stays at its start value in both methods).  The
+model update of a step of relative length eps is
+    vs <- clip(vs - eps * max|vs| / max|d| * d)       (src/calc_mat_change_test.c)
+for the L-BFGS direction d.  GPU-seconds are device time from CUDA events:
+the engine's own per-call timing (gradients, test forward models) plus the
+network inference, so the two methods are compared on the same clock.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import time
+
+import numpy as np
+
+from . import DshError, Engine, Shot, _check, lib, make_params
+
+
+class LineSearch(C.Structure):
+    _fields_ = [("epst", C.c_float * 3), ("L2t", C.c_float * 3), ("eps_scale", C.c_float), ("scalefac", C.c_float),
+                ("step1", C.c_int), ("step2", C.c_int), ("countstep", C.c_int), ("stepmax", C.c_int),
+                ("slot", C.c_int)]
+
+
+def _setup():
+    L = lib()
+    if not getattr(L, "_fwi_ready", False):
+        L.dsh_lbfgs_direction.argtypes = [C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_opt_step.restype = C.c_float
+        L.dsh_opt_step.argtypes = [C.c_void_p, C.c_void_p]
+        L.dsh_line_search_init.argtypes = [C.POINTER(LineSearch), C.c_float, C.c_float, C.c_float, C.c_int]
+        L.dsh_line_search_next.argtypes = [C.POINTER(LineSearch), C.c_float, C.POINTER(C.c_float),
+                                           C.POINTER(C.c_int)]
+        L._fwi_ready = True
+    return L
+
+
+def lbfgs_direction(S, Y, q):
+    """r = H q from pairs S, Y [count][n] (oldest first)."""
+    S = np.ascontiguousarray(S, np.float32)
+    Y = np.ascontiguousarray(Y, np.float32)
+    q = np.ascontiguousarray(q, np.float32).ravel()
+    r = np.empty_like(q)
+    count = S.shape[0] if S.ndim == 2 else 0
+    _check(_setup().dsh_lbfgs_direction(q.size, count, S.ctypes.data if count else None,
+                                        Y.ctypes.data if count else None, q.ctypes.data, r.ctypes.data),
+           "dsh_lbfgs_direction")
+    return r
+
+
+def opt_step(L2t, epst):
+    a = np.ascontiguousarray(L2t, np.float32)
+    e = np.ascontiguousarray(epst, np.float32)
+    return float(_setup().dsh_opt_step(a.ctypes.data, e.ctypes.data))
+
+
+def line_search(misfit, L2_now, eps_scale=0.01, scalefac=2.0, stepmax=6):
+    """Runs the reference's line search with misfit(eps) as the test forward
+    model; returns (chosen eps or 0 when no step reduced the misfit, tests)."""
+    L = _setup()
+    ls = LineSearch()
+    L.dsh_line_search_init(C.byref(ls), L2_now, eps_scale, scalefac, stepmax)
+    eps, slot = C.c_float(eps_scale), C.c_int(1)
+    tests = 0
+    while True:
+        l2 = misfit(float(eps.value))
+        tests += 1
+        rc = L.dsh_line_search_next(C.byref(ls), float(l2), C.byref(eps), C.byref(slot))
+        if rc == 1:
+            continue
+        return (float(eps.value) if rc == 0 else 0.0), tests
+
+
+def l2_misfit(syn, obs):
+    """Sum of squared residuals as src/calc_res.c forms it (first sample excluded)."""
+    d = syn[..., 1:].astype(np.float64) - obs[..., 1:].astype(np.float64)
+    return float(np.sum(d * d))
+
+
+class Problem:
+    """An FWI problem: model parameters, start/true models and shots."""
+
+    def __init__(self, cfg, test_shots=4):
+        self.cfg = cfg
+        self.p = dict(cfg["params"])
+        self.shots = cfg["shots"]
+        self.rho, self.qs = cfg["rho"], cfg["qs"]
+        self.vs0 = cfg["vs"].astype(np.float32)
+        ns = len(self.shots)
+        self.test_idx = sorted({int(round(k)) for k in np.linspace(0, ns - 1, min(test_shots, ns))})
+        self.obs = None
+        self.engines = {}
+
+    def engine(self, eprecond):
+        if eprecond not in self.engines:
+            p = dict(self.p, eprecond=eprecond, max_shots=len(self.shots))
+            self.engines[eprecond] = Engine(make_params(**p))
+        return self.engines[eprecond]
+
+    def observe(self):
+        """Observed data: the solver on the true model (every shot)."""
+        e = self.engine(1)
+        e.set_model(self.cfg["true"], self.rho, self.qs)
+        self.obs = e.forward(self.shots)
+        return self.obs
+
+    def close(self):
+        for e in self.engines.values():
+            e.close()
+        self.engines = {}
+
+
+class Clock:
+    """GPU-seconds of a method: engine call times plus timed network work."""
+
+    def __init__(self):
+        self.ms = 0.0
+
+    def add_engine(self, eng):
+        self.ms += eng.stats()["ms_total"]
+
+    @property
+    def seconds(self):
+        return self.ms / 1e3
+
+
+def learned_preconditioner(net, torch, g, ws, wr, vs, clock):
+    """H_vs predicted by the U-Net from (raw gradient, Ws, Wr, vs), device-timed."""
+    from . import nn as dnn
+
+    ny, nx = g.shape
+    x = dnn.pack_inputs(torch, g, ws, wr, vs)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    out = net.forward(x, 1, ny, nx)
+    e1.record()
+    torch.cuda.synchronize()
+    clock.ms += e0.elapsed_time(e1)
+    return dnn.hessian_from_prediction(out.cpu().numpy().reshape(ny, nx))
+
+
+def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, scalefac=2.0, stepmax=6, nlbfgs=5,
+        vmin=None, vmax=None, target_misfit=None, log=None):
+    """FWI iterations; returns the history [{iter, misfit, gpu_s, eps, tests, fallback}].
+    method "plain": EPRECOND=1 gradient; "learned": raw gradient / U-Net Hessian,
+    falling back to a plain gradient when the line search rejects the learned step."""
+    if problem.obs is None:
+        problem.observe()
+    shots, obs = problem.shots, problem.obs
+    test = problem.test_idx
+    vs = problem.vs0.copy()
+    vmin = float(vs.min()) * 0.5 if vmin is None else vmin
+    vmax = float(vs.max()) * 1.5 if vmax is None else vmax
+    c_vs = float(vs.mean())
+    clock = Clock()
+    S, Y = [], []
+    prev = None
+    hist = []
+    fwd_eng = problem.engine(1)
+
+    def gradient(kind):
+        eng = problem.engine(1 if kind == "plain" else 10)
+        eng.set_model(vs, problem.rho, problem.qs)
+        out = eng.gradient(shots, obs, want_seis=True, want_energy=(kind == "learned"))
+        clock.add_engine(eng)
+        if kind == "plain":
+            q = out["g_vs"]
+        else:
+            ws, wr = out["Ws"].sum(axis=0), out["Wr"].sum(axis=0)
+            h = learned_preconditioner(net, torch, out["g_vs"], ws, wr, vs, clock)
+            q = out["g_vs"] / (h + 0.005 * float(h.max()))
+        l2_test = sum(l2_misfit(out["seis"][k], obs[k]) for k in test)
+        return q.astype(np.float32), out["l2"], l2_test
+
+    def step_model(d, eps):
+        scale = eps * float(np.abs(vs).max()) / max(float(np.abs(d).max()), 1e-30)
+        return np.clip(vs - scale * d, vmin, vmax).astype(np.float32)
+
+    def test_misfit(d):
+        tshots = [shots[k] for k in test]
+
+        def f(eps):
+            fwd_eng.set_model(step_model(d, eps), problem.rho, problem.qs)
+            syn = fwd_eng.forward(tshots)
+            clock.add_engine(fwd_eng)
+            return sum(l2_misfit(s, obs[k]) for s, k in zip(syn, test))
+        return f
+
+    for it in range(1, niter + 1):
+        kind = method
+        q, l2, l2_test = gradient(kind)
+        fallback = False
+        for attempt in range(2):
+            qn = c_vs * q.ravel()
+            if prev is not None and prev[2] == kind:
+                S.append(((vs - prev[0]).ravel() / c_vs).astype(np.float32))
+                Y.append((qn - prev[1]).astype(np.float32))
+                S, Y = S[-nlbfgs:], Y[-nlbfgs:]
+            elif prev is not None:
+                S, Y = [], []
+            d = lbfgs_direction(np.array(S) if S else np.zeros((0, qn.size), np.float32),
+                                np.array(Y) if Y else np.zeros((0, qn.size), np.float32), qn)
+            if float(d @ qn) <= 0.0:        # not a descent direction: restart from the gradient
+                S, Y = [], []
+                d = qn.copy()
+            d = d.reshape(vs.shape)
+            eps, tests = line_search(test_misfit(d), l2_test, eps_scale, scalefac, stepmax)
+            if eps > 0.0 or kind == "plain":
+                break
+            # the line search rejected the learned step: plain gradient instead
+            fallback, kind = True, "plain"
+            S, Y = [], []
+            q, l2, l2_test = gradient("plain")
+        prev = (vs.copy(), c_vs * q.ravel(), kind)
+        if eps > 0.0:
+            vs = step_model(d, eps)
+        rec = {"iter": it, "misfit": l2, "gpu_s": clock.seconds, "eps": eps, "tests": tests, "fallback": fallback,
+               "wall_s": time.time()}
+        hist.append(rec)
+        if log:
+            log(rec)
+        if eps == 0.0 and kind == "plain":
+            break
+        if target_misfit is not None and l2 <= target_misfit:
+            break
+    # misfit of the final model
+    eng = problem.engine(1)
+    eng.set_model(vs, problem.rho, problem.qs)
+    syn = eng.forward(shots)
+    clock.add_engine(eng)
+    final = sum(l2_misfit(s, o) for s, o in zip(syn, obs))
+    hist.append({"iter": len(hist) + 1, "misfit": final, "gpu_s": clock.seconds, "final": True})
+    return hist, vs
+
+
+def training_pairs(torch, models, params, shots, log=None):
+    """(input bf16 [H*W][8] tensors, target float tensors) from the solver:
+    for each (true, start, rho) model, observed data on the true model, the
+    raw gradient with the energies Ws, Wr (EPRECOND energy-only mode) and the
+    pseudo-Hessian diagonal (dsh_hessian_diag) on the start model."""
+    from . import nn as dnn
+
+    qs = np.full((params["ny"], params["nx"]), 40.0, np.float32) if params["l"] else None
+    p = dict(params, max_shots=len(shots))
+    xs, ts = [], []
+    t0 = time.time()
+    with Engine(make_params(**dict(p, eprecond=10))) as eng:
+        for k, (seed, true, start, rho) in enumerate(models):
+            eng.set_model(true, rho, qs)
+            obs = eng.forward(shots)
+            eng.set_model(start, rho, qs)
+            out = eng.gradient(shots, obs, want_energy=True)
+            h_vs, _ = eng.hessian_diag(shots)
+            xs.append(dnn.pack_inputs(torch, out["g_vs"], out["Ws"].sum(axis=0), out["Wr"].sum(axis=0), start))
+            ts.append(torch.from_numpy(dnn.hessian_target(h_vs).ravel()).cuda())
+            if log and (k % 20 == 0):
+                log({"sample": k, "seed": seed, "elapsed_s": time.time() - t0})
+    return xs, ts
+
+
+def train(net, torch, xs, ts, ny, nx, epochs=10, batch=2, lr=1e-3, seed=0, log=None):
+    """Adam on the masked-free MSE of the log-Hessian target; returns per-epoch mean losses."""
+    rng = np.random.default_rng(seed)
+    n = len(xs)
+    hist = []
+    for ep in range(epochs):
+        order = rng.permutation(n)
+        tot = 0.0
+        nb = 0
+        for b0 in range(0, n - batch + 1, batch):
+            idx = order[b0:b0 + batch]
+            x = torch.cat([xs[i] for i in idx])
+            t = torch.cat([ts[i] for i in idx])
+            net.forward(x, batch, ny, nx)
+            loss, grad = net.loss_grad(t)
+            net.zero_grad()
+            net.backward(grad)
+            net.adam_step(lr=lr)
+            tot += float(loss.item())
+            nb += 1
+        hist.append(tot / max(nb, 1))
+        if log:
+            log({"epoch": ep, "loss": hist[-1]})
+    net.ctx.check()
+    return hist

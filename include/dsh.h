@@ -40,6 +40,8 @@ extern "C" {
 #define DSH_ERR_STATE (-5)     /* call out of order (e.g. no model set) */
 #define DSH_ERR_TIMEOUT (-6)   /* a bounded device wait expired */
 
+#define DSH_EPRECOND_ENERGY_ONLY 10   /* dsh_params.eprecond: raw gradient plus energy maps */
+
 /* Time-stepping parameters: the keys of the reference's .inp/.json files
  * that the hot path reads (src/read_par.c, src/globvar.h). */
 typedef struct dsh_params {
@@ -56,7 +58,9 @@ typedef struct dsh_params {
     int l;                    /* L: relaxation mechanisms (0 = elastic, <= 4) */
     float fl[8];              /* FL[1..L]: relaxation frequencies (Hz) */
     int quellart;             /* QUELLART: source wavelet (1 Ricker, 2, 4, 5, 6); 3 = caller supplies signals */
-    int eprecond;             /* EPRECOND: 0 or 1 (energy preconditioning) */
+    int eprecond;             /* EPRECOND: 0, 1 or 3 (energy preconditioning, src/eprecond1.c);
+                                 DSH_EPRECOND_ENERGY_ONLY: accumulate the energies Ws, Wr as
+                                 EPRECOND=1 does but leave the gradient unscaled */
     int max_shots;            /* shots advanced together in one launch (>= 1) */
     int compat_fd12;          /* 1: reuse hc[5] in the 6th y term of the FDORDER=12 velocity
                                  operator, as src/update_v_PML.c:469 does */

@@ -1,0 +1,46 @@
+/*
+ * dsh_fwi.h — host-side optimisation steps of the FWI loop, in plain C as in
+ * the reference (which keeps L-BFGS and the line search on the host):
+ *   dsh_lbfgs_direction   two-loop recursion (src/LBFGS.c:12-95), with the
+ *                         pairs of model and gradient differences stored as
+ *                         src/store_LBFGS_SH.c does (gradient x C_vs,
+ *                         model / C_vs)
+ *   dsh_opt_step          step length from three test misfits: the extremum
+ *                         of the parabola through them with the reference's
+ *                         guards (src/calc_opt_step.c:20-111)
+ *   dsh_line_search_next  one decision of the reference's bracketing loop
+ *                         (src/line_search.c:316-360)
+ */
+#ifndef DSH_FWI_H
+#define DSH_FWI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* r = H q for the stored pairs: S, Y hold `count` pairs [count][n], oldest
+ * first; gamma = (y.s)/(y.y) of the newest pair scales the initial inverse
+ * Hessian; rho_k = 1/(y_k.s_k), or 0 when y_k.s_k = 0.  count = 0 gives r = q.
+ * Dot products in double. */
+int dsh_lbfgs_direction(long long n, int count, const float *S, const float *Y, const float *q, float *r);
+
+/* epst[0..2], L2t[0..2]: test step lengths (epst[0] = 0) and their misfits */
+float dsh_opt_step(const float L2t[3], const float epst[3]);
+
+/* Line-search state of src/line_search.c: feed the misfits of the steps the
+ * previous call asked for; returns 1 while another test forward is needed
+ * (its relative step length in *eps_scale and its slot, 1 or 2, in *slot),
+ * 0 when done (*eps_scale = the chosen step) and -1 when no step reduced the
+ * misfit within stepmax tries (*eps_scale = 0). */
+typedef struct dsh_line_search {
+    float epst[3], L2t[3];
+    float eps_scale, scalefac;
+    int step1, step2, countstep, stepmax, slot;
+} dsh_line_search;
+void dsh_line_search_init(dsh_line_search *ls, float L2_now, float eps_scale, float scalefac, int stepmax);
+int dsh_line_search_next(dsh_line_search *ls, float L2_test, float *eps_scale, int *slot);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,70 @@
+"""FWI on the GPU engine: the energy-only EPRECOND mode (raw gradient plus
+the energies the plain preconditioner uses), the plain and the learned
+L-BFGS loops on a small problem, and the solver-generated training pairs."""
+import numpy as np
+import pytest
+
+import dsh
+from dsh import configs, fwi
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _small_problem(nshots=6, nt=500, seed=11):
+    cfg = configs.config5(seed=seed, nx=160, ny=80, nt=nt, nshots=nshots, ntr=60)
+    cfg["params"].update(fdorder=4, l=0, fl=())
+    cfg["qs"] = None
+    return cfg
+
+
+def test_energy_only_mode_is_raw_gradient_plus_energies():
+    cfg = _small_problem()
+    p = cfg["params"]
+    shots = cfg["shots"]
+    with dsh.Engine(dsh.make_params(**dict(p, eprecond=1, max_shots=3))) as e:
+        e.set_model(cfg["true"], cfg["rho"], None)
+        obs = e.forward(shots)
+        e.set_model(cfg["vs"], cfg["rho"], None)
+        pre = e.gradient(shots, obs, want_energy=True)
+    with dsh.Engine(dsh.make_params(**dict(p, eprecond=0, max_shots=3))) as e:
+        e.set_model(cfg["vs"], cfg["rho"], None)
+        raw = e.gradient(shots, obs)
+    with dsh.Engine(dsh.make_params(**dict(p, eprecond=dsh.EPRECOND_ENERGY_ONLY, max_shots=3))) as e:
+        e.set_model(cfg["vs"], cfg["rho"], None)
+        en = e.gradient(shots, obs, want_energy=True)
+    assert np.array_equal(en["g_vs"], raw["g_vs"]) and np.array_equal(en["g_rho"], raw["g_rho"])
+    assert np.array_equal(en["Ws"], pre["Ws"]) and np.array_equal(en["Wr"], pre["Wr"])
+    assert en["l2"] == raw["l2"]
+
+
+def test_plain_fwi_lowers_misfit():
+    prob = fwi.Problem(_small_problem(), test_shots=2)
+    try:
+        hist, vs = fwi.run(prob, 3, method="plain", eps_scale=0.02)
+    finally:
+        prob.close()
+    assert hist[-1]["final"] and hist[-1]["misfit"] < 0.9 * hist[0]["misfit"]
+    assert all(h["gpu_s"] > 0 for h in hist)
+    assert all(b["gpu_s"] >= a["gpu_s"] for a, b in zip(hist, hist[1:]))
+
+
+def test_training_pairs_and_learned_fwi():
+    from dsh import nn
+
+    cfg = _small_problem()
+    p = cfg["params"]
+    models = list(configs.training_models(count=4, first_seed=100, nx=p["nx"], ny=p["ny"]))
+    xs, ts = fwi.training_pairs(torch, models, p, cfg["shots"][:2])
+    assert len(xs) == 4 and xs[0].shape == (p["nx"] * p["ny"], nn.IN_CH)
+    assert all(bool(torch.isfinite(t).all()) for t in ts)
+    net = nn.UNet(torch, seed=1)
+    losses = fwi.train(net, torch, xs, ts, p["ny"], p["nx"], epochs=15, batch=2, lr=2e-3)
+    assert losses[-1] < losses[0]
+    prob = fwi.Problem(cfg, test_shots=2)
+    try:
+        hist, _ = fwi.run(prob, 3, method="learned", net=net, torch=torch, eps_scale=0.02)
+    finally:
+        prob.close()
+    assert hist[-1]["misfit"] < hist[0]["misfit"]
