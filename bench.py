@@ -14,6 +14,12 @@ Workloads (--config; seeded synthetic models, no dataset exists for this path):
                 forward modelling; NT per model = 1.5 x diagonal traveltime
                 (--nt-scale shortens all NTs alike).  Per-model throughput is
                 reported beside the aggregate.
+  c5            learned-preconditioner FWI: U-Net trained on solver-generated
+                (gradient, energies, vs) -> pseudo-Hessian pairs, then 20 L-BFGS
+                iterations of plain EPRECOND=1 FWI and of learned-preconditioned
+                FWI on NX=1200, NY=400, 32 shots, L=3; value = GPU-seconds the
+                learned method needs to reach the plain method's final misfit
+                (within 1%) / the plain method's GPU-seconds (lower is better).
   c3            batched gradient of 64 shots in one launch per half-step:
                 NX=1000, NY=300, FDORDER=8, L=2, NT=4000, 192 receivers, forward
                 wavefield checkpointed with recompute (full storage would need
@@ -58,7 +64,11 @@ def args_parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="dsh", choices=["dsh", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"])
+    ap.add_argument("--train-models", type=int, default=200, help="c5 only: training models")
+    ap.add_argument("--train-shots", type=int, default=8, help="c5 only: shots per training model")
+    ap.add_argument("--epochs", type=int, default=12, help="c5 only: training epochs")
+    ap.add_argument("--fwi-iters", type=int, default=20, help="c5 only: L-BFGS iterations")
     ap.add_argument("--nt-scale", type=float, default=1.0, help="c4 only: factor on every model's NT")
     ap.add_argument("--nt", type=int, default=None, help="time steps (default: the workload's NT)")
     ap.add_argument("--nx", type=int, default=2000, help="c2 only")
@@ -281,6 +291,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     if a.config == "c4":
         return bench_batch(a, rank, world, local)
+    if a.config == "c5":
+        return bench_learned(a, rank, world, local)
     cfg, wkind, label, fdo = workload(a.config, a.nt, a.nx, a.ny, a.shots)
     gradient = wkind == "gradient"
     p = cfg["params"]
@@ -620,6 +632,86 @@ def bench_batch(a, rank, world, local):
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def time_to_reach(hist, target):
+    """GPU-seconds after which the misfit is <= target: iteration k's model
+    update is done at hist[k]['gpu_s'] and its misfit is hist[k+1]['misfit']."""
+    if hist[0]["misfit"] <= target:
+        return 0.0
+    for k in range(len(hist) - 1):
+        if hist[k + 1]["misfit"] <= target:
+            return hist[k]["gpu_s"]
+    return None
+
+
+def bench_learned(a, rank, world, local):
+    """C5: training set from the solver, U-Net training, plain vs learned FWI."""
+    import numpy as np
+    import torch
+
+    import dsh
+    from dsh import configs, fwi
+    from dsh import nn as dnn
+
+    torch.cuda.set_device(local)
+    if rank != 0:
+        return
+    cfg = configs.config5(**({"nt": a.nt} if a.nt else {}))
+    p = dict(cfg["params"])
+    ny, nx = p["ny"], p["nx"]
+    ns = len(cfg["shots"])
+    pick = sorted({int(round(k)) for k in np.linspace(0, ns - 1, min(a.train_shots, ns))})
+    train_shots = [cfg["shots"][k] for k in pick]
+    log = lambda r: print(json.dumps(r), file=sys.stderr, flush=True)
+    t0 = time.time()
+    clock0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clock0[0].record()
+    models = configs.training_models(count=a.train_models, first_seed=100, nx=nx, ny=ny)
+    xs, ts = fwi.training_pairs(torch, models, p, train_shots, log=log)
+    clock0[1].record()
+    torch.cuda.synchronize()
+    gen_s = clock0[0].elapsed_time(clock0[1]) / 1e3
+    net = dnn.UNet(torch, seed=0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = fwi.train(net, torch, xs, ts, ny, nx, epochs=a.epochs, batch=2, lr=1e-3, log=log)
+    e1.record()
+    torch.cuda.synchronize()
+    train_s = e0.elapsed_time(e1) / 1e3
+    del xs, ts
+    prob = fwi.Problem(cfg, test_shots=4)
+    prob.observe()
+    w0 = time.time()
+    hp, _ = fwi.run(prob, a.fwi_iters, method="plain", log=log)
+    w1 = time.time()
+    target = hp[-1]["misfit"] * 1.01
+    hl, _ = fwi.run(prob, a.fwi_iters, method="learned", net=net, torch=torch, target_misfit=target, log=log)
+    w2 = time.time()
+    prob.close()
+    t_plain = hp[-1]["gpu_s"]
+    t_learned = time_to_reach(hl, target)
+    ratio = (t_learned / t_plain) if t_learned is not None else None
+    wall_ratio = ((w2 - w1) / (w1 - w0)) if t_learned is not None else None
+    curve = lambda h: [[round(r["gpu_s"], 3), r["misfit"]] for r in h]
+    line = {
+        "metric": "learned-vs-plain FWI: GPU-seconds to the plain method's final misfit (ratio)", "value": ratio,
+        "unit": "ratio", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 solver, bf16 network", "data": "synthetic",
+        "config": {"workload": f"learned-fwi-{nx}x{ny}-fd8-L3-{ns}shots-nt{p['nt']}", "fwi_iters": a.fwi_iters,
+                   "train_models": a.train_models, "train_shots": len(train_shots), "epochs": a.epochs,
+                   "unet": "4 levels, 32 base channels, bf16 weights/activations, fp32 accumulation",
+                   "target": "plain final misfit x 1.01"},
+        "plain": {"final_misfit": hp[-1]["misfit"], "gpu_s": t_plain, "iterations": len(hp) - 1, "curve": curve(hp)},
+        "learned": {"final_misfit": hl[-1]["misfit"], "gpu_s_to_target": t_learned, "gpu_s_total": hl[-1]["gpu_s"],
+                    "iterations": len(hl) - 1, "fallbacks": sum(1 for r in hl if r.get("fallback")),
+                    "curve": curve(hl)},
+        "training": {"data_gpu_s": gen_s, "train_gpu_s": train_s, "loss_first": losses[0], "loss_last": losses[-1]},
+        "e2e": {"value": wall_ratio, "unit": "ratio (host wall-clock of both FWI runs)", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": None},
+        "wall_s": time.time() - t0,
+    }
+    print(json.dumps(line), flush=True)
 
 
 if __name__ == "__main__":

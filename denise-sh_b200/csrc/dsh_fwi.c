@@ -100,7 +100,9 @@ void dsh_line_search_init(dsh_line_search *ls, float L2_now, float eps_scale, fl
 
 int dsh_line_search_next(dsh_line_search *ls, float L2_test, float *eps_scale, int *slot)
 {
-    /* the misfit of the step just tested goes into its slot (epst1/L2t[itest]) */
+    /* the misfit of the step just tested goes into its slot (epst1/L2t[itest]);
+     * a non-finite misfit counts as no reduction */
+    if (!isfinite(L2_test)) L2_test = INFINITY;
     ls->L2t[ls->slot] = L2_test;
     ls->epst[ls->slot] = ls->eps_scale;
     if (ls->step1 == 0 && ls->L2t[0] <= ls->L2t[1]) {          /* no reduction yet: shorter step */

@@ -32,11 +32,24 @@ class _RoundST(torch.autograd.Function):
         return g
 
 
+class _RoundGrad(torch.autograd.Function):
+    """Identity in the forward pass, BF16 rounding of the gradient in the
+    backward pass (the GPU path feeds BF16 output gradients to its GEMMs)."""
+
+    @staticmethod
+    def forward(ctx, x):
+        return x.clone()
+
+    @staticmethod
+    def backward(ctx, g):
+        return _bf(g)
+
+
 def _conv(x, w, b, cin, cout):
     """x [B][cin][H][W]; w [cout][9*cin] tap-major (k = tap*cin + c, tap = (dy+1)*3 + (dx+1))."""
     wk = w.view(cout, 3, 3, cin).permute(0, 3, 1, 2)           # [cout][cin][ky][kx]
-    y = F.conv2d(x, _RoundST.apply(wk), b, padding=1)
-    return _RoundST.apply(F.relu(y))
+    z = _RoundGrad.apply(F.conv2d(x, _RoundST.apply(wk), b, padding=1))
+    return _RoundST.apply(F.relu(z))
 
 
 def forward(state, x_nhwc, B, H, W):

@@ -76,3 +76,8 @@ def test_line_search_brackets_and_fits(emin):
 def test_line_search_gives_up_without_descent():
     eps, tests = fwi.line_search(lambda e: 1.0 + e, 1.0, eps_scale=0.01, scalefac=2.0, stepmax=4)
     assert eps == 0.0 and tests == 5
+
+
+def test_line_search_terminates_on_non_finite_misfits():
+    eps, tests = fwi.line_search(lambda e: float("nan"), 1.0, eps_scale=0.01, scalefac=2.0, stepmax=3)
+    assert eps == 0.0 and tests == 4

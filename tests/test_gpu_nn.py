@@ -109,11 +109,12 @@ def test_conv_layer_backward_matches_cpu(cin, cout):
     yg = y.float().cpu().view(B, H, W, cout).permute(0, 3, 1, 2)
     assert float((yg - yr).abs().max()) <= 1e-2 * float(yr.abs().max())
     mask = (yg > 0).float()
-    dz = (dy_in.cpu().view(B, H, W, cout).permute(0, 3, 1, 2) * mask).to(torch.bfloat16).float()
-    z.backward(dz)
+    dz32 = dy_in.cpu().view(B, H, W, cout).permute(0, 3, 1, 2) * mask
+    z.backward(dz32.to(torch.bfloat16).float())          # the GEMMs take the BF16-rounded dz
     gx = dx.cpu().view(B, H, W, cin).permute(0, 3, 1, 2)
     gw = layer.gwt.view(9 * cin, cout).t().contiguous().cpu().view(cout, 3, 3, cin).permute(0, 3, 1, 2)
-    for got, ref in ((gx, xc.grad), (gw, wc.grad), (layer.gb.cpu(), bc.grad)):
+    gb_ref = dz32.sum(dim=(0, 2, 3))                      # the bias gradient sums the FP32 dz
+    for got, ref in ((gx, xc.grad), (gw, wc.grad), (layer.gb.cpu(), gb_ref)):
         err = float((got - ref).abs().max())
         assert err <= 2e-5 * float(ref.abs().max()) + 1e-6, err
 
@@ -134,8 +135,9 @@ def test_unet_forward_backward_match_cpu_checker():
     ref_out, ref_g = unet_ref.gradients(net.state(), x.float().cpu().numpy(), B, H, W, dout.cpu().numpy())
     got = out.cpu().numpy()
     assert np.abs(got - ref_out).max() <= 2e-2 * np.abs(ref_out).max()
-    # BF16 rounding of every activation and of each layer's output gradient
-    # accumulates through the 17 layers: the bound is on direction and size
+    # the checker rounds activations and conv output gradients to BF16 where
+    # the GPU does; what remains is 1-ulp BF16 differences from the GEMMs' and
+    # conv2d's different FP32 summation orders, compounded through 17 layers
     g = net.grads()
     worst = []
     for k, r in ref_g.items():
