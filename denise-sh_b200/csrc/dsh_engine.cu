@@ -339,7 +339,7 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     ctx->m_vs = m; m += ctx->dstride;
     ctx->m_rho = m;
     if (cudaMalloc(&ctx->pml, 12 * (size_t)(2 * DSH_MAX_FW + 1) * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
-    if (cudaMalloc(&ctx->sums, 4 * (size_t)ctx->dstride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->sums, 6 * (size_t)ctx->dstride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     if (cudaMalloc(&ctx->d_out, 2 * (size_t)nx * ny * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     if (cudaMalloc(&ctx->d_nt, 2 * sizeof(int)) != cudaSuccess) return bail(DSH_ERR_OOM);
     ctx->d_status = ctx->d_nt + 1;
@@ -1077,8 +1077,12 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
     const dsh_params &p = ctx->p;
     const long long n = (long long)p.nx * p.ny;
     float *sum_u = ctx->sums, *sum_r = ctx->sums + ctx->dstride;
+    float *esum_s = ctx->sums + 4 * ctx->dstride, *esum_r = ctx->sums + 5 * ctx->dstride;
+    const bool energies = p.eprecond == 1 || p.eprecond == 3 || p.eprecond == DSH_EPRECOND_ENERGY_ONLY;
     CK(cudaMemsetAsync(ctx->sums, 0, 2 * (size_t)ctx->dstride * sizeof(float), ctx->st));
+    CK(cudaMemsetAsync(esum_s, 0, 2 * (size_t)ctx->dstride * sizeof(float), ctx->st));
     ctx->launches = 0;
+    ctx->shot_l2.clear();
     double l2_total = 0.0;
     float ms_f = 0, ms_a = 0;
     long long out = 0;
@@ -1137,11 +1141,17 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
         shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
                                                                ctx->slab + ctx->o_gu, ctx->slab + ctx->o_grho, sum_u, sum_r);
         ctx->launches++;
+        if (energies) {            /* shot sums of Ws and Wr (dsh_get_energy_sums) */
+            shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
+                                                                   ctx->slab + ctx->o_ws, ctx->slab + ctx->o_wr,
+                                                                   esum_s, esum_r);
+            ctx->launches++;
+        }
         CK(cudaGetLastError());
         std::vector<double> l2b(nb);
         CK(cudaMemcpyAsync(l2b.data(), ctx->d_l2, nb * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
         CK(cudaStreamSynchronize(ctx->st));
-        for (int s = 0; s < nb; s++) l2_total += l2b[s];
+        for (int s = 0; s < nb; s++) { l2_total += l2b[s]; ctx->shot_l2.push_back(l2b[s]); }
         float a = 0, b = 0;
         cudaEventElapsedTime(&a, e0, e1);
         cudaEventElapsedTime(&b, e1, e2);
@@ -1255,6 +1265,33 @@ extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
                          (size_t)p.nx * sizeof(float), p.ny, cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
     (void)n;
+    return DSH_OK;
+}
+
+extern "C" int dsh_get_shot_misfits(dsh_ctx *ctx, int nshots, double *out)
+{
+    if (!ctx || !out || nshots < 0) return DSH_ERR_PARAM;
+    if (nshots > (int)ctx->shot_l2.size()) return DSH_ERR_STATE;
+    for (int s = 0; s < nshots; s++) out[s] = ctx->shot_l2[s];
+    return DSH_OK;
+}
+
+extern "C" int dsh_get_energy_sums(dsh_ctx *ctx, float *ws_sum, float *wr_sum)
+{
+    if (!ctx || (!ws_sum && !wr_sum)) return DSH_ERR_PARAM;
+    const dsh_params &p = ctx->p;
+    if (p.eprecond != 1 && p.eprecond != 3 && p.eprecond != DSH_EPRECOND_ENERGY_ONLY) return DSH_ERR_STATE;
+    CK(cudaSetDevice(ctx->dev));
+    const long long n = (long long)p.nx * p.ny;
+    float *src[2] = {ctx->sums + 4 * ctx->dstride, ctx->sums + 5 * ctx->dstride};
+    float *dst[2] = {ws_sum, wr_sum};
+    for (int k = 0; k < 2; k++) {
+        if (!dst[k]) continue;
+        gather_dense_kernel<<<256, 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, src[k], ctx->d_out);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(dst[k], ctx->d_out, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+        CK(cudaStreamSynchronize(ctx->st));
+    }
     return DSH_OK;
 }
 

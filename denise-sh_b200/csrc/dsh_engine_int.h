@@ -55,6 +55,7 @@ struct dsh_ctx {
     double *d_part = nullptr, *d_l2 = nullptr;
     unsigned *d_wemax = nullptr;
     std::vector<int> ntr_b;
+    std::vector<double> shot_l2;          /* per-shot L2 misfits of the last gradient */
     std::map<long long, cudaGraphExec_t> graphs;
     cudaEvent_t ev[4];
     dsh_stats stats;

@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
         L.dsh_profile_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_residual_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]
+        L.dsh_get_shot_misfits.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
+        L.dsh_get_energy_sums.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_batch_create.restype = C.c_void_p
         L.dsh_batch_create.argtypes = [C.c_void_p, C.c_int, C.c_int, C.POINTER(C.c_int)]
         L.dsh_batch_destroy.argtypes = [C.c_void_p]
@@ -276,6 +278,17 @@ class Engine:
         out = np.zeros(3, np.float32)
         _check(lib().dsh_profile_step(self.h, self.PASSES[pass_name], nsteps, out.ctypes.data), "dsh_profile_step")
         return {"v_step": float(out[0]), "inject_sample": float(out[1]), "s_step": float(out[2])}
+
+    def shot_misfits(self, nshots):
+        out = np.zeros(nshots, np.float64)
+        _check(lib().dsh_get_shot_misfits(self.h, nshots, out.ctypes.data), "dsh_get_shot_misfits")
+        return out
+
+    def energy_sums(self):
+        ny, nx = self.shape
+        ws, wr = np.zeros((ny, nx), np.float32), np.zeros((ny, nx), np.float32)
+        _check(lib().dsh_get_energy_sums(self.h, ws.ctypes.data, wr.ctypes.data), "dsh_get_energy_sums")
+        return ws, wr
 
     def stats(self) -> dict:
         s = Stats()

@@ -166,15 +166,15 @@ def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, sc
     def gradient(kind):
         eng = problem.engine(1 if kind == "plain" else 10)
         eng.set_model(vs, problem.rho, problem.qs)
-        out = eng.gradient(shots, obs, want_seis=True, want_energy=(kind == "learned"))
+        out = eng.gradient(shots, obs)
         clock.add_engine(eng)
         if kind == "plain":
             q = out["g_vs"]
         else:
-            ws, wr = out["Ws"].sum(axis=0), out["Wr"].sum(axis=0)
+            ws, wr = eng.energy_sums()            # summed over shots on the device
             h = learned_preconditioner(net, torch, out["g_vs"], ws, wr, vs, clock)
             q = out["g_vs"] / (h + 0.005 * float(h.max()))
-        l2_test = sum(l2_misfit(out["seis"][k], obs[k]) for k in test)
+        l2_test = float(eng.shot_misfits(len(shots))[test].sum())
         return q.astype(np.float32), out["l2"], l2_test
 
     def step_model(d, eps):
@@ -254,9 +254,10 @@ def training_pairs(torch, models, params, shots, log=None):
             eng.set_model(true, rho, qs)
             obs = eng.forward(shots)
             eng.set_model(start, rho, qs)
-            out = eng.gradient(shots, obs, want_energy=True)
+            out = eng.gradient(shots, obs)
+            ws, wr = eng.energy_sums()
             h_vs, _ = eng.hessian_diag(shots)
-            xs.append(dnn.pack_inputs(torch, out["g_vs"], out["Ws"].sum(axis=0), out["Wr"].sum(axis=0), start))
+            xs.append(dnn.pack_inputs(torch, out["g_vs"], ws, wr, start))
             ts.append(torch.from_numpy(dnn.hessian_target(h_vs).ravel()).cuda())
             if log and (k % 20 == 0):
                 log({"sample": k, "seed": seed, "elapsed_s": time.time() - t0})

@@ -209,6 +209,15 @@ typedef struct dsh_batch_stats {
  * the last run until model k's last step completed */
 int dsh_batch_get_stats(dsh_batch *b, double *model_ms, dsh_batch_stats *out);
 
+/* Per-shot L2 misfits of the last dsh_gradient / dsh_gradient_device call
+ * (the terms of its l2 total, in shot order; double accumulation). */
+int dsh_get_shot_misfits(dsh_ctx *ctx, int nshots, double *out);
+
+/* Shot sums of the energies Ws and Wr of the last gradient call (host dense
+ * [ny][nx]; either pointer may be NULL).  Needs EPRECOND 1, 3 or
+ * DSH_EPRECOND_ENERGY_ONLY; summed on the device, so no per-shot copies. */
+int dsh_get_energy_sums(dsh_ctx *ctx, float *ws_sum, float *wr_sum);
+
 /* Statistics of the last dsh_forward / dsh_gradient call. */
 typedef struct dsh_stats {
     double ms_forward, ms_adjoint, ms_total;   /* device time (CUDA events) */

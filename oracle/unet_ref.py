@@ -16,8 +16,11 @@ import torch.nn.functional as F
 BASE = 32
 
 
+_ROUND = True
+
+
 def _bf(t):
-    return t.to(torch.bfloat16).to(torch.float32)
+    return t.to(torch.bfloat16).to(torch.float32) if _ROUND else t
 
 
 class _RoundST(torch.autograd.Function):
@@ -52,9 +55,12 @@ def _conv(x, w, b, cin, cout):
     return _RoundST.apply(F.relu(z))
 
 
-def forward(state, x_nhwc, B, H, W):
+def forward(state, x_nhwc, B, H, W, rounding=True):
     """state: dict of numpy FP32 parameters (UNet.state()); x_nhwc [B*H*W][8]
-    (already BF16-representable).  Returns (prediction [B*H*W], parameter tensors)."""
+    (already BF16-representable).  Returns (prediction [B*H*W], parameter tensors).
+    rounding=False gives the same network in plain FP32 (no BF16 rounding)."""
+    global _ROUND
+    _ROUND = rounding
     params = {k: torch.tensor(v, dtype=torch.float32, requires_grad=True) for k, v in state.items()}
     c = [BASE, 2 * BASE, 4 * BASE, 8 * BASE]
     x = torch.tensor(np.asarray(x_nhwc, np.float32)).view(B, H, W, -1).permute(0, 3, 1, 2)
@@ -85,8 +91,8 @@ def forward(state, x_nhwc, B, H, W):
     return out.reshape(-1), params
 
 
-def gradients(state, x_nhwc, B, H, W, dout):
+def gradients(state, x_nhwc, B, H, W, dout, rounding=True):
     """Parameter gradients of sum(pred * dout) (weights [cout][9cin])."""
-    out, params = forward(state, x_nhwc, B, H, W)
+    out, params = forward(state, x_nhwc, B, H, W, rounding)
     (out * torch.tensor(np.asarray(dout, np.float32))).sum().backward()
     return out.detach().numpy(), {k: v.grad.numpy() for k, v in params.items()}

@@ -34,9 +34,17 @@ def test_energy_only_mode_is_raw_gradient_plus_energies():
     with dsh.Engine(dsh.make_params(**dict(p, eprecond=dsh.EPRECOND_ENERGY_ONLY, max_shots=3))) as e:
         e.set_model(cfg["vs"], cfg["rho"], None)
         en = e.gradient(shots, obs, want_energy=True)
+        ws_sum, wr_sum = e.energy_sums()
+        per_shot = e.shot_misfits(len(shots))
     assert np.array_equal(en["g_vs"], raw["g_vs"]) and np.array_equal(en["g_rho"], raw["g_rho"])
     assert np.array_equal(en["Ws"], pre["Ws"]) and np.array_equal(en["Wr"], pre["Wr"])
     assert en["l2"] == raw["l2"]
+    # device shot sums of the energies (two batches of 3 slots) and per-shot misfits
+    ref_s, ref_r = np.zeros_like(ws_sum), np.zeros_like(wr_sum)
+    for k in range(len(shots)):
+        ref_s, ref_r = ref_s + en["Ws"][k], ref_r + en["Wr"][k]
+    assert np.allclose(ws_sum, ref_s, rtol=1e-6) and np.allclose(wr_sum, ref_r, rtol=1e-6)
+    assert per_shot.sum() == pytest.approx(en["l2"], rel=1e-12) and (per_shot > 0).all()
 
 
 def test_plain_fwi_lowers_misfit():

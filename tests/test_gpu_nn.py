@@ -135,21 +135,26 @@ def test_unet_forward_backward_match_cpu_checker():
     ref_out, ref_g = unet_ref.gradients(net.state(), x.float().cpu().numpy(), B, H, W, dout.cpu().numpy())
     got = out.cpu().numpy()
     assert np.abs(got - ref_out).max() <= 2e-2 * np.abs(ref_out).max()
-    # the checker rounds activations and conv output gradients to BF16 where
-    # the GPU does; what remains is 1-ulp BF16 differences from the GEMMs' and
-    # conv2d's different FP32 summation orders, compounded through 17 layers
+    # The checker rounds activations and conv output gradients to BF16 where
+    # the GPU does; what remains are 1-ulp BF16 differences from different FP32
+    # summation orders, compounded through 17 layers.  The bound is calibrated
+    # on the checker itself: the GPU gradient must be as close to the BF16
+    # checker as the BF16 checker is to the same network in plain FP32 (a
+    # wiring error - concatenation order, pooling routes - is far outside it).
+    _, ref32 = unet_ref.gradients(net.state(), x.float().cpu().numpy(), B, H, W, dout.cpu().numpy(), rounding=False)
     g = net.grads()
-    worst = []
+    bad = []
     for k, r in ref_g.items():
         a = g[k].ravel().astype(np.float64)
         b = r.ravel().astype(np.float64)
+        c32 = ref32[k].ravel().astype(np.float64)
         if np.abs(b).max() == 0:
             continue
-        cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
         rel = np.linalg.norm(a - b) / np.linalg.norm(b)
-        worst.append((cos, rel, k))
-    print(sorted(worst)[:6])
-    assert all(c > 0.99 and r < 0.15 for c, r, _ in worst), sorted(worst)[:6]
+        noise = np.linalg.norm(b - c32) / np.linalg.norm(b)
+        if rel > max(0.05, 1.5 * noise):
+            bad.append((k, rel, noise))
+    assert not bad, bad
 
 
 def test_unet_training_lowers_loss():
