@@ -114,6 +114,14 @@ def kernel_bytes(l, store=True):
     return v, s
 
 
+def fused_bytes(l, store=True):
+    """Per-point bytes of one fused step (each array once): vy, sxy, syz and
+    the 2L memory variables read and written, model parameters read (1/rho,
+    uip, ujp | 1/rho, muip, mujp, tausipjp, taus), and with storage the stored
+    acceleration and strains written and Ws read and written."""
+    return 8 * (3 + 2 * l) + (12 if l == 0 else 20) + (20 if store else 0)
+
+
 def workload(name, nt=None, nx=2000, ny=800, shots=64):
     """(cfg, kind, label, fdorder) of a named workload."""
     from dsh import configs
@@ -425,14 +433,26 @@ def main():
         bf -= 12 + 8                       # no storage, no energy in plain forward modelling
     step_bytes = n * nt * nsh * (bf + (ba if gradient else 0)) * a.steps
     step_gbs = step_bytes / ((ms_f + ms_a) / 1e3) / 1e9
-    prof = eng.profile_step("forward_store" if gradient else "forward", a.profile_steps)
-    kv, ks = kernel_bytes(L, store=gradient)
-    s_gbs = ks * n * nsh / (prof["s_step"] / 1e3) / 1e9
+    pname = "forward_store" if gradient else "forward"
+    fused_ms = eng.profile_fused(pname, a.profile_steps)
+    prof = eng.profile_step(pname, a.profile_steps)
+    if fused_ms is not None:        # one fused kernel per step: it is the dominant (only) step kernel
+        ks = fused_bytes(L, store=gradient)
+        kname = f"fs_step<{fdo},{L}> (fused velocity+stress, forward pass{' with storage' if gradient else ''})"
+        kms = fused_ms
+        prof["fs_step"] = fused_ms
+    else:
+        kv, ks = kernel_bytes(L, store=gradient)
+        kname = f"s_step<{fdo},{L}> (forward pass{' with storage' if gradient else ''})"
+        kms = prof["s_step"]
+    s_gbs = ks * n * nsh / (kms / 1e3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath) and a.config == "c2":
         try:
-            traffic = json.load(open(tpath)).get("s_step_forward_store_bytes_per_launch")
+            key = "fs_step_forward_store_bytes_per_launch" if fused_ms is not None else \
+                "s_step_forward_store_bytes_per_launch"
+            traffic = json.load(open(tpath)).get(key)
         except Exception:
             traffic = None
 
@@ -462,9 +482,8 @@ def main():
                        "shots_per_gpu": nsh, "receivers": shots[0].ntr, "parallelism": f"shots{world}",
                        "checkpoint_interval": ckpt, "storage_gb": storage / 1e9, "l2": l2note},
             "roofline": {"bound": "hbm", "achieved": s_gbs, "peak": hbm, "unit": "GB/s", "frac": s_gbs / hbm,
-                         "traffic": traffic,
-                         "kernel": f"s_step<{fdo},{L}> (forward pass{' with storage' if gradient else ''})",
-                         "bytes_per_point": ks, "ms_per_launch": prof["s_step"], "peak_source": peak_kind},
+                         "traffic": traffic, "kernel": kname, "bytes_per_point": ks, "ms_per_launch": kms,
+                         "peak_source": peak_kind},
             "step_roofline": {"achieved": step_gbs, "frac": step_gbs / hbm, "bytes_per_point_fwd": bf,
                               "bytes_per_point_adj": ba if gradient else None,
                               "ms_forward_pass": ms_f / a.steps,

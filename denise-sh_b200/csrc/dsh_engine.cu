@@ -16,6 +16,8 @@
  */
 #include "dsh.h"
 #include "dsh_engine_int.h"
+#include "dsh_fs.h"
+#include "dsh_fused.cuh"
 #include "dsh_setup.h"
 
 #include <algorithm>
@@ -315,6 +317,16 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     ctx->o_psxx = o; o += round_up((long long)ny * 2 * fw + 4, 32);
     ctx->o_pvyy = o; o += round_up((long long)2 * fw * ctx->pitch + 4, 32);
     ctx->o_psyy = o; o += round_up((long long)2 * fw * ctx->pitch + 4, 32);
+    /* second buffers of the fused step (vy, sxy, syz, velocity CPML memory);
+       inside the state region so checkpoints hold both */
+    ctx->fused_ok = p->fdorder <= 8;
+    if (ctx->fused_ok) {
+        ctx->o_vy_b = o; o += ctx->fstride;
+        ctx->o_sxy_b = o; o += ctx->fstride;
+        ctx->o_syz_b = o; o += ctx->fstride;
+        ctx->o_pvxx_b = o; o += round_up((long long)ny * 2 * fw + 4, 32);
+        ctx->o_pvyy_b = o; o += round_up((long long)2 * fw * ctx->pitch + 4, 32);
+    }
     ctx->o_state_end = o;
     ctx->o_ws = o; o += ctx->dstride;
     ctx->o_wr = o; o += ctx->dstride;
@@ -556,26 +568,58 @@ int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_h
     }
     rec_off[S] = (int)rec_pt.size();
 
-    /* one int buffer: fixed tables, then 7 variable sections of capacity cp */
-    const long long F = 3LL * (S + 1) + 3LL * S * (T + 1);
+    /* fused step: per slot and 128 x 16 tile, the groups whose point lies in
+     * the tile's velocity region (the tile grown by H-1 points left / above
+     * and H right / below) */
+    const int H = p.fdorder / 2;
+    const int fgx = (p.nx + FTX - 1) / FTX, fgy = (p.ny + FTY - 1) / FTY, FT = fgx * fgy;
+    std::vector<int> fvoff(2 * S * (FT + 1)), fvids;
+    for (int pass = 0; pass < 2; pass++) {
+        const std::vector<int> &goff_s = pass ? agrp_off : fgrp_off;
+        for (int s = 0; s < S; s++) {
+            std::vector<std::pair<int, int>> ent;     /* (tile, group) */
+            for (int g = goff_s[s]; g < goff_s[s + 1]; g++) {
+                const int i = gpk[g] & 0xffff, j = gpk[g] >> 16;
+                for (int ty = std::max(0, (j - 1) / FTY - 1); ty <= std::min(fgy - 1, (j - 1) / FTY + 1); ty++)
+                    for (int tx = std::max(0, (i - 1) / FTX - 1); tx <= std::min(fgx - 1, (i - 1) / FTX + 1); tx++)
+                        if (i >= tx * FTX + 2 - H && i <= tx * FTX + FTX + H && j >= ty * FTY + 2 - H &&
+                            j <= ty * FTY + FTY + H)
+                            ent.push_back({ty * fgx + tx, g});
+            }
+            std::stable_sort(ent.begin(), ent.end(), [](auto &x, auto &y) { return x.first < y.first; });
+            int *tab = &fvoff[(size_t)(pass * S + s) * (FT + 1)];
+            size_t k = 0;
+            for (int t = 0; t <= FT; t++) {
+                while (k < ent.size() && ent[k].first < t) k++;
+                tab[t] = (int)fvids.size() + (int)k;
+            }
+            for (auto &e : ent) fvids.push_back(e.second);
+        }
+    }
+
+    /* one int buffer: fixed tables, then 8 variable sections of capacity cp */
+    const long long F = 3LL * (S + 1) + 3LL * S * (T + 1) + 2LL * S * (FT + 1);
     const long long maxlen = (long long)std::max({grp_pt.size(), grp_beg.size(), src_id.size(), rec_pt.size(),
-                                                  gpk.size(), rpk.size(), rid.size()}) + 1;
+                                                  gpk.size(), rpk.size(), rid.size(), fvids.size()}) + 1;
     bool realloc = false;
-    if (F + 7 * maxlen > ctx->geo_cap) {
+    if (F + 8 * maxlen > ctx->geo_cap) {
         cudaFree(ctx->d_geo);
         ctx->d_geo = nullptr;
-        const long long cp_old = ctx->geo_cap > F ? (ctx->geo_cap - F) / 7 : 0;
-        ctx->geo_cap = F + 7 * std::max(maxlen, 2 * cp_old);
+        const long long cp_old = ctx->geo_cap > F ? (ctx->geo_cap - F) / 8 : 0;
+        ctx->geo_cap = F + 8 * std::max(maxlen, 2 * cp_old);
         CK(cudaMalloc(&ctx->d_geo, (size_t)ctx->geo_cap * sizeof(int)));
         realloc = true;
     }
-    const long long cp = (ctx->geo_cap - F) / 7;
+    const long long cp = (ctx->geo_cap - F) / 8;
     int *G = ctx->d_geo;
     ctx->d_fgrp_off = G; ctx->d_agrp_off = G + (S + 1); ctx->d_rec_off = G + 2 * (S + 1);
     ctx->d_ftile = G + 3 * (S + 1); ctx->d_atile = ctx->d_ftile + S * (T + 1); ctx->d_rtile = ctx->d_atile + S * (T + 1);
     ctx->d_grp_pt = G + F; ctx->d_grp_beg = ctx->d_grp_pt + cp; ctx->d_src_id = ctx->d_grp_beg + cp;
     ctx->d_rec_pt = ctx->d_src_id + cp; ctx->d_gpk = ctx->d_rec_pt + cp; ctx->d_rpk = ctx->d_gpk + cp;
     ctx->d_rid = ctx->d_rpk + cp;
+    ctx->d_fvoff = ctx->d_rtile + S * (T + 1); ctx->d_avoff = ctx->d_fvoff + S * (FT + 1);
+    ctx->d_fvids = ctx->d_rid + cp;
+    ctx->fvg_ntiles = FT;
     ctx->ntiles = T;
     ctx->fused_inject = fused && getenv("DSH_NO_FUSED_INJECT") == nullptr;
     std::vector<int> host((size_t)ctx->geo_cap, 0);
@@ -584,6 +628,7 @@ int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_h
     put(3 * (S + 1), ftile); put(3 * (S + 1) + S * (T + 1), atile); put(3 * (S + 1) + 2 * S * (T + 1), rtile);
     put(F, grp_pt); put(F + cp, grp_beg); put(F + 2 * cp, src_id); put(F + 3 * cp, rec_pt);
     put(F + 4 * cp, gpk); put(F + 5 * cp, rpk); put(F + 6 * cp, rid);
+    put(3 * (S + 1) + 3 * S * (T + 1), fvoff); put(F + 7 * cp, fvids);
     CK(cudaMemcpyAsync(ctx->d_geo, host.data(), (size_t)ctx->geo_cap * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
 
@@ -678,6 +723,13 @@ StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.psi_vxx = sl + ctx->o_pvxx; a.psi_sxx = sl + ctx->o_psxx;
     a.psi_vyy_v = sl + ctx->o_pvyy; a.psi_syy = sl + ctx->o_psyy;
     a.gu = sl + ctx->o_gu; a.grho = sl + ctx->o_grho; a.hu = sl + ctx->o_hu; a.hrho = sl + ctx->o_hrho;
+    if (ctx->fused_ok) {
+        a.vy_b = sl + ctx->o_vy_b; a.sxy_b = sl + ctx->o_sxy_b; a.syz_b = sl + ctx->o_syz_b;
+        a.psi_vxx_b = sl + ctx->o_pvxx_b; a.psi_vyy_v_b = sl + ctx->o_pvyy_b;
+        a.fvg_off = pass == P_ADJ ? ctx->d_avoff : ctx->d_fvoff;
+        a.fvg_ids = ctx->d_fvids;
+        a.fvg_ntiles = ctx->fvg_ntiles;
+    }
     a.brho = ctx->m_brho; a.uip = ctx->m_uip; a.ujp = ctx->m_ujp;
     a.muip = ctx->m_muip; a.mujp = ctx->m_mujp; a.tausipjp = ctx->m_tip; a.taus = ctx->m_taus;
     for (int l = 0; l < 4; l++) a.eta[l] = ctx->eta[l];
@@ -757,8 +809,52 @@ InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
 }
 }  // namespace dsh::eng
 
+/* The fused step (one kernel per time step, dsh_fused.cuh) serves every pass
+ * but the Hessian one when FDORDER <= 8 and injection/sampling are fused;
+ * DSH_FUSED=0 selects the velocity + stress kernel pair instead. */
+static bool use_fused(dsh_ctx *ctx, Pass pass)
+{
+    static const bool on = []() { const char *e = getenv("DSH_FUSED"); return e && atoi(e) != 0; }();
+    return on && ctx->fused_ok && ctx->fused_inject && pass != P_FWD_HESS;
+}
+
+static int fused_mode(Pass pass)
+{
+    return pass == P_ADJ ? FM_ADJ : (pass == P_FWD_STORE || pass == P_RECOMP) ? FM_STORE : FM_FWD;
+}
+
+static int launch_fused_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chunk, long long *nlaunch)
+{
+    const dsh_params &p = ctx->p;
+    KFn fk = fs_kernel(p.fdorder, p.l, fused_mode(pass), dh_pow2(p.dh));
+    if (!fk) return DSH_ERR_PARAM;
+    StepArgs sa = step_args(ctx, pass);
+    dim3 grid((unsigned)((p.nx + FTX - 1) / FTX), (unsigned)((p.ny + FTY - 1) / FTY), (unsigned)nb);
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(256, 1, 1);
+    cfg.stream = ctx->st;
+    static const bool use_pdl = getenv("DSH_NO_PDL") == nullptr;
+    for (int k = 0; k < nsteps_in_chunk; k++) {
+        int off = k;
+        void *args[2] = {&sa, &off};
+        cfg.attrs = (use_pdl && k > 0) ? &attr : nullptr;
+        cfg.numAttrs = (use_pdl && k > 0) ? 1 : 0;
+        CK(cudaLaunchKernelExC(&cfg, (const void *)fk, args));
+        *nlaunch += 1;
+    }
+    advance_step<<<1, 1, 0, ctx->st>>>(ctx->d_nt, nsteps_in_chunk);
+    *nlaunch += 1;
+    CK(cudaGetLastError());
+    return DSH_OK;
+}
+
 static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chunk, long long *nlaunch)
 {
+    if (use_fused(ctx, pass)) return launch_fused_chunk(ctx, pass, nb, nsteps_in_chunk, nlaunch);
     const dsh_params &p = ctx->p;
     int vflags = 0, sflags = 0;
     switch (pass) {
@@ -811,8 +907,9 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
 
 static int get_graph(dsh_ctx *ctx, Pass pass, int nb, int K, cudaGraphExec_t *out)
 {
-    const long long key = ((long long)pass << 48) | ((long long)ctx->fused_inject << 47) | ((long long)K << 32) |
-                          ((long long)nb << 16) | (long long)(ctx->geo_version & 0xffff);
+    const long long key = ((long long)pass << 48) | ((long long)ctx->fused_inject << 47) |
+                          ((long long)use_fused(ctx, pass) << 46) | ((long long)K << 32) | ((long long)nb << 16) |
+                          (long long)(ctx->geo_version & 0xffff);
     auto it = ctx->graphs.find(key);
     if (it != ctx->graphs.end()) { *out = it->second; return DSH_OK; }
     cudaGraph_t g;
@@ -837,7 +934,10 @@ static int run_steps(dsh_ctx *ctx, Pass pass, int nb, int n0, int count)
     if (count <= 0) return DSH_OK;
     const int K = std::min(ctx->chunk, count);
     const int nfull = count / K, rem = count % K;
-    const long long per_step = ctx->fused_inject ? 2 : 3;
+    const bool fused = use_fused(ctx, pass);
+    const long long per_step = fused ? 1 : ctx->fused_inject ? 2 : 3;
+    /* the fused step leaves the state of step n in buffer n & 1 */
+    if (pass != P_RECOMP) ctx->state_b = fused ? ((n0 + count - 1) & 1) : 0;
     set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, n0);
     ctx->launches += 1;
     static const bool use_graphs = getenv("DSH_NO_GRAPHS") == nullptr;
@@ -1243,9 +1343,9 @@ extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
     const float *src;
     int pitch = ctx->pitch;
     switch (which) {
-    case 0: src = base + ctx->o_vy + (long long)ctx->hy * pitch; break;
-    case 1: src = base + ctx->o_sxy + (long long)ctx->hy * pitch; break;
-    case 2: src = base + ctx->o_syz + (long long)ctx->hy * pitch; break;
+    case 0: src = base + (ctx->state_b ? ctx->o_vy_b : ctx->o_vy) + (long long)ctx->hy * pitch; break;
+    case 1: src = base + (ctx->state_b ? ctx->o_sxy_b : ctx->o_sxy) + (long long)ctx->hy * pitch; break;
+    case 2: src = base + (ctx->state_b ? ctx->o_syz_b : ctx->o_syz) + (long long)ctx->hy * pitch; break;
     case 12: src = base + ctx->o_ws; break;
     case 13: src = base + ctx->o_wr; break;
     case 14: src = base + ctx->o_we; break;
@@ -1266,6 +1366,41 @@ extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
     CK(cudaStreamSynchronize(ctx->st));
     (void)n;
     return DSH_OK;
+}
+
+extern "C" int dsh_profile_fused(dsh_ctx *ctx, int pass, int nsteps, float *out_ms)
+{
+    if (!ctx || !out_ms || pass < 0 || pass > 3 || pass == P_FWD_HESS || nsteps < 1 || nsteps > ctx->p.nt)
+        return DSH_ERR_PARAM;
+    if (ctx->ckpt_c && (pass == P_FWD_STORE || pass == P_ADJ) && nsteps > ctx->ckpt_c) nsteps = ctx->ckpt_c;
+    if (!ctx->model_set || ctx->ntr_b.empty() || ((pass == P_FWD_STORE || pass == P_ADJ) && !ctx->fwd)) return DSH_ERR_STATE;
+    if (!use_fused(ctx, (Pass)pass)) return DSH_ERR_STATE;
+    CK(cudaSetDevice(ctx->dev));
+    const dsh_params &p = ctx->p;
+    const int nb = (int)ctx->ntr_b.size();
+    KFn fk = fs_kernel(p.fdorder, p.l, fused_mode((Pass)pass), dh_pow2(p.dh));
+    if (!fk) return DSH_ERR_PARAM;
+    StepArgs sa = step_args(ctx, (Pass)pass);
+    dim3 grid((unsigned)((p.nx + FTX - 1) / FTX), (unsigned)((p.ny + FTY - 1) / FTY), (unsigned)nb);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
+    CK(cudaEventRecord(e0, ctx->st));
+    for (int k = 0; k < nsteps; k++) {
+        int off = k;
+        void *args[2] = {&sa, &off};
+        CK(cudaLaunchKernel((const void *)fk, grid, dim3(256), args, 0, ctx->st));
+    }
+    CK(cudaEventRecord(e1, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    *out_ms = ms / nsteps;
+    cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->st);
+    return check_status(ctx);
 }
 
 extern "C" int dsh_get_shot_misfits(dsh_ctx *ctx, int nshots, double *out)

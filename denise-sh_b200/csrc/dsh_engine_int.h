@@ -24,6 +24,9 @@ struct dsh_ctx {
     long long fstride = 0, dstride = 0, slot_stride = 0;
     long long o_vy, o_sxy, o_syz, o_r, o_q, o_pvxx, o_psxx, o_pvyy, o_psyy, o_state_end;
     long long o_ws, o_wr, o_we, o_gu, o_grho, o_hu, o_hrho;
+    long long o_vy_b = 0, o_sxy_b = 0, o_syz_b = 0, o_pvxx_b = 0, o_pvyy_b = 0;   /* fused step's second buffers */
+    int fused_ok = 0;                     /* FDORDER <= 8: the fused step kernel can run this context */
+    int state_b = 0;                      /* the slab's current state is in the second buffers */
     float *slab = nullptr;
     float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho */
     float *m_brho, *m_uip, *m_ujp, *m_muip, *m_mujp, *m_tip, *m_taus, *m_vs, *m_rho;
@@ -46,6 +49,8 @@ struct dsh_ctx {
     int *d_fgrp_off, *d_agrp_off, *d_grp_pt, *d_grp_beg, *d_src_id, *d_rec_off, *d_rec_pt;
     int *d_ftile, *d_atile, *d_rtile, *d_gpk, *d_rpk, *d_rid;
     int ntiles = 0, fused_inject = 0;
+    int *d_fvoff = nullptr, *d_avoff = nullptr, *d_fvids = nullptr;   /* fused-tile injection lists */
+    int fvg_ntiles = 0;
     long long *d_offs = nullptr;          /* sig_off[S], seis_off[S], obs_off[S], out_off[S] */
     float *d_sig = nullptr, *d_seis = nullptr, *d_res = nullptr, *d_obs = nullptr, *d_tmp = nullptr;
     float *d_out = nullptr;               /* 2 x [ny][nx] dense outputs */

@@ -100,6 +100,12 @@ struct StepArgs {
     float *out_acc, *out_uy, *out_uyx;
     int *status;                 /* device error word (non-finite detection) */
     TileLists tl;
+    /* fused step (dsh_fused.cuh): second buffers of the fields neighbouring
+       tiles read during a step, and the injection groups of each 128 x 16
+       tile's velocity region: fvg_ids[fvg_off[slot*(fvg_ntiles+1) + tile] ..] */
+    float *vy_b, *sxy_b, *syz_b, *psi_vxx_b, *psi_vyy_v_b;
+    const int *fvg_off, *fvg_ids;
+    int fvg_ntiles;
 };
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }

@@ -88,6 +88,7 @@ def lib() -> C.CDLL:
         L.dsh_profile_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_residual_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]
+        L.dsh_profile_fused.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_get_shot_misfits.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.dsh_get_energy_sums.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_batch_create.restype = C.c_void_p
@@ -278,6 +279,15 @@ class Engine:
         out = np.zeros(3, np.float32)
         _check(lib().dsh_profile_step(self.h, self.PASSES[pass_name], nsteps, out.ctypes.data), "dsh_profile_step")
         return {"v_step": float(out[0]), "inject_sample": float(out[1]), "s_step": float(out[2])}
+
+    def profile_fused(self, pass_name: str, nsteps: int):
+        """Mean device ms per launch of the fused step kernel, or None when it does not serve this pass."""
+        out = np.zeros(1, np.float32)
+        rc = lib().dsh_profile_fused(self.h, self.PASSES[pass_name], nsteps, out.ctypes.data)
+        if rc == -5:
+            return None
+        _check(rc, "dsh_profile_fused")
+        return float(out[0])
 
     def shot_misfits(self, nshots):
         out = np.zeros(nshots, np.float64)

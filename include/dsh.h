@@ -149,6 +149,12 @@ int dsh_set_stream(dsh_ctx *ctx, void *stream);
  * wavefield state, which is rebuilt by the next call. */
 int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
 
+/* The same for the fused step kernel (one launch per time step; used when
+ * FDORDER <= 8, injection/sampling positions lie inside the grid and
+ * DSH_FUSED is set): mean ms per launch in *out_ms; DSH_ERR_STATE when the
+ * fused kernel does not serve this context and pass. */
+int dsh_profile_fused(dsh_ctx *ctx, int pass, int nsteps, float *out_ms);
+
 /* Residual and L2 misfit with no device allocation at all.  This entry point
  * has no counterpart in the reference; it exists for callers that cannot
  * allocate device memory themselves or let a library do it — for instance an

@@ -1,0 +1,56 @@
+"""The GPU gradient against finite differences of the GPU misfit.
+
+The reference's gradient (src/denise.c:1589-1609, converted at :1743-1813) is
+a zero-lag correlation of the forward field with the back-propagated residual
+field; with the CPML, the staggered half-step offsets and the unscaled
+injection (src/update_v_PML.c:564-583) it is not the exact derivative of the
+discrete misfit, so its directional derivatives match central differences of
+the misfit in sign but only up to a direction-dependent factor.  The GPU
+reproduces the reference's gradient bit for bit (test_gpu_parity.py); this
+test pins what that implies: every tested direction has the sign of the
+finite difference, the factor stays within one order of magnitude across
+directions, and the finite difference itself is converged in the step size.
+"""
+import numpy as np
+import pytest
+from scipy.ndimage import gaussian_filter
+
+import dsh
+
+pytestmark = pytest.mark.gpu
+
+
+def test_gradient_directional_derivatives_vs_finite_differences():
+    nx, ny, nt, dh, dt = 80, 60, 600, 0.5, 2e-4
+    rng = np.random.default_rng(5)
+    vs0 = gaussian_filter(200 + 30 * rng.standard_normal((ny, nx)), 3).astype(np.float32)
+    rho = np.full((ny, nx), 1800, np.float32)
+    vst = vs0.copy()
+    vst[20:30, 35:45] *= 1.08
+    src = np.zeros((8, 1), np.float32)
+    src[:, 0] = [40, 2, 0, 0, 40.0, 1.0, 0, 3]
+    rec = np.array([np.arange(5, 76, 5), np.ones(15, int)], np.int32)
+    shot = dsh.Shot(src, rec)
+    p = dsh.make_params(nx=nx, ny=ny, nt=nt, dh=dh, dt=dt, fdorder=8, fw=12, free_surf=1, l=0, fpml=40.0,
+                        damping=260.0, eprecond=0)
+    with dsh.Engine(p) as e:
+        e.set_model(vst, rho)
+        obs = e.forward([shot])
+
+        def J(vs):
+            e.set_model(vs.astype(np.float32), rho)
+            return e.gradient([shot], obs)["l2"]
+
+        e.set_model(vs0, rho)
+        g = e.gradient([shot], obs)["g_vs"].astype(np.float64)
+        yy, xx = np.mgrid[0:ny, 0:nx]
+        ratios = []
+        for k, (cy, cx, s) in enumerate([(10, 20, 5), (35, 60, 7), (25, 40, 10), (15, 55, 4), (45, 30, 8)]):
+            d = np.exp(-((yy - cy) ** 2 + (xx - cx) ** 2) / (2 * s ** 2)) * (1 if k % 2 == 0 else -1)
+            fd = (J(vs0 + d) - J(vs0 - d)) / 2
+            fd2 = (J(vs0 + 0.5 * d) - J(vs0 - 0.5 * d)) / 1.0
+            an = float(np.sum(g * d))
+            assert np.sign(fd) == np.sign(an), (k, fd, an)
+            assert fd2 == pytest.approx(fd, rel=0.05)
+            ratios.append(fd / an)
+    assert max(ratios) / min(ratios) < 10.0, ratios
