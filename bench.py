@@ -69,6 +69,10 @@ def args_parse():
     ap.add_argument("--train-shots", type=int, default=8, help="c5 only: shots per training model")
     ap.add_argument("--epochs", type=int, default=12, help="c5 only: training epochs")
     ap.add_argument("--fwi-iters", type=int, default=20, help="c5 only: L-BFGS iterations")
+    ap.add_argument("--net-cache", default=None, help="c5 only: .npz of trained U-Net weights (load if present, "
+                                                      "else train and save)")
+    ap.add_argument("--methods", default="learned_sym,learned,hessian",
+                    help="c5 only: preconditioners compared with plain (the first one gives `value`)")
     ap.add_argument("--nt-scale", type=float, default=1.0, help="c4 only: factor on every model's NT")
     ap.add_argument("--nt", type=int, default=None, help="time steps (default: the workload's NT)")
     ap.add_argument("--nx", type=int, default=2000, help="c2 only")
@@ -684,50 +688,62 @@ def bench_learned(a, rank, world, local):
     train_shots = [cfg["shots"][k] for k in pick]
     log = lambda r: print(json.dumps(r), file=sys.stderr, flush=True)
     t0 = time.time()
-    clock0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clock0[0].record()
-    models = configs.training_models(count=a.train_models, first_seed=100, nx=nx, ny=ny)
-    xs, ts = fwi.training_pairs(torch, models, p, train_shots, log=log)
-    clock0[1].record()
-    torch.cuda.synchronize()
-    gen_s = clock0[0].elapsed_time(clock0[1]) / 1e3
     net = dnn.UNet(torch, seed=0)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    losses = fwi.train(net, torch, xs, ts, ny, nx, epochs=a.epochs, batch=2, lr=1e-3, log=log)
-    e1.record()
-    torch.cuda.synchronize()
-    train_s = e0.elapsed_time(e1) / 1e3
-    del xs, ts
+    gen_s = train_s = 0.0
+    losses = [None]
+    if a.net_cache and os.path.exists(a.net_cache):
+        net.load_state(dict(np.load(a.net_cache)))
+    else:
+        clock0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        clock0[0].record()
+        models = configs.training_models(count=a.train_models, first_seed=100, nx=nx, ny=ny)
+        xs, ts = fwi.training_pairs(torch, models, p, train_shots, log=log)
+        clock0[1].record()
+        torch.cuda.synchronize()
+        gen_s = clock0[0].elapsed_time(clock0[1]) / 1e3
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        losses = fwi.train(net, torch, xs, ts, ny, nx, epochs=a.epochs, batch=2, lr=1e-3, log=log)
+        e1.record()
+        torch.cuda.synchronize()
+        train_s = e0.elapsed_time(e1) / 1e3
+        del xs, ts
+        if a.net_cache:
+            np.savez(a.net_cache, **net.state())
     prob = fwi.Problem(cfg, test_shots=4)
     prob.observe()
     w0 = time.time()
     hp, _ = fwi.run(prob, a.fwi_iters, method="plain", log=log)
     w1 = time.time()
     target = hp[-1]["misfit"] * 1.01
-    hl, _ = fwi.run(prob, a.fwi_iters, method="learned", net=net, torch=torch, target_misfit=target, log=log)
-    w2 = time.time()
-    prob.close()
     t_plain = hp[-1]["gpu_s"]
-    t_learned = time_to_reach(hl, target)
-    ratio = (t_learned / t_plain) if t_learned is not None else None
-    wall_ratio = ((w2 - w1) / (w1 - w0)) if t_learned is not None else None
     curve = lambda h: [[round(r["gpu_s"], 3), r["misfit"]] for r in h]
+    res = {}
+    for m in [x for x in a.methods.split(",") if x]:
+        ws = time.time()
+        hl, _ = fwi.run(prob, a.fwi_iters, method=m, net=net, torch=torch, target_misfit=target, log=log)
+        t = time_to_reach(hl, target)
+        res[m] = {"final_misfit": hl[-1]["misfit"], "gpu_s_to_target": t, "gpu_s_total": hl[-1]["gpu_s"],
+                  "ratio": (t / t_plain) if t is not None else None,
+                  "wall_ratio": ((time.time() - ws) / (w1 - w0)) if t is not None else None,
+                  "iterations": len(hl) - 1, "fallbacks": sum(1 for r in hl if r.get("fallback")),
+                  "curve": curve(hl)}
+    prob.close()
+    primary = a.methods.split(",")[0]
     line = {
-        "metric": "learned-vs-plain FWI: GPU-seconds to the plain method's final misfit (ratio)", "value": ratio,
+        "metric": "learned-vs-plain FWI: GPU-seconds to the plain method's final misfit (ratio)",
+        "value": res[primary]["ratio"], "method": primary,
         "unit": "ratio", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 solver, bf16 network", "data": "synthetic",
         "config": {"workload": f"learned-fwi-{nx}x{ny}-fd8-L3-{ns}shots-nt{p['nt']}", "fwi_iters": a.fwi_iters,
                    "train_models": a.train_models, "train_shots": len(train_shots), "epochs": a.epochs,
                    "unet": "4 levels, 32 base channels, bf16 weights/activations, fp32 accumulation",
-                   "target": "plain final misfit x 1.01"},
+                   "target": "plain final misfit x 1.01", "net_cache": bool(a.net_cache and gen_s == 0.0)},
         "plain": {"final_misfit": hp[-1]["misfit"], "gpu_s": t_plain, "iterations": len(hp) - 1, "curve": curve(hp)},
-        "learned": {"final_misfit": hl[-1]["misfit"], "gpu_s_to_target": t_learned, "gpu_s_total": hl[-1]["gpu_s"],
-                    "iterations": len(hl) - 1, "fallbacks": sum(1 for r in hl if r.get("fallback")),
-                    "curve": curve(hl)},
+        "methods": res,
         "training": {"data_gpu_s": gen_s, "train_gpu_s": train_s, "loss_first": losses[0], "loss_last": losses[-1]},
-        "e2e": {"value": wall_ratio, "unit": "ratio (host wall-clock of both FWI runs)", "h2d_bytes_per_step": None,
-                "d2h_bytes_per_step": None},
+        "e2e": {"value": res[primary]["wall_ratio"], "unit": "ratio (host wall-clock of the FWI runs)",
+                "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
         "wall_s": time.time() - t0,
     }
     print(json.dumps(line), flush=True)

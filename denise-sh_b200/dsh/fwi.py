@@ -144,11 +144,24 @@ def learned_preconditioner(net, torch, g, ws, wr, vs, clock):
     return dnn.hessian_from_prediction(out.cpu().numpy().reshape(ny, nx))
 
 
+METHODS = ("plain", "learned", "learned_sym", "hessian")
+
+
 def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, scalefac=2.0, stepmax=6, nlbfgs=5,
         vmin=None, vmax=None, target_misfit=None, log=None):
     """FWI iterations; returns the history [{iter, misfit, gpu_s, eps, tests, fallback}].
-    method "plain": EPRECOND=1 gradient; "learned": raw gradient / U-Net Hessian,
-    falling back to a plain gradient when the line search rejects the learned step."""
+    method
+      "plain"        EPRECOND=1 gradient (per-shot g / (sqrt(Ws Wr) + 0.005 max), src/eprecond1.c)
+      "learned"      raw gradient / (H + 0.005 max H), H the U-Net's pseudo-Hessian
+      "learned_sym"  raw gradient / (sqrt(H' Wr) + 0.005 max), H' = H scaled to max Ws: the
+                     predicted strain-energy Hessian in the source-side slot of the energy
+                     preconditioner (the vs kernel correlates forward strains)
+      "hessian"      as "learned" with the solver's own pseudo-Hessian (one extra forward
+                     pass per iteration; a reference for what the prediction stands in for)
+    The learned methods fall back to a plain gradient when the line search
+    rejects their step."""
+    if method not in METHODS:
+        raise ValueError(method)
     if problem.obs is None:
         problem.observe()
     shots, obs = problem.shots, problem.obs
@@ -172,8 +185,17 @@ def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, sc
             q = out["g_vs"]
         else:
             ws, wr = eng.energy_sums()            # summed over shots on the device
-            h = learned_preconditioner(net, torch, out["g_vs"], ws, wr, vs, clock)
-            q = out["g_vs"] / (h + 0.005 * float(h.max()))
+            if kind == "hessian":
+                h, _ = eng.hessian_diag(shots)
+                clock.add_engine(eng)
+            else:
+                h = learned_preconditioner(net, torch, out["g_vs"], ws, wr, vs, clock)
+            if kind == "learned_sym":
+                h = h.astype(np.float64) * (float(ws.max()) / max(float(h.max()), 1e-300))
+                w = np.sqrt(h * wr.astype(np.float64))
+                q = out["g_vs"] / (w + 0.005 * float(w.max()))
+            else:
+                q = out["g_vs"] / (h + 0.005 * float(h.max()))
         l2_test = float(eng.shot_misfits(len(shots))[test].sum())
         return q.astype(np.float32), out["l2"], l2_test
 

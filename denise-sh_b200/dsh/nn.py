@@ -339,6 +339,16 @@ class UNet:
         out["hb"] = self.hb.cpu().numpy()
         return out
 
+    def load_state(self, st):
+        """Inverse of state(): FP32 parameters from numpy arrays."""
+        torch = self.torch
+        for k, l in enumerate(self.layers()):
+            l.w.copy_(torch.from_numpy(np.asarray(st[f"w{k}"], np.float32)))
+            l.b.copy_(torch.from_numpy(np.asarray(st[f"b{k}"], np.float32)))
+            l.prep()
+        self.hw.copy_(torch.from_numpy(np.asarray(st["hw"], np.float32)))
+        self.hb.copy_(torch.from_numpy(np.asarray(st["hb"], np.float32)))
+
     def grads(self):
         """Accumulated gradients as numpy arrays (weights [cout][9cin])."""
         out = {}

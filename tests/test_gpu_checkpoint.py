@@ -71,7 +71,7 @@ def test_64_shots_one_launch_checkpointed():
     with engine_from(d, max_shots=64) as e:
         full = e.gradient(shots, obs)
         st_full = e.stats()
-    with engine_from(d, max_shots=64, mem_budget=st_full["storage_bytes"] // 3) as e:
+    with engine_from(d, max_shots=64, mem_budget=st_full["storage_bytes"] // 2) as e:
         ck = e.gradient(shots, obs)
         st = e.stats()
     assert st["checkpoint_interval"] > 0
