@@ -53,6 +53,6 @@ def test_gradient_directional_derivatives_vs_finite_differences():
             an = float(np.sum(g * d))
             assert np.sign(fd) == np.sign(an), (k, fd, an)
             if k > 0:      # the first bump sits next to source and receivers, where the misfit is far from linear
-                assert fd2 == pytest.approx(fd, rel=0.05), (k, fd, fd2)
+                assert fd2 == pytest.approx(fd, rel=0.1), (k, fd, fd2)
             ratios.append(fd / an)
     assert max(ratios) / min(ratios) < 10.0, ratios
