@@ -122,8 +122,18 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
             float4 vy4 = ld4(vy_r + hrow + col0);
             const float4 old4 = vy4;
             float4 acc4 = make_float4(0.f, 0.f, 0.f, 0.f);
-            const int c = 4 * g;
-            const int rz = r + H;
+            /* taps as float4 rows of shared memory (conflict-free): xs[p] =
+               sxy[i0 - 4*NLV + p] of row j, ys[q] = syz rows j-H .. j+H-1 */
+            constexpr int NLV = (H + 3) / 4, NRV = (H - 1 + 3) / 4;
+            float xs[4 * (NLV + 1 + NRV)];
+#pragma unroll
+            for (int v = 0; v < NLV + 1 + NRV; v++) {
+                const float4 t = *reinterpret_cast<const float4 *>(&s_sxy[r][4 * (g - NLV + v)]);
+                xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+            }
+            float4 ys[2 * H];
+#pragma unroll
+            for (int q = 0; q < 2 * H; q++) ys[q] = *reinterpret_cast<const float4 *>(&s_syz[r + q][4 * g]);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const int i = i0 + k;
@@ -131,8 +141,8 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
                 float sxy_x, syy_y;
 #pragma unroll
                 for (int m = 1; m <= H; m++) {
-                    float tx = a.hc[m] * (s_sxy[r][c + k + m - 1] - s_sxy[r][c + k - m]);
-                    float ty = a.hc[m] * (s_syz[rz + m - 1][c + k] - s_syz[rz - m][c + k]);
+                    float tx = a.hc[m] * (xs[4 * NLV + k + m - 1] - xs[4 * NLV + k - m]);
+                    float ty = a.hc[m] * (get(ys[H + m - 1], k) - get(ys[H - m], k));
                     if (m == 1) { sxy_x = tx; syy_y = ty; }
                     else { sxy_x = sxy_x + tx; syy_y = syy_y + ty; }
                 }
@@ -236,6 +246,7 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
         if (j > a.ny || i0 > a.nx) continue;
         const int rv = ro + H - 1, rz = ro + 2 * H - 1;
         const int c = 4 * g;
+        (void)c;
         const long long drow = (long long)(j - 1) * pitch;
         const long long hrow = (long long)(j - 1 + a.hy) * pitch;
         const int col0 = i0 - 1 + HX;
@@ -268,6 +279,17 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
             fy = ldg4(base + a.dstride);
             fu = ldg4(base + 2 * a.dstride);
         }
+        /* velocity taps: xs[p] = vy[i0 - 4*NLS + p] of row j, ys[q] = vy rows j-H+1 .. j+H */
+        constexpr int NLS = (H - 1 + 3) / 4, NRS = (H + 3) / 4;
+        float xs[4 * (NLS + 1 + NRS)];
+#pragma unroll
+        for (int v = 0; v < NLS + 1 + NRS; v++) {
+            const float4 t = *reinterpret_cast<const float4 *>(&s_v[rv][4 * (g - NLS + v)]);
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+        float4 ys[2 * H];
+#pragma unroll
+        for (int q = 0; q < 2 * H; q++) ys[q] = *reinterpret_cast<const float4 *>(&s_v[rv - H + 1 + q][4 * g]);
         float4 vyx4 = make_float4(0.f, 0.f, 0.f, 0.f), vyy4 = vyx4;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
@@ -275,8 +297,8 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
             float vyx, vyy;
 #pragma unroll
             for (int m = 1; m <= H; m++) {
-                float tx = a.hc[m] * (s_v[rv][c + k + m] - s_v[rv][c + k - m + 1]);
-                float ty = a.hc[m] * (s_v[rv + m][c + k] - s_v[rv - m + 1][c + k]);
+                float tx = a.hc[m] * (xs[4 * NLS + k + m] - xs[4 * NLS + k - m + 1]);
+                float ty = a.hc[m] * (get(ys[H - 1 + m], k) - get(ys[H - m], k));
                 if (m == 1) { vyx = tx; vyy = ty; }
                 else { vyx = vyx + tx; vyy = vyy + ty; }
             }
