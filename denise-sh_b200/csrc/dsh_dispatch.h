@@ -5,8 +5,9 @@
 namespace dsh {
 using KFn = void (*)(StepArgs, int);
 
-#define DSH_DECLARE_FD(N)                  \
-    KFn v_kernel_fd##N(int flags, bool p2); \
+#define DSH_DECLARE_FD(N)                     \
+    KFn v_kernel_fd##N(int flags, bool p2);    \
+    KFn v_kernel_st_fd##N(int flags, bool p2); \
     KFn s_kernel_fd##N(int l, int flags);
 DSH_DECLARE_FD(2)
 DSH_DECLARE_FD(4)
@@ -25,6 +26,20 @@ inline KFn v_kernel(int fdo, int flags, bool p2)
     case 8: return v_kernel_fd8(flags, p2);
     case 10: return v_kernel_fd10(flags, p2);
     case 12: return v_kernel_fd12(flags, p2);
+    default: return nullptr;
+    }
+}
+
+/* velocity step with shared-memory staged stress taps */
+inline KFn v_kernel_st(int fdo, int flags, bool p2)
+{
+    switch (fdo) {
+    case 2: return v_kernel_st_fd2(flags, p2);
+    case 4: return v_kernel_st_fd4(flags, p2);
+    case 6: return v_kernel_st_fd6(flags, p2);
+    case 8: return v_kernel_st_fd8(flags, p2);
+    case 10: return v_kernel_st_fd10(flags, p2);
+    case 12: return v_kernel_st_fd12(flags, p2);
     default: return nullptr;
     }
 }

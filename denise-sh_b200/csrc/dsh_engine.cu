@@ -809,6 +809,15 @@ InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
 }
 }  // namespace dsh::eng
 
+/* Velocity kernel of the kernel pair: the shared-memory staged variant
+ * (v_step_st) unless DSH_VSTAGE=0; the compat flags use v_step. */
+static KFn pick_v(int fdo, int vflags, bool p2)
+{
+    static const bool staged = []() { const char *e = getenv("DSH_VSTAGE"); return !e || atoi(e) != 0; }();
+    KFn k = staged ? v_kernel_st(fdo, vflags, p2) : nullptr;
+    return k ? k : v_kernel(fdo, vflags, p2);
+}
+
 /* The fused step (one kernel per time step, dsh_fused.cuh) serves every pass
  * but the Hessian one when FDORDER <= 8 and injection/sampling are fused;
  * DSH_FUSED=0 selects the velocity + stress kernel pair instead. */
@@ -865,7 +874,7 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
     case P_FWD_CKPT: break;
     case P_RECOMP: sflags = SF_STRAIN_OUT; break;
     }
-    KFn vk = v_kernel(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
+    KFn vk = pick_v(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
     StepArgs sa = step_args(ctx, pass);
     InjectArgs ia = inject_args(ctx, pass);
@@ -1458,7 +1467,7 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
     if (pass == P_FWD_STORE) sflags = SF_STRAIN_OUT;
     if (pass == P_FWD_HESS) { vflags = VF_HESS; sflags = SF_HESS; }
     if (pass == P_ADJ) { vflags = VF_ADJOINT | VF_CORR; sflags = SF_CORR; }
-    KFn vk = v_kernel(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
+    KFn vk = pick_v(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
     StepArgs sa = step_args(ctx, (Pass)pass);
     InjectArgs ia = inject_args(ctx, (Pass)pass);

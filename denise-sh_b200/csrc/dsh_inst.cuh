@@ -18,6 +18,17 @@
         }                                                                                     \
     }                                                                                         \
     KFn v_kernel_fd##N(int flags, bool p2) { return p2 ? v_pick_##N<true>(flags) : v_pick_##N<false>(flags); } \
+    template <bool P2>                                                                        \
+    static KFn v_pick_st_##N(int flags)                                                       \
+    {                                                                                         \
+        switch (flags) {                                                                      \
+        case 0: return v_step_st<N, 0, P2>;                                                   \
+        case VF_HESS: return v_step_st<N, VF_HESS, P2>;                                       \
+        case VF_ADJOINT | VF_CORR: return v_step_st<N, VF_ADJOINT | VF_CORR, P2>;             \
+        default: return nullptr;                                                              \
+        }                                                                                     \
+    }                                                                                         \
+    KFn v_kernel_st_fd##N(int flags, bool p2) { return p2 ? v_pick_st_##N<true>(flags) : v_pick_st_##N<false>(flags); } \
     template <int L>                                                                          \
     static KFn s_pick_##N(int flags)                                                          \
     {                                                                                         \

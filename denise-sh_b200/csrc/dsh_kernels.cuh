@@ -159,8 +159,48 @@ __device__ __forceinline__ float div_dh(float x, const StepArgs &a) { return P2 
  * them, ((j-1)/8) * ceil(nx/128) + (i0-1)/128.
  * All global loads are issued before any store so their latencies overlap.
  */
-template <int FDO, int FLAGS, bool P2>
-__device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, int j, int slot, int tile)
+/* Stress taps of the velocity update straight from global memory:
+ * xs[p] = sxy[i0 - 4*NL + p] of row j, ys[r] = syz rows j-H .. j+H-1. */
+struct GlobalTaps {
+    template <int H, int NL, int NR>
+    __device__ __forceinline__ void load(const StepArgs &a, long long so, long long hrow, int col0, int j, float *xs,
+                                         float4 *ys) const
+    {
+        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
+#pragma unroll
+        for (int v = 0; v < NL + 1 + NR; v++) {
+            float4 t = ld4(row + 4 * v);
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * a.pitch + col0;
+#pragma unroll
+        for (int r = 0; r < 2 * H; r++) ys[r] = ld4(col + (long long)r * a.pitch);
+    }
+};
+
+/* The same taps from a block's shared-memory staging (v_step_st): sx[ty][v]
+ * = sxy row of thread row ty, float4 group v counted from the block's first
+ * point minus 4*NL; sy[r][tx] = syz row j0-H+r at the thread's four points. */
+struct SharedTaps {
+    const float4 *sx, *sy;
+    int sx_pitch, tx, ty;
+    template <int H, int NL, int NR>
+    __device__ __forceinline__ void load(const StepArgs &, long long, long long, int, int, float *xs,
+                                         float4 *ys) const
+    {
+#pragma unroll
+        for (int v = 0; v < NL + 1 + NR; v++) {
+            const float4 t = sx[ty * sx_pitch + tx + v];
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+#pragma unroll
+        for (int r = 0; r < 2 * H; r++) ys[r] = sy[(ty + r) * BX + tx];
+    }
+};
+
+template <int FDO, int FLAGS, bool P2, class Taps = GlobalTaps>
+__device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, int j, int slot, int tile,
+                                       const Taps &taps = Taps())
 {
     constexpr int H = FDO / 2;
     constexpr int NL = (H + 3) / 4;          /* float4s left of the own vector (needs H)   */
@@ -199,20 +239,8 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
 
     /* ---- stress taps ---- */
     float xs[NXS];                           /* xs[p] = sxy[i0 - 4*NL + p] */
-    {
-        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
-#pragma unroll
-        for (int v = 0; v < NL + 1 + NR; v++) {
-            float4 t = ld4(row + 4 * v);
-            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
-        }
-    }
     float4 ys[2 * H];                        /* syz rows j-H .. j+H-1 */
-    {
-        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * pitch + col0;
-#pragma unroll
-        for (int r = 0; r < 2 * H; r++) ys[r] = ld4(col + (long long)r * pitch);
-    }
+    taps.template load<H, NL, NR>(a, so, hrow, col0, j, xs, ys);
 
     /* ---- compute ---- */
     float4 acc4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -312,6 +340,46 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
 {
     v_body<FDO, FLAGS, P2>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
                            blockIdx.z, blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+/* The velocity step with the block's stress taps staged in shared memory
+ * first: 8 sxy rows of 128 + 4*(NL+NR) points and 8+2H-1 syz rows of 128
+ * points, loaded once per block (about 3 float4 loads per thread instead of
+ * NL+1+NR+2H), then read by every thread of the block. */
+template <int FDO, int FLAGS, bool P2>
+__global__ void __launch_bounds__(BX *BY, 3) v_step_st(StepArgs a, int nt_off)
+{
+    constexpr int H = FDO / 2;
+    constexpr int NL = (H + 3) / 4, NR = (H - 1 + 3) / 4;
+    constexpr int SXP = BX + NL + NR;                 /* float4 groups per staged sxy row */
+    constexpr int SYR = BY + 2 * H - 1;               /* staged syz rows */
+    __shared__ float4 sx[BY * SXP];
+    __shared__ float4 sy[SYR * BX];
+    const int nt = *a.nt_base + nt_off;
+    if (nt > a.nt_last) return;
+    const int tid = threadIdx.y * BX + threadIdx.x;
+    const int slot = blockIdx.z;
+    const long long so = (long long)slot * a.slot_stride;
+    const int j0 = 1 + blockIdx.y * BY;
+    const int cb = 4 * blockIdx.x * BX + HX;          /* column of the block's first point */
+    const int rows_total = a.ny + 2 * a.hy;
+    pdl_wait();                                       /* stresses of the previous step are complete */
+    for (int idx = tid; idx < BY * SXP; idx += BX * BY) {
+        const int r = idx / SXP, v = idx % SXP;
+        const int row = j0 + r - 1 + a.hy, col = cb - 4 * NL + 4 * v;
+        sx[idx] = (row < rows_total && col + 3 < a.pitch) ? ld4(a.sxy + so + (long long)row * a.pitch + col)
+                                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    for (int idx = tid; idx < SYR * BX; idx += BX * BY) {
+        const int r = idx / BX, v = idx % BX;
+        const int row = j0 - H + r - 1 + a.hy, col = cb + 4 * v;
+        sy[idx] = (row < rows_total && col + 3 < a.pitch) ? ld4(a.syz + so + (long long)row * a.pitch + col)
+                                                         : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    __syncthreads();
+    SharedTaps taps{sx, sy, SXP, (int)threadIdx.x, (int)threadIdx.y};
+    v_body<FDO, FLAGS, P2>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
+                           slot, blockIdx.y * gridDim.x + blockIdx.x, taps);
 }
 
 /*
