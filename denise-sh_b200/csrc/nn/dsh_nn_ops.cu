@@ -204,42 +204,56 @@ __global__ void head_fwd_k(const bf16 *x, long long P, int C, const float *w, co
     }
 }
 
-/* dx and the per-block partial sums of the weight / bias gradients */
-__global__ void head_bwd_k(const float *dout, const bf16 *x, long long P, int C, const float *w, float *dx, float *gw,
-                           float *gb)
+/* dx[p][c] = dout[p] w[c], and per block b the partial sums
+ * part[b][c] = sum over its rows of dout[p] x[p][c] (c < C) and
+ * part[b][C] = sum of dout[p]: thread t of a block owns column t % (C+1) and
+ * the rows r = t / (C+1) + k * (256 / (C+1)) of the block's chunk, partials
+ * are combined in a fixed order, so the result does not depend on timing. */
+__global__ void head_bwd_k(const float *dout, const bf16 *x, long long P, int C, const float *w, float *dx, float *part)
 {
-    extern __shared__ float acc[];                 /* C + 1 per block */
-    for (int c = threadIdx.x; c <= C; c += blockDim.x) acc[c] = 0.0f;
-    __syncthreads();
-    GRID_LOOP(p, P)
-    {
-        const float d = dout[p];
-        for (int c = 0; c < C; c++) {
-            dx[p * C + c] = d * w[c];
-            atomicAdd(&acc[c], d * __bfloat162float(x[p * C + c]));
-        }
-        atomicAdd(&acc[C], d);
-    }
-    __syncthreads();
-    for (int c = threadIdx.x; c < C; c += blockDim.x) atomicAdd(&gw[c], acc[c]);
-    if (threadIdx.x == 0) atomicAdd(gb, acc[C]);
-}
-
-/* column sums of dy [P][N]: each block a strip of rows, shared-memory partials */
-__global__ void colsum_k(const float *dy, long long P, int N, float *g)
-{
-    extern __shared__ float acc[];
-    for (int n = threadIdx.x; n < N; n += blockDim.x) acc[n] = 0.0f;
-    __syncthreads();
     const long long rows = (P + gridDim.x - 1) / gridDim.x;
     const long long r0 = (long long)blockIdx.x * rows, r1 = min(P, r0 + rows);
-    for (long long idx = threadIdx.x; idx < (r1 - r0) * N; idx += blockDim.x) {
-        const long long p = r0 + idx / N;
-        const int n = (int)(idx % N);
-        atomicAdd(&acc[n], dy[p * N + n]);
+    for (long long idx = r0 * C + threadIdx.x; idx < r1 * C; idx += blockDim.x) {
+        const long long p = idx / C;
+        dx[idx] = dout[p] * w[idx % C];
     }
+    extern __shared__ float acc[];                 /* blockDim.x */
+    const int W = C + 1, lanes = blockDim.x / W;
+    float s = 0.0f;
+    if ((int)threadIdx.x < lanes * W) {
+        const int c = threadIdx.x % W, lane = threadIdx.x / W;
+        for (long long p = r0 + lane; p < r1; p += lanes)
+            s += c < C ? dout[p] * __bfloat162float(x[p * C + c]) : dout[p];
+    }
+    acc[threadIdx.x] = s;
     __syncthreads();
-    for (int n = threadIdx.x; n < N; n += blockDim.x) atomicAdd(&g[n], acc[n]);
+    if ((int)threadIdx.x < W) {
+        float t = 0.0f;
+        for (int lane = 0; lane < lanes; lane++) t += acc[lane * W + threadIdx.x];
+        part[(long long)blockIdx.x * W + threadIdx.x] = t;
+    }
+}
+
+/* per-block partial column sums of dy [P][N] (fixed order, as head_bwd_k) */
+__global__ void colsum_k(const float *dy, long long P, int N, float *part)
+{
+    const long long rows = (P + gridDim.x - 1) / gridDim.x;
+    const long long r0 = (long long)blockIdx.x * rows, r1 = min(P, r0 + rows);
+    for (int n = threadIdx.x; n < N; n += blockDim.x) {
+        float s = 0.0f;
+        for (long long p = r0; p < r1; p++) s += dy[p * N + n];
+        part[(long long)blockIdx.x * N + n] = s;
+    }
+}
+
+/* g[n] += sum over blocks of part[b*stride + n], blocks in order */
+__global__ void sum_parts_k(const float *part, int nblocks, int N, int stride, float *g)
+{
+    for (int n = blockIdx.x * blockDim.x + threadIdx.x; n < N; n += gridDim.x * blockDim.x) {
+        float s = 0.0f;
+        for (int b = 0; b < nblocks; b++) s += part[(long long)b * stride + n];
+        g[n] += s;
+    }
 }
 
 __global__ void mse_k(const float *pred, const float *target, const unsigned char *mask, long long n, float count,
@@ -386,19 +400,23 @@ extern "C" int dsh_nn_head_fwd(const void *x, long long P, int C, const float *w
     return status();
 }
 
+constexpr int RED_BLOCKS = DSH_NN_RED_BLOCKS;
+
 extern "C" int dsh_nn_head_bwd(const float *dout, const void *x, long long P, int C, const float *w, float *dx,
-                               float *gw, float *gb, void *stream)
+                               float *gw, float *gb, float *part, void *stream)
 {
-    if (!dout || !x || !w || !dx || !gw || !gb || P <= 0 || C <= 0 || C > 4096) return DSH_NN_ERR_PARAM;
-    head_bwd_k<<<grid_for(P), 256, (C + 1) * sizeof(float), ST>>>(dout, (const bf16 *)x, P, C, w, dx, gw, gb);
+    if (!dout || !x || !w || !dx || !gw || !gb || !part || P <= 0 || C <= 0 || C + 1 > 256) return DSH_NN_ERR_PARAM;
+    head_bwd_k<<<RED_BLOCKS, 256, 256 * sizeof(float), ST>>>(dout, (const bf16 *)x, P, C, w, dx, part);
+    sum_parts_k<<<1, 256, 0, ST>>>(part, RED_BLOCKS, C, C + 1, gw);
+    sum_parts_k<<<1, 32, 0, ST>>>(part + C, RED_BLOCKS, 1, C + 1, gb);   /* column C of the (C+1)-wide table */
     return status();
 }
 
-extern "C" int dsh_nn_colsum(const float *dy, long long P, int N, float *g, void *stream)
+extern "C" int dsh_nn_colsum(const float *dy, long long P, int N, float *g, float *part, void *stream)
 {
-    if (!dy || !g || P <= 0 || N <= 0 || N > 8192) return DSH_NN_ERR_PARAM;
-    const int blocks = (int)std::min<long long>(148 * 4, (P + 255) / 256);
-    colsum_k<<<blocks, 256, N * sizeof(float), ST>>>(dy, P, N, g);
+    if (!dy || !g || !part || P <= 0 || N <= 0) return DSH_NN_ERR_PARAM;
+    colsum_k<<<RED_BLOCKS, 256, 0, ST>>>(dy, P, N, part);
+    sum_parts_k<<<(N + 255) / 256, 256, 0, ST>>>(part, RED_BLOCKS, N, N, g);
     return status();
 }
 

@@ -25,6 +25,7 @@ import numpy as np
 PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 NN_LIB_PATH = os.path.join(PKG_DIR, "libdsh_nn.so")
 BASE = 32
+RED_BLOCKS = 296     # DSH_NN_RED_BLOCKS: row chunks of the fixed-order gradient reductions
 IN_CH = 8            # 4 input maps padded to 8 channels (72-element rows, 16-byte aligned)
 
 _nn = None
@@ -52,8 +53,8 @@ def nnlib() -> C.CDLL:
         L.dsh_nn_concat.argtypes = [v, i, v, i, ll, v, v]
         L.dsh_nn_split.argtypes = [v, i, i, ll, v, v, v]
         L.dsh_nn_head_fwd.argtypes = [v, ll, i, v, v, v, v]
-        L.dsh_nn_head_bwd.argtypes = [v, v, ll, i, v, v, v, v, v]
-        L.dsh_nn_colsum.argtypes = [v, ll, i, v, v]
+        L.dsh_nn_head_bwd.argtypes = [v, v, ll, i, v, v, v, v, v, v]
+        L.dsh_nn_colsum.argtypes = [v, ll, i, v, v, v]
         L.dsh_nn_mse.argtypes = [v, v, v, ll, f, v, v, v]
         L.dsh_nn_adam.argtypes = [v, v, v, v, i, i, i, f, f, f, f, i, v]
         _nn = L
@@ -155,7 +156,8 @@ class Conv3x3:
         P = B * H * W
         dz = ctx.scratch("dz16", P * self.cout, torch.bfloat16)
         _ck(nnlib().dsh_nn_relu_bwd(_p(dy), _p(y), _p(dz), _p(dy), P * self.cout, ctx.st), "relu_bwd")
-        _ck(nnlib().dsh_nn_colsum(_p(dy), P, self.cout, _p(self.gb), ctx.st), "colsum")
+        red = ctx.scratch("red", RED_BLOCKS * (self.cout + 1), torch.float32)
+        _ck(nnlib().dsh_nn_colsum(_p(dy), P, self.cout, _p(self.gb), _p(red), ctx.st), "colsum")
         # weight gradient (transposed): colT [9cin][P] . dzT [cout][P]^T, split over P
         ldp = _rup(P, 8)                      # 16-byte row pitch for the tensor-map operands
         colT = ctx.scratch("colT", self.K * ldp, torch.bfloat16)
@@ -264,8 +266,9 @@ class UNet:
         L = nnlib()
         f32 = lambda n: torch.empty(n, dtype=torch.float32, device=self.ctx.device)
         g = f32(P[0] * c[0])
-        _ck(L.dsh_nn_head_bwd(_p(dout), _p(a["d0c"]), P[0], c[0], _p(self.hw), _p(g), _p(self.ghw), _p(self.ghb), st),
-            "head_bwd")
+        red = self.ctx.scratch("red", RED_BLOCKS * (c[0] + 1), torch.float32)
+        _ck(L.dsh_nn_head_bwd(_p(dout), _p(a["d0c"]), P[0], c[0], _p(self.hw), _p(g), _p(self.ghw), _p(self.ghb),
+                              _p(red), st), "head_bwd")
         skip = {}
         for l in (0, 1, 2):
             h, w = H >> l, W >> l

@@ -71,11 +71,15 @@ int dsh_nn_concat(const void *a, int C1, const void *b, int C2, long long P, voi
 int dsh_nn_split(const float *dy, int C1, int C2, long long P, float *da, float *db, void *stream);
 /* out[p] = sum_c x[p][c] w[c] + b (1x1 convolution to one channel, x bf16, out float) */
 int dsh_nn_head_fwd(const void *x, long long P, int C, const float *w, const float *b, float *out, void *stream);
-/* dx[p][c] = dout[p] w[c] (float); gw[c] += sum_p dout[p] x[p][c]; gb += sum_p dout[p] */
+/* dx[p][c] = dout[p] w[c] (float); gw[c] += sum_p dout[p] x[p][c]; gb += sum_p dout[p].
+ * part: scratch of DSH_NN_RED_BLOCKS*(C+1) floats; the sums are formed in a
+ * fixed order (no atomics), so training is reproducible run to run. */
+#define DSH_NN_RED_BLOCKS 296
 int dsh_nn_head_bwd(const float *dout, const void *x, long long P, int C, const float *w, float *dx, float *gw,
-                    float *gb, void *stream);
-/* column sums: g[n] += sum_p dy[p][n] (bias gradient), dy float [P][N] */
-int dsh_nn_colsum(const float *dy, long long P, int N, float *g, void *stream);
+                    float *gb, float *part, void *stream);
+/* column sums: g[n] += sum_p dy[p][n] (bias gradient), dy float [P][N];
+ * part: scratch of DSH_NN_RED_BLOCKS*N floats, fixed summation order */
+int dsh_nn_colsum(const float *dy, long long P, int N, float *g, float *part, void *stream);
 /* masked mean-square loss: d = pred - target on mask != 0; loss[0] += sum d^2 / count,
  * grad = 2 d / count (0 outside the mask) */
 int dsh_nn_mse(const float *pred, const float *target, const unsigned char *mask, long long n, float count,

@@ -175,3 +175,26 @@ def test_unet_training_lowers_loss():
         losses.append(float(loss.item()))
     net.ctx.check()
     assert losses[-1] < 0.2 * losses[0], losses[::10]
+
+
+def test_training_is_reproducible():
+    """Fixed-order reductions: two trainings from the same seed and data give
+    bit-identical weights."""
+    from dsh import nn
+
+    B, H, W = 2, 16, 24
+    x = _inputs(B, H, W, 9)
+    t = x.float().view(B, H, W, -1)[..., 2].contiguous().view(-1)
+    states = []
+    for _ in range(2):
+        net = nn.UNet(torch, seed=6)
+        for _ in range(5):
+            net.forward(x, B, H, W)
+            loss, grad = net.loss_grad(t)
+            net.zero_grad()
+            net.backward(grad)
+            net.adam_step(lr=1e-3)
+        net.ctx.check()
+        states.append(net.state())
+    for k in states[0]:
+        assert np.array_equal(states[0][k], states[1][k]), k
