@@ -809,11 +809,14 @@ InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
 }
 }  // namespace dsh::eng
 
-/* Velocity kernel of the kernel pair: the shared-memory staged variant
- * (v_step_st) unless DSH_VSTAGE=0; the compat flags use v_step. */
+/* Velocity kernel of the kernel pair: v_step (stress taps from global
+ * memory through L1); DSH_VSTAGE=1 selects the shared-memory staged
+ * v_step_st, which measured slower on B200 (19.2 vs 14.7 us per launch at
+ * 2000 x 800, FDORDER 8: the block-wide staging and barrier cost more than the
+ * L1 hits they replace). */
 static KFn pick_v(int fdo, int vflags, bool p2)
 {
-    static const bool staged = []() { const char *e = getenv("DSH_VSTAGE"); return !e || atoi(e) != 0; }();
+    static const bool staged = []() { const char *e = getenv("DSH_VSTAGE"); return e && atoi(e) != 0; }();
     KFn k = staged ? v_kernel_st(fdo, vflags, p2) : nullptr;
     return k ? k : v_kernel(fdo, vflags, p2);
 }
