@@ -17,6 +17,7 @@
 #include "dsh.h"
 #include "dsh_engine_int.h"
 #include "dsh_fs.h"
+#include "dsh_pf.h"
 #include "dsh_fused.cuh"
 #include "dsh_setup.h"
 
@@ -353,9 +354,10 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     if (cudaMalloc(&ctx->pml, 12 * (size_t)(2 * DSH_MAX_FW + 1) * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     if (cudaMalloc(&ctx->sums, 6 * (size_t)ctx->dstride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     if (cudaMalloc(&ctx->d_out, 2 * (size_t)nx * ny * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
-    if (cudaMalloc(&ctx->d_nt, 2 * sizeof(int)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->d_nt, 4 * sizeof(int)) != cudaSuccess) return bail(DSH_ERR_OOM);
     ctx->d_status = ctx->d_nt + 1;
-    cudaMemset(ctx->d_nt, 0, 2 * sizeof(int));
+    ctx->d_bar = reinterpret_cast<unsigned *>(ctx->d_nt + 2);
+    cudaMemset(ctx->d_nt, 0, 4 * sizeof(int));
     if (cudaMalloc(&ctx->d_part, (size_t)ctx->S * RED_BLOCKS * sizeof(double)) != cudaSuccess) return bail(DSH_ERR_OOM);
     if (cudaMalloc(&ctx->d_l2, (size_t)ctx->S * sizeof(double)) != cudaSuccess) return bail(DSH_ERR_OOM);
     if (cudaMalloc(&ctx->d_wemax, (size_t)ctx->S * sizeof(unsigned)) != cudaSuccess) return bail(DSH_ERR_OOM);
@@ -939,11 +941,45 @@ static int get_graph(dsh_ctx *ctx, Pass pass, int nb, int K, cudaGraphExec_t *ou
     return DSH_OK;
 }
 
+/* Small grids, plain forward modelling: the whole pass in one cooperative
+ * launch of persist_fwd when all tiles of all slots fit in one wave
+ * (DSH_PERSIST=0 turns it off).  Returns the grid size, 0 when not used. */
+static int persistent_grid(dsh_ctx *ctx, Pass pass, int nb)
+{
+    static const bool on = []() { const char *e = getenv("DSH_PERSIST"); return !e || atoi(e) != 0; }();
+    const dsh_params &p = ctx->p;
+    if (!on || pass != P_FWD_PLAIN || !ctx->fused_inject || p.fdorder > 8) return 0;
+    PFn fk = pf_kernel(p.fdorder, p.l, dh_pow2(p.dh));
+    if (!fk) return 0;
+    int per_sm = 0, nsm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fk, BX * BY, 0) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->dev) != cudaSuccess) return 0;
+    const long long tiles = (long long)((p.nx + 4 * BX - 1) / (4 * BX)) * ((p.ny + BY - 1) / BY) * nb;
+    return tiles <= (long long)per_sm * nsm ? (int)tiles : 0;
+}
+
+static int run_persistent(dsh_ctx *ctx, Pass pass, int nb, int n0, int count, int grid)
+{
+    const dsh_params &p = ctx->p;
+    PFn fk = pf_kernel(p.fdorder, p.l, dh_pow2(p.dh));
+    StepArgs sa = step_args(ctx, pass);
+    sa.nslots = nb;
+    set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, n0);
+    CK(cudaMemsetAsync(ctx->d_bar, 0, 2 * sizeof(unsigned), ctx->st));
+    unsigned *bar = ctx->d_bar;
+    void *args[3] = {&sa, &count, &bar};
+    CK(cudaLaunchCooperativeKernel((const void *)fk, dim3(grid), dim3(BX, BY), args, 0, ctx->st));
+    ctx->launches += 2;
+    ctx->state_b = 0;
+    return DSH_OK;
+}
+
 /* Steps n0 .. n0+count-1 of a pass: graphs of `chunk` steps replayed
  * count/chunk times, then one graph for the remaining steps. */
 static int run_steps(dsh_ctx *ctx, Pass pass, int nb, int n0, int count)
 {
     if (count <= 0) return DSH_OK;
+    if (const int grid = persistent_grid(ctx, pass, nb)) return run_persistent(ctx, pass, nb, n0, count, grid);
     const int K = std::min(ctx->chunk, count);
     const int nfull = count / K, rem = count % K;
     const bool fused = use_fused(ctx, pass);
@@ -1047,7 +1083,7 @@ int check_status(dsh_ctx *ctx)
     if (h) {
         cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->st);
         cudaStreamSynchronize(ctx->st);
-        return DSH_ERR_UNSTABLE;
+        return (h & 2) ? DSH_ERR_TIMEOUT : DSH_ERR_UNSTABLE;   /* bit 2: a bounded grid barrier expired */
     }
     return DSH_OK;
 }

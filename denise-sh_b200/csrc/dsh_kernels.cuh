@@ -109,6 +109,14 @@ struct StepArgs {
 };
 
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+/* state loads of the persistent kernel: other blocks wrote them earlier in the
+ * same launch, so they bypass L1 (ld.global.cg) */
+template <bool CG>
+__device__ __forceinline__ float4 lds4(const float *p)
+{
+    if (CG) return __ldcg(reinterpret_cast<const float4 *>(p));
+    return *reinterpret_cast<const float4 *>(p);
+}
 __device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
 __device__ __forceinline__ float get(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
@@ -161,6 +169,7 @@ __device__ __forceinline__ float div_dh(float x, const StepArgs &a) { return P2 
  */
 /* Stress taps of the velocity update straight from global memory:
  * xs[p] = sxy[i0 - 4*NL + p] of row j, ys[r] = syz rows j-H .. j+H-1. */
+template <bool CG = false>
 struct GlobalTaps {
     template <int H, int NL, int NR>
     __device__ __forceinline__ void load(const StepArgs &a, long long so, long long hrow, int col0, int j, float *xs,
@@ -169,12 +178,12 @@ struct GlobalTaps {
         const float *row = a.sxy + so + hrow + col0 - 4 * NL;
 #pragma unroll
         for (int v = 0; v < NL + 1 + NR; v++) {
-            float4 t = ld4(row + 4 * v);
+            float4 t = lds4<CG>(row + 4 * v);
             xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
         }
         const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * a.pitch + col0;
 #pragma unroll
-        for (int r = 0; r < 2 * H; r++) ys[r] = ld4(col + (long long)r * a.pitch);
+        for (int r = 0; r < 2 * H; r++) ys[r] = lds4<CG>(col + (long long)r * a.pitch);
     }
 };
 
@@ -198,7 +207,7 @@ struct SharedTaps {
     }
 };
 
-template <int FDO, int FLAGS, bool P2, class Taps = GlobalTaps>
+template <int FDO, int FLAGS, bool P2, class Taps = GlobalTaps<>, bool CG = false>
 __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, int j, int slot, int tile,
                                        const Taps &taps = Taps())
 {
@@ -216,7 +225,7 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
 
     /* ---- loads of data the preceding stress kernel does not write ---- */
     const float4 b4 = ldg4(a.brho + drow + col0);
-    float4 vy4 = ld4(a.vy + so + hrow + col0);
+    float4 vy4 = lds4<CG>(a.vy + so + hrow + col0);
     float4 g4, h4, f4;
     if (FLAGS & VF_CORR) g4 = ld4(a.grho + so + drow + col0);
     if (FLAGS & VF_HESS) h4 = ld4(a.hrho + so + drow + col0);
@@ -393,7 +402,7 @@ __global__ void __launch_bounds__(BX *BY, 3) v_step_st(StepArgs a, int nt_off)
  * All loads (taps, stresses, memory variables, coefficients, accumulators)
  * are issued before the first store.
  */
-template <int FDO, int L, int FLAGS>
+template <int FDO, int L, int FLAGS, bool CG = false>
 __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, int j, int slot)
 {
     constexpr int H = FDO / 2;
@@ -413,7 +422,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     /* ---- loads of data the preceding velocity kernel does not write ---- */
     float *sxy_p = a.sxy + so + hrow + col0;
     float *syz_p = a.syz + so + hrow + col0;
-    float4 sxy4 = ld4(sxy_p), syz4 = ld4(syz_p);
+    float4 sxy4 = lds4<CG>(sxy_p), syz4 = lds4<CG>(syz_p);
     float4 c1, c2;                           /* uip/ujp (elastic) or fipjp/f (visc) */
     float4 rr[LL], qq[LL], dip4[LL], d4[LL];
     float4 mi4, mj4, ti4, tj4;               /* muip, mujp, tausipjp, taus */
@@ -461,7 +470,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
         const float *row = a.vy + so + hrow + col0 - 4 * NL;
 #pragma unroll
         for (int v = 0; v < NL + 1 + NR; v++) {
-            float4 t = ld4(row + 4 * v);
+            float4 t = lds4<CG>(row + 4 * v);
             xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
         }
     }
@@ -469,7 +478,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     {
         const float *col = a.vy + so + (long long)(j - 1 + a.hy - H + 1) * pitch + col0;
 #pragma unroll
-        for (int r = 0; r < 2 * H; r++) ys[r] = ld4(col + (long long)r * pitch);
+        for (int r = 0; r < 2 * H; r++) ys[r] = lds4<CG>(col + (long long)r * pitch);
     }
 
     /* ---- derivatives and CPML ---- */

@@ -215,3 +215,24 @@ def test_unstable_model_reports_error():
     d2["dt"] = np.float32(2e-4)
     with engine_from(d2) as e:
         assert np.all(np.isfinite(e.forward(shots)[0]))
+
+
+@pytest.mark.parametrize("nx,ny", [(70, 40), (1100, 300)])
+def test_forward_persistent_and_pair_paths(nx, ny):
+    """Plain forward modelling takes the one-launch persistent kernel when all
+    tiles fit in one wave (70 x 40: 6 tiles) and the per-step kernel pair
+    otherwise (1100 x 300: 342 tiles); both are bit-identical to the oracle."""
+    d, shots = _case(500 + nx, nx=nx, ny=ny, nt=90, fdo=8, L=2, fs=1, fw=10)
+    m = oracle_model(d)
+    o = O.Oracle(m, "port")
+    ref = o.forward(shots[0].srcpos, shots[0].recpos)
+    o.close()
+    with engine_from(d) as e:
+        seis = e.forward(shots)[0]
+        st = e.stats()
+    assert np.array_equal(seis, ref)
+    tiles = ((nx + 127) // 128) * ((ny + 7) // 8)
+    if tiles <= 148:
+        assert st["kernel_launches"] <= 8      # one cooperative launch (+ counter, transpose)
+    else:
+        assert st["kernel_launches"] >= 2 * 90
