@@ -315,3 +315,32 @@ int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *src
     }
     return 0;
 }
+
+/* SPATFILTER=3 (src/gauss_filt.c:58-141): filter length and normalised
+ * kernel [n][n] (row jj, column ii), in the reference's float/double mix;
+ * the normalising sum starts at 0 (the reference leaves it uninitialised). */
+int dsh_setup_gauss_size(float wd_damp, float c_vs, float fc_end, float dh)
+{
+    const float lam = c_vs / fc_end;
+    int f = (int)round((wd_damp * lam) / dh);
+    if (f == 0) return 0;
+    if (!(f % 2)) f += f > 0 ? 1 : -1;
+    return f;
+}
+
+int dsh_setup_gauss_kernel(int filt, float *kernel)
+{
+    if (filt == 0 || !kernel) return -1;
+    const int hfs = abs(filt) / 2;
+    const float sigma = hfs / 2;
+    const float s = 2.0f * sigma * sigma;
+    const int n = 2 * hfs + 1;
+    float sum = 0.0f;
+    for (int ii = -hfs; ii <= hfs; ii++)
+        for (int jj = -hfs; jj <= hfs; jj++) {
+            kernel[(jj + hfs) * n + (ii + hfs)] = exp(-((ii * ii) / s) - ((jj * jj) / s));
+            sum += kernel[(jj + hfs) * n + (ii + hfs)];
+        }
+    for (int k = 0; k < n * n; k++) kernel[k] /= sum;
+    return 0;
+}

@@ -52,6 +52,12 @@ int dsh_setup_visc_base(int nx, int ny, int l, const float *fl, float dt, const 
 /* Source time functions (src/wavelet.c:26-84): out [nsrc][nt]. */
 int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *srcpos8, float *out);
 
+/* SPATFILTER=3 Gaussian gradient smoothing (src/gauss_filt.c): odd filter
+ * length round(WD_DAMP*(C_vs/FC_END)/DH), and its normalised kernel [n][n],
+ * n = 2*(|filt|/2)+1 (row jj, column ii). */
+int dsh_setup_gauss_size(float wd_damp, float c_vs, float fc_end, float dh);
+int dsh_setup_gauss_kernel(int filt, float *kernel);
+
 /* Largest stable DT of the staggered scheme (src/checkfd_ssg_elastic.c):
  * DH / (sqrt(2) * sum|hc| * vmax). */
 double dsh_setup_dt_limit(int fdorder, int maxrelerror, float dh, float vmax);

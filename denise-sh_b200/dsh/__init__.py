@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
         L.dsh_profile_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_residual_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]
+        L.dsh_smooth_gauss.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_gauss_filter_size.argtypes = [C.c_float] * 4
         L.dsh_profile_fused.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_get_shot_misfits.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.dsh_get_energy_sums.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -381,6 +383,22 @@ class Batch:
         return {"ms_total": s.ms_total, "kernel_launches": s.kernel_launches, "point_updates": s.point_updates,
                 "v_variant": s.v_variant, "s_variant": s.s_variant, "phases": s.phases,
                 "v_ms": list(s.v_ms)[:3], "s_ms": list(s.s_ms)[:3], "model_ms": ms}
+
+
+def smooth_gauss(grad, filt, stream=None):
+    """SPATFILTER=3 Gaussian smoothing of a [ny, nx] gradient on the GPU (dsh_smooth_gauss)."""
+    import torch
+
+    g = torch.from_numpy(np.ascontiguousarray(grad, np.float32)).cuda()
+    out = torch.empty_like(g)
+    ny, nx = g.shape
+    _check(lib().dsh_smooth_gauss(nx, ny, int(filt), g.data_ptr(), out.data_ptr(), stream), "dsh_smooth_gauss")
+    torch.cuda.synchronize()
+    return out.cpu().numpy()
+
+
+def gauss_filter_size(wd_damp, c_vs, fc_end, dh):
+    return int(lib().dsh_gauss_filter_size(wd_damp, c_vs, fc_end, dh))
 
 
 NOALLOC_MAX_SHOTS = 64

@@ -224,6 +224,15 @@ int dsh_get_shot_misfits(dsh_ctx *ctx, int nshots, double *out);
  * DSH_EPRECOND_ENERGY_ONLY; summed on the device, so no per-shot copies. */
 int dsh_get_energy_sums(dsh_ctx *ctx, float *ws_sum, float *wr_sum);
 
+/* Gradient smoothing SPATFILTER=3 (src/smooth_grad.c:27-29, src/gauss_filt.c):
+ * out = in convolved with the normalised Gaussian of the given odd filter
+ * length (dsh_gauss_filter_size: round(WD_DAMP*(C_vs/FC_END)/DH) made odd),
+ * edges replicated; device arrays [ny][nx], in != out, |filt| <= 45
+ * (0 copies).  The reference never initialises the kernel's normalising sum
+ * (src/gauss_filt.c:26,130); here it starts at 0. */
+int dsh_smooth_gauss(int nx, int ny, int filt, const float *in_dev, float *out_dev, void *stream);
+int dsh_gauss_filter_size(float wd_damp, float c_vs, float fc_end, float dh);
+
 /* Statistics of the last dsh_forward / dsh_gradient call. */
 typedef struct dsh_stats {
     double ms_forward, ms_adjoint, ms_total;   /* device time (CUDA events) */

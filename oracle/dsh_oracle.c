@@ -592,3 +592,59 @@ int dsho_psource(int nt, float *sxx, float *syy, int nsrc, const float *srcpos8,
     }
     return 0;
 }
+
+/* ---- SPATFILTER=3 Gaussian smoothing of a gradient (src/gauss_filt.c:58-160) ----
+ * Filter length FILT_SIZE_GRAD = round(WD_DAMP*lam/DH) with lam = C_vs/FC_END,
+ * made odd (:61-69); hfs = |filt|/2, sigma = hfs/2 in integer arithmetic, s =
+ * 2 sigma^2 (:71-73); the model is extended by replicating its edge rows and
+ * columns (:98-123); kernel exp(-(ii^2)/s - (jj^2)/s) normalised by its sum
+ * (:126-141; the reference never initialises that sum, here it starts at 0);
+ * conv summed in float with ii outer and jj inner (:144-157). */
+int dsho_gauss_filter_size(float wd_damp, float c_vs, float fc_end, float dh)
+{
+    const float lam = c_vs / fc_end;
+    int f = (int)round((wd_damp * lam) / dh);
+    if (f == 0) return 0;
+    if (!(f % 2)) f += f > 0 ? 1 : -1;
+    return f;
+}
+
+int dsho_gauss_kernel(int filt, float *kernel /* [filt][filt], row jj, column ii */)
+{
+    if (filt == 0) return -1;
+    const int hfs = abs(filt) / 2;
+    const float sigma = hfs / 2;
+    const float s = 2.0f * sigma * sigma;
+    const int n = 2 * hfs + 1;
+    float sum = 0.0f;
+    for (int ii = -hfs; ii <= hfs; ii++)
+        for (int jj = -hfs; jj <= hfs; jj++) {
+            kernel[(jj + hfs) * n + (ii + hfs)] = exp(-((ii * ii) / s) - ((jj * jj) / s));
+            sum += kernel[(jj + hfs) * n + (ii + hfs)];
+        }
+    for (int k = 0; k < n * n; k++) kernel[k] /= sum;
+    return 0;
+}
+
+int dsho_gauss_filt(int nx, int ny, int filt, const float *in /* [ny][nx] */, float *out)
+{
+    if (filt == 0) { memcpy(out, in, (size_t)nx * ny * sizeof(float)); return 0; }
+    const int hfs = abs(filt) / 2, n = 2 * hfs + 1;
+    float *k = (float *)malloc((size_t)n * n * sizeof(float));
+    if (!k) return -1;
+    dsho_gauss_kernel(filt, k);
+    for (int j = 1; j <= ny; j++)
+        for (int i = 1; i <= nx; i++) {
+            float conv = 0.0f;
+            for (int ii = -hfs; ii <= hfs; ii++)
+                for (int jj = -hfs; jj <= hfs; jj++) {
+                    int jy = j + jj, ix = i + ii;
+                    jy = jy < 1 ? 1 : jy > ny ? ny : jy;
+                    ix = ix < 1 ? 1 : ix > nx ? nx : ix;
+                    conv += in[(size_t)(jy - 1) * nx + (ix - 1)] * k[(jj + hfs) * n + (ii + hfs)];
+                }
+            out[(size_t)(j - 1) * nx + (i - 1)] = conv;
+        }
+    free(k);
+    return 0;
+}

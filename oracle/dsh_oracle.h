@@ -49,4 +49,8 @@ int dsho_convert(const float *wu, const float *wrho, float *g_vs, float *g_rho);
 int dsho_hessian_out(float *h_vs, float *h_rho);
 int dsho_psource(int nt, float *sxx, float *syy, int nsrc, const float *srcpos8, const float *signals);
 
+/* SPATFILTER=3 gradient smoothing (src/gauss_filt.c) */
+int dsho_gauss_filter_size(float wd_damp, float c_vs, float fc_end, float dh);
+int dsho_gauss_kernel(int filt, float *kernel);
+int dsho_gauss_filt(int nx, int ny, int filt, const float *in, float *out);
 #endif

@@ -257,3 +257,21 @@ class Oracle:
 
     def close(self):
         self._fn("free")()
+
+
+def gauss_filter_size(wd_damp, c_vs, fc_end, dh):
+    """SPATFILTER=3 filter length (src/gauss_filt.c:58-69), from the restatement."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdsh_oracle.so"))
+    lib.dsho_gauss_filter_size.argtypes = [C.c_float] * 4
+    return int(lib.dsho_gauss_filter_size(wd_damp, c_vs, fc_end, dh))
+
+
+def gauss_filt(grad, filt):
+    """SPATFILTER=3 Gaussian smoothing of a [ny, nx] gradient (src/gauss_filt.c), restatement."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdsh_oracle.so"))
+    g = _f32(grad)
+    out = np.empty_like(g)
+    ny, nx = g.shape
+    if lib.dsho_gauss_filt(nx, ny, int(filt), _ptr(g), _ptr(out)) != 0:
+        raise ValueError("gauss_filt failed")
+    return out
