@@ -22,22 +22,32 @@ namespace dsh {
 
 constexpr long long BARRIER_LIMIT = 1LL << 24;   /* polls of the generation word */
 
-/* count[0]: arrivals of the current barrier, count[1]: generation */
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+/* count[0]: arrivals of the current barrier, count[1]: generation.  The
+ * block barrier before thread 0's fence makes the block's stores part of its
+ * release (fences are cumulative); waiting threads poll the generation with
+ * acquire loads. */
 __device__ __forceinline__ bool grid_barrier(unsigned *count, int *status)
 {
     __shared__ int ok;
-    __threadfence();                 /* this thread's stores before the arrival */
     __syncthreads();
     if (threadIdx.x == 0 && threadIdx.y == 0) {
-        const unsigned g = atomicOr(count + 1, 0u);
+        const unsigned g = ld_acquire(count + 1);
         ok = 1;
+        __threadfence();
         if (atomicAdd(count, 1u) == gridDim.x - 1) {
             atomicExch(count, 0u);
             __threadfence();
             atomicAdd(count + 1, 1u);
         } else {
             long long it = 0;
-            while (atomicOr(count + 1, 0u) == g) {
+            while (ld_acquire(count + 1) == g) {
                 if (++it > BARRIER_LIMIT) { atomicOr(status, 2); ok = 0; break; }
             }
         }

@@ -1,6 +1,8 @@
 /*
- * dsh_post.cu — gradient post-processing on the device: the SPATFILTER=3
- * Gaussian smoothing of src/gauss_filt.c (src/smooth_grad.c:27-29).
+ * dsh_post.cu — processing around the gradient on the device: the
+ * SPATFILTER=3 Gaussian smoothing of src/gauss_filt.c (src/smooth_grad.c:27-29)
+ * and the Butterworth filtering of source signals and traces of the
+ * multi-scale workflow stages (src/timedomain_filt.c, libcseife).
  * Each output point sums the (2h+1)^2 taps of the edge-replicated gradient
  * in the reference's order (ii outer, jj inner) in FP32 without contraction,
  * so it is bit-identical to the reference's loop (with its normalising sum
@@ -41,7 +43,88 @@ __global__ void gauss_filt_kernel(int nx, int ny, int hfs, const __grid_constant
     }
 }
 
+struct IIRChain {
+    int n;
+    double c[9][5];                  /* f0, f1, f2, g1, g2 per section */
+};
+
+/* [ntr][ns] float -> [ns][ntr] double; the highpass first subtracts each
+ * trace's first sample (cseife.c:139-144) */
+__global__ void iir_load(const float *d, int ntr, int ns, int highpass, double *x)
+{
+    const long long total = (long long)ntr * ns;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(idx / ntr), t = (int)(idx % ntr);
+        double v = (double)d[(long long)t * ns + j];
+        if (highpass) v -= (double)d[(long long)t * ns];
+        x[idx] = v;
+    }
+}
+
+/* the recursive sections of one trace per thread (cseife_rekfl.c:62-73),
+ * in place, samples [ns][ntr] so neighbouring threads touch neighbouring words */
+__global__ void iir_run(double *x, int ntr, int ns, const __grid_constant__ IIRChain ch)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= ntr) return;
+    for (int s = 0; s < ch.n; s++) {
+        const double f0 = ch.c[s][0], f1 = ch.c[s][1], f2 = ch.c[s][2], g1 = ch.c[s][3], g2 = ch.c[s][4];
+        double xa = 0., xaa = 0., ya = 0., yaa = 0.;
+        for (int j = 0; j < ns; j++) {
+            double *p = x + (long long)j * ntr + t;
+            const double xn = *p;
+            const double y = f0 * xn + f1 * xa + f2 * xaa + g1 * ya + g2 * yaa;
+            *p = y;
+            xaa = xa;
+            xa = xn;
+            yaa = ya;
+            ya = y;
+        }
+    }
+}
+
+__global__ void iir_store(const double *x, int ntr, int ns, float *d)
+{
+    const long long total = (long long)ntr * ns;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(idx / ntr), t = (int)(idx % ntr);
+        d[(long long)t * ns + j] = (float)x[idx];
+    }
+}
+
 }  // namespace
+
+/* Butterworth filtering of traces (src/timedomain_filt.c with libcseife's
+ * seife_lpb / seife_hpb): data_dev [ntr][ns] float on the device, filtered in
+ * double like the reference and rounded back; method 1 lowpass, 2 highpass.
+ * compat = 1 reproduces the reference's indexing (it passes its 1-based
+ * vector as 0-based: a zero lead-in sample is filtered instead of the last
+ * one, which is returned unfiltered, and the highpass removes that zero
+ * instead of the first sample). */
+extern "C" int dsh_timedomain_filt(float *data_dev, int ntr, int ns, float dt, float fc, int order, int method,
+                                   int compat, void *stream)
+{
+    if (!data_dev || ntr < 1 || ns < 1 || (method != 1 && method != 2)) return DSH_ERR_PARAM;
+    IIRChain ch;
+    ch.n = dsh_setup_butterworth((double)dt, fc, order, method == 2, &ch.c[0][0]);
+    if (ch.n < 0) return DSH_ERR_PARAM;
+    const cudaStream_t st = (cudaStream_t)stream;
+    double *x = nullptr;
+    if (cudaMallocAsync(&x, (size_t)ntr * ns * sizeof(double), st) != cudaSuccess) return DSH_ERR_OOM;
+    const long long total = (long long)ntr * ns;
+    const int blocks = (int)((total + 255) / 256 < 148 * 16 ? (total + 255) / 256 : 148 * 16);
+    /* compat: samples 0 .. ns-2 are filtered (a zero lead-in with zero
+       filter state changes nothing), sample ns-1 stays, no offset removal */
+    const int nf = compat ? ns - 1 : ns;
+    iir_load<<<blocks, 256, 0, st>>>(data_dev, ntr, ns, method == 2 && !compat, x);
+    if (nf > 0) iir_run<<<(ntr + 127) / 128, 128, 0, st>>>(x, ntr, nf, ch);
+    iir_store<<<blocks, 256, 0, st>>>(x, ntr, ns, data_dev);
+    const cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(x, st);
+    return e == cudaSuccess ? DSH_OK : DSH_ERR_CUDA;
+}
 
 extern "C" int dsh_smooth_gauss(int nx, int ny, int filt, const float *in_dev, float *out_dev, void *stream)
 {

@@ -344,3 +344,39 @@ int dsh_setup_gauss_kernel(int filt, float *kernel)
     for (int k = 0; k < n * n; k++) kernel[k] /= sum;
     return 0;
 }
+
+/* Butterworth sections of libcseife (cseife.c:147-177, cseife_rfk.c) for
+ * timedomain_filt.c: period t0 = 1/fc, order m; an odd order adds a first
+ * order section first, then m/2 second-order sections with damping
+ * h_j = sin(pi/2 (2j-1)/m).  Each section: f0, f1, f2, g1, g2 (double). */
+int dsh_setup_butterworth(double dt, float fc, int order, int highpass, double *coef /* [max 9][5] */)
+{
+    if (order < 1 || order > 16 || !(fc > 0) || !(dt > 0)) return -1;
+    const double one = 1., two = 2., four = 4., eight = 8.;
+    const double T0 = 1.0 / fc;
+    const double t0 = T0 / dt;
+    const double zpi = eight * atan(one), eps = zpi / t0;
+    int n = 0;
+    const int mm = order / 2;
+    if (order > 2 * mm) {
+        double *c = coef + 5 * n++;
+        c[2] = 0.; c[4] = 0.;
+        c[3] = (two - eps) / (two + eps);
+        if (!highpass) { c[0] = eps / (two + eps); c[1] = c[0]; }
+        else { c[0] = two / (two + eps); c[1] = -(c[0]); }
+    }
+    const double pih = 2. * atan(1.);
+    for (int j = 1; j <= mm; ++j) {
+        const double h = sin(pih * (2 * j - 1) / order);
+        const double epsq = eps * eps;
+        const double a = one - eps * h + epsq / four;
+        const double b = -two + epsq / two;
+        const double c0 = one + eps * h + epsq / four;
+        double *c = coef + 5 * n++;
+        c[3] = -b / c0;
+        c[4] = -a / c0;
+        if (!highpass) { c[0] = epsq / four / c0; c[1] = c[0] + c[0]; c[2] = c[0]; }
+        else { c[0] = one / c0; c[1] = -(c[0]) - c[0]; c[2] = c[0]; }
+    }
+    return n;
+}

@@ -58,6 +58,10 @@ int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *src
 int dsh_setup_gauss_size(float wd_damp, float c_vs, float fc_end, float dh);
 int dsh_setup_gauss_kernel(int filt, float *kernel);
 
+/* Butterworth low-/highpass sections of timedomain_filt.c (libcseife):
+ * returns the number of sections written to coef [n][5] = f0 f1 f2 g1 g2. */
+int dsh_setup_butterworth(double dt, float fc, int order, int highpass, double *coef);
+
 /* Largest stable DT of the staggered scheme (src/checkfd_ssg_elastic.c):
  * DH / (sqrt(2) * sum|hc| * vmax). */
 double dsh_setup_dt_limit(int fdorder, int maxrelerror, float dh, float vmax);

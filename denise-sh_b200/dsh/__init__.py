@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
         L.dsh_profile_step.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_residual_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                            C.c_void_p, C.c_void_p]
+        L.dsh_timedomain_filt.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int,
+                                          C.c_int, C.c_void_p]
         L.dsh_smooth_gauss.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_gauss_filter_size.argtypes = [C.c_float] * 4
         L.dsh_profile_fused.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]

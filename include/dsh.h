@@ -233,6 +233,18 @@ int dsh_get_energy_sums(dsh_ctx *ctx, float *ws_sum, float *wr_sum);
 int dsh_smooth_gauss(int nx, int ny, int filt, const float *in_dev, float *out_dev, void *stream);
 int dsh_gauss_filter_size(float wd_damp, float c_vs, float fc_end, float dh);
 
+/* Butterworth filtering of traces or source signals (TIME_FILT stages;
+ * src/timedomain_filt.c with libcseife's seife_lpb/seife_hpb,
+ * src/denise.c:908-918,1056-1059): data_dev [ntr][ns] device floats,
+ * filtered in double by the reference's recursive sections (corner fc Hz,
+ * order 1..16; method 1 lowpass, 2 highpass) and rounded back to float.
+ * compat = 1 reproduces the reference's off-by-one (src/timedomain_filt.c:31,
+ * :42-45 pass its 1-based vector to 0-based libcseife: the last sample is
+ * returned unfiltered and the highpass removes a zero, not the first sample);
+ * compat = 0 filters all ns samples as libcseife intends. */
+int dsh_timedomain_filt(float *data_dev, int ntr, int ns, float dt, float fc, int order, int method, int compat,
+                        void *stream);
+
 /* Statistics of the last dsh_forward / dsh_gradient call. */
 typedef struct dsh_stats {
     double ms_forward, ms_adjoint, ms_total;   /* device time (CUDA events) */

@@ -275,3 +275,13 @@ def gauss_filt(grad, filt):
     if lib.dsho_gauss_filt(nx, ny, int(filt), _ptr(g), _ptr(out)) != 0:
         raise ValueError("gauss_filt failed")
     return out
+
+
+def timedomain_filt(data, dt, fc, order, method):
+    """The reference's Butterworth trace filter (src/timedomain_filt.c + libcseife), data [ntr, ns]."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_timedomain_filt.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_int, C.c_int]
+    d = _f32(data).copy()
+    ntr, ns = d.shape
+    lib.refh_timedomain_filt(d.ctypes.data, ntr, ns, dt, fc, order, method)
+    return d

@@ -696,3 +696,23 @@ int refh_write_su(const char *path, int ntr, int ns, const float *section, const
     free_imatrix(rp, 1, 3, 1, ntr);
     return 0;
 }
+
+/* The reference's Butterworth filtering of traces (timedomain_filt.c with
+ * libcseife's seife_lpb / seife_hpb), on dense data [ntr][ns]. */
+void timedomain_filt(float **data, float fc, int order, int ntr, int ns, int method);
+int refh_timedomain_filt(float *data, int ntr, int ns, float dt, float fc, int order, int method)
+{
+    float **d = matrix(1, ntr, 1, ns);
+    int t, j;
+    for (t = 1; t <= ntr; t++) for (j = 1; j <= ns; j++) d[t][j] = data[(t - 1) * ns + j - 1];
+    DT = dt;
+    /* timedomain_filt hands libcseife its 1-based dvector as a 0-based array,
+     * so element 0 of that allocation (never initialised) is filtered as the
+     * first sample; releasing a zeroed block of the same size first makes the
+     * allocator hand that block back, so the element is 0 as in a fresh process */
+    free(calloc((size_t)ns + 1, sizeof(double)));
+    timedomain_filt(d, fc, order, ntr, ns, method);
+    for (t = 1; t <= ntr; t++) for (j = 1; j <= ns; j++) data[(t - 1) * ns + j - 1] = d[t][j];
+    free_matrix(d, 1, ntr, 1, ns);
+    return 0;
+}
