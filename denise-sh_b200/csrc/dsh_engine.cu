@@ -942,11 +942,14 @@ static int get_graph(dsh_ctx *ctx, Pass pass, int nb, int K, cudaGraphExec_t *ou
 }
 
 /* Small grids, plain forward modelling: the whole pass in one cooperative
- * launch of persist_fwd when all tiles of all slots fit in one wave
- * (DSH_PERSIST=0 turns it off).  Returns the grid size, 0 when not used. */
+ * launch of persist_fwd when all tiles of all slots fit in one wave.  Opt-in
+ * (DSH_PERSIST=1): on the 500 x 200 FDORDER 4 case it measured 16.8 us per
+ * step against 12.5 us for the graph-replayed kernel pair — two bounded grid
+ * barriers per step cost more than the two launches they replace.  Returns
+ * the grid size, 0 when not used. */
 static int persistent_grid(dsh_ctx *ctx, Pass pass, int nb)
 {
-    static const bool on = []() { const char *e = getenv("DSH_PERSIST"); return !e || atoi(e) != 0; }();
+    static const bool on = []() { const char *e = getenv("DSH_PERSIST"); return e && atoi(e) != 0; }();
     const dsh_params &p = ctx->p;
     if (!on || pass != P_FWD_PLAIN || !ctx->fused_inject || p.fdorder > 8) return 0;
     PFn fk = pf_kernel(p.fdorder, p.l, dh_pow2(p.dh));
@@ -1434,6 +1437,11 @@ extern "C" int dsh_profile_fused(dsh_ctx *ctx, int pass, int nsteps, float *out_
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
+    {   /* one untimed launch first (lazy module loading) */
+        int off = 0;
+        void *args[2] = {&sa, &off};
+        CK(cudaLaunchKernel((const void *)fk, grid, dim3(256), args, 0, ctx->st));
+    }
     CK(cudaEventRecord(e0, ctx->st));
     for (int k = 0; k < nsteps; k++) {
         int off = k;
@@ -1516,6 +1524,14 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
     cudaEvent_t ev[6];
     for (auto &e : ev) CK(cudaEventCreate(&e));
     set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, 1);
+    {   /* one untimed launch of each kernel first (lazy module loading) */
+        int off = 0;
+        void *args[2] = {&sa, &off};
+        void *iargs[2] = {&ia, &off};
+        CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
+        if (!sa.tl.on) CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
+        CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
+    }
     for (int q = 0; q < 3; q++) {
         CK(cudaEventRecord(ev[2 * q], ctx->st));
         for (int k = 0; k < nsteps; k++) {

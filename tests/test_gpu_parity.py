@@ -9,6 +9,8 @@ multiple of the 4-point vector width, and multi-shot batches.  The L2 misfit
 is summed in double on the device while the reference adds its n terms one by
 one in float, so it is compared within the float summation bound
 (n-1)*2^-24 relative (non-negative terms)."""
+import os
+
 import numpy as np
 import pytest
 
@@ -219,9 +221,10 @@ def test_unstable_model_reports_error():
 
 @pytest.mark.parametrize("nx,ny", [(70, 40), (1100, 300)])
 def test_forward_persistent_and_pair_paths(nx, ny):
-    """Plain forward modelling takes the one-launch persistent kernel when all
-    tiles fit in one wave (70 x 40: 6 tiles) and the per-step kernel pair
-    otherwise (1100 x 300: 342 tiles); both are bit-identical to the oracle."""
+    """With DSH_PERSIST=1 (set for the GPU test run), plain forward modelling
+    takes the one-launch persistent kernel when all tiles fit in one wave
+    (70 x 40: 5 tiles) and the per-step kernel pair otherwise (1100 x 300:
+    342 tiles); both are bit-identical to the oracle."""
     d, shots = _case(500 + nx, nx=nx, ny=ny, nt=90, fdo=8, L=2, fs=1, fw=10)
     rec = shots[0].recpos.copy()
     rec[1] = np.clip(rec[1], 1, ny)              # all receivers inside the grid: fused sampling lists
@@ -235,7 +238,23 @@ def test_forward_persistent_and_pair_paths(nx, ny):
         st = e.stats()
     assert np.array_equal(seis, ref)
     tiles = ((nx + 127) // 128) * ((ny + 7) // 8)
-    if tiles <= 148:
+    if tiles <= 148 and os.environ.get("DSH_PERSIST") == "1":
         assert st["kernel_launches"] <= 8      # one cooperative launch (+ counter, transpose)
     else:
         assert st["kernel_launches"] >= 2 * 90
+
+
+def test_persistent_forward_in_subprocess():
+    """The opt-in persistent kernel (DSH_PERSIST=1 is read once per process,
+    so it runs in a child process): one cooperative launch for the whole
+    forward pass, bit-identical to the oracle."""
+    import subprocess
+    import sys
+
+    env = dict(os.environ, DSH_PERSIST="1")
+    code = ("import sys; sys.argv=['x']; import pytest; "
+            "sys.exit(pytest.main(['-q', '-p', 'no:cacheprovider', '-m', 'gpu', "
+            "'tests/test_gpu_parity.py::test_forward_persistent_and_pair_paths']))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
