@@ -25,6 +25,12 @@ namespace dsh {
 constexpr int HX = 8;            /* left halo / alignment columns */
 constexpr int BX = 32;           /* threads per block along x (4 points each) */
 constexpr int BY = 8;            /* threads per block along depth */
+#ifndef SSTEP_MIN_BLOCKS
+#define SSTEP_MIN_BLOCKS 2       /* resident stress-kernel blocks per SM the register budget targets */
+#endif
+#ifndef VSTEP_MIN_BLOCKS
+#define VSTEP_MIN_BLOCKS 3       /* resident velocity-kernel blocks per SM the register budget targets */
+#endif
 
 /* flags of the velocity kernel */
 constexpr int VF_ADJOINT = 1;    /* sw=1: vyp1 = old vy (update_v_PML.c:189-192) */
@@ -345,7 +351,7 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
 
 /* one thread block = 128 x 8 points of one shot slot (grid z) */
 template <int FDO, int FLAGS, bool P2>
-__global__ void __launch_bounds__(BX *BY, 3) v_step(StepArgs a, int nt_off)
+__global__ void __launch_bounds__(BX *BY, VSTEP_MIN_BLOCKS) v_step(StepArgs a, int nt_off)
 {
     v_body<FDO, FLAGS, P2>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
                            blockIdx.z, blockIdx.y * gridDim.x + blockIdx.x);
@@ -639,7 +645,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
 
 /* one thread block = 128 x 8 points of one shot slot (grid z) */
 template <int FDO, int L, int FLAGS>
-__global__ void __launch_bounds__(BX *BY, 2) s_step(StepArgs a, int nt_off)
+__global__ void __launch_bounds__(BX *BY, SSTEP_MIN_BLOCKS) s_step(StepArgs a, int nt_off)
 {
     s_body<FDO, L, FLAGS>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
                           blockIdx.z);
