@@ -324,6 +324,8 @@ def main():
     eng = dsh.Engine(params, device=local)
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
+    eng.set_model(cfg["vs"], cfg["rho"], cfg["qs"])
+    variant, variant_ms = eng.autotune(shots, nsteps=min(64, nt))   # step-kernel variant for this grid
 
     seis = torch.empty(ntr_all * nt, device="cuda", dtype=torch.float32)
     if gradient:
@@ -484,6 +486,7 @@ def main():
             "dtype": "f32", "data": "synthetic",
             "config": {"workload": f"{label}-nt{nt}", "nx": nx, "ny": ny, "nt": nt, "fdorder": fdo, "l": L,
                        "shots_per_gpu": nsh, "receivers": shots[0].ntr, "parallelism": f"shots{world}",
+                       "step_variant": variant, "autotune_ms_per_step": variant_ms,
                        "checkpoint_interval": ckpt, "storage_gb": storage / 1e9, "l2": l2note},
             "roofline": {"bound": "hbm", "achieved": s_gbs, "peak": hbm, "unit": "GB/s", "frac": s_gbs / hbm,
                          "traffic": traffic, "kernel": kname, "bytes_per_point": ks, "ms_per_launch": kms,

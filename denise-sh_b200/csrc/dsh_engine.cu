@@ -816,9 +816,16 @@ InjectArgs inject_args(dsh_ctx *ctx, Pass pass)
  * v_step_st, which measured slower on B200 (19.2 vs 14.7 us per launch at
  * 2000 x 800, FDORDER 8: the block-wide staging and barrier cost more than the
  * L1 hits they replace). */
-static KFn pick_v(int fdo, int vflags, bool p2)
+static int env_flag(const char *name)
 {
-    static const bool staged = []() { const char *e = getenv("DSH_VSTAGE"); return e && atoi(e) != 0; }();
+    const char *e = getenv(name);
+    return e && atoi(e) != 0;
+}
+
+static KFn pick_v(const dsh_ctx *ctx, int fdo, int vflags, bool p2)
+{
+    static const int env = env_flag("DSH_VSTAGE");
+    const bool staged = ctx->sel_staged >= 0 ? ctx->sel_staged != 0 : env != 0;
     KFn k = staged ? v_kernel_st(fdo, vflags, p2) : nullptr;
     return k ? k : v_kernel(fdo, vflags, p2);
 }
@@ -828,7 +835,8 @@ static KFn pick_v(int fdo, int vflags, bool p2)
  * DSH_FUSED=0 selects the velocity + stress kernel pair instead. */
 static bool use_fused(dsh_ctx *ctx, Pass pass)
 {
-    static const bool on = []() { const char *e = getenv("DSH_FUSED"); return e && atoi(e) != 0; }();
+    static const int env = env_flag("DSH_FUSED");
+    const bool on = ctx->sel_fused >= 0 ? ctx->sel_fused != 0 : env != 0;
     return on && ctx->fused_ok && ctx->fused_inject && pass != P_FWD_HESS;
 }
 
@@ -879,7 +887,7 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
     case P_FWD_CKPT: break;
     case P_RECOMP: sflags = SF_STRAIN_OUT; break;
     }
-    KFn vk = pick_v(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
+    KFn vk = pick_v(ctx, p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
     StepArgs sa = step_args(ctx, pass);
     InjectArgs ia = inject_args(ctx, pass);
@@ -921,9 +929,10 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
 
 static int get_graph(dsh_ctx *ctx, Pass pass, int nb, int K, cudaGraphExec_t *out)
 {
+    const long long staged = pick_v(ctx, ctx->p.fdorder, 0, dh_pow2(ctx->p.dh)) != v_kernel(ctx->p.fdorder, 0, dh_pow2(ctx->p.dh));
     const long long key = ((long long)pass << 48) | ((long long)ctx->fused_inject << 47) |
-                          ((long long)use_fused(ctx, pass) << 46) | ((long long)K << 32) | ((long long)nb << 16) |
-                          (long long)(ctx->geo_version & 0xffff);
+                          ((long long)use_fused(ctx, pass) << 46) | (staged << 45) | ((long long)K << 32) |
+                          ((long long)nb << 16) | (long long)(ctx->geo_version & 0xffff);
     auto it = ctx->graphs.find(key);
     if (it != ctx->graphs.end()) { *out = it->second; return DSH_OK; }
     cudaGraph_t g;
@@ -949,7 +958,8 @@ static int get_graph(dsh_ctx *ctx, Pass pass, int nb, int K, cudaGraphExec_t *ou
  * the grid size, 0 when not used. */
 static int persistent_grid(dsh_ctx *ctx, Pass pass, int nb)
 {
-    static const bool on = []() { const char *e = getenv("DSH_PERSIST"); return e && atoi(e) != 0; }();
+    static const int env = env_flag("DSH_PERSIST");
+    const bool on = ctx->sel_persist >= 0 ? ctx->sel_persist != 0 : env != 0;
     const dsh_params &p = ctx->p;
     if (!on || pass != P_FWD_PLAIN || !ctx->fused_inject || p.fdorder > 8) return 0;
     PFn fk = pf_kernel(p.fdorder, p.l, dh_pow2(p.dh));
@@ -1419,6 +1429,59 @@ extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
     return DSH_OK;
 }
 
+/* Times plain forward steps of each step-kernel variant the context can run
+ * on these shots — kernel pair (v_step), pair with v_step_st, fused step,
+ * persistent launch — and keeps the fastest for the context's later calls
+ * (the fused choice also serves the gradient passes, the persistent one only
+ * plain forward modelling).  ms_per_step[4] (optional): mean device ms per
+ * step of each variant, 0 where it does not apply. */
+extern "C" int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int nsteps, float *ms_per_step,
+                            int *choice)
+{
+    if (!ctx || !shots || nshots < 1 || nsteps < 1) return DSH_ERR_PARAM;
+    if (!ctx->model_set) return DSH_ERR_STATE;
+    CK(cudaSetDevice(ctx->dev));
+    const int nb = std::min(ctx->S, nshots);
+    int rc = upload_batch(ctx, shots, nb, nullptr, nullptr, 0);
+    if (rc != DSH_OK) return rc;
+    nsteps = std::min(nsteps, ctx->p.nt);
+    const int sel[4][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};   /* staged, fused, persistent */
+    float ms[4] = {0, 0, 0, 0};
+    int best = 0;
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int v = 0; v < 4; v++) {
+        ctx->sel_staged = sel[v][0];
+        ctx->sel_fused = sel[v][1];
+        ctx->sel_persist = sel[v][2];
+        drop_graphs(ctx);                              /* graphs hold the previous variant's kernels */
+        if (v == 2 && !use_fused(ctx, P_FWD_PLAIN)) continue;
+        if (v == 3 && !persistent_grid(ctx, P_FWD_PLAIN, nb)) continue;
+        for (int rep = 0; rep < 2; rep++) {            /* first round warms up (graphs, lazy loading) */
+            if ((rc = zero_slots(ctx, nb, false)) != DSH_OK) break;
+            CK(cudaEventRecord(e0, ctx->st));
+            if ((rc = run_steps(ctx, P_FWD_PLAIN, nb, 1, nsteps)) != DSH_OK) break;
+            CK(cudaEventRecord(e1, ctx->st));
+        }
+        if (rc != DSH_OK) break;
+        CK(cudaEventSynchronize(e1));
+        cudaEventElapsedTime(&ms[v], e0, e1);
+        ms[v] /= nsteps;
+        if (ms[v] < ms[best]) best = v;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->sel_staged = sel[best][0];
+    ctx->sel_fused = sel[best][1];
+    ctx->sel_persist = sel[best][2];
+    drop_graphs(ctx);
+    if (ms_per_step) for (int v = 0; v < 4; v++) ms_per_step[v] = ms[v];
+    if (choice) *choice = best;
+    if (rc != DSH_OK) return rc;
+    return check_status(ctx);
+}
+
 extern "C" int dsh_profile_fused(dsh_ctx *ctx, int pass, int nsteps, float *out_ms)
 {
     if (!ctx || !out_ms || pass < 0 || pass > 3 || pass == P_FWD_HESS || nsteps < 1 || nsteps > ctx->p.nt)
@@ -1514,7 +1577,7 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
     if (pass == P_FWD_STORE) sflags = SF_STRAIN_OUT;
     if (pass == P_FWD_HESS) { vflags = VF_HESS; sflags = SF_HESS; }
     if (pass == P_ADJ) { vflags = VF_ADJOINT | VF_CORR; sflags = SF_CORR; }
-    KFn vk = pick_v(p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
+    KFn vk = pick_v(ctx, p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
     StepArgs sa = step_args(ctx, (Pass)pass);
     InjectArgs ia = inject_args(ctx, (Pass)pass);

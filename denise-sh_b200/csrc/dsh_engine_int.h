@@ -27,6 +27,8 @@ struct dsh_ctx {
     long long o_vy_b = 0, o_sxy_b = 0, o_syz_b = 0, o_pvxx_b = 0, o_pvyy_b = 0;   /* fused step's second buffers */
     int fused_ok = 0;                     /* FDORDER <= 8: the fused step kernel can run this context */
     int state_b = 0;                      /* the slab's current state is in the second buffers */
+    int sel_staged = -1, sel_fused = -1, sel_persist = -1;   /* step-kernel variants chosen by dsh_autotune
+                                                               (-1: the DSH_VSTAGE / DSH_FUSED / DSH_PERSIST defaults) */
     float *slab = nullptr;
     float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho */
     float *m_brho, *m_uip, *m_ujp, *m_muip, *m_mujp, *m_tip, *m_taus, *m_vs, *m_rho;

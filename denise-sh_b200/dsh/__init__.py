@@ -92,6 +92,7 @@ def lib() -> C.CDLL:
                                           C.c_int, C.c_void_p]
         L.dsh_smooth_gauss.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_gauss_filter_size.argtypes = [C.c_float] * 4
+        L.dsh_autotune.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
         L.dsh_profile_fused.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_get_shot_misfits.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.dsh_get_energy_sums.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -283,6 +284,16 @@ class Engine:
         out = np.zeros(3, np.float32)
         _check(lib().dsh_profile_step(self.h, self.PASSES[pass_name], nsteps, out.ctypes.data), "dsh_profile_step")
         return {"v_step": float(out[0]), "inject_sample": float(out[1]), "s_step": float(out[2])}
+
+    VARIANTS = ("kernel pair", "kernel pair, staged velocity taps", "fused step", "persistent launch")
+
+    def autotune(self, shots, nsteps=64):
+        """Times each step-kernel variant on these shots, keeps the fastest; returns (name, ms per step each)."""
+        ms = np.zeros(4, np.float32)
+        ch = C.c_int(0)
+        _check(lib().dsh_autotune(self.h, _shots_c(list(shots)), len(shots), nsteps, ms.ctypes.data, C.byref(ch)),
+               "dsh_autotune")
+        return self.VARIANTS[ch.value], {n: float(t) for n, t in zip(self.VARIANTS, ms)}
 
     def profile_fused(self, pass_name: str, nsteps: int):
         """Mean device ms per launch of the fused step kernel, or None when it does not serve this pass."""

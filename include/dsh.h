@@ -149,6 +149,15 @@ int dsh_set_stream(dsh_ctx *ctx, void *stream);
  * wavefield state, which is rebuilt by the next call. */
 int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
 
+/* Step-kernel autotuner: times nsteps plain forward steps of every variant
+ * this context can run on these shots (0 kernel pair, 1 pair with the
+ * shared-memory staged velocity kernel, 2 fused velocity+stress step,
+ * 3 one persistent launch per pass for grids that fit one wave), keeps the
+ * fastest for the context's later calls and reports ms_per_step[4] (0 where a
+ * variant does not apply) and *choice.  Results do not depend on the choice
+ * (all variants are bit-identical). */
+int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int nsteps, float *ms_per_step, int *choice);
+
 /* The same for the fused step kernel (one launch per time step; used when
  * FDORDER <= 8, injection/sampling positions lie inside the grid and
  * DSH_FUSED is set): mean ms per launch in *out_ms; DSH_ERR_STATE when the

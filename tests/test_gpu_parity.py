@@ -258,3 +258,26 @@ def test_persistent_forward_in_subprocess():
     root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+
+
+def test_autotune_picks_a_variant_and_keeps_parity():
+    """dsh_autotune times every applicable step-kernel variant and keeps the
+    fastest; forward and gradient afterwards are still bit-identical."""
+    d, shots = _case(611, nx=70, ny=40, nt=120, fdo=8, L=2, fs=1, fw=10)
+    rec = shots[0].recpos.copy()
+    rec[1] = np.clip(rec[1], 1, d["ny"])
+    shots = [dsh.Shot(shots[0].srcpos, rec)]
+    m = oracle_model(d)
+    o = O.Oracle(m, "port")
+    seis_ref = o.forward(shots[0].srcpos, shots[0].recpos)
+    o.close()
+    obs = [(seis_ref * np.float32(0.9)).astype(np.float32)]
+    gv, gr, l2, _ = _oracle_gradient(d, shots, obs)
+    with engine_from(d) as e:
+        name, ms = e.autotune(shots, nsteps=40)
+        assert name in dsh.Engine.VARIANTS
+        assert ms["kernel pair"] > 0 and ms["fused step"] > 0 and ms["persistent launch"] > 0
+        assert ms[name] == min(t for t in ms.values() if t > 0)
+        assert np.array_equal(e.forward(shots)[0], seis_ref)
+        out = e.gradient(shots, obs)
+    assert np.array_equal(out["g_vs"], gv) and np.array_equal(out["g_rho"], gr)
