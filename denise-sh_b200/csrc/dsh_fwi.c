@@ -18,10 +18,8 @@ int dsh_lbfgs_direction(long long n, int count, const float *S, const float *Y, 
 {
     if (n <= 0 || count < 0 || !q || !r || (count > 0 && (!S || !Y)) || count > 64) return -1;
     double alpha[64], rho[64];
-    double *w = NULL;
     for (long long i = 0; i < n; i++) r[i] = q[i];
     if (count == 0) return 0;
-    (void)w;
     for (int k = 0; k < count; k++) {
         const double ys = dot(n, Y + (long long)k * n, S + (long long)k * n);
         rho[k] = fabs(ys) > 0.0 ? 1.0 / ys : 0.0;
@@ -42,6 +40,39 @@ int dsh_lbfgs_direction(long long n, int count, const float *S, const float *Y, 
         const float *s = S + (long long)k * n, *y = Y + (long long)k * n;
         const double beta = rho[k] * dot(n, y, r);
         for (long long i = 0; i < n; i++) r[i] = (float)((double)r[i] + (double)s[i] * (alpha[k] - beta));
+    }
+    return 0;
+}
+
+int dsh_pcg_direction(long long n, int nclass, const float *g_new, const float *g_old, float *dir, int beta_kind,
+                      float *beta_out)
+{
+    if (n <= 0 || nclass < 1 || nclass > DSH_PCG_MAX_CLASSES || !g_new || !g_old || !dir || beta_kind < 1 ||
+        beta_kind > 4)
+        return -1;
+    float beta[DSH_PCG_MAX_CLASSES];
+    /* beta per class from float sums in vector order (src/PCG.c:25-83) */
+    for (int k = 0; k < nclass; k++) {
+        const float *a = g_new + (long long)k * n, *b = g_old + (long long)k * n, *d = dir + (long long)k * n;
+        float num = 0.0f, den = 0.0f;
+        for (long long i = 0; i < n; i++) {
+            switch (beta_kind) {
+            case 1: num += a[i] * a[i]; den += b[i] * b[i]; break;                    /* Fletcher-Reeves */
+            case 2: num += a[i] * (a[i] - b[i]); den += b[i] * b[i]; break;           /* Polak-Ribiere */
+            case 3: num += -a[i] * (a[i] - b[i]); den += d[i] * (a[i] - b[i]); break; /* Hestenes-Stiefel */
+            default: num += -a[i] * a[i]; den += d[i] * (a[i] - b[i]); break;         /* Dai-Yuan */
+            }
+        }
+        beta[k] = 0.0f;
+        if (den != 0.0f) beta[k] = num / den;
+        if (beta_kind == 2 && beta[k] < 0.0f) beta[k] = 0.0f;                     /* direction reset */
+        if (beta_out) beta_out[k] = beta[k];
+    }
+    /* new conjugate direction (src/PCG.c:88-102) */
+    for (int k = 0; k < nclass; k++) {
+        const float *a = g_new + (long long)k * n;
+        float *d = dir + (long long)k * n;
+        for (long long i = 0; i < n; i++) d[i] = a[i] + beta[k] * d[i];
     }
     return 0;
 }

@@ -31,6 +31,8 @@ def _setup():
     L = lib()
     if not getattr(L, "_fwi_ready", False):
         L.dsh_lbfgs_direction.argtypes = [C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_pcg_direction.argtypes = [C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                        C.c_void_p]
         L.dsh_opt_step.restype = C.c_float
         L.dsh_opt_step.argtypes = [C.c_void_p, C.c_void_p]
         L.dsh_line_search_init.argtypes = [C.POINTER(LineSearch), C.c_float, C.c_float, C.c_float, C.c_int]
@@ -51,6 +53,27 @@ def lbfgs_direction(S, Y, q):
                                         Y.ctypes.data if count else None, q.ctypes.data, r.ctypes.data),
            "dsh_lbfgs_direction")
     return r
+
+
+PCG_BETA = {"fletcher_reeves": 1, "polak_ribiere": 2, "hestenes_stiefel": 3, "dai_yuan": 4}
+
+
+def pcg_direction(g_new, g_old, direction, beta="polak_ribiere"):
+    """Conjugate-gradient direction (src/PCG.c): g_new, g_old, direction are
+    [nclass][...] arrays (one parameter class per leading index, e.g. vs and
+    rho); returns (new direction, beta per class).  The reference stores each
+    class x-major (src/store_PCG_SH.c), so pass the [ny][nx] fields transposed
+    to reproduce its float sums bit for bit."""
+    a = np.ascontiguousarray(g_new, np.float32)
+    b = np.ascontiguousarray(g_old, np.float32)
+    d = np.array(direction, np.float32, order="C", copy=True)
+    if a.shape != b.shape or a.shape != d.shape or a.ndim < 1:
+        raise ValueError("g_new, g_old and direction must have one shape [nclass][...]")
+    nclass = a.shape[0]
+    betas = np.zeros(nclass, np.float32)
+    _check(_setup().dsh_pcg_direction(a.size // nclass, nclass, a.ctypes.data, b.ctypes.data, d.ctypes.data,
+                                      PCG_BETA[beta], betas.ctypes.data), "dsh_pcg_direction")
+    return d, betas
 
 
 def opt_step(L2t, epst):

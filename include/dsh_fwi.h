@@ -5,6 +5,8 @@
  *                         pairs of model and gradient differences stored as
  *                         src/store_LBFGS_SH.c does (gradient x C_vs,
  *                         model / C_vs)
+ *   dsh_pcg_direction     conjugate-gradient direction update per
+ *                         parameter class (src/PCG.c:10-107)
  *   dsh_opt_step          step length from three test misfits: the extremum
  *                         of the parabola through them with the reference's
  *                         guards (src/calc_opt_step.c:20-111)
@@ -23,6 +25,24 @@ extern "C" {
  * Hessian; rho_k = 1/(y_k.s_k), or 0 when y_k.s_k = 0.  count = 0 gives r = q.
  * Dot products in double. */
 int dsh_lbfgs_direction(long long n, int count, const float *S, const float *Y, const float *q, float *r);
+
+/* Conjugate-gradient direction (src/PCG.c:10-107, called at
+ * src/denise.c:1850-1871 on the steepest-descent directions of vs and rho):
+ * the vectors hold nclass parameter classes of n values each, class after
+ * class, in the caller's point order (the reference stores each class x-major,
+ * src/store_PCG_SH.c).  Per class, beta = num/den from float sums taken in
+ * vector order, 0 when den = 0:
+ *   beta_kind 1 Fletcher-Reeves   num = g_new.g_new          den = g_old.g_old
+ *             2 Polak-Ribiere     num = g_new.(g_new-g_old)  den = g_old.g_old,
+ *                                 beta < 0 reset to 0 (the reference's setting,
+ *                                 PCG_BETA = 2 at src/PCG.c:17)
+ *             3 Hestenes-Stiefel  num = -g_new.(g_new-g_old) den = dir.(g_new-g_old)
+ *             4 Dai-Yuan          num = -g_new.g_new         den = dir.(g_new-g_old)
+ * then dir = g_new + beta*dir in place.  beta_out (nclass floats) may be NULL.
+ * Returns 0, or -1 for invalid arguments (nclass outside 1..DSH_PCG_MAX_CLASSES). */
+#define DSH_PCG_MAX_CLASSES 8
+int dsh_pcg_direction(long long n, int nclass, const float *g_new, const float *g_old, float *dir, int beta_kind,
+                      float *beta_out);
 
 /* epst[0..2], L2t[0..2]: test step lengths (epst[0] = 0) and their misfits */
 float dsh_opt_step(const float L2t[3], const float epst[3]);

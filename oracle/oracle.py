@@ -285,3 +285,44 @@ def timedomain_filt(data, dt, fc, order, method):
     ntr, ns = d.shape
     lib.refh_timedomain_filt(d.ctypes.data, ntr, ns, dt, fc, order, method)
     return d
+
+
+def pcg(g_new, g_old, dir, nx, ny):
+    """The reference's PCG direction update (src/PCG.c, Polak-Ribiere with
+    reset): vectors of nclass*nx*ny floats, each class x-major as
+    src/store_PCG_SH.c stores it.  Returns the new direction."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_pcg.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    a, b = _f32(g_new).ravel(), _f32(g_old).ravel()
+    d = _f32(dir).ravel().copy()
+    nclass = a.size // (nx * ny)
+    lib.refh_pcg(nx, ny, nclass, a.ctypes.data, b.ctypes.data, d.ctypes.data)
+    return d
+
+
+def pcg_port(g_new, g_old, dir, nclass, beta_kind):
+    """Restatement of src/PCG.c:25-102 for every beta choice (the reference
+    compiles only Polak-Ribiere): float32 sums in vector order, one Python
+    step per element, so only for small vectors."""
+    f = np.float32
+    a = _f32(g_new).ravel().reshape(nclass, -1)
+    b = _f32(g_old).ravel().reshape(nclass, -1)
+    d = _f32(dir).ravel().reshape(nclass, -1).copy()
+    betas = []
+    for k in range(nclass):
+        num, den = f(0), f(0)
+        for x, y, z in zip(a[k], b[k], d[k]):
+            if beta_kind == 1:
+                num, den = f(num + x * x), f(den + y * y)
+            elif beta_kind == 2:
+                num, den = f(num + x * f(x - y)), f(den + y * y)
+            elif beta_kind == 3:
+                num, den = f(num + f(-x) * f(x - y)), f(den + z * f(x - y))
+            else:
+                num, den = f(num + f(-x) * x), f(den + z * f(x - y))
+        beta = f(num / den) if den != 0 else f(0)
+        if beta_kind == 2 and beta < 0:
+            beta = f(0)
+        betas.append(beta)
+        d[k] = a[k] + beta * d[k]
+    return d.ravel(), np.array(betas, np.float32)

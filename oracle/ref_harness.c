@@ -716,3 +716,22 @@ int refh_timedomain_filt(float *data, int ntr, int ns, float dt, float fc, int o
     free_matrix(d, 1, ntr, 1, ns);
     return 0;
 }
+
+/* The reference's conjugate-gradient direction update (src/PCG.c, which fixes
+ * PCG_BETA = 2, Polak-Ribiere with reset) on nclass classes of nx*ny values,
+ * in the order src/store_PCG_SH.c stores them; dir is updated in place and
+ * the reference's 1-based vectors are filled from and copied back to it. */
+void PCG(float *PCG_new, float *PCG_old, float *PCG_dir, int PCG_class);
+int refh_pcg(int nx, int ny, int nclass, const float *g_new, const float *g_old, float *dir)
+{
+    const int n = nclass * nx * ny, nx0 = NX, ny0 = NY, idx0 = IDX, idy0 = IDY, myid0 = MYID;
+    float *a = vector(1, n), *b = vector(1, n), *d = vector(1, n);
+    int h;
+    for (h = 1; h <= n; h++) { a[h] = g_new[h - 1]; b[h] = g_old[h - 1]; d[h] = dir[h - 1]; }
+    NX = nx; NY = ny; IDX = IDY = 1; MYID = 1;   /* MYID != 0: no progress printout */
+    PCG(a, b, d, nclass);
+    NX = nx0; NY = ny0; IDX = idx0; IDY = idy0; MYID = myid0;
+    for (h = 1; h <= n; h++) dir[h - 1] = d[h];
+    free_vector(a, 1, n); free_vector(b, 1, n); free_vector(d, 1, n);
+    return 0;
+}

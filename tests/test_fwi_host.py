@@ -1,13 +1,17 @@
 """Host-side optimisation steps of the FWI loop (include/dsh_fwi.h): the
-L-BFGS two-loop recursion against a textbook numpy version, the parabolic
-step length (src/calc_opt_step.c) and the bracketing line search
-(src/line_search.c) on misfit curves with a known minimum."""
+L-BFGS two-loop recursion against a textbook numpy version, the
+conjugate-gradient direction against the reference's src/PCG.c (compiled into
+the oracle) bit for bit and against the oracle's restatement for the beta
+choices the reference does not compile, the parabolic step length
+(src/calc_opt_step.c) and the bracketing line search (src/line_search.c) on
+misfit curves with a known minimum."""
 import ctypes as C
 
 import numpy as np
 import pytest
 
 import dsh
+import oracle as O
 from dsh import fwi
 
 
@@ -50,6 +54,51 @@ def test_lbfgs_satisfies_newest_secant_equation():
     Y = (S * h).astype(np.float32)
     r = fwi.lbfgs_direction(S, Y, Y[-1])
     assert np.allclose(r, S[-1], rtol=1e-4, atol=1e-4)
+
+
+def _pcg_fields(seed, ny=37, nx=53, reset=False):
+    """vs and rho descent directions [2][ny][nx] of two iterations and the
+    previous search direction; with reset the new gradient is half the old
+    one (Polak-Ribiere beta < 0)."""
+    rng = np.random.default_rng(seed)
+    old = rng.standard_normal((2, ny, nx)).astype(np.float32) * np.float32([[[3e-3]], [[4e2]]])
+    new = (0.5 * old if reset else 0.7 * old + 0.4 * old.std() * rng.standard_normal((2, ny, nx))).astype(np.float32)
+    if not reset:
+        new[1] = 0.9 * old[1] + 0.2 * old[1].std() * rng.standard_normal((ny, nx)).astype(np.float32)
+    d = (old + 0.1 * rng.standard_normal((2, ny, nx)) * old.std(axis=(1, 2), keepdims=True)).astype(np.float32)
+    return new, old, d
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference build not present")
+@pytest.mark.parametrize("seed,reset", [(1, False), (2, False), (3, True)])
+def test_pcg_direction_bit_identical_to_reference(seed, reset):
+    new, old, d = _pcg_fields(seed, reset=reset)
+    ny, nx = new.shape[1:]
+    xm = lambda a: np.ascontiguousarray(a.transpose(0, 2, 1))     # the reference's x-major class order
+    got, betas = fwi.pcg_direction(xm(new), xm(old), xm(d))
+    ref = O.pcg(xm(new), xm(old), xm(d), nx, ny)
+    assert np.array_equal(got.ravel(), ref)
+    assert (betas >= 0).all()
+    if reset:
+        assert (betas == 0).all() and np.array_equal(got, xm(new))
+
+
+@pytest.mark.parametrize("beta", ["fletcher_reeves", "polak_ribiere", "hestenes_stiefel", "dai_yuan"])
+def test_pcg_direction_beta_choices_match_restatement(beta):
+    new, old, d = _pcg_fields(4, ny=9, nx=13)
+    got, betas = fwi.pcg_direction(new, old, d, beta=beta)
+    ref, ref_b = O.pcg_port(new, old, d, 2, fwi.PCG_BETA[beta])
+    assert np.array_equal(got.ravel(), ref) and np.array_equal(betas, ref_b)
+
+
+def test_pcg_direction_zero_denominator_and_bad_arguments():
+    new = np.ones((1, 10), np.float32)
+    got, betas = fwi.pcg_direction(new, np.zeros_like(new), np.full_like(new, 5.0))   # g_old = 0: beta = 0
+    assert betas[0] == 0 and np.array_equal(got, new)
+    with pytest.raises(dsh.DshError):
+        fwi.pcg_direction(np.ones((9, 4), np.float32), np.ones((9, 4), np.float32), np.ones((9, 4), np.float32))
+    with pytest.raises(KeyError):
+        fwi.pcg_direction(new, new, new, beta="newton")
 
 
 def test_opt_step_parabola():
