@@ -162,6 +162,41 @@ __global__ void shot_sum_kernel(int nx, int ny, int pitch, long long slot_stride
     }
 }
 
+/* per-shot circular taper of one slot (src/taper_grad_shot.c) */
+struct TaperShot {
+    int i1, j1;
+    float minm, maxm;
+};
+
+/* sum += tapered per-shot field: the shot's coefficient (min(1, box value)
+ * - minm) / maxm, 0 within filt points of its source
+ * (src/taper_grad_shot.c:126-190, then denise.c:1689-1694) */
+__global__ void shot_sum_taper_kernel(int nx, int ny, int pitch, long long slot_stride, int nslots, const float *a_u,
+                                      const float *a_r, float *sum_u, float *sum_r, const float *box, int g, int ijc,
+                                      int filt, const TaperShot *ts)
+{
+    const long long n = (long long)nx * ny;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nx) + 1, j = (int)(idx / nx) + 1;
+        const long long o = (long long)(j - 1) * pitch + (i - 1 + HX);
+        float su = sum_u[o], sr = sum_r[o];
+        for (int s = 0; s < nslots; s++) {
+            const TaperShot t = ts[s];
+            const int ix = i - t.i1 + ijc, iy = j - t.j1 + ijc;
+            float mm = 1.0f;
+            if (ix >= 1 && ix <= g && iy >= 1 && iy <= g) mm = box[(iy - 1) * g + (ix - 1)];
+            float ms = 1.0f;
+            if (ms > mm) ms = mm;
+            const float c = (ms - t.minm) / t.maxm;
+            const bool z = abs(i - t.i1) <= filt && abs(j - t.j1) <= filt;
+            su = su + (z ? 0.0f : a_u[(long long)s * slot_stride + o] * c);
+            sr = sr + (z ? 0.0f : a_r[(long long)s * slot_stride + o] * c);
+        }
+        sum_u[o] = su;
+        sum_r[o] = sr;
+    }
+}
+
 /* waveconv_mu = -DT*sum_u; g_vs = 2 rho vs mu (double, as the reference's
  * double literal promotes it); g_rho = vs^2 mu - DT*sum_rho (denise.c:1752-1800) */
 __global__ void convert_kernel(int nx, int ny, int pitch, float dt, const float *vs, const float *rho,
@@ -387,6 +422,7 @@ extern "C" int dsh_destroy(dsh_ctx *ctx)
     cudaFree(ctx->d_geo); cudaFree(ctx->d_offs); cudaFree(ctx->d_sig); cudaFree(ctx->d_seis); cudaFree(ctx->d_res);
     cudaFree(ctx->d_obs); cudaFree(ctx->d_tmp); cudaFree(ctx->d_out); cudaFree(ctx->d_nt); cudaFree(ctx->d_part); cudaFree(ctx->d_l2);
     cudaFree(ctx->d_wemax);
+    cudaFree(ctx->d_taper_box); cudaFree(ctx->d_taper_shot);
     for (int k = 0; k < 4; k++) if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     if (ctx->own_st) cudaStreamDestroy(ctx->own_st);
     delete ctx;
@@ -1299,8 +1335,25 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
             eprecond_scale_kernel<<<epi_grid(ctx, nb), 256, 0, ctx->st>>>(ea);
             ctx->launches += 2;
         }
-        shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
-                                                               ctx->slab + ctx->o_gu, ctx->slab + ctx->o_grho, sum_u, sum_r);
+        if (ctx->taper_on) {
+            std::vector<TaperShot> ts(nb);
+            for (int s = 0; s < nb; s++) {
+                const dsh_shot &sh = shots[b0 + s];
+                ts[s].i1 = (int)sh.srcpos[0];
+                ts[s].j1 = (int)sh.srcpos[sh.nsrc];
+                dsh_setup_taper_norm(p.nx, p.ny, ctx->taper_g, ctx->taper_ijc, ctx->taper_box.data(), ts[s].i1,
+                                     ts[s].j1, &ts[s].minm, &ts[s].maxm);
+            }
+            CK(cudaMemcpyAsync(ctx->d_taper_shot, ts.data(), nb * sizeof(TaperShot), cudaMemcpyHostToDevice, ctx->st));
+            shot_sum_taper_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(
+                p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb, ctx->slab + ctx->o_gu, ctx->slab + ctx->o_grho, sum_u,
+                sum_r, ctx->d_taper_box, ctx->taper_g, ctx->taper_ijc, ctx->taper_filt,
+                (const TaperShot *)ctx->d_taper_shot);
+        } else {
+            shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
+                                                                   ctx->slab + ctx->o_gu, ctx->slab + ctx->o_grho,
+                                                                   sum_u, sum_r);
+        }
         ctx->launches++;
         if (energies) {            /* shot sums of Ws and Wr (dsh_get_energy_sums) */
             shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
@@ -1354,6 +1407,35 @@ extern "C" int dsh_gradient_device(dsh_ctx *ctx, const dsh_shot *shots, int nsho
     if (!obs_dev) return DSH_ERR_PARAM;
     return gradient_impl(ctx, shots, nshots, nullptr, obs_dev, nullptr, nullptr, g_vs_dev, g_rho_dev, l2, nullptr,
                          nullptr, nullptr);
+}
+
+extern "C" int dsh_set_shot_taper(dsh_ctx *ctx, int enable, int srtshape, float srtradius, int filtsize)
+{
+    if (!ctx) return DSH_ERR_PARAM;
+    if (!enable) {
+        ctx->taper_on = 0;
+        return DSH_OK;
+    }
+    int g = 0, ijc = 0;
+    if (filtsize < 0 || dsh_setup_taper_box(srtshape, srtradius, ctx->p.dh, &g, &ijc, nullptr) != 0)
+        return DSH_ERR_PARAM;
+    if (g > 4096) return DSH_ERR_PARAM;
+    std::vector<float> box((size_t)g * g);
+    dsh_setup_taper_box(srtshape, srtradius, ctx->p.dh, &g, &ijc, box.data());
+    CK(cudaSetDevice(ctx->dev));
+    CK(cudaStreamSynchronize(ctx->st));
+    cudaFree(ctx->d_taper_box);
+    ctx->d_taper_box = nullptr;
+    if (cudaMalloc(&ctx->d_taper_box, box.size() * sizeof(float)) != cudaSuccess) return DSH_ERR_OOM;
+    if (!ctx->d_taper_shot && cudaMalloc(&ctx->d_taper_shot, (size_t)ctx->S * sizeof(TaperShot)) != cudaSuccess)
+        return DSH_ERR_OOM;
+    CK(cudaMemcpy(ctx->d_taper_box, box.data(), box.size() * sizeof(float), cudaMemcpyHostToDevice));
+    ctx->taper_box.swap(box);
+    ctx->taper_g = g;
+    ctx->taper_ijc = ijc;
+    ctx->taper_filt = filtsize;
+    ctx->taper_on = 1;
+    return DSH_OK;
 }
 
 extern "C" int dsh_hessian_diag(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *h_vs, float *h_rho)

@@ -63,6 +63,12 @@ struct dsh_ctx {
     double *d_part = nullptr, *d_l2 = nullptr;
     unsigned *d_wemax = nullptr;
     std::vector<int> ntr_b;
+    /* per-shot circular gradient taper (dsh_set_shot_taper): box [g][g] and,
+       per slot, the first source's grid point and the normalisation */
+    int taper_on = 0, taper_g = 0, taper_ijc = 0, taper_filt = 0;
+    std::vector<float> taper_box;
+    float *d_taper_box = nullptr;
+    void *d_taper_shot = nullptr;         /* S x TaperShot */
     std::vector<double> shot_l2;          /* per-shot L2 misfits of the last gradient */
     std::map<long long, cudaGraphExec_t> graphs;
     cudaEvent_t ev[4];

@@ -1,7 +1,8 @@
 /*
  * dsh_post.cu — processing around the gradient on the device: the
- * SPATFILTER=3 Gaussian smoothing of src/gauss_filt.c (src/smooth_grad.c:27-29)
- * and the Butterworth filtering of source signals and traces of the
+ * SPATFILTER=3 Gaussian smoothing of src/gauss_filt.c (src/smooth_grad.c:27-29),
+ * the application of the gradient tapers (src/taper_grad.c; coefficients from
+ * dsh_taper.c) and the Butterworth filtering of source signals and traces of the
  * multi-scale workflow stages (src/timedomain_filt.c, libcseife).
  * Each output point sums the (2h+1)^2 taps of the edge-replicated gradient
  * in the reference's order (ii outer, jj inner) in FP32 without contraction,
@@ -94,7 +95,25 @@ __global__ void iir_store(const double *x, int ntr, int ns, float *d)
     }
 }
 
+/* g = zero ? 0 : g*coeff (src/taper_grad.c: waveconv *= taper_coeff, then
+ * the zeroed points are set to 0.0) */
+__global__ void taper_kernel(long long n, float *g, const float *c, const unsigned char *z)
+{
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        g[k] = z[k] ? 0.0f : g[k] * c[k];
+}
+
 }  // namespace
+
+extern "C" int dsh_taper_apply(float *g_dev, int nx, int ny, const float *coeff_dev, const unsigned char *zero_dev,
+                               void *stream)
+{
+    if (nx < 1 || ny < 1 || !g_dev || !coeff_dev || !zero_dev) return DSH_ERR_PARAM;
+    const long long total = (long long)nx * ny;
+    const int blocks = (int)((total + 255) / 256 < 148 * 8 ? (total + 255) / 256 : 148 * 8);
+    taper_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(total, g_dev, coeff_dev, zero_dev);
+    return cudaGetLastError() == cudaSuccess ? DSH_OK : DSH_ERR_CUDA;
+}
 
 /* Butterworth filtering of traces (src/timedomain_filt.c with libcseife's
  * seife_lpb / seife_hpb): data_dev [ntr][ns] float on the device, filtered in

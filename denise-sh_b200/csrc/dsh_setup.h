@@ -62,6 +62,17 @@ int dsh_setup_gauss_kernel(int filt, float *kernel);
  * returns the number of sections written to coef [n][5] = f0 f1 f2 g1 g2. */
 int dsh_setup_butterworth(double dt, float fc, int order, int highpass, double *coef);
 
+/* Circular source taper box of src/taper_grad.c:298-351 and
+ * src/taper_grad_shot.c:47-96: size g (>= 5) and centre ijc in grid points,
+ * and, when m is not NULL, the normalised box values m [g][g] (row iy-1,
+ * column ix-1). */
+int dsh_setup_taper_box(int srtshape, float srtradius, float dh, int *g, int *ijc, float *m);
+/* For one source at grid point (i1, j1): the minimum of the source's
+ * min-combined mask over the grid and the maximum after subtracting it
+ * (src/taper_grad_shot.c:126-140); the coefficient at a point is then
+ * (min(1, box value or 1) - minm) / maxm. */
+void dsh_setup_taper_norm(int nx, int ny, int g, int ijc, const float *m, int i1, int j1, float *minm, float *maxm);
+
 /* Largest stable DT of the staggered scheme (src/checkfd_ssg_elastic.c):
  * DH / (sqrt(2) * sum|hc| * vmax). */
 double dsh_setup_dt_limit(int fdorder, int maxrelerror, float dh, float vmax);

@@ -92,6 +92,10 @@ def lib() -> C.CDLL:
                                           C.c_int, C.c_void_p]
         L.dsh_smooth_gauss.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_gauss_filter_size.argtypes = [C.c_float] * 4
+        L.dsh_taper_coeff.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_int, C.c_float, C.c_int,
+                                      C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_taper_apply.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_set_shot_taper.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]
         L.dsh_autotune.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
         L.dsh_profile_fused.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_get_shot_misfits.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -304,6 +308,12 @@ class Engine:
         _check(rc, "dsh_profile_fused")
         return float(out[0])
 
+    def set_shot_taper(self, srtshape=1, srtradius=5.0, filtsize=1, enable=True):
+        """SWS_TAPER_CIRCULAR_PER_SHOT: taper every shot's gradient around its
+        first source before the shot sum (src/taper_grad_shot.c)."""
+        _check(lib().dsh_set_shot_taper(self.h, int(bool(enable)), int(srtshape), float(srtradius), int(filtsize)),
+               "dsh_set_shot_taper")
+
     def shot_misfits(self, nshots):
         out = np.zeros(nshots, np.float64)
         _check(lib().dsh_get_shot_misfits(self.h, nshots, out.ctypes.data), "dsh_get_shot_misfits")
@@ -412,6 +422,43 @@ def smooth_gauss(grad, filt, stream=None):
 
 def gauss_filter_size(wd_damp, c_vs, fc_end, dh):
     return int(lib().dsh_gauss_filter_size(wd_damp, c_vs, fc_end, dh))
+
+
+TAPER_VERTICAL, TAPER_HORIZONTAL, TAPER_SOURCES, TAPER_FILE_VS, TAPER_FILE_RHO = 1, 2, 3, 5, 6
+
+
+def taper_coeff(sws, nx, ny, dh, gradt=(0, 0, 0, 0), srtshape=1, srtradius=5.0, filtsize=1, src_xy=None,
+                recpos=None, file_vals=None):
+    """Host coefficients of the gradient taper sws (src/taper_grad.c):
+    returns (coeff [ny, nx] float32, zero [ny, nx] bool).  src_xy [2, nsrc]
+    source x, y in metres; recpos [2, ntr] 1-based grid points; file_vals
+    nx*ny floats, x outer (sws 5, 6)."""
+    coeff = np.zeros((ny, nx), np.float32)
+    zero = np.zeros((ny, nx), np.uint8)
+    sxy = np.ascontiguousarray(src_xy if src_xy is not None else np.zeros((2, 0)), np.float32)
+    rp = np.ascontiguousarray(recpos if recpos is not None else np.zeros((2, 0)), np.int32)
+    gt = np.ascontiguousarray(gradt, np.int32)
+    fv = np.ascontiguousarray(file_vals, np.float32) if file_vals is not None else None
+    _check(lib().dsh_taper_coeff(sws, nx, ny, dh, gt.ctypes.data, srtshape, srtradius, filtsize, sxy.shape[1],
+                                 sxy.ctypes.data, rp.shape[1], rp.ctypes.data,
+                                 fv.ctypes.data if fv is not None else None, coeff.ctypes.data, zero.ctypes.data),
+           "dsh_taper_coeff")
+    return coeff, zero.astype(bool)
+
+
+def taper_apply(g_dev, coeff, zero, stream=None):
+    """g = zero ? 0 : g*coeff in place on a CUDA tensor g_dev [ny, nx]
+    (dsh_taper_apply); coeff, zero: host arrays from taper_coeff."""
+    import torch
+
+    ny, nx = g_dev.shape
+    if g_dev.dtype != torch.float32 or not g_dev.is_cuda or not g_dev.is_contiguous():
+        raise ValueError("g_dev must be a contiguous float32 CUDA tensor")
+    c = torch.from_numpy(np.ascontiguousarray(coeff, np.float32)).to(g_dev.device)
+    z = torch.from_numpy(np.ascontiguousarray(zero, np.uint8)).to(g_dev.device)
+    _check(lib().dsh_taper_apply(g_dev.data_ptr(), nx, ny, c.data_ptr(), z.data_ptr(), stream), "dsh_taper_apply")
+    torch.cuda.synchronize(g_dev.device)
+    return g_dev
 
 
 NOALLOC_MAX_SHOTS = 64

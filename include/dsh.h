@@ -254,6 +254,39 @@ int dsh_gauss_filter_size(float wd_damp, float c_vs, float fc_end, float dh);
 int dsh_timedomain_filt(float *data_dev, int ntr, int ns, float dt, float fc, int order, int method, int compat,
                         void *stream);
 
+/* Gradient tapers applied after the shot sum and the smoothing
+ * (src/taper_grad.c, called at src/denise.c:1822-1846).  dsh_taper_coeff
+ * computes on the host the coefficients coeff [ny][nx] and the mask
+ * zero [ny][nx] (1 = the taper sets the point to 0) of
+ *   sws 1     the vertical frame: Gaussian ramps over columns GRADT1..GRADT2
+ *             and GRADT3..GRADT4, 0 outside, zero at every source and receiver
+ *   sws 2     the horizontal taper: 0 above row GRADT1, a Gaussian ramp over
+ *             rows GRADT1..GRADT2, the depth j*DH below
+ *   sws 3     circular tapers around the sources (srtshape 1 erf, 2 log,
+ *             radius srtradius m), zero within filtsize points of a source
+ *   sws 5, 6  the values of a taper file (file_vals: nx*ny floats, x outer,
+ *             as the reference reads taper.bin)
+ * gradt = GRADT1..GRADT4; src_xy [2][nsrc] source x and y in metres (the
+ * reference's srcpos rows 1-2, rounded to grid points as it does); recpos
+ * [2][ntr] 1-based receiver grid points.  Points outside the grid are
+ * ignored: the reference's zeroing writes for box points left of column 1
+ * land in the halo or in the previous row's last columns, which is not
+ * reproduced.  dsh_taper_apply then sets g = zero ? 0 : g*coeff on device
+ * arrays [ny][nx] (coeff_dev, zero_dev: copies of the host arrays). */
+int dsh_taper_coeff(int sws, int nx, int ny, float dh, const int gradt[4], int srtshape, float srtradius,
+                    int filtsize, int nsrc, const float *src_xy, int ntr, const int *recpos, const float *file_vals,
+                    float *coeff, unsigned char *zero);
+int dsh_taper_apply(float *g_dev, int nx, int ny, const float *coeff_dev, const unsigned char *zero_dev,
+                    void *stream);
+
+/* Per-shot circular taper (SWS_TAPER_CIRCULAR_PER_SHOT, src/taper_grad_shot.c,
+ * applied at src/denise.c:1681-1687): in dsh_gradient / dsh_gradient_device
+ * every shot's gradients, after the eprecond scaling and before the shot sum,
+ * are multiplied by the circular taper (srtshape 1 erf, 2 log, radius
+ * srtradius m) around the shot's first source and set to 0 within filtsize
+ * points of it.  enable = 0 switches it off (the default). */
+int dsh_set_shot_taper(dsh_ctx *ctx, int enable, int srtshape, float srtradius, int filtsize);
+
 /* Statistics of the last dsh_forward / dsh_gradient call. */
 typedef struct dsh_stats {
     double ms_forward, ms_adjoint, ms_total;   /* device time (CUDA events) */

@@ -326,3 +326,32 @@ def pcg_port(g_new, g_old, dir, nclass, beta_kind):
         betas.append(beta)
         d[k] = a[k] + beta * d[k]
     return d.ravel(), np.array(betas, np.float32)
+
+
+def taper(g, sws, dh, gradt=(0, 0, 0, 0), srtshape=1, srtradius=5.0, filtsize=1, src_xy=None, recpos=None,
+          shot=0, file_vals=None):
+    """The reference's gradient taper (src/taper_grad.c; shot = k >= 1:
+    src/taper_grad_shot.c for source k) applied to g [ny, nx].  Returns
+    (tapered g, coefficient field).  Files the reference writes or reads
+    (its coefficient files, taper.bin for sws 5/6) go to a temporary
+    directory."""
+    import tempfile
+
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_taper.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_int,
+                               C.c_float, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    out = _f32(g).copy()
+    ny, nx = out.shape
+    tc = np.zeros_like(out)
+    sxy = _f32(src_xy if src_xy is not None else np.zeros((2, 0)))
+    rp = np.ascontiguousarray(recpos if recpos is not None else np.zeros((2, 0)), np.int32)
+    gt = np.ascontiguousarray(gradt, np.int32)
+    with tempfile.TemporaryDirectory() as d:
+        if file_vals is not None:
+            _f32(file_vals).tofile(os.path.join(d, "taper.bin"))
+        rc = lib.refh_taper(d.encode(), sws, shot, nx, ny, dh, gt.ctypes.data, srtshape, srtradius, filtsize,
+                            sxy.shape[1], sxy.ctypes.data, rp.shape[1], rp.ctypes.data, out.ctypes.data,
+                            tc.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("refh_taper failed")
+    return out, tc

@@ -735,3 +735,50 @@ int refh_pcg(int nx, int ny, int nclass, const float *g_new, const float *g_old,
     free_vector(a, 1, n); free_vector(b, 1, n); free_vector(d, 1, n);
     return 0;
 }
+
+/* The reference's gradient tapers on a dense gradient g [ny][nx] (in place):
+ * shot = 0 runs src/taper_grad.c with the given sws, shot = k >= 1 runs
+ * src/taper_grad_shot.c for source k.  src_xy [2][nsrc] in metres, recpos
+ * [2][ntr]; the coefficient field comes back in taper [ny][nx].  The
+ * coefficient files taper_grad writes (and taper.bin it reads for sws 5/6)
+ * live in the directory dir. */
+void taper_grad(float **waveconv, float **taper_coeff, float **srcpos, int nshots, int **recpos, int ntr, int iter,
+                int sws);
+void taper_grad_shot(float **waveconv, float **taper_coeff, float **srcpos, int nshots, int **recpos, int ntr,
+                     int ishot);
+extern int GRADT1, GRADT2, GRADT3, GRADT4, SRTSHAPE, FILTSIZE;
+extern float SRTRADIUS;
+#include <unistd.h>
+int refh_taper(const char *dir, int sws, int shot, int nx, int ny, float dh, const int *gradt, int srtshape,
+               float srtradius, int filtsize, int nsrc, const float *src_xy, int ntr, const int *recpos, float *g,
+               float *taper)
+{
+    char cwd[4096];
+    int i, j, k;
+    const int nx0 = NX, ny0 = NY, nxg0 = NXG, nyg0 = NYG, myid0 = MYID;
+    const float dh0 = DH;
+    FILE *fp0 = FP, *quiet;
+    float **w, **tc, **sp;
+    int **rp;
+    if (!getcwd(cwd, sizeof cwd) || chdir(dir) != 0) return -1;
+    quiet = fopen("/dev/null", "w");
+    NX = NXG = nx; NY = NYG = ny; DH = dh; POS[1] = POS[2] = 0; IDX = IDY = 1;
+    NPROCX = NPROCY = 1; MYID = 1;   /* MYID != 0: no merge of the per-rank coefficient files */
+    FP = quiet ? quiet : stderr;
+    GRADT1 = gradt[0]; GRADT2 = gradt[1]; GRADT3 = gradt[2]; GRADT4 = gradt[3];
+    SRTSHAPE = srtshape; SRTRADIUS = srtradius; FILTSIZE = filtsize;
+    w = matrix(1, ny, 1, nx); tc = matrix(1, ny, 1, nx);
+    sp = matrix(1, 8, 1, nsrc > 0 ? nsrc : 1); rp = imatrix(1, 3, 1, ntr > 0 ? ntr : 1);
+    for (j = 1; j <= ny; j++) for (i = 1; i <= nx; i++) { w[j][i] = g[(j - 1) * nx + i - 1]; tc[j][i] = 0.0f; }
+    for (k = 1; k <= nsrc; k++) { sp[1][k] = src_xy[k - 1]; sp[2][k] = src_xy[nsrc + k - 1]; }
+    for (k = 1; k <= ntr; k++) { rp[1][k] = recpos[k - 1]; rp[2][k] = recpos[ntr + k - 1]; rp[3][k] = 0; }
+    if (shot == 0) taper_grad(w, tc, sp, nsrc, rp, ntr, 1, sws);
+    else taper_grad_shot(w, tc, sp, nsrc, rp, ntr, shot);
+    for (j = 1; j <= ny; j++) for (i = 1; i <= nx; i++) { g[(j - 1) * nx + i - 1] = w[j][i]; taper[(j - 1) * nx + i - 1] = tc[j][i]; }
+    free_matrix(w, 1, ny, 1, nx); free_matrix(tc, 1, ny, 1, nx);
+    free_matrix(sp, 1, 8, 1, nsrc > 0 ? nsrc : 1); free_imatrix(rp, 1, 3, 1, ntr > 0 ? ntr : 1);
+    FP = fp0;
+    NX = nx0; NY = ny0; NXG = nxg0; NYG = nyg0; MYID = myid0; DH = dh0;
+    if (quiet) fclose(quiet);
+    return chdir(cwd) == 0 ? 0 : -1;
+}
