@@ -1424,6 +1424,7 @@ extern "C" int dsh_set_shot_taper(dsh_ctx *ctx, int enable, int srtshape, float 
     dsh_setup_taper_box(srtshape, srtradius, ctx->p.dh, &g, &ijc, box.data());
     CK(cudaSetDevice(ctx->dev));
     CK(cudaStreamSynchronize(ctx->st));
+    ctx->taper_on = 0;
     cudaFree(ctx->d_taper_box);
     ctx->d_taper_box = nullptr;
     if (cudaMalloc(&ctx->d_taper_box, box.size() * sizeof(float)) != cudaSuccess) return DSH_ERR_OOM;
