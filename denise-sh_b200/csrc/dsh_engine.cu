@@ -76,6 +76,81 @@ __global__ void residual_kernel(int nt_total, const int *rec_off, const float *s
     if (threadIdx.x == 0) part[(long long)s * gridDim.x + blockIdx.x] = sh[0];
 }
 
+/* Residual of LNORM 1, 3, 4 (calc_res.c:156-189) with the same layout and
+ * first-sample replacement: sign(obs - syn), (obs - syn)/(1 + (obs - syn)^2),
+ * tanh(obs - syn) (double tanh rounded to float, as the reference's C call).
+ * The reference adds nothing to the misfit for these norms (:250-260). */
+__global__ void residual_elem_kernel(int lnorm, int nt_total, const int *rec_off, const float *seis,
+                                     const long long *seis_off, const float *obs, const long long *obs_off, float *res,
+                                     double *part)
+{
+    const int s = blockIdx.y;
+    const int ntr = rec_off[s + 1] - rec_off[s];
+    const long long n = (long long)ntr * nt_total;
+    const float *syn = seis + seis_off[s];
+    const float *ob = obs + obs_off[s];
+    float *rs = res + seis_off[s];
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(idx / nt_total);
+        const int t = (int)(idx % nt_total) + 1;
+        const int tf = nt_total - t + 1;
+        const float sy = syn[(long long)(tf - 1) * ntr + r];
+        const float od = (tf == 1) ? sy : ob[(long long)r * nt_total + (tf - 1)];
+        float v;
+        if (lnorm == 1) v = (od - sy) > 0.0f ? 1.0f : ((od - sy) < 0.0f ? -1.0f : 0.0f);
+        else if (lnorm == 3) v = (od - sy) / (1.0f + ((od - sy) * (od - sy)));
+        else v = (float)tanh((double)(od - sy));
+        rs[(long long)r * nt_total + (t - 1)] = v;
+    }
+    if (threadIdx.x == 0) part[(long long)s * gridDim.x + blockIdx.x] = 0.0;
+}
+
+/* Global-correlation residual, LNORM=5 (calc_res.c:119-147,192-217): per
+ * trace the float norms |obs|, |syn| and syn.obs in sample order (before the
+ * first observed sample is replaced), then
+ *   res = syn (syn.obs) / (|syn|^3 |obs|) - obs / (|syn| |obs|)
+ * time-reversed, and the misfit term -obs syn / (|obs| |syn|) per sample
+ * (summed in double; the reference subtracts it from its float L2).  One
+ * thread per trace. */
+__global__ void residual_gc_kernel(int nt_total, const int *rec_off, const float *seis, const long long *seis_off,
+                                   const float *obs, const long long *obs_off, float *res, double *part)
+{
+    const int s = blockIdx.y;
+    const int ntr = rec_off[s + 1] - rec_off[s];
+    const float *syn = seis + seis_off[s];
+    float *rs = res + seis_off[s];
+    double acc = 0.0;
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < ntr; r += gridDim.x * blockDim.x) {
+        const float *ob = obs + obs_off[s] + (long long)r * nt_total;
+        float ad = 0.0f, as = 0.0f, dms = 0.0f;
+#pragma unroll 8
+        for (int t = 0; t < nt_total; t++) {
+            const float d = ob[t], y = syn[(long long)t * ntr + r];
+            ad = ad + d * d;
+            as = as + y * y;
+            dms = dms + y * d;
+        }
+        ad = (float)sqrt((double)ad);
+        as = (float)sqrt((double)as);
+        const float tmp = as * as * as * ad, tmp1 = as * ad, tmp2 = ad * as;
+#pragma unroll 4
+        for (int tf = 1; tf <= nt_total; tf++) {
+            const float y = syn[(long long)(tf - 1) * ntr + r];
+            const float d = (tf == 1) ? y : ob[tf - 1];
+            rs[(long long)r * nt_total + (nt_total - tf)] = ((y * dms) / (tmp + 0.0f)) - (d / (tmp1 + 0.0f));
+            acc -= (double)((d * y) / (tmp2 + 0.0f));
+        }
+    }
+    __shared__ double sh[RED_THREADS];
+    sh[threadIdx.x] = acc;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if (threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(long long)s * gridDim.x + blockIdx.x] = sh[0];
+}
+
 __global__ void reduce_parts(const double *part, int nparts, int nslots, double *out)
 {
     const int s = blockIdx.x;
@@ -1295,10 +1370,20 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
         cudaEventRecord(e0, ctx->st);
         if ((rc = forward_for_gradient(ctx, nb)) != DSH_OK) return rc;
         cudaEventRecord(e1, ctx->st);
-        /* residual + L2 */
-        residual_kernel<<<dim3(RED_BLOCKS, nb), RED_THREADS, 0, ctx->st>>>(p.nt, ctx->d_rec_off, ctx->d_seis,
-                                                                          ctx->d_offs + ctx->S, obs_base,
-                                                                          ctx->d_offs + 2 * ctx->S, ctx->d_res, ctx->d_part);
+        /* residual + misfit (LNORM of dsh_set_misfit) */
+        if (ctx->lnorm == 2)
+            residual_kernel<<<dim3(RED_BLOCKS, nb), RED_THREADS, 0, ctx->st>>>(p.nt, ctx->d_rec_off, ctx->d_seis,
+                                                                              ctx->d_offs + ctx->S, obs_base,
+                                                                              ctx->d_offs + 2 * ctx->S, ctx->d_res,
+                                                                              ctx->d_part);
+        else if (ctx->lnorm == 5)
+            residual_gc_kernel<<<dim3(RED_BLOCKS, nb), RED_THREADS, 0, ctx->st>>>(
+                p.nt, ctx->d_rec_off, ctx->d_seis, ctx->d_offs + ctx->S, obs_base, ctx->d_offs + 2 * ctx->S,
+                ctx->d_res, ctx->d_part);
+        else
+            residual_elem_kernel<<<dim3(RED_BLOCKS, nb), RED_THREADS, 0, ctx->st>>>(
+                ctx->lnorm, p.nt, ctx->d_rec_off, ctx->d_seis, ctx->d_offs + ctx->S, obs_base,
+                ctx->d_offs + 2 * ctx->S, ctx->d_res, ctx->d_part);
         reduce_parts<<<nb, RED_THREADS, 0, ctx->st>>>(ctx->d_part, RED_BLOCKS, nb, ctx->d_l2);
         ctx->launches += 2;
         CK(cudaGetLastError());
@@ -1407,6 +1492,13 @@ extern "C" int dsh_gradient_device(dsh_ctx *ctx, const dsh_shot *shots, int nsho
     if (!obs_dev) return DSH_ERR_PARAM;
     return gradient_impl(ctx, shots, nshots, nullptr, obs_dev, nullptr, nullptr, g_vs_dev, g_rho_dev, l2, nullptr,
                          nullptr, nullptr);
+}
+
+extern "C" int dsh_set_misfit(dsh_ctx *ctx, int lnorm)
+{
+    if (!ctx || lnorm < 1 || lnorm > 5) return DSH_ERR_PARAM;
+    ctx->lnorm = lnorm;
+    return DSH_OK;
 }
 
 extern "C" int dsh_set_shot_taper(dsh_ctx *ctx, int enable, int srtshape, float srtradius, int filtsize)

@@ -63,6 +63,7 @@ struct dsh_ctx {
     double *d_part = nullptr, *d_l2 = nullptr;
     unsigned *d_wemax = nullptr;
     std::vector<int> ntr_b;
+    int lnorm = 2;                        /* misfit norm of the residual (dsh_set_misfit) */
     /* per-shot circular gradient taper (dsh_set_shot_taper): box [g][g] and,
        per slot, the first source's grid point and the normalisation */
     int taper_on = 0, taper_g = 0, taper_ijc = 0, taper_filt = 0;

@@ -96,6 +96,7 @@ def lib() -> C.CDLL:
                                       C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_taper_apply.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_set_shot_taper.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]
+        L.dsh_set_misfit.argtypes = [C.c_void_p, C.c_int]
         L.dsh_autotune.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
         L.dsh_profile_fused.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_get_shot_misfits.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -307,6 +308,12 @@ class Engine:
             return None
         _check(rc, "dsh_profile_fused")
         return float(out[0])
+
+    LNORM = {"l1": 1, "l2": 2, "cauchy": 3, "sech": 4, "global_correlation": 5}
+
+    def set_misfit(self, lnorm):
+        """Misfit norm of the residual (calc_res.c LNORM 1..5, or a key of LNORM)."""
+        _check(lib().dsh_set_misfit(self.h, self.LNORM.get(lnorm, lnorm)), "dsh_set_misfit")
 
     def set_shot_taper(self, srtshape=1, srtradius=5.0, filtsize=1, enable=True):
         """SWS_TAPER_CIRCULAR_PER_SHOT: taper every shot's gradient around its

@@ -279,6 +279,18 @@ int dsh_taper_coeff(int sws, int nx, int ny, float dh, const int gradt[4], int s
 int dsh_taper_apply(float *g_dev, int nx, int ny, const float *coeff_dev, const unsigned char *zero_dev,
                     void *stream);
 
+/* Misfit norm of dsh_gradient / dsh_gradient_device (LNORM of calc_res.c,
+ * GRAD_FORM=2; default 2): 1 L1 (residual sign(obs - syn)), 2 L2 (syn - obs),
+ * 3 Cauchy, 4 sech (tanh residual), 5 global correlation
+ * (syn (syn.obs)/(|syn|^3 |obs|) - obs/(|syn| |obs|) per trace).  The
+ * misfit reported is the reference's: sum res^2 for 2, -sum obs syn/(|obs|
+ * |syn|) for 5, and 0 for 1, 3 and 4 (src/calc_res.c:213-257 adds nothing
+ * for them).  A trace with |syn| or |obs| = 0 (or whose norms underflow in
+ * float) gives NaN residuals under LNORM=5, as in the reference.  LNORM=6 is
+ * rejected: the reference reads integrated traces there that it allocates
+ * only for LNORM=5 with GRAD_FORM=1 (src/calc_res.c:69-72,221). */
+int dsh_set_misfit(dsh_ctx *ctx, int lnorm);
+
 /* Per-shot circular taper (SWS_TAPER_CIRCULAR_PER_SHOT, src/taper_grad_shot.c,
  * applied at src/denise.c:1681-1687): in dsh_gradient / dsh_gradient_device
  * every shot's gradients, after the eprecond scaling and before the shot sum,

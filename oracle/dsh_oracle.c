@@ -55,7 +55,7 @@ static const double HOLBERG[5][6][6] = {
 
 /* Global oracle session (one model at a time; test infrastructure). */
 static struct {
-    int alive, fp64, fd12_compat;
+    int alive, fp64, fd12_compat, lnorm;
     int nx, ny, nt, fdorder, maxrelerror, fw, free_surf, l, quellart, eprecond;
     float dh, dt, damping, fpml, npower, k_max_pml, fl[8];
     int pitch, rows;
@@ -67,7 +67,7 @@ static struct {
     float bip[8], bjm[8], cip[8], cjm[8], eta[8];
     float c_vs, c_rho;
     int ntr, *recpos;
-} G = {.fd12_compat = 1};
+} G = {.fd12_compat = 1, .lnorm = 2};
 
 #define REAL float
 #define SFX f32
@@ -81,6 +81,12 @@ static struct {
 #undef SFX
 
 void dsho_set_fd12_compat(int on) { G.fd12_compat = on; }
+int dsho_set_lnorm(int lnorm)
+{
+    if (lnorm < 1 || lnorm > 5) return -1;
+    G.lnorm = lnorm;
+    return 0;
+}
 
 void dsho_free(void)
 {
@@ -243,6 +249,7 @@ int dsho_init(const dsho_params *p, const float *vs, const float *rho, const flo
     int i, j, l, k;
     const size_t n = (size_t)p->nx * p->ny;
     dsho_free();
+    G.lnorm = 2;
     if (p->fdorder < 2 || p->fdorder > 12 || (p->fdorder & 1) || p->maxrelerror < 0 || p->maxrelerror > 4 ||
         p->fw < 0 || p->fw > 64 || p->l < 0 || p->l > 8 || p->nx < 1 || p->ny < 1 || p->nt < 1)
         return -1;

@@ -30,6 +30,8 @@ typedef struct {
 int dsho_init(const dsho_params *p, const float *vs, const float *rho, const float *qs, int fp64);
 void dsho_free(void);
 void dsho_set_fd12_compat(int on);
+/* misfit norm of dsho_residual (calc_res.c LNORM 1..5, GRAD_FORM=2); dsho_init resets it to 2 */
+int dsho_set_lnorm(int lnorm);
 void dsho_get_hc(float *out7);
 void dsho_get_cnorm(float *out2);
 int dsho_get_pml(int which, float *out);

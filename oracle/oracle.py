@@ -207,6 +207,11 @@ class Oracle:
         self.ntr = ntr
         return seis[:ntr]
 
+    def set_lnorm(self, lnorm):
+        """Misfit norm of residual() (calc_res.c LNORM 1..5; default 2)."""
+        if self._fn("set_lnorm")(int(lnorm)) != 0:
+            raise ValueError("LNORM must be 1..5")
+
     def residual(self, obs):
         ob = _f32(obs)
         res = np.zeros((self.ntr, self.m.nt), np.float32)
@@ -243,10 +248,12 @@ class Oracle:
         self._fn("psource")(nt, _ptr(a), _ptr(b), sp.shape[1], _ptr(sp), _ptr(sig))
         return a, b
 
-    def shot_gradient(self, srcpos8, recpos, obs, signals=None, nsteps=None):
+    def shot_gradient(self, srcpos8, recpos, obs, signals=None, nsteps=None, lnorm=None):
         """Forward + residual + adjoint + eprecond scaling for one shot (denise.c:875-1694).
 
         Returns dict(seis, res, l2, g_u, g_rho, Ws, Wr, We)."""
+        if lnorm is not None:
+            self.set_lnorm(lnorm)
         seis = self.forward(srcpos8, recpos, signals=signals, nsteps=nsteps, store=True)
         res, l2 = self.residual(obs)
         self.adjoint(nsteps=nsteps)

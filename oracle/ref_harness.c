@@ -59,6 +59,7 @@ static fn_se_t impl_se = NULL;
 static fn_sv_t impl_sv = NULL;
 static fn_ep_t impl_ep = NULL;
 static fn_ep1_t impl_ep1 = NULL;
+static int cur_lnorm = 2;         /* LNORM of refh_residual (refh_set_lnorm; reset by refh_init) */
 
 void refh_set_impl(void *v, void *s_el, void *s_visc, void *ep, void *ep1)
 {
@@ -178,6 +179,7 @@ int refh_init(const refh_params *p, const float *vs, const float *rho, const flo
 {
     int i, j, l;
     refh_free();
+    cur_lnorm = 2;
     FP = stderr;
     NX = NXG = p->nx; NY = NYG = p->ny; NT = p->nt;
     FDORDER = p->fdorder; MAXRELERROR = p->maxrelerror; FW = p->fw; FREE_SURF = p->free_surf;
@@ -483,8 +485,15 @@ int refh_forward(int nsrc, const float *srcpos8, const float *signals_in, int nt
     return 0;
 }
 
-/* Residual and L2 (calc_res.c, LNORM=2, GRAD_FORM=2): obs [ntr][NT]; res out [ntr][NT]
- * (time-reversed); the reference also overwrites obs sample 1 with the synthetic one. */
+/* Residual and misfit (calc_res.c, GRAD_FORM=2, LNORM from refh_set_lnorm,
+ * default 2): obs [ntr][NT]; res out [ntr][NT] (time-reversed); the reference
+ * also overwrites obs sample 1 with the synthetic one. */
+int refh_set_lnorm(int lnorm)
+{
+    if (lnorm < 1 || lnorm > 5) return -1;
+    cur_lnorm = lnorm;
+    return 0;
+}
 int refh_residual(const float *obs, float *res, double *l2)
 {
     int k, nt, ntr = cur_ntr;
@@ -496,7 +505,7 @@ int refh_residual(const float *obs, float *res, double *l2)
     {
         int **recpos_glob = recpos_loc;
         float **srcdummy = matrix(1, 8, 1, 1);
-        *l2 = calc_res(sectionvydata, sectionvy, sectionvydiff, sectionvydiffold, ntr, NT, 2, 0.0, 0, 1, 1, ntr,
+        *l2 = calc_res(sectionvydata, sectionvy, sectionvydiff, sectionvydiffold, ntr, NT, cur_lnorm, 0.0, 0, 1, 1, ntr,
                        recpos_glob, recpos_loc, srcdummy, 1, 1, 1);
         free_matrix(srcdummy, 1, 8, 1, 1);
     }
