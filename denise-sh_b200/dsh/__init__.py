@@ -22,6 +22,7 @@ DSH_OK = 0
 EPRECOND_ENERGY_ONLY = 10      # dsh_params.eprecond: raw gradient plus the energies Ws, Wr
 ERRORS = {-1: "invalid parameter", -2: "CUDA error", -3: "out of device memory or budget",
           -4: "simulation is unstable (non-finite wavefield)", -5: "call out of order", -6: "device wait timed out"}
+ERR_PARAM, ERR_CUDA, ERR_OOM, ERR_UNSTABLE, ERR_STATE, ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
 
 FIELD = {"vy": 0, "sxy": 1, "syz": 2, "Ws": 12, "Wr": 13, "We": 14, "g_u": 15, "g_rho": 16, "hess_u": 17,
          "hess_rho": 18}

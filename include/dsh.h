@@ -286,7 +286,9 @@ int dsh_taper_apply(float *g_dev, int nx, int ny, const float *coeff_dev, const 
  * misfit reported is the reference's: sum res^2 for 2, -sum obs syn/(|obs|
  * |syn|) for 5, and 0 for 1, 3 and 4 (src/calc_res.c:213-257 adds nothing
  * for them).  A trace with |syn| or |obs| = 0 (or whose norms underflow in
- * float) gives NaN residuals under LNORM=5, as in the reference.  LNORM=6 is
+ * float) gives NaN residuals under LNORM=5, as in the reference, which carries
+ * them into its gradient; here the adjoint pass then returns DSH_ERR_UNSTABLE.
+ * LNORM=6 is
  * rejected: the reference reads integrated traces there that it allocates
  * only for LNORM=5 with GRAD_FORM=1 (src/calc_res.c:69-72,221). */
 int dsh_set_misfit(dsh_ctx *ctx, int lnorm);
