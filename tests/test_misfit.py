@@ -131,7 +131,10 @@ def test_engine_global_correlation_nan_trace_is_reported():
 
 @pytest.mark.gpu
 def test_set_misfit_rejects_lnorm_6():
-    with dsh.Engine(dsh.make_params(nx=32, ny=16, nt=10, dh=0.5, dt=1e-4)) as e:
+    from test_gpu_parity import engine_from
+
+    d, _, _, _ = _problem(5)
+    with engine_from(d) as e:
         for bad in (0, 6):
             with pytest.raises(dsh.DshError):
                 e.set_misfit(bad)
