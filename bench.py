@@ -73,6 +73,9 @@ def args_parse():
                                                       "else train and save)")
     ap.add_argument("--methods", default="learned_sym,learned,hessian",
                     help="c5 only: preconditioners compared with plain (the first one gives `value`)")
+    ap.add_argument("--targets", default="log_h",
+                    help="c5 only: comma list of network output modes (dsh.nn.TARGETS); the learned methods run "
+                         "once per network, the first target's runs unsuffixed")
     ap.add_argument("--nt-scale", type=float, default=1.0, help="c4 only: factor on every model's NT")
     ap.add_argument("--nt", type=int, default=None, help="time steps (default: the workload's NT)")
     ap.add_argument("--nx", type=int, default=2000, help="c2 only")
@@ -691,12 +694,18 @@ def bench_learned(a, rank, world, local):
     train_shots = [cfg["shots"][k] for k in pick]
     log = lambda r: print(json.dumps(r), file=sys.stderr, flush=True)
     t0 = time.time()
-    net = dnn.UNet(torch, seed=0)
-    gen_s = train_s = 0.0
-    losses = [None]
-    if a.net_cache and os.path.exists(a.net_cache):
-        net.load_state(dict(np.load(a.net_cache)))
-    else:
+    targets = [t for t in a.targets.split(",") if t]
+    nets = {t: dnn.UNet(torch, seed=0) for t in targets}
+    for t, n in nets.items():
+        n.target = t
+    cache = {t: (f"{os.path.splitext(a.net_cache)[0]}_{t}.npz" if a.net_cache else None) for t in targets}
+    gen_s = 0.0
+    train_s, losses = {t: 0.0 for t in targets}, {t: [None] for t in targets}
+    todo = [t for t in targets if not (cache[t] and os.path.exists(cache[t]))]
+    for t in targets:
+        if t not in todo:
+            nets[t].load_state(dict(np.load(cache[t])))
+    if todo:
         clock0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         clock0[0].record()
         models = configs.training_models(count=a.train_models, first_seed=100, nx=nx, ny=ny)
@@ -704,15 +713,18 @@ def bench_learned(a, rank, world, local):
         clock0[1].record()
         torch.cuda.synchronize()
         gen_s = clock0[0].elapsed_time(clock0[1]) / 1e3
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        losses = fwi.train(net, torch, xs, ts, ny, nx, epochs=a.epochs, batch=2, lr=1e-3, log=log)
-        e1.record()
-        torch.cuda.synchronize()
-        train_s = e0.elapsed_time(e1) / 1e3
+        for t in todo:
+            tt = dnn.residual_targets(torch, xs, ts) if t == "log_h_over_ws" else ts
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            losses[t] = fwi.train(nets[t], torch, xs, tt, ny, nx, epochs=a.epochs, batch=2, lr=1e-3, log=log)
+            e1.record()
+            torch.cuda.synchronize()
+            train_s[t] = e0.elapsed_time(e1) / 1e3
+            if cache[t]:
+                np.savez(cache[t], **nets[t].state())
+            del tt
         del xs, ts
-        if a.net_cache:
-            np.savez(a.net_cache, **net.state())
     prob = fwi.Problem(cfg, test_shots=4)
     prob.observe()
     w0 = time.time()
@@ -722,15 +734,21 @@ def bench_learned(a, rank, world, local):
     t_plain = hp[-1]["gpu_s"]
     curve = lambda h: [[round(r["gpu_s"], 3), r["misfit"]] for r in h]
     res = {}
+    runs = []
     for m in [x for x in a.methods.split(",") if x]:
+        if m.startswith("learned"):
+            runs += [(m if k == 0 else f"{m}@{t}", m, nets[t]) for k, t in enumerate(targets)]
+        else:
+            runs.append((m, m, None))
+    for key, m, net in runs:
         ws = time.time()
         hl, _ = fwi.run(prob, a.fwi_iters, method=m, net=net, torch=torch, target_misfit=target, log=log)
         t = time_to_reach(hl, target)
-        res[m] = {"final_misfit": hl[-1]["misfit"], "gpu_s_to_target": t, "gpu_s_total": hl[-1]["gpu_s"],
-                  "ratio": (t / t_plain) if t is not None else None,
-                  "wall_ratio": ((time.time() - ws) / (w1 - w0)) if t is not None else None,
-                  "iterations": len(hl) - 1, "fallbacks": sum(1 for r in hl if r.get("fallback")),
-                  "curve": curve(hl)}
+        res[key] = {"final_misfit": hl[-1]["misfit"], "gpu_s_to_target": t, "gpu_s_total": hl[-1]["gpu_s"],
+                    "ratio": (t / t_plain) if t is not None else None,
+                    "wall_ratio": ((time.time() - ws) / (w1 - w0)) if t is not None else None,
+                    "iterations": len(hl) - 1, "fallbacks": sum(1 for r in hl if r.get("fallback")),
+                    "network_target": net.target if net is not None else None, "curve": curve(hl)}
     prob.close()
     primary = a.methods.split(",")[0]
     line = {
@@ -740,11 +758,14 @@ def bench_learned(a, rank, world, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 solver, bf16 network", "data": "synthetic",
         "config": {"workload": f"learned-fwi-{nx}x{ny}-fd8-L3-{ns}shots-nt{p['nt']}", "fwi_iters": a.fwi_iters,
                    "train_models": a.train_models, "train_shots": len(train_shots), "epochs": a.epochs,
+                   "network_targets": targets,
                    "unet": "4 levels, 32 base channels, bf16 weights/activations, fp32 accumulation",
                    "target": "plain final misfit x 1.01", "net_cache": bool(a.net_cache and gen_s == 0.0)},
         "plain": {"final_misfit": hp[-1]["misfit"], "gpu_s": t_plain, "iterations": len(hp) - 1, "curve": curve(hp)},
         "methods": res,
-        "training": {"data_gpu_s": gen_s, "train_gpu_s": train_s, "loss_first": losses[0], "loss_last": losses[-1]},
+        "training": {"data_gpu_s": gen_s, "train_gpu_s": train_s,
+                     "loss_first": {t: v[0] for t, v in losses.items()},
+                     "loss_last": {t: v[-1] for t, v in losses.items()}},
         "e2e": {"value": res[primary]["wall_ratio"], "unit": "ratio (host wall-clock of the FWI runs)",
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
         "wall_s": time.time() - t0,

@@ -164,10 +164,10 @@ def learned_preconditioner(net, torch, g, ws, wr, vs, clock):
     e1.record()
     torch.cuda.synchronize()
     clock.ms += e0.elapsed_time(e1)
-    return dnn.hessian_from_prediction(out.cpu().numpy().reshape(ny, nx))
+    return dnn.prediction_to_hessian(torch, getattr(net, "target", "log_h"), out, x, (ny, nx))
 
 
-METHODS = ("plain", "learned", "learned_sym", "hessian")
+METHODS = ("plain", "learned", "learned_sym", "hessian", "energy_src")
 
 
 def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, scalefac=2.0, stepmax=6, nlbfgs=5,
@@ -181,6 +181,8 @@ def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, sc
                      preconditioner (the vs kernel correlates forward strains)
       "hessian"      as "learned" with the solver's own pseudo-Hessian (one extra forward
                      pass per iteration; a reference for what the prediction stands in for)
+      "energy_src"   raw gradient / (Ws + 0.005 max Ws): the forward energy alone in place
+                     of the Hessian (what a "log_h_over_ws" network corrects; no network)
     The learned methods fall back to a plain gradient when the line search
     rejects their step."""
     if method not in METHODS:
@@ -211,6 +213,8 @@ def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, sc
             if kind == "hessian":
                 h, _ = eng.hessian_diag(shots)
                 clock.add_engine(eng)
+            elif kind == "energy_src":
+                h = ws
             else:
                 h = learned_preconditioner(net, torch, out["g_vs"], ws, wr, vs, clock)
             if kind == "learned_sym":

@@ -200,6 +200,7 @@ class UNet:
         self.mhb, self.vhb = torch.zeros_like(self.hb), torch.zeros_like(self.hb)
         self.step_count = 0
         self.shape = None
+        self.target = "log_h"            # meaning of the output, one of TARGETS
 
     def layers(self):
         out = [l for lev in self.enc for l in lev]
@@ -389,3 +390,27 @@ def hessian_target(h):
 def hessian_from_prediction(pred):
     """Inverse of hessian_target (up to the unknown scale)."""
     return np.power(10.0, 8.0 * np.asarray(pred, np.float64)).astype(np.float32)
+
+
+# What the network's output stands for:
+#   "log_h"          hessian_target(H) itself
+#   "log_h_over_ws"  hessian_target(H) minus input channel 1 (log10 Ws / max Ws, / 8):
+#                    the correction to the forward energy Ws, which carries most of
+#                    the pseudo-Hessian's dynamic range (the vs kernel correlates
+#                    forward strains, and strain ~ particle velocity / vs)
+TARGETS = ("log_h", "log_h_over_ws")
+
+
+def residual_targets(torch, xs, ts):
+    """Training targets of the "log_h_over_ws" mode from (inputs, hessian_target) pairs."""
+    return [t - x.view(-1, IN_CH)[:, 1].float() for x, t in zip(xs, ts)]
+
+
+def prediction_to_hessian(torch, target, out, x16, shape):
+    """Pseudo-Hessian (up to scale) from the network output of a `target` mode network."""
+    pred = out.float()
+    if target == "log_h_over_ws":
+        pred = pred + x16.view(-1, IN_CH)[:, 1].float()
+    elif target != "log_h":
+        raise ValueError(target)
+    return hessian_from_prediction(pred.cpu().numpy().reshape(shape))

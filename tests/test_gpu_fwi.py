@@ -70,9 +70,20 @@ def test_training_pairs_and_learned_fwi():
     net = nn.UNet(torch, seed=1)
     losses = fwi.train(net, torch, xs, ts, p["ny"], p["nx"], epochs=15, batch=2, lr=2e-3)
     assert losses[-1] < losses[0]
+    # the residual mode learns the correction to the forward energy Ws
+    res_net = nn.UNet(torch, seed=1)
+    res_net.target = "log_h_over_ws"
+    tr = nn.residual_targets(torch, xs, ts)
+    assert float(sum(float((t * t).mean()) for t in tr)) < float(sum(float((t * t).mean()) for t in ts))
+    res_losses = fwi.train(res_net, torch, xs, tr, p["ny"], p["nx"], epochs=15, batch=2, lr=2e-3)
+    assert res_losses[-1] < res_losses[0]
     prob = fwi.Problem(cfg, test_shots=2)
     try:
         hist, _ = fwi.run(prob, 3, method="learned", net=net, torch=torch, eps_scale=0.02)
+        hist_res, _ = fwi.run(prob, 3, method="learned_sym", net=res_net, torch=torch, eps_scale=0.02)
+        hist_ws, _ = fwi.run(prob, 3, method="energy_src", eps_scale=0.02)
     finally:
         prob.close()
     assert hist[-1]["misfit"] < hist[0]["misfit"]
+    assert hist_res[-1]["misfit"] < hist_res[0]["misfit"]
+    assert hist_ws[-1]["misfit"] < hist_ws[0]["misfit"]
