@@ -76,6 +76,8 @@ def args_parse():
     ap.add_argument("--targets", default="log_h",
                     help="c5 only: comma list of network output modes (dsh.nn.TARGETS); the learned methods run "
                          "once per network, the first target's runs unsuffixed")
+    ap.add_argument("--problem-seeds", default="6",
+                    help="c5 only: comma list of FWI problem seeds (config5(seed)); value = median ratio")
     ap.add_argument("--nt-scale", type=float, default=1.0, help="c4 only: factor on every model's NT")
     ap.add_argument("--nt", type=int, default=None, help="time steps (default: the workload's NT)")
     ap.add_argument("--nx", type=int, default=2000, help="c2 only")
@@ -725,48 +727,66 @@ def bench_learned(a, rank, world, local):
                 np.savez(cache[t], **nets[t].state())
             del tt
         del xs, ts
-    prob = fwi.Problem(cfg, test_shots=4)
-    prob.observe()
-    w0 = time.time()
-    hp, _ = fwi.run(prob, a.fwi_iters, method="plain", log=log)
-    w1 = time.time()
-    target = hp[-1]["misfit"] * 1.01
-    t_plain = hp[-1]["gpu_s"]
     curve = lambda h: [[round(r["gpu_s"], 3), r["misfit"]] for r in h]
-    res = {}
     runs = []
     for m in [x for x in a.methods.split(",") if x]:
         if m.startswith("learned"):
             runs += [(m if k == 0 else f"{m}@{t}", m, nets[t]) for k, t in enumerate(targets)]
         else:
             runs.append((m, m, None))
-    for key, m, net in runs:
-        ws = time.time()
-        hl, _ = fwi.run(prob, a.fwi_iters, method=m, net=net, torch=torch, target_misfit=target, log=log)
-        t = time_to_reach(hl, target)
-        res[key] = {"final_misfit": hl[-1]["misfit"], "gpu_s_to_target": t, "gpu_s_total": hl[-1]["gpu_s"],
-                    "ratio": (t / t_plain) if t is not None else None,
-                    "wall_ratio": ((time.time() - ws) / (w1 - w0)) if t is not None else None,
-                    "iterations": len(hl) - 1, "fallbacks": sum(1 for r in hl if r.get("fallback")),
-                    "network_target": net.target if net is not None else None, "curve": curve(hl)}
-    prob.close()
+    seeds = [int(x) for x in a.problem_seeds.split(",") if x]
+    per_seed = []
+    for seed in seeds:
+        pcfg = configs.config5(seed=seed, **({"nt": a.nt} if a.nt else {}))
+        prob = fwi.Problem(pcfg, test_shots=4)
+        prob.observe()
+        w0 = time.time()
+        hp, _ = fwi.run(prob, a.fwi_iters, method="plain", log=log)
+        w1 = time.time()
+        target = hp[-1]["misfit"] * 1.01
+        t_plain = hp[-1]["gpu_s"]
+        res = {}
+        for key, m, net in runs:
+            ws = time.time()
+            hl, _ = fwi.run(prob, a.fwi_iters, method=m, net=net, torch=torch, target_misfit=target, log=log)
+            t = time_to_reach(hl, target)
+            res[key] = {"final_misfit": hl[-1]["misfit"], "gpu_s_to_target": t, "gpu_s_total": hl[-1]["gpu_s"],
+                        "ratio": (t / t_plain) if t is not None else None,
+                        "wall_ratio": ((time.time() - ws) / (w1 - w0)) if t is not None else None,
+                        "iterations": len(hl) - 1, "fallbacks": sum(1 for r in hl if r.get("fallback")),
+                        "network_target": net.target if net is not None else None, "curve": curve(hl)}
+        prob.close()
+        per_seed.append({"seed": seed, "plain": {"final_misfit": hp[-1]["misfit"], "gpu_s": t_plain,
+                                                 "iterations": len(hp) - 1, "curve": curve(hp)},
+                         "methods": res})
     primary = a.methods.split(",")[0]
+
+    def median_ratio(key, field="ratio"):
+        v = sorted(float("inf") if r["methods"][key][field] is None else r["methods"][key][field] for r in per_seed)
+        med = v[len(v) // 2] if len(v) % 2 else 0.5 * (v[len(v) // 2 - 1] + v[len(v) // 2])
+        return None if med == float("inf") else med
+
+    summary = {key: {"median_ratio": median_ratio(key), "ratios": [r["methods"][key]["ratio"] for r in per_seed]}
+               for key, _, _ in runs}
     line = {
         "metric": "learned-vs-plain FWI: GPU-seconds to the plain method's final misfit (ratio)",
-        "value": res[primary]["ratio"], "method": primary,
+        "value": summary[primary]["median_ratio"], "method": primary,
         "unit": "ratio", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 solver, bf16 network", "data": "synthetic",
         "config": {"workload": f"learned-fwi-{nx}x{ny}-fd8-L3-{ns}shots-nt{p['nt']}", "fwi_iters": a.fwi_iters,
                    "train_models": a.train_models, "train_shots": len(train_shots), "epochs": a.epochs,
-                   "network_targets": targets,
+                   "network_targets": targets, "problem_seeds": seeds,
                    "unet": "4 levels, 32 base channels, bf16 weights/activations, fp32 accumulation",
-                   "target": "plain final misfit x 1.01", "net_cache": bool(a.net_cache and gen_s == 0.0)},
-        "plain": {"final_misfit": hp[-1]["misfit"], "gpu_s": t_plain, "iterations": len(hp) - 1, "curve": curve(hp)},
-        "methods": res,
+                   "target": "plain final misfit x 1.01", "value": "median over the problem seeds",
+                   "net_cache": bool(a.net_cache and gen_s == 0.0)},
+        "summary": summary,
+        "plain": per_seed[0]["plain"],
+        "methods": per_seed[0]["methods"],
+        "per_seed": per_seed[1:],
         "training": {"data_gpu_s": gen_s, "train_gpu_s": train_s,
                      "loss_first": {t: v[0] for t, v in losses.items()},
                      "loss_last": {t: v[-1] for t, v in losses.items()}},
-        "e2e": {"value": res[primary]["wall_ratio"], "unit": "ratio (host wall-clock of the FWI runs)",
+        "e2e": {"value": median_ratio(primary, "wall_ratio"), "unit": "ratio (host wall-clock of the FWI runs)",
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
         "wall_s": time.time() - t0,
     }
