@@ -71,12 +71,12 @@ def args_parse():
     ap.add_argument("--fwi-iters", type=int, default=20, help="c5 only: L-BFGS iterations")
     ap.add_argument("--net-cache", default=None, help="c5 only: .npz of trained U-Net weights (load if present, "
                                                       "else train and save)")
-    ap.add_argument("--methods", default="learned_sym,learned,hessian",
+    ap.add_argument("--methods", default="learned,hessian,energy_src",
                     help="c5 only: preconditioners compared with plain (the first one gives `value`)")
-    ap.add_argument("--targets", default="log_h",
+    ap.add_argument("--targets", default="log_h_over_ws",
                     help="c5 only: comma list of network output modes (dsh.nn.TARGETS); the learned methods run "
                          "once per network, the first target's runs unsuffixed")
-    ap.add_argument("--problem-seeds", default="6",
+    ap.add_argument("--problem-seeds", default="6,7,8,9",
                     help="c5 only: comma list of FWI problem seeds (config5(seed)); value = median ratio")
     ap.add_argument("--nt-scale", type=float, default=1.0, help="c4 only: factor on every model's NT")
     ap.add_argument("--nt", type=int, default=None, help="time steps (default: the workload's NT)")
