@@ -8,7 +8,10 @@ gradient of its shots with its own engine, and one all-reduce (NCCL on GPUs,
 gloo on CPU) sums gradients and misfits.  No halo exchange exists: each grid
 lives on one GPU.  The conversion to (vs, rho) is linear in the shot sums, so
 summing converted per-rank gradients equals converting the global sum up to
-float rounding.
+float rounding.  Per iteration the updated model goes out from rank 0 in one
+broadcast (broadcast_model) and the line search's test-shot misfits come back
+in one scalar all-reduce per test step (distributed_misfit), as the reference
+sums them over ranks (src/line_search.c:300-306).
 """
 from __future__ import annotations
 
@@ -81,3 +84,52 @@ def distributed_gradient(local_gradient: Callable[[list[int]], dict], nshots: in
     buf = buf.cpu().numpy()
     n = gv.size
     return GradientResult(buf[:n].reshape(shape), buf[n:].reshape(shape), float(l2t.item()), mine)
+
+
+def _device(group, device):
+    import torch
+    import torch.distributed as dist
+
+    if device is not None:
+        return device
+    return "cuda" if torch.cuda.is_available() and dist.get_backend(group) == "nccl" else "cpu"
+
+
+def broadcast_model(vs: np.ndarray, rho: np.ndarray, qs: np.ndarray | None = None, src: int = 0, group=None,
+                    device=None):
+    """Rank src's model (vs, rho[, qs]) on every rank of `group`, in one
+    broadcast of the concatenated fields; returns the received arrays."""
+    import torch
+    import torch.distributed as dist
+
+    fields = [vs, rho] + ([qs] if qs is not None else [])
+    shape = np.asarray(vs).shape
+    if not dist.is_initialized() or dist.get_world_size(group) == 1:
+        return tuple(np.asarray(f, np.float32) for f in fields) + ((None,) if qs is None else ())
+    buf = torch.from_numpy(np.concatenate([np.asarray(f, np.float32).ravel() for f in fields])).to(_device(group, device))
+    dist.broadcast(buf, src=src, group=group)
+    out = buf.cpu().numpy()
+    n = int(np.prod(shape))
+    arrs = [out[k * n:(k + 1) * n].reshape(shape).copy() for k in range(len(fields))]
+    return tuple(arrs) + ((None,) if qs is None else ())
+
+
+def distributed_misfit(local_misfit: Callable[[list[int]], float], indices: Sequence[int],
+                       costs: Sequence[float] | None = None, group=None, device=None) -> float:
+    """Sum over ranks of local_misfit(my share of `indices`) (e.g. the test
+    shots of one line-search step): the shots are partitioned like the
+    gradient's, a rank without shots contributes 0, one scalar all-reduce."""
+    import torch
+    import torch.distributed as dist
+
+    idx = list(indices)
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    parts = partition(costs if costs is not None else [1.0] * len(idx), world)
+    mine = [idx[k] for k in parts[rank]]
+    val = float(local_misfit(mine)) if mine else 0.0
+    if world == 1:
+        return val
+    t = torch.tensor([val], dtype=torch.float64, device=_device(group, device))
+    dist.all_reduce(t, group=group)
+    return float(t.item())

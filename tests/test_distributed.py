@@ -1,5 +1,6 @@
 """Shot-parallel gradient across processes (CPU, gloo, world size 2): shot
-partitioning, the all-reduce of gradients and misfit, and failure detection
+partitioning, the all-reduce of gradients and misfit, the model broadcast and
+the line search's scalar misfit all-reduce, and failure detection
 when a rank dies before the collective (the survivor gets an error from a
 short process-group timeout instead of hanging).  The per-rank gradient comes
 from the CPU oracle, standing in for a GPU engine."""
@@ -69,7 +70,7 @@ def _worker(rank, world, port, outdir, fail_rank):
     sys.path[:0] = [os.path.join(root, "denise-sh_b200"), os.path.join(root, "oracle")]
     import torch.distributed as dist
 
-    from dsh.distributed import distributed_gradient
+    from dsh.distributed import broadcast_model, distributed_gradient, distributed_misfit
 
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=8))
@@ -79,8 +80,15 @@ def _worker(rank, world, port, outdir, fail_rank):
             raise RuntimeError("injected failure before the collective")
         res = distributed_gradient(lambda idx: _local_gradient(m, shots, obs, idx), len(shots), (m.ny, m.nx),
                                    costs=[1.0] * len(shots))
+        # rank 0's updated model reaches every rank in one broadcast
+        vs_new = (m.vs * np.float32(1.01)).astype(np.float32) if rank == 0 else np.zeros_like(m.vs)
+        rho_new = m.rho if rank == 0 else np.zeros_like(m.rho)
+        bvs, brho, bqs = broadcast_model(vs_new, rho_new)
+        # line-search misfit of three test shots: partitioned, one scalar all-reduce
+        test = [0, 2, 4]
+        mis = distributed_misfit(lambda idx: _local_gradient(m, shots, obs, idx)["l2"], test)
         np.savez(os.path.join(outdir, f"r{rank}.npz"), g_vs=res.g_vs, g_rho=res.g_rho, l2=res.l2,
-                 mine=np.array(res.my_shots))
+                 mine=np.array(res.my_shots), bvs=bvs, brho=brho, bqs_none=np.array(bqs is None), mis=mis)
     except Exception as e:   # noqa: BLE001 - report any failure to the parent
         with open(os.path.join(outdir, f"err{rank}.txt"), "w") as f:
             f.write(repr(e))
@@ -117,6 +125,11 @@ def test_two_ranks_match_single_process(tmp_path):
         assert np.allclose(o["g_rho"], ref["g_rho"], rtol=1e-5, atol=1e-6 * np.abs(ref["g_rho"]).max())
         assert abs(float(o["l2"]) - ref["l2"]) <= 1e-12 * ref["l2"] + 1e-30
     assert np.array_equal(outs[0]["g_vs"], outs[1]["g_vs"])
+    for o in outs:
+        assert np.array_equal(o["bvs"], (m.vs * np.float32(1.01)).astype(np.float32))
+        assert np.array_equal(o["brho"], m.rho) and bool(o["bqs_none"])
+        ref_mis = _local_gradient(m, shots, obs, [0, 2, 4])["l2"]
+        assert abs(float(o["mis"]) - ref_mis) <= 1e-12 * ref_mis
 
 
 @pytest.mark.timeout(120)
