@@ -63,6 +63,13 @@ def _lib():
         L.dsh_write_model.argtypes = [cp, ci, ci, vp]
         L.dsh_write_su.argtypes = [cp, ci, ci, vp, vp, vp, cf, cf, cf, cf, ci, vp]
         L.dsh_read_su.argtypes = [cp, ci, ci, vp]
+        L.dsh_stager_create.restype = vp
+        L.dsh_stager_create.argtypes = [ci, C.c_longlong, ci, C.POINTER(ci)]
+        L.dsh_stager_submit.argtypes = [vp, ci, C.POINTER(cp), vp, ci]
+        L.dsh_stager_acquire.argtypes = [vp, vp, C.POINTER(vp), C.POINTER(C.c_longlong)]
+        L.dsh_stager_acquire_host.argtypes = [vp, C.POINTER(vp), C.POINTER(C.c_longlong)]
+        L.dsh_stager_release.argtypes = [vp, vp]
+        L.dsh_stager_destroy.argtypes = [vp]
         _configured = True
     return L
 
@@ -140,3 +147,48 @@ def read_su(path: str, ntr: int, ns: int):
     sec = np.zeros((ntr, ns), np.float32)
     _check(_lib().dsh_read_su(_b(path), ntr, ns, sec.ctypes.data), "dsh_read_su")
     return sec
+
+
+class Stager:
+    """Asynchronous reader of observed SU data (dsh_stager): submit batches of
+    files, then acquire them in order - on the device (use_device=True: a
+    device pointer the given CUDA stream may use once the upload completes)
+    or as host arrays - and release each before the next acquire."""
+
+    def __init__(self, nbuf: int, max_floats: int, use_device: bool = True):
+        st = C.c_int(0)
+        self.h = _lib().dsh_stager_create(nbuf, max_floats, int(use_device), C.byref(st))
+        if not self.h:
+            _check(st.value or -1, "dsh_stager_create")
+        self.device = use_device
+
+    def submit(self, paths, ntr, ns: int) -> None:
+        arr = (C.c_char_p * len(paths))(*[_b(p) for p in paths])
+        n = np.ascontiguousarray(ntr, np.int32)
+        _check(_lib().dsh_stager_submit(self.h, len(paths), arr, n.ctypes.data, ns), "dsh_stager_submit")
+
+    def acquire(self, stream: int | None = None):
+        """(device pointer, number of floats) of the oldest batch."""
+        ptr, n = C.c_void_p(), C.c_longlong()
+        _check(_lib().dsh_stager_acquire(self.h, stream, C.byref(ptr), C.byref(n)), "dsh_stager_acquire")
+        return ptr.value, n.value
+
+    def acquire_host(self):
+        """A copy of the oldest batch as a float32 array."""
+        ptr, n = C.c_void_p(), C.c_longlong()
+        _check(_lib().dsh_stager_acquire_host(self.h, C.byref(ptr), C.byref(n)), "dsh_stager_acquire_host")
+        return np.ctypeslib.as_array((C.c_float * n.value).from_address(ptr.value)).copy()
+
+    def release(self, stream: int | None = None) -> None:
+        _check(_lib().dsh_stager_release(self.h, stream), "dsh_stager_release")
+
+    def close(self) -> None:
+        if self.h:
+            _lib().dsh_stager_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()

@@ -104,6 +104,29 @@ int dsh_write_su(const char *path, int ntr, int ns, const float *section, const 
 /* SU input as src/inseis.c:73-82 fills it: section [ntr][ns], sample 1 set to 0. */
 int dsh_read_su(const char *path, int ntr, int ns, float *section);
 
+/* Asynchronous staging of observed data for the shot loop, in place of the
+ * synchronous inseis reads before each residual (src/denise.c:1364-1420).
+ * A host thread reads the SU files of submitted batches (dsh_read_su, the
+ * same values) into nbuf buffers of max_floats floats; with use_device = 1
+ * the buffers are page-locked and dsh_stager_acquire copies the oldest batch
+ * to device memory on the stager's own stream and makes `stream` (a
+ * cudaStream_t as void*) wait for that copy, so reading and uploading overlap
+ * the computation on the previous batch.  A batch is the files' sections
+ * concatenated ([ntr[0]][ns], [ntr[1]][ns], ...), the layout dsh_gradient
+ * takes as observed data.  Acquire and release alternate; the buffer returns
+ * to the reader once `stream` has passed dsh_stager_release, and batch i is
+ * read once batch i - nbuf is released.  acquire returns the batch's read
+ * status (DSH_ERR_PARAM when a file could not be read; release it all the
+ * same); with use_device = 0, dsh_stager_acquire_host returns the host
+ * buffer instead (release with stream NULL).  Submitting needs no GPU. */
+typedef struct dsh_stager dsh_stager;
+dsh_stager *dsh_stager_create(int nbuf, long long max_floats, int use_device, int *status);
+int dsh_stager_submit(dsh_stager *s, int nfiles, const char *const *paths, const int *ntr, int ns);
+int dsh_stager_acquire(dsh_stager *s, void *stream, const float **dev, long long *nfloats);
+int dsh_stager_acquire_host(dsh_stager *s, const float **host, long long *nfloats);
+int dsh_stager_release(dsh_stager *s, void *stream);
+int dsh_stager_destroy(dsh_stager *s);
+
 #ifdef __cplusplus
 }
 #endif
