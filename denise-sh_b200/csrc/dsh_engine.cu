@@ -518,10 +518,13 @@ extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, co
     const dsh_params &p = ctx->p;
     const int L = p.l;
     const size_t n = (size_t)p.nx * p.ny;
-    for (size_t k = 0; k < n; k++) {
-        if (!std::isfinite(vs[k]) || !std::isfinite(rho[k]) || vs[k] < 0 || rho[k] < 0) return DSH_ERR_PARAM;
-        if (L > 0 && !(qs[k] > 0)) return DSH_ERR_PARAM;
+    int bad = 0;
+#pragma omp parallel for schedule(static) reduction(| : bad)
+    for (long long k = 0; k < (long long)n; k++) {
+        if (!std::isfinite(vs[k]) || !std::isfinite(rho[k]) || vs[k] < 0 || rho[k] < 0) bad |= 1;
+        if (L > 0 && !(qs[k] > 0)) bad |= 1;
     }
+    if (bad) return DSH_ERR_PARAM;
     std::vector<float> brho(n), uip(n), ujp(n), muip(L ? n : 1), mujp(L ? n : 1), tip(L ? n : 1), taus(L ? n : 1);
     if (dsh_setup_holberg(p.fdorder, p.maxrelerror, ctx->hc) != 0) return DSH_ERR_PARAM;
     if (dsh_setup_model(p.nx, p.ny, L, p.fl, p.dt, vs, rho, qs, brho.data(), uip.data(), ujp.data(), nullptr, nullptr,

@@ -5,6 +5,10 @@
  * libm calls and double literals) and the same operation order as the
  * reference, so the device kernels see bit-identical inputs.  Compiled as C
  * (C++ would pick float overloads of pow/exp/log) with -ffp-contract=off.
+ * The per-point loops run on the host's cores (OpenMP); every point is
+ * computed by the same expression either way, and the reductions (the mean
+ * model of the gradient normalisation) stay sequential in the reference's
+ * order.
  */
 #include "dsh_setup.h"
 
@@ -158,24 +162,27 @@ int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const floa
 {
     const size_t n = (size_t)nx * ny;
     float *mu_ip = NULL, *mu_jp = NULL, *taus = NULL, *tausipjp = NULL;
-    size_t k;
     int i, j, m;
     if (nx < 1 || ny < 1 || l < 0 || l > DSH_MAX_L) return -1;
 
-    if (brho)
-        for (k = 0; k < n; k++) {
-            float b = 1.0 / rho[k];
-            if (rho[k] < 1e-20) b = 0.0;
-            brho[k] = b;
+    if (brho) {
+#pragma omp parallel for schedule(static)
+        for (long long kk = 0; kk < (long long)n; kk++) {
+            float b = 1.0 / rho[kk];
+            if (rho[kk] < 1e-20) b = 0.0;
+            brho[kk] = b;
         }
+    }
 
     /* shear modulus mu = rho*vs^2 and its harmonic means at (i+1/2, j) and
      * (i, j+1/2); zero if either side is zero */
     mu_ip = uip ? uip : (float *)malloc(n * sizeof(float));
     mu_jp = ujp ? ujp : (float *)malloc(n * sizeof(float));
     if (!mu_ip || !mu_jp) return -1;
-    for (j = 1; j <= ny; j++)
-        for (i = 1; i <= nx; i++) {
+#pragma omp parallel for schedule(static)
+    for (int jj = 1; jj <= ny; jj++)
+        for (int ii = 1; ii <= nx; ii++) {
+            const int i = ii, j = jj;
             size_t c = nb(nx, ny, i, j), e = nb(nx, ny, i + 1, j), s = nb(nx, ny, i, j + 1);
             float mu_c = rho[c] * vs[c] * vs[c];
             float mu_e = rho[e] * vs[e] * vs[e];
@@ -196,11 +203,13 @@ int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const floa
             tau_sls[m] = 1.0 / (2.0 * DSH_PI * fl[m]);
             eta[m] = dt / tau_sls[m];
         }
-        for (k = 0; k < n; k++) taus[k] = 2.0 / qs[k];
-        for (j = 1; j <= ny; j++)
-            for (i = 1; i <= nx; i++)
-                tausipjp[nb(nx, ny, i, j)] = 0.25 * (taus[nb(nx, ny, i, j)] + taus[nb(nx, ny, i + 1, j)] +
-                                                     taus[nb(nx, ny, i, j + 1)] + taus[nb(nx, ny, i + 1, j + 1)]);
+#pragma omp parallel for schedule(static)
+        for (long long kk = 0; kk < (long long)n; kk++) taus[kk] = 2.0 / qs[kk];
+#pragma omp parallel for schedule(static)
+        for (int jj = 1; jj <= ny; jj++)
+            for (int ii = 1; ii <= nx; ii++)
+                tausipjp[nb(nx, ny, ii, jj)] = 0.25 * (taus[nb(nx, ny, ii, jj)] + taus[nb(nx, ny, ii + 1, jj)] +
+                                                       taus[nb(nx, ny, ii, jj + 1)] + taus[nb(nx, ny, ii + 1, jj + 1)]);
         /* relaxed-modulus correction at the reference frequency FL[1] */
         omega = 2.0 * DSH_PI * fl[0];
         for (m = 0; m < l; m++)
@@ -212,14 +221,16 @@ int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const floa
             if (cip) cip[m] = 1.0 - (eta[m] * 0.5);
             if (cjm) cjm[m] = 1.0 - (eta[m] * 0.5);
         }
-        for (k = 0; k < n; k++) {
-            float mujp = mu_jp[k] / (1.0 + sumu * taus[k]);
-            float muip = mu_ip[k] / (1.0 + sumu * tausipjp[k]);
-            if (fipjp) fipjp[k] = muip * dt * (1.0 + l * tausipjp[k]);
-            if (f) f[k] = mujp * dt * (1.0 + l * taus[k]);
-            for (m = 0; m < l; m++) {
-                if (dip) dip[(size_t)m * n + k] = muip * eta[m] * tausipjp[k];
-                if (d) d[(size_t)m * n + k] = mujp * eta[m] * taus[k];
+#pragma omp parallel for schedule(static)
+        for (long long kk = 0; kk < (long long)n; kk++) {
+            const size_t q = (size_t)kk;
+            float mujp = mu_jp[q] / (1.0 + sumu * taus[q]);
+            float muip = mu_ip[q] / (1.0 + sumu * tausipjp[q]);
+            if (fipjp) fipjp[q] = muip * dt * (1.0 + l * tausipjp[q]);
+            if (f) f[q] = mujp * dt * (1.0 + l * taus[q]);
+            for (int mm = 0; mm < l; mm++) {
+                if (dip) dip[(size_t)mm * n + q] = muip * eta[mm] * tausipjp[q];
+                if (d) d[(size_t)mm * n + q] = mujp * eta[mm] * taus[q];
             }
         }
         free(taus);
@@ -250,8 +261,7 @@ int dsh_setup_visc_base(int nx, int ny, int l, const float *fl, float dt, const 
 {
     const size_t n = (size_t)nx * ny;
     float tau_sls[DSH_MAX_L], omega, sumu = 0.0;
-    size_t k;
-    int i, j, m;
+    int m;
     if (nx < 1 || ny < 1 || l < 1 || l > DSH_MAX_L) return -1;
     if (dsh_setup_model(nx, ny, 0, fl, dt, vs, rho, qs, NULL, muip, mujp, NULL, NULL, NULL, NULL, NULL, NULL, NULL,
                         NULL, NULL) != 0)
@@ -260,19 +270,22 @@ int dsh_setup_visc_base(int nx, int ny, int l, const float *fl, float dt, const 
         tau_sls[m] = 1.0 / (2.0 * DSH_PI * fl[m]);
         eta[m] = dt / tau_sls[m];
     }
-    for (k = 0; k < n; k++) taus[k] = 2.0 / qs[k];
-    for (j = 1; j <= ny; j++)
-        for (i = 1; i <= nx; i++)
-            tausipjp[nb(nx, ny, i, j)] = 0.25 * (taus[nb(nx, ny, i, j)] + taus[nb(nx, ny, i + 1, j)] +
-                                                 taus[nb(nx, ny, i, j + 1)] + taus[nb(nx, ny, i + 1, j + 1)]);
+#pragma omp parallel for schedule(static)
+    for (long long kk = 0; kk < (long long)n; kk++) taus[kk] = 2.0 / qs[kk];
+#pragma omp parallel for schedule(static)
+    for (int jj = 1; jj <= ny; jj++)
+        for (int ii = 1; ii <= nx; ii++)
+            tausipjp[nb(nx, ny, ii, jj)] = 0.25 * (taus[nb(nx, ny, ii, jj)] + taus[nb(nx, ny, ii + 1, jj)] +
+                                                   taus[nb(nx, ny, ii, jj + 1)] + taus[nb(nx, ny, ii + 1, jj + 1)]);
     omega = 2.0 * DSH_PI * fl[0];
     for (m = 0; m < l; m++)
         sumu = sumu + ((omega * omega * tau_sls[m] * tau_sls[m]) / (1.0 + omega * omega * tau_sls[m] * tau_sls[m]));
-    for (k = 0; k < n; k++) {
-        float u_jp = mujp[k] / (1.0 + sumu * taus[k]);
-        float u_ip = muip[k] / (1.0 + sumu * tausipjp[k]);
-        mujp[k] = u_jp;
-        muip[k] = u_ip;
+#pragma omp parallel for schedule(static)
+    for (long long kk = 0; kk < (long long)n; kk++) {
+        float u_jp = mujp[kk] / (1.0 + sumu * taus[kk]);
+        float u_ip = muip[kk] / (1.0 + sumu * tausipjp[kk]);
+        mujp[kk] = u_jp;
+        muip[kk] = u_ip;
     }
     return 0;
 }
