@@ -261,6 +261,10 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
     float4 acc4 = make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 old4 = vy4;
     const int nvalid = min(4, a.nx - i0 + 1);
+    /* whether a CPML strip holds any of the four points (false for the whole
+       warp almost everywhere: one branch instead of four tests per point) */
+    const bool in_pml = a.fw > 0 && (i0 <= a.fw || i0 + 3 >= a.nx - a.fw + 1 || (!a.free_surf && j <= a.fw) ||
+                                     j >= a.ny - a.fw + 1);
 #pragma unroll
     for (int k = 0; k < 4; k++) {
         const int i = i0 + k;
@@ -274,7 +278,7 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
             else { sxy_x = sxy_x + tx; syy_y = syy_y + ty; }
         }
         const int fw = a.fw;
-        if (fw > 0 && i <= a.nx) {
+        if (in_pml && i <= a.nx) {
             if (i <= fw) {
                 float *p = a.psi_vxx + so + (long long)(j - 1) * 2 * fw + (i - 1);
                 float ps = __ldg(a.pml.b_x + i) * *p + __ldg(a.pml.a_x + i) * sxy_x;
@@ -489,6 +493,8 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
 
     /* ---- derivatives and CPML ---- */
     const float dhi = (L > 0) ? a.dhi_visc : a.dhi_el;
+    const bool in_pml = a.fw > 0 && (i0 <= a.fw || i0 + 3 >= a.nx - a.fw + 1 || (!a.free_surf && j <= a.fw) ||
+                                     j >= a.ny - a.fw + 1);
     float4 vyx4 = make_float4(0.f, 0.f, 0.f, 0.f), vyy4 = vyx4;
 #pragma unroll
     for (int k = 0; k < 4; k++) {
@@ -504,7 +510,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
         vyx = vyx * dhi;
         vyy = vyy * dhi;
         const int fw = a.fw;
-        if (fw > 0 && i <= a.nx) {
+        if (in_pml && i <= a.nx) {
             if (i <= fw) {
                 float *p = a.psi_sxx + so + (long long)(j - 1) * 2 * fw + (i - 1);
                 float ps = __ldg(a.pml.b_x_half + i) * *p + __ldg(a.pml.a_x_half + i) * vyx;
