@@ -820,6 +820,7 @@ StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.l = p.l; a.fd12_compat = p.compat_fd12;
     a.fdo = p.fdorder; a.p2 = dh_pow2(p.dh) ? 1 : 0; a.nslots = ctx->S;
     a.nt_last = p.nt; a.nt_total = p.nt; a.nt_base = ctx->d_nt;
+    a.chk_mask = 15;
     a.fstride = ctx->fstride; a.dstride = ctx->dstride; a.slot_stride = ctx->slot_stride;
     for (int k = 0; k < 7; k++) a.hc[k] = ctx->hc[k];
     a.dt = p.dt; a.dh = p.dh;

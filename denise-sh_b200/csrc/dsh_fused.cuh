@@ -215,12 +215,12 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
                     }
                 }
                 if (MODE == FM_STORE) {      /* forward storage of vyp1 */
-                    const long long k = (nt - 1) % a.fwd_mod;
+                    const long long k = store_idx(nt - 1, a.fwd_mod);
                     st4m(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4,
                          nvalid);
                 }
                 if (MODE == FM_ADJ) {        /* g_rho += vyp1 * forward acceleration (denise.c:1589) */
-                    const long long k = (a.nt_total - nt) % a.fwd_mod;
+                    const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
                     const float4 f4 =
                         ldg4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
                     float4 g4 = ld4(a.grho + so + drow + col0);
@@ -274,7 +274,7 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
         if (a.ws) w4 = ld4(a.ws + so + drow + col0);
         if (MODE == FM_ADJ) {
             g4 = ld4(a.gu + so + drow + col0);
-            const long long k = (a.nt_total - nt) % a.fwd_mod;
+            const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
             const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
             fy = ldg4(base + a.dstride);
             fu = ldg4(base + 2 * a.dstride);
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
               isfinite(syz4.y) && isfinite(syz4.z) && isfinite(syz4.w) && isfinite(vnow.x)))
             atomicOr(a.status, 1);
         if (MODE == FM_STORE) {
-            const long long k = (nt - 1) % a.fwd_mod;
+            const long long k = store_idx(nt - 1, a.fwd_mod);
             float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
             st4m(base + a.dstride, vyy4, nvalid);
             st4m(base + 2 * a.dstride, vyx4, nvalid);

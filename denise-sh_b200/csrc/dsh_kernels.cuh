@@ -80,6 +80,8 @@ struct StepArgs {
     int nslots;                  /* shot slots allocated (multi-model launches skip slots >= nslots) */
     int nt_last;                 /* last valid step of this pass (1-based) */
     int nt_total;                /* NT of the pass (for the Hessian's nt < NTDTINV) */
+    int chk_mask;                /* finite check of the updated fields on steps with (nt & chk_mask) == 0
+                                    and on the pass's last step (0: every step) */
     const int *nt_base;          /* device step counter; step = *nt_base + nt_off */
     long long fstride;           /* floats per haloed field */
     long long dstride;           /* floats per interior field */
@@ -155,6 +157,10 @@ __device__ __forceinline__ void set_lane(float4 &v, int k, float x)
 {
     if (k == 0) v.x = x; else if (k == 1) v.y = x; else if (k == 2) v.z = x; else v.w = x;
 }
+
+/* stored-step index s % mod (s >= 0); no division when the pass stores
+ * every step (mod = NT > s), the case of full storage */
+__device__ __forceinline__ long long store_idx(int s, int mod) { return s < mod ? s : s % mod; }
 
 /* x / DH: when DH is a power of two the product with the exact reciprocal is
  * the same correctly rounded value, so P2 kernels multiply. */
@@ -246,7 +252,7 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
     }
     if (nt > a.nt_last) return;
     if (FLAGS & VF_CORR) {                   /* stored forward acceleration of step NT-nt+1 */
-        const long long k = (a.nt_total - nt) % a.fwd_mod;
+        const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
         f4 = ldg4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
     }
     pdl_wait();                              /* stresses of the previous step are complete */
@@ -343,7 +349,7 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
         st4m(a.grho + so + drow + col0, g4, nvalid);
     }
     if (!(FLAGS & VF_ADJOINT) && a.fwd && !(FLAGS & VF_CORR)) {   /* forward storage of vyp1 */
-        const long long k = (nt - 1) % a.fwd_mod;
+        const long long k = store_idx(nt - 1, a.fwd_mod);
         st4m(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4, nvalid);
     }
     if ((FLAGS & VF_HESS) && nt < a.nt_total) {
@@ -466,7 +472,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     if (FLAGS & SF_HESS) h4 = ld4(a.hu + so + drow + col0);
     if (nt > a.nt_last) return;
     if (FLAGS & SF_CORR) {
-        const long long k = (a.nt_total - nt) % a.fwd_mod;
+        const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
         const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
         fy = ldg4(base + a.dstride);
         fu = ldg4(base + 2 * a.dstride);
@@ -611,7 +617,10 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
         st4m(a.r + so + l * a.dstride + drow + col0, rr[l], nvalid);
         st4m(a.q + so + l * a.dstride + drow + col0, qq[l], nvalid);
     }
-    if (!(isfinite(sxy4.x) && isfinite(sxy4.y) && isfinite(sxy4.z) && isfinite(sxy4.w) && isfinite(syz4.x) &&
+    /* a non-finite value never turns finite again in these updates, so a
+       check every few steps and on the last one finds every instability */
+    if (((nt & a.chk_mask) == 0 || nt >= a.nt_last) &&
+        !(isfinite(sxy4.x) && isfinite(sxy4.y) && isfinite(sxy4.z) && isfinite(sxy4.w) && isfinite(syz4.x) &&
           isfinite(syz4.y) && isfinite(syz4.z) && isfinite(syz4.w) && isfinite(xs[4 * NL])))
         atomicOr(a.status, 1);
     if (FLAGS & SF_STRAIN_OUT) {
@@ -619,7 +628,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
             st4m(a.out_uy + so + hrow + col0, vyy4, nvalid);
             st4m(a.out_uyx + so + hrow + col0, vyx4, nvalid);
         } else {                      /* forward storage: uy at +dstride, uyx at +2*dstride */
-            const long long k = (nt - 1) % a.fwd_mod;
+            const long long k = store_idx(nt - 1, a.fwd_mod);
             float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
             st4m(base + a.dstride, vyy4, nvalid);
             st4m(base + 2 * a.dstride, vyx4, nvalid);
