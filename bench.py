@@ -84,6 +84,9 @@ def args_parse():
     ap.add_argument("--ny", type=int, default=800, help="c2 only")
     ap.add_argument("--shots", type=int, default=64, help="c3 only: shots per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="c1-c3: keep the default kernel pair instead of timing the step-kernel variants "
+                         "(for runs under a profiler)")
     ap.add_argument("--cpu-steps", type=int, default=24, help="time steps per pass in the CPU sample")
     ap.add_argument("--profile-steps", type=int, default=20)
     return ap.parse_args()
@@ -330,7 +333,10 @@ def main():
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
     eng.set_model(cfg["vs"], cfg["rho"], cfg["qs"])
-    variant, variant_ms = eng.autotune(shots, nsteps=min(64, nt))   # step-kernel variant for this grid
+    if a.no_autotune:            # profiling runs: a profiler's serialised timings would mislead the tuner
+        variant, variant_ms = "kernel pair (autotuner skipped)", None
+    else:
+        variant, variant_ms = eng.autotune(shots, nsteps=min(64, nt))   # step-kernel variant for this grid
 
     seis = torch.empty(ntr_all * nt, device="cuda", dtype=torch.float32)
     if gradient:
