@@ -8,6 +8,7 @@ using KFn = void (*)(StepArgs, int);
 #define DSH_DECLARE_FD(N)                     \
     KFn v_kernel_fd##N(int flags, bool p2);    \
     KFn v_kernel_st_fd##N(int flags, bool p2); \
+    KFn v_kernel_tp_fd##N(int flags, bool p2); \
     KFn s_kernel_fd##N(int l, int flags);
 DSH_DECLARE_FD(2)
 DSH_DECLARE_FD(4)
@@ -40,6 +41,21 @@ inline KFn v_kernel_st(int fdo, int flags, bool p2)
     case 8: return v_kernel_st_fd8(flags, p2);
     case 10: return v_kernel_st_fd10(flags, p2);
     case 12: return v_kernel_st_fd12(flags, p2);
+    default: return nullptr;
+    }
+}
+
+/* persistent velocity step with TMA-staged taps (dsh_vtma.cuh); grid (blocks per slot, slots),
+ * block (32, 9) */
+inline KFn v_kernel_tp(int fdo, int flags, bool p2)
+{
+    switch (fdo) {
+    case 2: return v_kernel_tp_fd2(flags, p2);
+    case 4: return v_kernel_tp_fd4(flags, p2);
+    case 6: return v_kernel_tp_fd6(flags, p2);
+    case 8: return v_kernel_tp_fd8(flags, p2);
+    case 10: return v_kernel_tp_fd10(flags, p2);
+    case 12: return v_kernel_tp_fd12(flags, p2);
     default: return nullptr;
     }
 }

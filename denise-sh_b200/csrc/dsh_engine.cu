@@ -21,6 +21,8 @@
 #include "dsh_fused.cuh"
 #include "dsh_setup.h"
 
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -31,6 +33,8 @@
 
 using namespace dsh;
 using namespace dsh::eng;
+
+static void build_tmaps(dsh_ctx *ctx);
 
 namespace {
 
@@ -448,6 +452,7 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     ctx->o_hrho = o; o += ctx->dstride;
     ctx->slot_stride = o;
     if (cudaMalloc(&ctx->slab, (size_t)ctx->S * ctx->slot_stride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    build_tmaps(ctx);
     const long long nmodel = 9LL * ctx->dstride;
     if (cudaMalloc(&ctx->model, (size_t)nmodel * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     cudaMemset(ctx->model, 0, (size_t)nmodel * sizeof(float));
@@ -497,11 +502,71 @@ extern "C" int dsh_destroy(dsh_ctx *ctx)
     cudaFree(ctx->d_geo); cudaFree(ctx->d_offs); cudaFree(ctx->d_sig); cudaFree(ctx->d_seis); cudaFree(ctx->d_res);
     cudaFree(ctx->d_obs); cudaFree(ctx->d_tmp); cudaFree(ctx->d_out); cudaFree(ctx->d_nt); cudaFree(ctx->d_part); cudaFree(ctx->d_l2);
     cudaFree(ctx->d_wemax);
-    cudaFree(ctx->d_taper_box); cudaFree(ctx->d_taper_shot);
+    cudaFree(ctx->d_taper_box); cudaFree(ctx->d_taper_shot); cudaFree(ctx->d_tmap);
     for (int k = 0; k < 4; k++) if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     if (ctx->own_st) cudaStreamDestroy(ctx->own_st);
     delete ctx;
     return DSH_OK;
+}
+
+/* ---------------- tensor maps of the TMA-staged velocity kernel ---------------- */
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn tmap_encoder()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+/* one haloed field of every shot slot: dims (pitch, ny + 2hy, S) floats,
+ * row and slot strides in bytes (multiples of 16), box (bx floats, by rows,
+ * 1 slot), zero fill outside */
+static bool field_map(CUtensorMap *m, const dsh_ctx *ctx, const float *field, int bx, int by)
+{
+    EncodeTiledFn enc = tmap_encoder();
+    if (!enc || !field) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)ctx->pitch, (cuuint64_t)(ctx->p.ny + 2 * ctx->hy), (cuuint64_t)ctx->S};
+    const cuuint64_t strides[2] = {(cuuint64_t)ctx->pitch * 4, (cuuint64_t)ctx->slot_stride * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(field), dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+/* maps of sxy and syz for the slab and the shadow state (the slab's again
+ * while no shadow exists); on any failure the TMA variant stays off */
+static void build_tmaps(dsh_ctx *ctx)
+{
+    ctx->tma_ok = 0;
+    const int H = ctx->p.fdorder / 2, NL = (H + 3) / 4, NR = (H - 1 + 3) / 4;
+    const int bxs = 4 * (BX + NL + NR), bys = BY, bxy = 4 * BX, byy = BY + 2 * H - 1;
+    alignas(64) CUtensorMap maps[4];
+    const float *sh = ctx->shadow ? ctx->shadow : ctx->slab;
+    if (!field_map(&maps[0], ctx, ctx->slab + ctx->o_sxy, bxs, bys) ||
+        !field_map(&maps[1], ctx, ctx->slab + ctx->o_syz, bxy, byy) ||
+        !field_map(&maps[2], ctx, sh + ctx->o_sxy, bxs, bys) || !field_map(&maps[3], ctx, sh + ctx->o_syz, bxy, byy))
+        return;
+    if (!ctx->d_tmap && cudaMalloc(&ctx->d_tmap, sizeof(maps)) != cudaSuccess) {
+        cudaGetLastError();
+        ctx->d_tmap = nullptr;
+        return;
+    }
+    if (cudaMemcpy(ctx->d_tmap, maps, sizeof(maps), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaGetLastError();
+        return;
+    }
+    ctx->tma_ok = 1;
 }
 
 static int upload_field(dsh_ctx *ctx, float *dst, const float *src)
@@ -856,6 +921,11 @@ StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.fwd_mod = ctx->fwd_mod > 0 ? ctx->fwd_mod : p.nt;
     a.fwd_step_stride = ctx->fwd_step_stride;
     a.status = ctx->d_status;
+    if (ctx->tma_ok) {
+        const CUtensorMap *tm = (const CUtensorMap *)ctx->d_tmap + (pass == P_RECOMP ? 2 : 0);
+        a.tm_sxy = tm;
+        a.tm_syz = tm + 1;
+    }
     /* fused injection / sampling lists */
     a.tl.on = ctx->fused_inject;
     a.tl.ntiles = ctx->ntiles;
@@ -937,13 +1007,45 @@ static int env_flag(const char *name)
     return e && atoi(e) != 0;
 }
 
-static KFn pick_v(const dsh_ctx *ctx, int fdo, int vflags, bool p2)
+/* the velocity kernel of the pair: code 0 v_step, 1 v_step_st (DSH_VSTAGE=1
+ * or the autotuner), 2 the persistent TMA-staged v_step_tp (DSH_VTMA=1; it
+ * needs the context's tensor maps) */
+struct VPick {
+    KFn k;
+    int code;
+};
+
+static VPick pick_v(const dsh_ctx *ctx, int fdo, int vflags, bool p2)
 {
     static const int env = env_flag("DSH_VSTAGE");
+    static const int env_tma = env_flag("DSH_VTMA");
     const bool staged = ctx->sel_staged >= 0 ? ctx->sel_staged != 0 : env != 0;
     KFn k = staged ? v_kernel_st(fdo, vflags, p2) : nullptr;
-    return k ? k : v_kernel(fdo, vflags, p2);
+    if (k) return {k, 1};
+    if (env_tma && ctx->tma_ok && (k = v_kernel_tp(fdo, vflags, p2))) return {k, 2};
+    return {v_kernel(fdo, vflags, p2), 0};
 }
+
+/* launch shape of the picked velocity kernel for nb slots: the tile grid, or
+ * for the persistent one about two blocks per SM shared among the slots */
+static void v_shape(const dsh_ctx *ctx, const VPick &v, int nb, dim3 *grid, dim3 *block)
+{
+    const dsh_params &p = ctx->p;
+    const unsigned gx = (unsigned)((p.nx + 4 * BX - 1) / (4 * BX)), gy = (unsigned)((p.ny + BY - 1) / BY);
+    if (v.code == 2) {
+        int nsm = 148;
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->dev);
+        const unsigned per = (unsigned)std::max(1, 2 * nsm / std::max(1, nb));
+        *grid = dim3(std::min(per, gx * gy), (unsigned)nb, 1);
+        *block = dim3(BX, BY + 1, 1);           /* 8 computing warps + 1 producer warp */
+    } else {
+        *grid = dim3(gx, gy, (unsigned)nb);
+        *block = dim3(BX, BY, 1);
+    }
+}
+
+/* graph key code of the velocity kernel in use */
+static long long v_code(const dsh_ctx *ctx) { return pick_v(ctx, ctx->p.fdorder, 0, dh_pow2(ctx->p.dh)).code; }
 
 /* The fused step (one kernel per time step, dsh_fused.cuh) serves every pass
  * but the Hessian one when FDORDER <= 8 and injection/sampling are fused;
@@ -1002,12 +1104,15 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
     case P_FWD_CKPT: break;
     case P_RECOMP: sflags = SF_STRAIN_OUT; break;
     }
-    KFn vk = pick_v(ctx, p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
+    const VPick vp = pick_v(ctx, p.fdorder, vflags, dh_pow2(p.dh));
+    KFn vk = vp.k, sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
     StepArgs sa = step_args(ctx, pass);
     InjectArgs ia = inject_args(ctx, pass);
     dim3 block(BX, BY, 1);
     dim3 grid((unsigned)((p.nx + 4 * BX - 1) / (4 * BX)), (unsigned)((p.ny + BY - 1) / BY), (unsigned)nb);
+    dim3 vgrid, vblock;
+    v_shape(ctx, vp, nb, &vgrid, &vblock);
     /* velocity and stress kernels overlap their prologues with the
      * predecessor through programmatic dependent launch; the first velocity
      * kernel of a chunk follows the step-counter update and is launched plainly */
@@ -1025,7 +1130,11 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
         void *args[2] = {&sa, &off};
         cfg.attrs = (use_pdl && k > 0) ? &attr : nullptr;
         cfg.numAttrs = (use_pdl && k > 0) ? 1 : 0;
+        cfg.gridDim = vgrid;
+        cfg.blockDim = vblock;
         CK(cudaLaunchKernelExC(&cfg, (const void *)vk, args));
+        cfg.gridDim = grid;
+        cfg.blockDim = block;
         if (!sa.tl.on) {
             void *iargs[2] = {&ia, &off};
             CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
@@ -1044,9 +1153,9 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
 
 static int get_graph(dsh_ctx *ctx, Pass pass, int nb, int K, cudaGraphExec_t *out)
 {
-    const long long staged = pick_v(ctx, ctx->p.fdorder, 0, dh_pow2(ctx->p.dh)) != v_kernel(ctx->p.fdorder, 0, dh_pow2(ctx->p.dh));
-    const long long key = ((long long)pass << 48) | ((long long)ctx->fused_inject << 47) |
-                          ((long long)use_fused(ctx, pass) << 46) | (staged << 45) | ((long long)K << 32) |
+    const long long vcode = v_code(ctx);
+    const long long key = ((long long)pass << 52) | ((long long)ctx->fused_inject << 51) |
+                          ((long long)use_fused(ctx, pass) << 50) | (vcode << 45) | ((long long)K << 32) |
                           ((long long)nb << 16) | (long long)(ctx->geo_version & 0xffff);
     auto it = ctx->graphs.find(key);
     if (it != ctx->graphs.end()) { *out = it->second; return DSH_OK; }
@@ -1266,6 +1375,7 @@ static int ensure_storage(dsh_ctx *ctx)
         ctx->ckpt_c = C;
     }
     ctx->fwd_slot_stride = (long long)ctx->fwd_mod * ctx->fwd_step_stride;
+    build_tmaps(ctx);                     /* the shadow state may have changed */
     return DSH_OK;
 }
 
@@ -1756,12 +1866,15 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
     if (pass == P_FWD_STORE) sflags = SF_STRAIN_OUT;
     if (pass == P_FWD_HESS) { vflags = VF_HESS; sflags = SF_HESS; }
     if (pass == P_ADJ) { vflags = VF_ADJOINT | VF_CORR; sflags = SF_CORR; }
-    KFn vk = pick_v(ctx, p.fdorder, vflags, dh_pow2(p.dh)), sk = s_kernel(p.fdorder, p.l, sflags);
+    const VPick vp = pick_v(ctx, p.fdorder, vflags, dh_pow2(p.dh));
+    KFn vk = vp.k, sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
     StepArgs sa = step_args(ctx, (Pass)pass);
     InjectArgs ia = inject_args(ctx, (Pass)pass);
     dim3 block(BX, BY, 1);
     dim3 grid((unsigned)((p.nx + 4 * BX - 1) / (4 * BX)), (unsigned)((p.ny + BY - 1) / BY), (unsigned)nb);
+    dim3 vgrid, vblock;
+    v_shape(ctx, vp, nb, &vgrid, &vblock);
     /* each kernel launched nsteps times back to back between one event pair */
     cudaEvent_t ev[6];
     for (auto &e : ev) CK(cudaEventCreate(&e));
@@ -1770,7 +1883,7 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
         int off = 0;
         void *args[2] = {&sa, &off};
         void *iargs[2] = {&ia, &off};
-        CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
+        CK(cudaLaunchKernel((const void *)vk, vgrid, vblock, args, 0, ctx->st));
         if (!sa.tl.on) CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
         CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
     }
@@ -1780,7 +1893,7 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
             int off = k;
             void *args[2] = {&sa, &off};
             void *iargs[2] = {&ia, &off};
-            if (q == 0) CK(cudaLaunchKernel((const void *)vk, grid, block, args, 0, ctx->st));
+            if (q == 0) CK(cudaLaunchKernel((const void *)vk, vgrid, vblock, args, 0, ctx->st));
             if (q == 1 && !sa.tl.on) CK(cudaLaunchKernel((const void *)inject_sample, dim3(nb), dim3(128), iargs, 0, ctx->st));
             if (q == 2) CK(cudaLaunchKernel((const void *)sk, grid, block, args, 0, ctx->st));
         }

@@ -64,6 +64,8 @@ struct dsh_ctx {
     unsigned *d_wemax = nullptr;
     std::vector<int> ntr_b;
     int lnorm = 2;                        /* misfit norm of the residual (dsh_set_misfit) */
+    void *d_tmap = nullptr;               /* 4 CUtensorMap: sxy, syz of the slab, then of the shadow state */
+    int tma_ok = 0;                       /* the maps are built (the TMA-staged velocity kernel can run) */
     /* per-shot circular gradient taper (dsh_set_shot_taper): box [g][g] and,
        per slot, the first source's grid point and the normalisation */
     int taper_on = 0, taper_g = 0, taper_ijc = 0, taper_filt = 0;

@@ -2,6 +2,7 @@
  * dsh_fd<N>.cu so the orders compile in parallel). */
 #pragma once
 #include "dsh_dispatch.h"
+#include "dsh_vtma.cuh"
 
 #define DSH_INSTANTIATE_FD(N)                                                                 \
     namespace dsh {                                                                           \
@@ -29,6 +30,17 @@
         }                                                                                     \
     }                                                                                         \
     KFn v_kernel_st_fd##N(int flags, bool p2) { return p2 ? v_pick_st_##N<true>(flags) : v_pick_st_##N<false>(flags); } \
+    template <bool P2>                                                                        \
+    static KFn v_pick_tp_##N(int flags)                                                       \
+    {                                                                                         \
+        switch (flags) {                                                                      \
+        case 0: return v_step_tp<N, 0, P2>;                                                   \
+        case VF_HESS: return v_step_tp<N, VF_HESS, P2>;                                       \
+        case VF_ADJOINT | VF_CORR: return v_step_tp<N, VF_ADJOINT | VF_CORR, P2>;             \
+        default: return nullptr;                                                              \
+        }                                                                                     \
+    }                                                                                         \
+    KFn v_kernel_tp_fd##N(int flags, bool p2) { return p2 ? v_pick_tp_##N<true>(flags) : v_pick_tp_##N<false>(flags); } \
     template <int L>                                                                          \
     static KFn s_pick_##N(int flags)                                                          \
     {                                                                                         \

@@ -107,6 +107,8 @@ struct StepArgs {
     /* compat outputs (Layer-1): explicit vyp1/uy/uyx haloed fields */
     float *out_acc, *out_uy, *out_uyx;
     int *status;                 /* device error word (non-finite detection) */
+    const void *tm_sxy, *tm_syz;   /* tensor maps (CUtensorMap, device memory) of sxy / syz over all slots,
+                                      for the TMA-staged velocity kernel; NULL when not built */
     TileLists tl;
     /* fused step (dsh_fused.cuh): second buffers of the fields neighbouring
        tiles read during a step, and the injection groups of each 128 x 16

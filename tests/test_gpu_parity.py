@@ -280,6 +280,24 @@ def test_persistent_forward_in_subprocess():
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
 
 
+def test_tma_velocity_kernel_in_subprocess():
+    """The opt-in persistent velocity kernel whose stress taps the tensor-memory
+    accelerator stages in shared memory (DSH_VTMA=1, read once per process, so
+    in a child process): every FD order and relaxation count, multi-shot
+    batches and checkpointed gradients stay bit-identical to the oracle."""
+    import subprocess
+    import sys
+
+    env = dict(os.environ, DSH_VTMA="1")
+    code = ("import sys; sys.argv=['x']; import pytest; "
+            "sys.exit(pytest.main(['-q', '-p', 'no:cacheprovider', '-m', 'gpu', "
+            "'tests/test_gpu_parity.py::test_random_cases_vs_oracle', "
+            "'tests/test_gpu_parity.py::test_multi_shot_batches', 'tests/test_gpu_checkpoint.py']))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True, timeout=900)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+
+
 def test_autotune_picks_a_variant_and_keeps_parity():
     """dsh_autotune times every applicable step-kernel variant and keeps the
     fastest; forward and gradient afterwards are still bit-identical."""
