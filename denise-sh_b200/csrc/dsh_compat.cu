@@ -20,11 +20,14 @@
  * grid range (nx1..nx2 = 1..NX, ny1..ny2 = 1..NY), L <= 4.  Unsupported
  * settings print a message on stderr and leave the arrays unchanged.
  */
+#include "dsh.h"
+#include "dsh_compat.h"
 #include "dsh_dispatch.h"
 #include "dsh_setup.h"
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -51,6 +54,28 @@ struct Compat {
 };
 Compat G;
 
+int last_status = DSH_OK;                 /* first error since the last dsh_compat_status() */
+
+/* Records an error for dsh_compat_status() and prints it.  With
+ * DSH_COMPAT_ABORT=1 in the environment the run ends as the reference ends
+ * it on a fatal error (src/util.c:7-15: the rank, a run-time error banner
+ * and the message on stdout, then a non-zero exit, which an MPI launcher
+ * turns into the abort of the whole job). */
+void fail(int code, const char *msg)
+{
+    if (last_status == DSH_OK) last_status = code;
+    fprintf(stderr, "dsh compat: %s\n", msg);
+    static const bool abort_mode = getenv("DSH_COMPAT_ABORT") && atoi(getenv("DSH_COMPAT_ABORT")) != 0;
+    if (abort_mode) {
+        fprintf(stdout, "Message from PE %d\n", MYID);
+        fprintf(stdout, "R U N - T I M E  E R R O R: \n");
+        fprintf(stdout, "%s\n", msg);
+        fprintf(stdout, "...now exiting to system.\n");
+        fflush(stdout);
+        exit(1);
+    }
+}
+
 void release()
 {
     cudaFree(G.buf);
@@ -64,8 +89,10 @@ bool supported(const char *fn, int nx1, int nx2, int ny1, int ny2)
 {
     if (NPROCX != 1 || NPROCY != 1 || BOUNDARY != 0 || nx1 != 1 || ny1 != 1 || nx2 != NX || ny2 != NY ||
         FDORDER < 2 || FDORDER > 12 || (FDORDER & 1) || L < 0 || L > DSH_MAX_L || FW < 0 || FW > DSH_MAX_FW) {
-        fprintf(stderr, "dsh compat %s: only the one-rank full-grid configuration is supported "
-                        "(NPROCX=NPROCY=1, BOUNDARY=0, ranges 1..NX/1..NY, L<=4)\n", fn);
+        char msg[256];
+        snprintf(msg, sizeof msg, "%s: only the one-rank full-grid configuration is supported "
+                                  "(NPROCX=NPROCY=1, BOUNDARY=0, ranges 1..NX/1..NY, L<=4)", fn);
+        fail(DSH_ERR_PARAM, msg);
         return false;
     }
     return true;
@@ -85,8 +112,8 @@ bool ensure()
     const long long vlen = 2 * DSH_MAX_FW + 1;
     const long long total = 6 * G.fstride + (5 + 4 * (long long)L + 2) * G.dstride + 2 * psix + 2 * psiy + 12 * vlen;
     if (cudaMalloc(&G.buf, total * sizeof(float)) != cudaSuccess || cudaMalloc(&G.ints, 2 * sizeof(int)) != cudaSuccess) {
-        fprintf(stderr, "dsh compat: device allocation failed\n");
         release();
+        fail(DSH_ERR_OOM, "device allocation failed");
         return false;
     }
     cudaMemset(G.buf, 0, total * sizeof(float));
@@ -236,8 +263,8 @@ StepArgs base_args(const float *hc)
 
 bool launch(KFn fn, StepArgs &a)
 {
-    int zero = 0;
-    cudaMemcpy(G.ints, &zero, sizeof(int), cudaMemcpyHostToDevice);
+    const int zero[2] = {0, 0};           /* step counter, status word */
+    cudaMemcpy(G.ints, zero, sizeof(zero), cudaMemcpyHostToDevice);
     dim3 block(BX, BY, 1);
     dim3 grid((unsigned)((NX + 4 * BX - 1) / (4 * BX)), (unsigned)((NY + BY - 1) / BY), 1);
     int off = 1;                           /* the kernels read step = *nt_base + off */
@@ -245,7 +272,15 @@ bool launch(KFn fn, StepArgs &a)
     cudaError_t e = cudaLaunchKernel((const void *)fn, grid, block, args, 0, 0);
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
-        fprintf(stderr, "dsh compat: kernel failed (%s)\n", cudaGetErrorString(e));
+        char msg[256];
+        snprintf(msg, sizeof msg, "kernel failed (%s)", cudaGetErrorString(e));
+        fail(DSH_ERR_CUDA, msg);
+        return false;
+    }
+    int st = 0;
+    cudaMemcpy(&st, G.ints + 1, sizeof(int), cudaMemcpyDeviceToHost);
+    if (st) {   /* a non-finite stress or velocity (the reference's check at src/denise.c:1183-1185) */
+        fail(DSH_ERR_UNSTABLE, " Simulation is unstable !");
         return false;
     }
     return true;
@@ -272,7 +307,7 @@ bool device_ok()
 {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n < 1) {
-        fprintf(stderr, "dsh compat: no CUDA device\n");
+        fail(DSH_ERR_CUDA, "no CUDA device");
         return false;
     }
     return true;
@@ -292,7 +327,7 @@ void update_v_PML(int nx1, int nx2, int ny1, int ny2, int nt, float **vy, float 
     (void)vym1; (void)utty; (void)absorb_coeff; (void)infoout;
     if (!device_ok() || !supported("update_v_PML", nx1, nx2, ny1, ny2) || !ensure()) return;
     if (GRAD_FORM != 2 && sw == 1) {
-        fprintf(stderr, "dsh compat update_v_PML: only GRAD_FORM=2 is supported\n");
+        fail(DSH_ERR_PARAM, "update_v_PML: only GRAD_FORM=2 is supported");
         return;
     }
     const int H = G.hy;
@@ -523,3 +558,10 @@ void psource(int nt, float **sxx, float **syy, float **srcpos_loc, float **signa
 }
 
 }  /* extern "C" */
+
+extern "C" int dsh_compat_status(void)
+{
+    const int st = last_status;
+    last_status = DSH_OK;
+    return st;
+}

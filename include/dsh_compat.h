@@ -66,6 +66,18 @@ void zero_fdveps_visc(int ny1, int ny2, int nx1, int nx2, float **vy, float **sy
 /* replaces src/psource.c:9 (P-SV explosive source; not used by the SH program) */
 void psource(int nt, float **sxx, float **syy, float **srcpos_loc, float **signals, int nsrc);
 
+/* Errors of the functions above, which keep the reference's void
+ * signatures: the first error code (dsh.h's DSH_ERR_*) since the previous
+ * call, then cleared — DSH_ERR_UNSTABLE when a stress or velocity update left
+ * a non-finite value, DSH_ERR_PARAM for an unsupported configuration,
+ * DSH_ERR_CUDA / DSH_ERR_OOM for device failures.  Each error is also
+ * printed.  With DSH_COMPAT_ABORT=1 in the environment an error ends the
+ * run the way the reference's err() does (src/util.c:7-15: the rank and the
+ * message on stdout, then a non-zero exit), as the reference does for its
+ * own fatal errors (src/denise.c:1183-1185 for an unstable simulation).
+ * No counterpart in the reference. */
+int dsh_compat_status(void);
+
 #ifdef __cplusplus
 }
 #endif

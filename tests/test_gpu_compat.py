@@ -55,3 +55,61 @@ def test_compat_layer_is_drop_in(name):
         assert np.array_equal(np.asarray(gpu[k]), np.asarray(base[k])), k
     assert np.array_equal(gpu["seis"], d["seis"])
     assert np.array_equal(gpu["g_u"], d["g_u"])
+
+
+def _use_compat(ref, comp):
+    ptr = lambda f: C.c_void_p(C.cast(getattr(comp, f), C.c_void_p).value)
+    ref.refh_set_impl(ptr("update_v_PML"), ptr("update_s_elastic_PML"), ptr("update_s_visc_PML"), ptr("eprecond"),
+                      ptr("eprecond1"))
+
+
+def _unstable_forward(d):
+    """The reference's forward loop with DT 20x beyond the stability limit."""
+    d = dict(d, dt=np.float32(d["dt"] * 20))
+    o = O.Oracle(oracle_model(d), "ref")
+    o.forward(d["srcpos"], d["recpos"])
+    o.close()
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference not compiled here")
+def test_compat_status_reports_instability():
+    """The layer keeps the reference's void signatures; dsh_compat_status
+    reports (and clears) the first error: none after a stable run,
+    DSH_ERR_UNSTABLE after a run whose wavefield became non-finite."""
+    ref, comp = _libs()
+    comp.dsh_compat_status.restype = C.c_int
+    d = golden("elastic_fd4_fs")
+    _use_compat(ref, comp)
+    try:
+        comp.dsh_compat_status()
+        _run(d)
+        assert comp.dsh_compat_status() == 0
+        _unstable_forward(d)
+        assert comp.dsh_compat_status() == -4            # DSH_ERR_UNSTABLE
+        assert comp.dsh_compat_status() == 0             # cleared by the read
+    finally:
+        ref.refh_set_impl(None, None, None, None, None)
+
+
+@pytest.mark.skipif(os.environ.get("DSH_COMPAT_ABORT") != "1", reason="run by the abort-mode test in a child")
+def test_compat_abort_mode_child():
+    ref, comp = _libs()
+    _use_compat(ref, comp)
+    _unstable_forward(golden("elastic_fd4_fs"))
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference not compiled here")
+def test_compat_abort_mode_exits_like_the_reference():
+    """With DSH_COMPAT_ABORT=1 an error ends the process as the reference's
+    err() does: the run-time error banner with the message on stdout and
+    exit status 1 (in a child process)."""
+    import subprocess
+    import sys
+
+    env = dict(os.environ, DSH_COMPAT_ABORT="1")
+    code = ("import sys; sys.argv=['x']; import pytest; "
+            "sys.exit(pytest.main(['-q', '-s', '-p', 'no:cacheprovider', '-m', 'gpu', "
+            "'tests/test_gpu_compat.py::test_compat_abort_mode_child']))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 1, out.stdout[-2000:] + out.stderr[-2000:]
+    assert "R U N - T I M E  E R R O R" in out.stdout and "Simulation is unstable" in out.stdout
