@@ -14,6 +14,9 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <vector>
+
 namespace {
 
 constexpr int GAUSS_MAX = 45;                 /* largest filter length (odd) */
@@ -95,6 +98,34 @@ __global__ void iir_store(const double *x, int ntr, int ns, float *d)
     }
 }
 
+/* SPATFILTER=4: out = sum_k w_k in(edge-replicated tap k) / sum_k w_k with the
+ * point's own kernel (ii outer, jj inner, float, no contraction), or the
+ * input where the point has none (src/gauss_filt_var.c:150-205) */
+__global__ void gauss_var_kernel(int nx, int ny, const int *map, const int *pairs, const float *w, const float *in,
+                                 float *out)
+{
+    const long long total = (long long)nx * ny;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const int k = map[idx];
+        if (k < 0) { out[idx] = in[idx]; continue; }
+        const int i = (int)(idx % nx), j = (int)(idx / nx);
+        const int hx = pairs[4 * k], hz = pairs[4 * k + 1];
+        const float *wk = w + pairs[4 * k + 2];
+        const float sum = __int_as_float(pairs[4 * k + 3]);
+        float conv = 0.0f;
+        int q = 0;
+        for (int ii = -hx; ii <= hx; ii++) {
+            const int ic = min(max(i + ii, 0), nx - 1);
+            for (int jj = -hz; jj <= hz; jj++) {
+                const int jc = min(max(j + jj, 0), ny - 1);
+                conv = conv + in[(long long)jc * nx + ic] * wk[q++];
+            }
+        }
+        out[idx] = conv / sum;
+    }
+}
+
 /* g = zero ? 0 : g*coeff (src/taper_grad.c: waveconv *= taper_coeff, then
  * the zeroed points are set to 0.0) */
 __global__ void taper_kernel(long long n, float *g, const float *c, const unsigned char *z)
@@ -160,6 +191,44 @@ extern "C" int dsh_smooth_gauss(int nx, int ny, int filt, const float *in_dev, f
     const int blocks = (int)((total + 255) / 256 < 148 * 16 ? (total + 255) / 256 : 148 * 16);
     gauss_filt_kernel<<<blocks, 256, 0, st>>>(nx, ny, hfs, k, in_dev, out_dev);
     return cudaGetLastError() == cudaSuccess ? DSH_OK : DSH_ERR_CUDA;
+}
+
+extern "C" int dsh_smooth_gauss_var(int nx, int ny, float dh, float wd_damp, float wd_damp1, float fc_end,
+                                    const float *vel_host, const float *in_dev, float *out_dev, void *stream)
+{
+    if (nx < 1 || ny < 1 || !vel_host || !in_dev || !out_dev || in_dev == out_dev || !(dh > 0) || !(fc_end > 0))
+        return DSH_ERR_PARAM;
+    const long long n = (long long)nx * ny;
+    const int max_pairs = 4096, max_weights = 1 << 22;
+    std::vector<int> map((size_t)n), pairs(4 * (size_t)max_pairs);
+    std::vector<float> w((size_t)max_weights);
+    const int np = dsh_setup_gauss_var(nx, ny, dh, wd_damp, wd_damp1, fc_end, vel_host, map.data(), max_pairs,
+                                       pairs.data(), max_weights, w.data());
+    if (np < 0) return DSH_ERR_PARAM;
+    int nw = 0;
+    for (int k = 0; k < np; k++) nw = std::max(nw, pairs[4 * k + 2] + (2 * pairs[4 * k] + 1) * (2 * pairs[4 * k + 1] + 1));
+    const cudaStream_t st = (cudaStream_t)stream;
+    int *d_map = nullptr, *d_pairs = nullptr;
+    float *d_w = nullptr;
+    if (cudaMallocAsync(&d_map, (size_t)n * sizeof(int), st) != cudaSuccess ||
+        cudaMallocAsync(&d_pairs, (size_t)std::max(np, 1) * 4 * sizeof(int), st) != cudaSuccess ||
+        cudaMallocAsync(&d_w, (size_t)std::max(nw, 1) * sizeof(float), st) != cudaSuccess) {
+        cudaFreeAsync(d_map, st); cudaFreeAsync(d_pairs, st); cudaFreeAsync(d_w, st);
+        cudaGetLastError();
+        return DSH_ERR_OOM;
+    }
+    cudaMemcpyAsync(d_map, map.data(), (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st);
+    if (np > 0) {
+        cudaMemcpyAsync(d_pairs, pairs.data(), (size_t)np * 4 * sizeof(int), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(d_w, w.data(), (size_t)nw * sizeof(float), cudaMemcpyHostToDevice, st);
+    }
+    const int blocks = (int)((n + 255) / 256 < 148 * 16 ? (n + 255) / 256 : 148 * 16);
+    gauss_var_kernel<<<blocks, 256, 0, st>>>(nx, ny, d_map, d_pairs, d_w, in_dev, out_dev);
+    const cudaError_t e = cudaGetLastError();
+    cudaFreeAsync(d_map, st); cudaFreeAsync(d_pairs, st); cudaFreeAsync(d_w, st);
+    /* the host tables must outlive the asynchronous copies */
+    if (cudaStreamSynchronize(st) != cudaSuccess || e != cudaSuccess) return DSH_ERR_CUDA;
+    return DSH_OK;
 }
 
 extern "C" int dsh_gauss_filter_size(float wd_damp, float c_vs, float fc_end, float dh)

@@ -358,6 +358,62 @@ int dsh_setup_gauss_kernel(int filt, float *kernel)
     return 0;
 }
 
+/* Spatially variable Gaussian smoothing, SPATFILTER=4 (src/gauss_filt_var.c:
+ * 150-205).  Per point: lam = vel/FC_END, filter sizes round(WD_DAMP1 lam/DH)
+ * along x and round(WD_DAMP lam/DH) in depth (odd, at least 6); no filtering
+ * where the depth size is <= 0.  The kernels depend only on the half sizes
+ * (hx, hz); each distinct pair gets one entry: weights exp(-(ii^2)/sx -
+ * (jj^2)/sz) for ii = -hx..hx (outer), jj = -hz..hz (inner) and their float
+ * sum in that order, as the reference forms them at every point.
+ * map[p] = pair index or -1; pairs[4k..4k+3] = hx, hz, offset of the
+ * weights in `weights`, and the sum's bits.  Returns the number of pairs, or
+ * -1 when more than max_pairs pairs or max_weights weights are needed. */
+int dsh_setup_gauss_var(int nx, int ny, float dh, float wd_damp, float wd_damp1, float fc_end, const float *vel,
+                        int *map, int max_pairs, int *pairs, int max_weights, float *weights)
+{
+    int npairs = 0, nw = 0;
+    if (nx < 1 || ny < 1 || !vel || !map || !pairs || !weights) return -1;
+    int (*slot)[256] = (int (*)[256])malloc(sizeof(int) * 256 * 256);   /* pair index by (hx, hz), -1 = none */
+    if (!slot) return -1;
+    for (int a = 0; a < 256; a++)
+        for (int b = 0; b < 256; b++) slot[a][b] = -1;
+    for (long long p = 0; p < (long long)nx * ny; p++) {
+        const float lam = vel[p] / fc_end;
+        int fx = (int)round((wd_damp1 * lam) / dh);
+        int fz = (int)round((wd_damp * lam) / dh);
+        if (!(fz > 0)) { map[p] = -1; continue; }
+        if (!(fx % 2)) fx += 1;
+        if (!(fz % 2)) fz += 1;
+        if (fx < 6) fx = 6;
+        if (fz < 6) fz = 6;
+        const int hx = abs(fx) / 2, hz = abs(fz) / 2;
+        if (hx > 255 || hz > 255) { free(slot); return -1; }
+        if (slot[hx][hz] < 0) {
+            const int need = (2 * hx + 1) * (2 * hz + 1);
+            if (npairs >= max_pairs || nw + need > max_weights) { free(slot); return -1; }
+            const float sigmax = hx / 2, sigmaz = hz / 2;
+            const float sx = 2.0 * sigmax * sigmax, sz = 2.0 * sigmaz * sigmaz;
+            float sum = 0.0;
+            int k = nw;
+            for (int ii = -hx; ii <= hx; ii++)
+                for (int jj = -hz; jj <= hz; jj++) {
+                    const float kernel = exp(-((ii * ii) / sx) - ((jj * jj) / sz));
+                    weights[k++] = kernel;
+                    sum += kernel;
+                }
+            pairs[4 * npairs] = hx;
+            pairs[4 * npairs + 1] = hz;
+            pairs[4 * npairs + 2] = nw;
+            memcpy(&pairs[4 * npairs + 3], &sum, sizeof(float));
+            slot[hx][hz] = npairs++;
+            nw += need;
+        }
+        map[p] = slot[hx][hz];
+    }
+    free(slot);
+    return npairs;
+}
+
 /* Butterworth sections of libcseife (cseife.c:147-177, cseife_rfk.c) for
  * timedomain_filt.c: period t0 = 1/fc, order m; an odd order adds a first
  * order section first, then m/2 second-order sections with damping

@@ -58,6 +58,11 @@ int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *src
 int dsh_setup_gauss_size(float wd_damp, float c_vs, float fc_end, float dh);
 int dsh_setup_gauss_kernel(int filt, float *kernel);
 
+/* SPATFILTER=4 spatially variable Gaussian smoothing (src/gauss_filt_var.c):
+ * per-point kernel index and the distinct kernels' weights and sums. */
+int dsh_setup_gauss_var(int nx, int ny, float dh, float wd_damp, float wd_damp1, float fc_end, const float *vel,
+                        int *map, int max_pairs, int *pairs, int max_weights, float *weights);
+
 /* Butterworth low-/highpass sections of timedomain_filt.c (libcseife):
  * returns the number of sections written to coef [n][5] = f0 f1 f2 g1 g2. */
 int dsh_setup_butterworth(double dt, float fc, int order, int highpass, double *coef);

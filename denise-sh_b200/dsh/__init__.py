@@ -93,6 +93,9 @@ def lib() -> C.CDLL:
                                           C.c_int, C.c_void_p]
         L.dsh_smooth_gauss.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_gauss_filter_size.argtypes = [C.c_float] * 4
+        L.dsh_smooth_gauss_var.argtypes = [C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_void_p] * 4
+        L.dsh_setup_gauss_var.argtypes = [C.c_int, C.c_int] + [C.c_float] * 4 + [C.c_void_p, C.c_void_p, C.c_int,
+                                                                                    C.c_void_p, C.c_int, C.c_void_p]
         L.dsh_taper_coeff.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_int, C.c_float, C.c_int,
                                       C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_taper_apply.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -426,6 +429,37 @@ def smooth_gauss(grad, filt, stream=None):
     _check(lib().dsh_smooth_gauss(nx, ny, int(filt), g.data_ptr(), out.data_ptr(), stream), "dsh_smooth_gauss")
     torch.cuda.synchronize()
     return out.cpu().numpy()
+
+
+def smooth_gauss_var(grad, vel, dh, wd_damp, wd_damp1, fc_end, stream=None):
+    """SPATFILTER=4 Gaussian smoothing whose size follows the velocity vel
+    [ny, nx], on the GPU (dsh_smooth_gauss_var)."""
+    import torch
+
+    g = torch.from_numpy(np.ascontiguousarray(grad, np.float32)).cuda()
+    out = torch.empty_like(g)
+    v = np.ascontiguousarray(vel, np.float32)
+    ny, nx = g.shape
+    _check(lib().dsh_smooth_gauss_var(nx, ny, dh, wd_damp, wd_damp1, fc_end, v.ctypes.data, g.data_ptr(),
+                                      out.data_ptr(), stream), "dsh_smooth_gauss_var")
+    return out.cpu().numpy()
+
+
+def gauss_var_tables(vel, dh, wd_damp, wd_damp1, fc_end, max_pairs=4096, max_weights=1 << 22):
+    """Host tables of SPATFILTER=4 (dsh_setup_gauss_var): per-point kernel
+    index (-1: none) [ny, nx], per kernel (hx, hz, weight offset, weight
+    sum), and the weights."""
+    v = np.ascontiguousarray(vel, np.float32)
+    ny, nx = v.shape
+    mp = np.zeros((ny, nx), np.int32)
+    pairs = np.zeros(4 * max_pairs, np.int32)
+    w = np.zeros(max_weights, np.float32)
+    n = lib().dsh_setup_gauss_var(nx, ny, dh, wd_damp, wd_damp1, fc_end, v.ctypes.data, mp.ctypes.data, max_pairs,
+                                  pairs.ctypes.data, max_weights, w.ctypes.data)
+    if n < 0:
+        raise DshError(ERR_PARAM, "dsh_setup_gauss_var")
+    pr = pairs[:4 * n].reshape(n, 4)
+    return mp, [(int(a), int(b), int(c), float(np.int32(d).view(np.float32))) for a, b, c, d in pr], w
 
 
 def gauss_filter_size(wd_damp, c_vs, fc_end, dh):

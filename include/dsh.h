@@ -242,6 +242,18 @@ int dsh_get_energy_sums(dsh_ctx *ctx, float *ws_sum, float *wr_sum);
 int dsh_smooth_gauss(int nx, int ny, int filt, const float *in_dev, float *out_dev, void *stream);
 int dsh_gauss_filter_size(float wd_damp, float c_vs, float fc_end, float dh);
 
+/* Gradient smoothing SPATFILTER=4 (src/smooth_grad.c:31-33,
+ * src/gauss_filt_var.c): a Gaussian whose size follows the local velocity
+ * vel_host [ny][nx] (host): lam = vel/FC_END, kernel lengths
+ * round(WD_DAMP1 lam/DH) along x and round(WD_DAMP lam/DH) in depth (odd, at
+ * least 6; no smoothing where the depth length is <= 0), weights
+ * exp(-ii^2/sx - jj^2/sz) normalised by their sum, edges replicated; device
+ * arrays [ny][nx], in != out.  The kernels are tabulated on the host (glibc
+ * exp, the reference's float/double mix); at most 4096 distinct kernel
+ * sizes and 4 M weights (DSH_ERR_PARAM beyond).  Synchronises `stream`. */
+int dsh_smooth_gauss_var(int nx, int ny, float dh, float wd_damp, float wd_damp1, float fc_end, const float *vel_host,
+                         const float *in_dev, float *out_dev, void *stream);
+
 /* Butterworth filtering of traces or source signals (TIME_FILT stages;
  * src/timedomain_filt.c with libcseife's seife_lpb/seife_hpb,
  * src/denise.c:908-918,1056-1059): data_dev [ntr][ns] device floats,

@@ -362,3 +362,23 @@ def taper(g, sws, dh, gradt=(0, 0, 0, 0), srtshape=1, srtradius=5.0, filtsize=1,
     if rc != 0:
         raise RuntimeError("refh_taper failed")
     return out, tc
+
+
+def gauss_filt_var(grad, vel, dh, wd_damp, wd_damp1, fc_end):
+    """The reference's spatially variable Gaussian smoothing (src/gauss_filt_var.c,
+    SPATFILTER=4) of grad [ny, nx] for the velocity vel [ny, nx]; its
+    temporary files go to a temporary directory."""
+    import tempfile
+
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_gauss_filt_var.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
+                                        C.c_void_p, C.c_void_p]
+    g = _f32(grad).copy()
+    v = _f32(vel)
+    ny, nx = g.shape
+    with tempfile.TemporaryDirectory(dir="/tmp") as d:      # a short path: the reference's names are char[74]
+        rc = lib.refh_gauss_filt_var(d.encode(), nx, ny, dh, wd_damp, wd_damp1, fc_end, v.ctypes.data,
+                                     g.ctypes.data)
+    if rc != 0:
+        raise RuntimeError("refh_gauss_filt_var failed")
+    return g

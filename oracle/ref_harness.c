@@ -791,3 +791,33 @@ int refh_taper(const char *dir, int sws, int shot, int nx, int ny, float dh, con
     if (quiet) fclose(quiet);
     return chdir(cwd) == 0 ? 0 : -1;
 }
+
+/* The reference's spatially variable Gaussian smoothing (src/gauss_filt_var.c,
+ * SPATFILTER=4) of a dense gradient g [ny][nx] (in place) for the velocity
+ * model vel [ny][nx]; the files it writes and reads back go to the directory
+ * dir (JACOBIAN = dir/jac). */
+void gauss_filt_var(float **waveconv, float **vel_mod);
+extern float WD_DAMP, WD_DAMP1, FC_END;
+extern char JACOBIAN[];
+int refh_gauss_filt_var(const char *dir, int nx, int ny, float dh, float wd_damp, float wd_damp1, float fc_end,
+                        const float *vel, float *g)
+{
+    int i, j;
+    if (strlen(dir) + 4 + 18 >= STRING_SIZE) return -1;   /* its file names live in char[STRING_SIZE] */
+    const int nx0 = NX, ny0 = NY, nxg0 = NXG, nyg0 = NYG, myid0 = MYID;
+    const float dh0 = DH;
+    FILE *fp0 = FP, *quiet = fopen("/dev/null", "w");
+    float **w = matrix(1, ny, 1, nx), **v = matrix(1, ny, 1, nx);
+    NX = NXG = nx; NY = NYG = ny; DH = dh; POS[1] = POS[2] = 0; IDX = IDY = 1;
+    NPROCX = NPROCY = 1; MYID = 0;
+    FP = quiet ? quiet : stderr;
+    WD_DAMP = wd_damp; WD_DAMP1 = wd_damp1; FC_END = fc_end;
+    snprintf(JACOBIAN, STRING_SIZE, "%s/jac", dir);   /* the reference appends up to 18 characters */
+    for (j = 1; j <= ny; j++) for (i = 1; i <= nx; i++) { w[j][i] = g[(j - 1) * nx + i - 1]; v[j][i] = vel[(j - 1) * nx + i - 1]; }
+    gauss_filt_var(w, v);
+    for (j = 1; j <= ny; j++) for (i = 1; i <= nx; i++) g[(j - 1) * nx + i - 1] = w[j][i];
+    free_matrix(w, 1, ny, 1, nx); free_matrix(v, 1, ny, 1, nx);
+    NX = nx0; NY = ny0; NXG = nxg0; NYG = nyg0; MYID = myid0; DH = dh0; FP = fp0;
+    if (quiet) fclose(quiet);
+    return 0;
+}
