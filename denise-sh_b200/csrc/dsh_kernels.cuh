@@ -31,6 +31,10 @@ constexpr int BY = 8;            /* threads per block along depth */
 #ifndef VSTEP_MIN_BLOCKS
 #define VSTEP_MIN_BLOCKS 3       /* resident velocity-kernel blocks per SM the register budget targets */
 #endif
+#ifndef VSTEP_MIN_BLOCKS_FWD
+#define VSTEP_MIN_BLOCKS_FWD 4   /* the same for the forward velocity kernel (no correlation), which fits
+                                    64 registers */
+#endif
 
 /* flags of the velocity kernel */
 constexpr int VF_ADJOINT = 1;    /* sw=1: vyp1 = old vy (update_v_PML.c:189-192) */
@@ -363,7 +367,8 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
 
 /* one thread block = 128 x 8 points of one shot slot (grid z) */
 template <int FDO, int FLAGS, bool P2>
-__global__ void __launch_bounds__(BX *BY, VSTEP_MIN_BLOCKS) v_step(StepArgs a, int nt_off)
+__global__ void __launch_bounds__(BX *BY, (FLAGS & (VF_CORR | VF_HESS)) ? VSTEP_MIN_BLOCKS : VSTEP_MIN_BLOCKS_FWD)
+    v_step(StepArgs a, int nt_off)
 {
     v_body<FDO, FLAGS, P2>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
                            blockIdx.z, blockIdx.y * gridDim.x + blockIdx.x);
