@@ -216,13 +216,13 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
                 }
                 if (MODE == FM_STORE) {      /* forward storage of vyp1 */
                     const long long k = store_idx(nt - 1, a.fwd_mod);
-                    st4m(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4,
-                         nvalid);
+                    st4ms(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4,
+                          nvalid);
                 }
                 if (MODE == FM_ADJ) {        /* g_rho += vyp1 * forward acceleration (denise.c:1589) */
                     const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
                     const float4 f4 =
-                        ldg4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
+                        ldcs4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
                     float4 g4 = ld4(a.grho + so + drow + col0);
                     g4.x = g4.x + (old4.x * f4.x); g4.y = g4.y + (old4.y * f4.y);
                     g4.z = g4.z + (old4.z * f4.z); g4.w = g4.w + (old4.w * f4.w);
@@ -276,8 +276,8 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
             g4 = ld4(a.gu + so + drow + col0);
             const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
             const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
-            fy = ldg4(base + a.dstride);
-            fu = ldg4(base + 2 * a.dstride);
+            fy = ldcs4(base + a.dstride);
+            fu = ldcs4(base + 2 * a.dstride);
         }
         /* velocity taps: xs[p] = vy[i0 - 4*NLS + p] of row j, ys[q] = vy rows j-H+1 .. j+H */
         constexpr int NLS = (H - 1 + 3) / 4, NRS = (H + 3) / 4;
@@ -404,8 +404,8 @@ __global__ void __launch_bounds__(256, 2) fs_step(StepArgs a, int nt_off)
         if (MODE == FM_STORE) {
             const long long k = store_idx(nt - 1, a.fwd_mod);
             float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
-            st4m(base + a.dstride, vyy4, nvalid);
-            st4m(base + 2 * a.dstride, vyx4, nvalid);
+            st4ms(base + a.dstride, vyy4, nvalid);
+            st4ms(base + 2 * a.dstride, vyx4, nvalid);
         }
         if (a.ws) {                       /* energy W += vy^2 (eprecond.c:11) */
 #pragma unroll

@@ -122,17 +122,61 @@ struct StepArgs {
     int fvg_ntiles;
 };
 
+#ifndef DSH_L2_KEEP
+#define DSH_L2_KEEP 1
+#endif
+#if DSH_L2_KEEP
+/* The fields that every time step reads again (wavefield state, memory
+ * variables, model factors, energies, gradient sums) are loaded and stored
+ * with an L2 evict-last policy, so that a working set smaller than the L2
+ * stays there from one step to the next; the stored forward wavefield is
+ * streamed (st4ms / ldcs4 below). */
+__device__ __forceinline__ uint64_t l2_keep()
+{
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ float4 ld4(const float *p)
+{
+    float4 v;
+    asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(l2_keep()));
+    return v;
+}
+__device__ __forceinline__ float4 ldg4(const float *p)
+{
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(l2_keep()));
+    return v;
+}
+__device__ __forceinline__ void st4(float *p, float4 v)
+{
+    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(v.x), "f"(v.y),
+                 "f"(v.z), "f"(v.w), "l"(l2_keep())
+                 : "memory");
+}
+__device__ __forceinline__ void st1(float *p, float v)
+{
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(l2_keep()) : "memory");
+}
+#else
 __device__ __forceinline__ float4 ld4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
+__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
+__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
+__device__ __forceinline__ void st1(float *p, float v) { *p = v; }
+#endif
 /* state loads of the persistent kernel: other blocks wrote them earlier in the
  * same launch, so they bypass L1 (ld.global.cg) */
 template <bool CG>
 __device__ __forceinline__ float4 lds4(const float *p)
 {
     if (CG) return __ldcg(reinterpret_cast<const float4 *>(p));
-    return *reinterpret_cast<const float4 *>(p);
+    return ld4(p);
 }
-__device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpret_cast<const float4 *>(p)); }
-__device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
 __device__ __forceinline__ float get(const float4 &v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
 __device__ __forceinline__ void set(float4 &v, int k, float x)
 {
@@ -143,10 +187,22 @@ __device__ __forceinline__ void set(float4 &v, int k, float x)
 __device__ __forceinline__ void st4m(float *p, float4 v, int nvalid)
 {
     if (nvalid >= 4) { st4(p, v); return; }
-    if (nvalid > 0) p[0] = v.x;
-    if (nvalid > 1) p[1] = v.y;
-    if (nvalid > 2) p[2] = v.z;
+    if (nvalid > 0) st1(p, v.x);
+    if (nvalid > 1) st1(p + 1, v.y);
+    if (nvalid > 2) st1(p + 2, v.z);
 }
+
+/* forward-storage traffic is written once per pass and read once by the
+ * adjoint, so it is streamed (st.global.cs / ld.global.cs: evict-first in L2)
+ * and leaves the L2 to the fields that every time step reads again */
+__device__ __forceinline__ void st4ms(float *p, float4 v, int nvalid)
+{
+    if (nvalid >= 4) { __stcs(reinterpret_cast<float4 *>(p), v); return; }
+    if (nvalid > 0) __stcs(p, v.x);
+    if (nvalid > 1) __stcs(p + 1, v.y);
+    if (nvalid > 2) __stcs(p + 2, v.z);
+}
+__device__ __forceinline__ float4 ldcs4(const float *p) { return __ldcs(reinterpret_cast<const float4 *>(p)); }
 
 /* Programmatic dependent launch (PTX griddepcontrol): a kernel launched with
  * programmatic stream serialization may start while its predecessor drains.
@@ -259,7 +315,7 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
     if (nt > a.nt_last) return;
     if (FLAGS & VF_CORR) {                   /* stored forward acceleration of step NT-nt+1 */
         const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
-        f4 = ldg4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
+        f4 = ldcs4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
     }
     pdl_wait();                              /* stresses of the previous step are complete */
     pdl_trigger();
@@ -356,7 +412,7 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
     }
     if (!(FLAGS & VF_ADJOINT) && a.fwd && !(FLAGS & VF_CORR)) {   /* forward storage of vyp1 */
         const long long k = store_idx(nt - 1, a.fwd_mod);
-        st4m(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4, nvalid);
+        st4ms(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4, nvalid);
     }
     if ((FLAGS & VF_HESS) && nt < a.nt_total) {
         h4.x = h4.x + (acc4.x * acc4.x); h4.y = h4.y + (acc4.y * acc4.y);
@@ -481,8 +537,8 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     if (FLAGS & SF_CORR) {
         const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
         const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
-        fy = ldg4(base + a.dstride);
-        fu = ldg4(base + 2 * a.dstride);
+        fy = ldcs4(base + a.dstride);
+        fu = ldcs4(base + 2 * a.dstride);
     }
     pdl_wait();                              /* velocities of this step are complete */
     pdl_trigger();
@@ -637,8 +693,8 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
         } else {                      /* forward storage: uy at +dstride, uyx at +2*dstride */
             const long long k = store_idx(nt - 1, a.fwd_mod);
             float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
-            st4m(base + a.dstride, vyy4, nvalid);
-            st4m(base + 2 * a.dstride, vyx4, nvalid);
+            st4ms(base + a.dstride, vyy4, nvalid);
+            st4ms(base + 2 * a.dstride, vyx4, nvalid);
         }
     }
     if (a.ws) {                       /* energy W += vy^2 (eprecond.c:11); vy at the point is xs[4NL+k] */
