@@ -409,6 +409,28 @@ int dsh_write_model(const char *path, int nx, int ny, const float *field)
     return DSH_OK;
 }
 
+int dsh_builtin_model(int l, int nx, int ny, float dh, float *vs, float *rho, float *qs)
+{
+    int i, j;
+    if (l < 0 || nx < 1 || ny < 1 || !vs || !rho || (l > 0 && !qs)) return DSH_ERR_PARAM;
+    for (j = 0; j < ny; j++)
+        for (i = 0; i < nx; i++) {
+            const size_t k = (size_t)j * nx + i;
+            if (l > 0) {
+                /* model_grad_visc.c:21,46: float constants, float arithmetic */
+                const float grad0 = 2.80f, vs0 = 170.0f;
+                vs[k] = grad0 * ((float)j * dh) + vs0;
+                rho[k] = 1900.0f;
+                qs[k] = 10.0f;
+            } else {
+                vs[k] = 164.0f;
+                rho[k] = 1900.0f;
+                if (qs) qs[k] = 0.0f;
+            }
+        }
+    return DSH_OK;
+}
+
 /* ---------------- SU ---------------- */
 
 static void put_i32(unsigned char *h, int off, int v) { memcpy(h + off, &v, 4); }

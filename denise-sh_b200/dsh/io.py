@@ -61,6 +61,7 @@ def _lib():
         L.dsh_read_receivers.argtypes = [cp, cf, vp, ci, vp, vp]
         L.dsh_read_model.argtypes = [cp, ci, ci, ci, vp, vp, vp]
         L.dsh_write_model.argtypes = [cp, ci, ci, vp]
+        L.dsh_builtin_model.argtypes = [ci, ci, ci, cf, vp, vp, vp]
         L.dsh_write_su.argtypes = [cp, ci, ci, vp, vp, vp, cf, cf, cf, cf, ci, vp]
         L.dsh_read_su.argtypes = [cp, ci, ci, vp]
         L.dsh_stager_create.restype = vp
@@ -124,6 +125,18 @@ def read_model(mfile: str, nx: int, ny: int, l: int = 0):
     qs = np.zeros((ny, nx), np.float32) if l > 0 else None
     _check(_lib().dsh_read_model(_b(mfile), nx, ny, l, vs.ctypes.data, rho.ctypes.data,
                                 qs.ctypes.data if qs is not None else None), "dsh_read_model")
+    return vs, rho, qs
+
+
+def builtin_model(l: int, nx: int, ny: int, dh: float):
+    """The reference's start model for READMOD=0 (src/model_grad_visc.c for
+    l > 0, src/check_start.c for l == 0): (vs, rho, qs) as [ny, nx] float32,
+    qs None when l == 0."""
+    vs = np.empty((ny, nx), np.float32)
+    rho = np.empty((ny, nx), np.float32)
+    qs = np.empty((ny, nx), np.float32) if l > 0 else None
+    _check(_lib().dsh_builtin_model(l, nx, ny, dh, vs.ctypes.data, rho.ctypes.data,
+                                    qs.ctypes.data if qs is not None else None), "dsh_builtin_model")
     return vs, rho, qs
 
 

@@ -93,6 +93,15 @@ int dsh_read_model(const char *mfile, int nx, int ny, int l, float *vs, float *r
 /* dense [ny][nx] -> float32 file, x outer / depth inner (src/writemod.c) */
 int dsh_write_model(const char *path, int nx, int ny, const float *field);
 
+/* The reference's built-in start models, used when READMOD=0
+ * (src/denise.c:609-615), as dense [ny][nx] arrays: l > 0 the 1-D gradient
+ * model of src/model_grad_visc.c:26-55 (vs = 2.8 (j-1) DH + 170 m/s,
+ * rho = 1900 kg/m^3, Qs = 10, i.e. taus = 2/Qs), l == 0 the homogeneous
+ * model of src/check_start.c:68-92 (vs = 164 m/s, rho = 1900); qs may be
+ * NULL when l == 0.  The reference also writes these models to files
+ * (writemod/mergemod); dsh_write_model does that here when wanted. */
+int dsh_builtin_model(int l, int nx, int ny, float dh, float *vs, float *rho, float *qs);
+
 /* SU output of one shot (SEIS_FORMAT=1): section [ntr][ns] (ns samples, every
  * ndt-th step), recpos [2][ntr] grid indices, tracl[k] trace numbers (NULL:
  * 1..ntr), source position (xs, ys) in metres; header values as

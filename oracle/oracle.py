@@ -382,3 +382,28 @@ def gauss_filt_var(grad, vel, dh, wd_damp, wd_damp1, fc_end):
     if rc != 0:
         raise RuntimeError("refh_gauss_filt_var failed")
     return g
+
+
+def builtin_model(l, nx, ny, dh, dt, fl=()):
+    """The reference's built-in start model for READMOD=0: model() of
+    src/model_grad_visc.c (l > 0) or model_elastic() of src/check_start.c
+    (l == 0).  Returns vs, rho, taus (None for l == 0), eta (None for l == 0)
+    and the bytes of the vs file the reference writes (merged, x outer)."""
+    import tempfile
+
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_builtin_model.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_void_p,
+                                       C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    vs = np.zeros((ny, nx), np.float32)
+    rho = np.zeros((ny, nx), np.float32)
+    taus = np.zeros((ny, nx), np.float32)
+    eta = np.zeros(max(l, 1), np.float32)
+    flv = np.asarray(list(fl) + [0.0] * (8 - len(fl)), np.float32)
+    with tempfile.TemporaryDirectory(dir="/tmp") as d:      # a short path: the reference's names are char[74]
+        rc = lib.refh_builtin_model(d.encode(), l, nx, ny, dh, dt, flv.ctypes.data, vs.ctypes.data,
+                                    rho.ctypes.data, taus.ctypes.data, eta.ctypes.data)
+        name = os.path.join(d, "inv_vs_it_0.bin" if l > 0 else "mod.mu")
+        vs_file = open(name, "rb").read() if rc == 0 else b""
+    if rc != 0:
+        raise RuntimeError("refh_builtin_model failed")
+    return vs, rho, (taus if l > 0 else None), (eta[:l] if l > 0 else None), vs_file

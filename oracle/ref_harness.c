@@ -821,3 +821,54 @@ int refh_gauss_filt_var(const char *dir, int nx, int ny, float dh, float wd_damp
     if (quiet) fclose(quiet);
     return 0;
 }
+
+/* The reference's built-in start models (READMOD=0, src/denise.c:609-615):
+ * model() of src/model_grad_visc.c when l > 0 (vs, rho, taus, eta) and
+ * model_elastic() of src/check_start.c when l == 0 (vs, rho), as dense
+ * [ny][nx] arrays; the model files they write go to dir (INV_MODELFILE =
+ * dir/inv, MFILE = dir/mod). */
+void model(float **rho, float **u, float **taus, float *eta);
+void model_elastic(float **rho, float **u);
+extern char MFILE[], INV_MODELFILE[];
+int refh_builtin_model(const char *dir, int l, int nx, int ny, float dh, float dt, const float *fl, float *vs,
+                       float *rho, float *taus, float *eta)
+{
+    int i, j, k;
+    if (strlen(dir) + 4 + 17 >= STRING_SIZE) return -1;   /* dir/inv_rho_it_0.bin.0.0 in char[STRING_SIZE] */
+    const int nx0 = NX, ny0 = NY, nxg0 = NXG, nyg0 = NYG, myid0 = MYID, l0 = L;
+    const float dh0 = DH, dt0 = DT;
+    float *fl0 = FL;
+    FILE *fp0 = FP, *quiet = fopen("/dev/null", "w");
+    NX = NXG = nx; NY = NYG = ny; DH = dh; DT = dt; L = l; POS[1] = POS[2] = 0; IDX = IDY = 1;
+    NPROCX = NPROCY = 1; NPROC = 1; MYID = 0;
+    FP = quiet ? quiet : stderr;
+    snprintf(INV_MODELFILE, STRING_SIZE, "%s/inv", dir);
+    snprintf(MFILE, STRING_SIZE, "%s/mod", dir);
+    float **r = matrix(1, ny, 1, nx), **u = matrix(1, ny, 1, nx), **t = NULL, *e = NULL;
+    if (l > 0) {
+        FL = vector(1, l);
+        for (k = 1; k <= l; k++) FL[k] = fl[k - 1];
+        t = matrix(1, ny, 1, nx);
+        e = vector(1, l);
+        model(r, u, t, e);
+    } else {
+        model_elastic(r, u);
+    }
+    for (j = 1; j <= ny; j++)
+        for (i = 1; i <= nx; i++) {
+            vs[(j - 1) * nx + i - 1] = u[j][i];
+            rho[(j - 1) * nx + i - 1] = r[j][i];
+            if (l > 0) taus[(j - 1) * nx + i - 1] = t[j][i];
+        }
+    if (l > 0) {
+        for (k = 1; k <= l; k++) eta[k - 1] = e[k];
+        free_matrix(t, 1, ny, 1, nx);
+        free_vector(e, 1, l);
+        free_vector(FL, 1, l);
+    }
+    free_matrix(r, 1, ny, 1, nx); free_matrix(u, 1, ny, 1, nx);
+    FL = fl0;
+    NX = nx0; NY = ny0; NXG = nxg0; NYG = nyg0; MYID = myid0; L = l0; DH = dh0; DT = dt0; FP = fp0;
+    if (quiet) fclose(quiet);
+    return 0;
+}
