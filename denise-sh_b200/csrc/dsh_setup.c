@@ -11,6 +11,7 @@
  * order.
  */
 #include "dsh_setup.h"
+#include "dsh.h"
 
 #include <math.h>
 #include <stdlib.h>
@@ -74,6 +75,56 @@ double dsh_setup_dt_limit(int fdorder, int maxrelerror, float dh, float vmax)
     if (dsh_setup_holberg(fdorder, maxrelerror, hc) != 0 || vmax <= 0) return 0.0;
     for (k = 1; k <= 6; k++) gamma += fabs(hc[k]);
     return dh / (sqrt(2.0) * gamma * vmax);
+}
+
+/* FD grid check of the starting model (checkfd_ssg_visc.c:14-140,
+ * checkfd_ssg_elastic.c), the reference's float/double mix kept: sumu, c,
+ * gamma, dtstab and dhstab are floats formed from double expressions. */
+int dsh_check_fd(int nx, int ny, int l, const float *fl, float dh, float dt, float ts, int fdorder, int maxrelerror,
+                 int fw, const float *vs, const float *rho, const float *qs, float out[4], int *warn)
+{
+    float hc[7], peta[DSH_MAX_L];
+    float cmax = 0.0f, cmin = 1e9f, c, ws, fmax, gamma, dtstab, dhstab;
+    size_t k, n;
+    int m;
+    if (nx < 1 || ny < 1 || l < 0 || l > DSH_MAX_L || !vs || !rho || !out || !(ts > 0.0f) || !(dh > 0.0f) ||
+        (l > 0 && (!fl || !qs)) || dsh_setup_holberg(fdorder, maxrelerror, hc) != 0)
+        return DSH_ERR_PARAM;
+    for (m = 0; m < l; m++) {                       /* readmod.c:32-33 */
+        const float pts = 1.0 / (2.0 * DSH_PI * fl[m]);
+        peta[m] = dt / pts;
+    }
+    ws = 2.0 * DSH_PI / ts;                         /* checkfd_ssg_visc.c:27 */
+    n = (size_t)nx * ny;
+    for (k = 0; k < n; k++) {
+        const float u = vs[k], r = rho[k];
+        if (l > 0) {
+            const float taus = 2.0 / qs[k];         /* readmod.c:99 */
+            const float pu_ref = r * u * u;
+            float sumu = 0.0f;
+            for (m = 0; m < l; m++) {
+                const float tsl = dt / peta[m];
+                sumu = sumu + ((ws * ws * tsl * tsl * taus) / (1.0 + ws * ws * tsl * tsl));
+            }
+            c = sqrt(pu_ref / (r * (1.0 + sumu)));
+            if (cmin > c) cmin = c;
+            c = sqrt(pu_ref * (1.0 + l * taus) / (r * (1.0 + sumu)));
+            if (cmax < c) cmax = c;
+        } else {
+            c = u;
+            if (cmax < c) cmax = c;
+            if (cmin > c) cmin = c;
+        }
+    }
+    fmax = 2.0 / ts;
+    dhstab = (cmin / (hc[0] * fmax));
+    gamma = fabs(hc[1]) + fabs(hc[2]) + fabs(hc[3]) + fabs(hc[4]) + fabs(hc[5]) + fabs(hc[6]);
+    dtstab = dh / (sqrt(2) * gamma * cmax);
+    out[0] = cmin; out[1] = cmax; out[2] = dtstab; out[3] = dhstab;
+    if (warn) *warn = (dh > dhstab ? 1 : 0) | (fw < 10 ? 2 : 0);
+    if (dt > dtstab) return DSH_ERR_UNSTABLE;
+    if (fw > nx || fw > ny) return DSH_ERR_PARAM;
+    return DSH_OK;
 }
 
 /* One C-PML node: damping d = d0 * x^npower, stretching K, frequency shift

@@ -574,3 +574,27 @@ def wavelet(quellart: int, nt: int, dt: float, srcpos8) -> np.ndarray:
 
 def dt_limit(fdorder: int, maxrelerror: int, dh: float, vmax: float) -> float:
     return lib().dsh_setup_dt_limit(fdorder, maxrelerror, dh, vmax)
+
+
+def check_fd(vs, rho, qs=None, fl=(), *, dh: float, dt: float, ts: float, fdorder: int, maxrelerror: int = 1,
+             fw: int = 20):
+    """The reference's FD grid check of a starting model (checkfd_ssg_visc /
+    checkfd_ssg_elastic): returns (status, dict(cmin, cmax, dtstab, dhstab),
+    warn bits); status is DSH_OK, ERR_UNSTABLE (DT above the stability
+    limit) or ERR_PARAM (FW wider than the grid), as the reference's stops."""
+    vs = np.ascontiguousarray(vs, np.float32)
+    rho = np.ascontiguousarray(rho, np.float32)
+    ny, nx = vs.shape
+    l = len(fl)
+    q = np.ascontiguousarray(qs, np.float32) if l > 0 else None
+    flv = (C.c_float * 8)(*fl)
+    out = (C.c_float * 4)()
+    warn = C.c_int(0)
+    L = lib()
+    L.dsh_check_fd.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_int,
+                               C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_int)]
+    rc = L.dsh_check_fd(nx, ny, l, C.cast(flv, C.c_void_p), dh, dt, ts, fdorder, maxrelerror, fw, vs.ctypes.data,
+                        rho.ctypes.data, q.ctypes.data if q is not None else None, C.cast(out, C.c_void_p),
+                        C.byref(warn))
+    vals = dict(zip(("cmin", "cmax", "dtstab", "dhstab"), (np.float32(v) for v in out)))
+    return rc, vals, warn.value

@@ -313,6 +313,22 @@ int dsh_set_misfit(dsh_ctx *ctx, int lnorm);
  * points of it.  enable = 0 switches it off (the default). */
 int dsh_set_shot_taper(dsh_ctx *ctx, int enable, int srtshape, float srtradius, int filtsize);
 
+/* The FD grid check the reference runs once on the starting model
+ * (src/denise.c:617-622: checkfd_ssg_visc, src/checkfd_ssg_visc.c:14-140,
+ * for l > 0; checkfd_ssg_elastic, src/checkfd_ssg_elastic.c, for l == 0;
+ * INVMAT1=1), on dense [ny][nx] vs, rho, qs with the reference's float /
+ * double mix: out[0] = cmin, the smallest S velocity at zero frequency;
+ * out[1] = cmax, the largest at infinite frequency; out[2] = dtstab =
+ * DH / (sqrt(2) gamma cmax), gamma = sum |hc[1..6]|; out[3] = dhstab =
+ * cmin / (hc[0] * 2/TS), the grid spacing for hc[0] points per minimum
+ * wavelength.  Returns DSH_ERR_UNSTABLE where the reference stops with "The
+ * simulation will get unstable" (DT > dtstab), DSH_ERR_PARAM where it stops
+ * because FW exceeds NX or NY (and for invalid arguments); *warn (optional)
+ * gets bit 0 for its grid-dispersion warning (DH > dhstab) and bit 1 for
+ * FW < 10.  ts = the source duration TS of the parameter file. */
+int dsh_check_fd(int nx, int ny, int l, const float *fl, float dh, float dt, float ts, int fdorder, int maxrelerror,
+                 int fw, const float *vs, const float *rho, const float *qs, float out[4], int *warn);
+
 /* Statistics of the last dsh_forward / dsh_gradient call. */
 typedef struct dsh_stats {
     double ms_forward, ms_adjoint, ms_total;   /* device time (CUDA events) */

@@ -407,3 +407,24 @@ def builtin_model(l, nx, ny, dh, dt, fl=()):
     if rc != 0:
         raise RuntimeError("refh_builtin_model failed")
     return vs, rho, (taus if l > 0 else None), (eta[:l] if l > 0 else None), vs_file
+
+
+def checkfd(vs, rho, qs, fl, dh, dt, ts, fdorder, maxrelerror, fw):
+    """The reference's FD grid check (checkfd_ssg_visc for fl non-empty, else
+    checkfd_ssg_elastic) on arguments that pass it; returns its report."""
+    import tempfile
+
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_checkfd.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_float, C.c_float, C.c_float,
+                                 C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    vs, rho = _f32(vs), _f32(rho)
+    ny, nx = vs.shape
+    l = len(fl)
+    q = _f32(qs) if l > 0 else np.ones_like(vs)
+    flv = np.asarray(list(fl) + [0.0] * (8 - l), np.float32)
+    with tempfile.TemporaryDirectory() as d:
+        log = os.path.join(d, "checkfd.log")
+        if lib.refh_checkfd(log.encode(), l, nx, ny, flv.ctypes.data, dh, dt, ts, fdorder, maxrelerror, fw,
+                            vs.ctypes.data, rho.ctypes.data, q.ctypes.data) != 0:
+            raise RuntimeError("refh_checkfd failed")
+        return open(log).read()

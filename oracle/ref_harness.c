@@ -872,3 +872,48 @@ int refh_builtin_model(const char *dir, int l, int nx, int ny, float dh, float d
     if (quiet) fclose(quiet);
     return 0;
 }
+
+/* The reference's FD grid check (src/checkfd_ssg_visc.c for l > 0,
+ * src/checkfd_ssg_elastic.c for l == 0) on dense [ny][nx] vs, rho, qs; its
+ * report goes to the file log.  Only for arguments that pass the check: where
+ * it fails the reference ends the process (err). */
+void checkfd_ssg_visc(FILE *fp, float **prho, float **pu, float **ptaus, float *peta, float *hc);
+void checkfd_ssg_elastic(FILE *fp, float **prho, float **pu, float *hc);
+extern float TS;
+int refh_checkfd(const char *log, int l, int nx, int ny, const float *fl, float dh, float dt, float ts, int fdorder,
+                 int maxrelerror, int fw, const float *vs, const float *rho, const float *qs)
+{
+    int i, j, k;
+    FILE *fp = fopen(log, "w");
+    if (!fp) return -1;
+    const int nx0 = NX, ny0 = NY, myid0 = MYID, l0 = L, fdo0 = FDORDER, mre0 = MAXRELERROR, fw0 = FW, inv0 = INVMAT1;
+    const float dh0 = DH, dt0 = DT, ts0 = TS;
+    NX = nx; NY = ny; DH = dh; DT = dt; TS = ts; L = l; MYID = 0; FDORDER = fdorder; MAXRELERROR = maxrelerror;
+    FW = fw; INVMAT1 = 1;
+    float *h = holbergcoeff();
+    float **r = matrix(1, ny, 1, nx), **u = matrix(1, ny, 1, nx);
+    for (j = 1; j <= ny; j++)
+        for (i = 1; i <= nx; i++) {
+            u[j][i] = vs[(j - 1) * nx + i - 1];
+            r[j][i] = rho[(j - 1) * nx + i - 1];
+        }
+    if (l > 0) {
+        float **t = matrix(1, ny, 1, nx), *e = vector(1, l);
+        for (j = 1; j <= ny; j++)
+            for (i = 1; i <= nx; i++) t[j][i] = 2.0 / qs[(j - 1) * nx + i - 1];   /* readmod.c:99 */
+        for (k = 1; k <= l; k++) {                                                 /* readmod.c:32-33 */
+            float pts = 1.0 / (2.0 * PI * fl[k - 1]);
+            e[k] = DT / pts;
+        }
+        checkfd_ssg_visc(fp, r, u, t, e, h);
+        free_matrix(t, 1, ny, 1, nx);
+        free_vector(e, 1, l);
+    } else {
+        checkfd_ssg_elastic(fp, r, u, h);
+    }
+    fclose(fp);
+    free_matrix(r, 1, ny, 1, nx); free_matrix(u, 1, ny, 1, nx); free_vector(h, 0, 6);
+    NX = nx0; NY = ny0; MYID = myid0; L = l0; FDORDER = fdo0; MAXRELERROR = mre0; FW = fw0; INVMAT1 = inv0;
+    DH = dh0; DT = dt0; TS = ts0;
+    return 0;
+}
