@@ -169,3 +169,48 @@ int dsh_line_search_next(dsh_line_search *ls, float L2_test, float *eps_scale, i
     *slot = ls->slot;
     return 1;
 }
+
+/* calc_misfit.c:51-86 for itest = 0, sws = 1, swstestshot = 1: float
+ * running integrals and sums; the LNORM=5 correction is formed in double and
+ * stored back to the float sum. */
+double dsh_calc_misfit(const float *obs, const float *syn, int ntr, int ns, int lnorm, float dt, float l2_in)
+{
+    float L2 = l2_in;
+    int i, j;
+    if (!obs || !syn || ntr < 0 || ns < 0) return NAN;
+    for (i = 0; i < ntr; i++) {
+        const float *d = obs + (size_t)i * ns, *s = syn + (size_t)i * ns;
+        float intseis = 0.0f, intseis_data = 0.0f, intseis_synthetics = 0.0f, abs_data = 0.0f, abs_synthetics = 0.0f;
+        float L2_dummy = 0.0f;
+        for (j = 0; j < ns; j++) {
+            if (lnorm == 2 || lnorm == 6) intseis += s[j] - d[j];
+            if (lnorm == 5) {
+                intseis_data += d[j] * dt;
+                intseis_synthetics += s[j] * dt;
+                abs_data += intseis_data * intseis_data;
+                abs_synthetics += intseis_synthetics * intseis_synthetics;
+                L2_dummy += (intseis_data * intseis_synthetics);
+            }
+            if (lnorm == 2 || lnorm == 6) L2 += intseis * intseis * dt * dt;
+        }
+        if (lnorm == 5) L2 -= L2_dummy / (sqrt(abs_data) * sqrt(abs_synthetics));
+    }
+    return L2;
+}
+
+/* calc_energy.c:51-59 */
+double dsh_calc_energy(const float *obs, int ntr, int ns, float dt, float energy_in)
+{
+    float energy = energy_in;
+    int i, j;
+    if (!obs || ntr < 0 || ns < 0) return NAN;
+    for (i = 0; i < ntr; i++) {
+        const float *d = obs + (size_t)i * ns;
+        float intseis = 0.0f;
+        for (j = 0; j < ns; j++) {
+            intseis += d[j];
+            energy += intseis * intseis * dt * dt;
+        }
+    }
+    return energy;
+}

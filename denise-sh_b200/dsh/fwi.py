@@ -38,8 +38,31 @@ def _setup():
         L.dsh_line_search_init.argtypes = [C.POINTER(LineSearch), C.c_float, C.c_float, C.c_float, C.c_int]
         L.dsh_line_search_next.argtypes = [C.POINTER(LineSearch), C.c_float, C.POINTER(C.c_float),
                                            C.POINTER(C.c_int)]
+        L.dsh_calc_misfit.restype = C.c_double
+        L.dsh_calc_misfit.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float]
+        L.dsh_calc_energy.restype = C.c_double
+        L.dsh_calc_energy.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
         L._fwi_ready = True
     return L
+
+
+def calc_misfit(obs, syn, lnorm: int, dt: float, l2_in: float = 0.0) -> float:
+    """Misfit of traces [ntr, ns] as src/calc_misfit.c forms it (running
+    integrals, float sums), added to l2_in."""
+    o = np.ascontiguousarray(obs, np.float32)
+    s = np.ascontiguousarray(syn, np.float32)
+    if o.shape != s.shape or o.ndim != 2:
+        raise ValueError("obs and syn must be [ntr, ns] of one shape")
+    return _setup().dsh_calc_misfit(o.ctypes.data, s.ctypes.data, o.shape[0], o.shape[1], lnorm, dt, l2_in)
+
+
+def calc_energy(obs, dt: float, energy_in: float = 0.0) -> float:
+    """Energy of the running integrals of traces [ntr, ns] (src/calc_energy.c),
+    added to energy_in; the reference reports L2 / energy for LNORM=2."""
+    o = np.ascontiguousarray(obs, np.float32)
+    if o.ndim != 2:
+        raise ValueError("obs must be [ntr, ns]")
+    return _setup().dsh_calc_energy(o.ctypes.data, o.shape[0], o.shape[1], dt, energy_in)
 
 
 def lbfgs_direction(S, Y, q):

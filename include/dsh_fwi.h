@@ -60,6 +60,23 @@ typedef struct dsh_line_search {
 void dsh_line_search_init(dsh_line_search *ls, float L2_now, float eps_scale, float scalefac, int stepmax);
 int dsh_line_search_next(dsh_line_search *ls, float L2_test, float *eps_scale, int *slot);
 
+/* Misfit and data energy of the FWI loop's reported objective and of the
+ * line search's test shots (called at src/denise.c:1423-1425 and in
+ * src/line_search.c), over traces [ntr][ns] (row-major, sample 1 first), with
+ * the reference's float accumulation; trace killing (TRKILL) is not built.
+ *   dsh_calc_misfit (src/calc_misfit.c:7-100, itest = 0, sws = 1,
+ *   swstestshot = 1): LNORM 2 and 6 add, per trace, the squared running
+ *   integral of syn - obs times DT^2; LNORM 5 subtracts, per trace, the
+ *   normalised correlation of the running integrals of obs and syn; other
+ *   LNORMs add nothing.  The sum starts from l2_in (the running total the
+ *   reference passes in).
+ *   dsh_calc_energy (src/calc_energy.c:7-65): adds the squared running
+ *   integral of obs times DT^2 to energy_in.
+ * The L2 misfit the reference reports is L2 / energy for LNORM=2
+ * (src/denise.c:1719-1723). */
+double dsh_calc_misfit(const float *obs, const float *syn, int ntr, int ns, int lnorm, float dt, float l2_in);
+double dsh_calc_energy(const float *obs, int ntr, int ns, float dt, float energy_in);
+
 #ifdef __cplusplus
 }
 #endif

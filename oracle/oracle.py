@@ -428,3 +428,21 @@ def checkfd(vs, rho, qs, fl, dh, dt, ts, fdorder, maxrelerror, fw):
                             vs.ctypes.data, rho.ctypes.data, q.ctypes.data) != 0:
             raise RuntimeError("refh_checkfd failed")
         return open(log).read()
+
+
+def calc_misfit(obs, syn, lnorm, dt, l2_in=0.0):
+    """The reference's calc_misfit (src/calc_misfit.c) of traces [ntr, ns]."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_calc_misfit.restype = C.c_double
+    lib.refh_calc_misfit.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float]
+    o, s = _f32(obs), _f32(syn)
+    return lib.refh_calc_misfit(o.ctypes.data, s.ctypes.data, o.shape[0], o.shape[1], lnorm, dt, l2_in)
+
+
+def calc_energy(obs, dt, energy_in=0.0):
+    """The reference's calc_energy (src/calc_energy.c) of traces [ntr, ns]."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_calc_energy.restype = C.c_double
+    lib.refh_calc_energy.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
+    o = _f32(obs)
+    return lib.refh_calc_energy(o.ctypes.data, o.shape[0], o.shape[1], dt, energy_in)

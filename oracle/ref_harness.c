@@ -917,3 +917,40 @@ int refh_checkfd(const char *log, int l, int nx, int ny, const float *fl, float 
     DH = dh0; DT = dt0; TS = ts0;
     return 0;
 }
+
+/* The reference's misfit and data energy of traces [ntr][ns]
+ * (src/calc_misfit.c, src/calc_energy.c; TRKILL off), called as
+ * src/denise.c:1423-1425 calls them. */
+double calc_misfit(float **sectiondata, float **section, int ntr, int ns, int LNORM, float L2, int itest, int sws,
+                   int swstestshot, int ntr_glob, int **recpos_loc, int nsrc_glob, int ishot);
+double calc_energy(float **sectiondata, int ntr, int ns, float energy, int ntr_glob, int **recpos_loc, int nsrc_glob,
+                   int ishot);
+static float **traces_in(const float *a, int ntr, int ns)
+{
+    int i, j;
+    float **m = matrix(1, ntr, 1, ns);
+    for (i = 1; i <= ntr; i++) for (j = 1; j <= ns; j++) m[i][j] = a[(i - 1) * ns + j - 1];
+    return m;
+}
+double refh_calc_misfit(const float *obs, const float *syn, int ntr, int ns, int lnorm, float dt, float l2_in)
+{
+    const float dt0 = DT;
+    const int trk0 = TRKILL;
+    float **d = traces_in(obs, ntr, ns), **s = traces_in(syn, ntr, ns);
+    DT = dt; TRKILL = 0;
+    const double r = calc_misfit(d, s, ntr, ns, lnorm, l2_in, 0, 1, 1, ntr, NULL, 1, 1);
+    DT = dt0; TRKILL = trk0;
+    free_matrix(d, 1, ntr, 1, ns); free_matrix(s, 1, ntr, 1, ns);
+    return r;
+}
+double refh_calc_energy(const float *obs, int ntr, int ns, float dt, float energy_in)
+{
+    const float dt0 = DT;
+    const int trk0 = TRKILL;
+    float **d = traces_in(obs, ntr, ns);
+    DT = dt; TRKILL = 0;
+    const double r = calc_energy(d, ntr, ns, energy_in, ntr, NULL, 1, 1);
+    DT = dt0; TRKILL = trk0;
+    free_matrix(d, 1, ntr, 1, ns);
+    return r;
+}
