@@ -214,3 +214,47 @@ double dsh_calc_energy(const float *obs, int ntr, int ns, float dt, float energy
     }
     return energy;
 }
+
+/* calc_mat_change_test.c:31-170 (itest = 1: the caller keeps or adopts the
+ * new fields); maxima over the grid in the reference's order, float steps */
+float dsh_model_update(int nx, int ny, const float *vs, const float *rho, const float *d_vs, const float *d_rho,
+                       float eps_scale, float scalerho, int iter, int inv_vs_iter, int inv_rho_iter,
+                       const float limits[4], float *vs_new, float *rho_new, float *eps_rho)
+{
+    float umax = 0.0f, rhomax = 0.0f, gradmax_u = 0.0f, gradmax_rho = 0.0f, eps_u, eps_r;
+    int i, j;
+    if (nx < 1 || ny < 1 || !vs || !rho || !d_vs || !d_rho || !limits || !vs_new || !rho_new) return NAN;
+    for (i = 0; i < nx; i++)
+        for (j = 0; j < ny; j++) {
+            const size_t k = (size_t)j * nx + i;
+            const float gu = fabs(d_vs[k]), gr = fabs(d_rho[k]);
+            if (vs[k] > umax) umax = vs[k];
+            if ((i == 0 && j == 0) || gradmax_u == 0.0f) gradmax_u = gu;
+            else if (gu > gradmax_u) gradmax_u = gu;
+            if (rho[k] > rhomax) rhomax = rho[k];
+            if ((i == 0 && j == 0) || gradmax_rho == 0.0f) gradmax_rho = gr;
+            else if (gr > gradmax_rho) gradmax_rho = gr;
+        }
+    eps_u = eps_scale * (umax / gradmax_u);
+    if (iter < inv_vs_iter) eps_u = 0.0f;
+    eps_r = eps_scale * (rhomax / gradmax_rho) * scalerho;
+    if (iter < inv_rho_iter) eps_r = 0.0f;
+    for (i = 0; i < nx; i++)
+        for (j = 0; j < ny; j++) {
+            const size_t k = (size_t)j * nx + i;
+            float un = vs[k] - eps_u * d_vs[k];
+            float rn = rho[k] - eps_r * d_rho[k];
+            if (un < limits[0] && un > 1e-6) un = vs[k];
+            if (un > limits[1]) un = vs[k];
+            if (rn < limits[2]) rn = rho[k];
+            if (rn > limits[3]) rn = rho[k];
+            if (inv_vs_iter > iter) un = vs[k];
+            if (inv_rho_iter > iter) rn = rho[k];
+            if (un < 0.0f) un = vs[k];
+            if (rn < 0.0f) rn = rho[k];
+            vs_new[k] = un;
+            rho_new[k] = rn;
+        }
+    if (eps_rho) *eps_rho = eps_r;
+    return eps_u;
+}

@@ -42,8 +42,29 @@ def _setup():
         L.dsh_calc_misfit.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_float, C.c_float]
         L.dsh_calc_energy.restype = C.c_double
         L.dsh_calc_energy.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
+        L.dsh_model_update.restype = C.c_float
+        L.dsh_model_update.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_float, C.c_float, C.c_int,
+                                                                                C.c_int, C.c_int] + [C.c_void_p] * 4
         L._fwi_ready = True
     return L
+
+
+def model_update(vs, rho, d_vs, d_rho, eps_scale: float, scalerho: float = 1.0, it: int = 1, inv_vs_iter: int = 0,
+                 inv_rho_iter: int = 0, limits=(0.0, 1e9, 0.0, 1e9)):
+    """Model update along the directions d_vs, d_rho [ny, nx] as
+    src/calc_mat_change_test.c does it (step relative to max(vs)/max|d_vs|,
+    the reference's bounds); limits = (VSLOWERLIM, VSUPPERLIM, RHOLOWERLIM,
+    RHOUPPERLIM).  Returns vs_new, rho_new, eps_u, eps_rho."""
+    a = [np.ascontiguousarray(x, np.float32) for x in (vs, rho, d_vs, d_rho)]
+    if any(x.shape != a[0].shape for x in a) or a[0].ndim != 2:
+        raise ValueError("vs, rho, d_vs, d_rho must be [ny, nx] of one shape")
+    ny, nx = a[0].shape
+    lim = np.asarray(limits, np.float32)
+    vn, rn = np.empty_like(a[0]), np.empty_like(a[0])
+    er = C.c_float()
+    eu = _setup().dsh_model_update(nx, ny, *[x.ctypes.data for x in a], eps_scale, scalerho, it, inv_vs_iter,
+                                   inv_rho_iter, lim.ctypes.data, vn.ctypes.data, rn.ctypes.data, C.addressof(er))
+    return vn, rn, np.float32(eu), np.float32(er.value)
 
 
 def calc_misfit(obs, syn, lnorm: int, dt: float, l2_in: float = 0.0) -> float:

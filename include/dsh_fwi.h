@@ -75,6 +75,20 @@ int dsh_line_search_next(dsh_line_search *ls, float L2_test, float *eps_scale, i
  * The L2 misfit the reference reports is L2 / energy for LNORM=2
  * (src/denise.c:1719-1723). */
 double dsh_calc_misfit(const float *obs, const float *syn, int ntr, int ns, int lnorm, float dt, float l2_in);
+
+/* Model update along the search direction (src/calc_mat_change_test.c:9-170,
+ * INVMAT1=1), on dense [ny][nx] fields: eps_u = eps_scale * max(vs)/max|d_vs|
+ * and eps_rho = eps_scale * max(rho)/max|d_rho| * SCALERHO (0 before
+ * INV_VS_ITER / INV_RHO_ITER), vs_new = vs - eps_u d_vs, rho_new = rho -
+ * eps_rho d_rho, then the reference's bounds in its order: a new vs below
+ * VSLOWERLIM (but above 1e-6) or above VSUPPERLIM keeps the old value, a new
+ * rho outside [RHOLOWERLIM, RHOUPPERLIM] keeps the old value, before the
+ * INV_*_ITER iterations the old values are kept, negative values keep the old
+ * ones.  Returns eps_u (the reference's eps_true); *eps_rho (optional) gets
+ * eps_rho.  limits = {VSLOWERLIM, VSUPPERLIM, RHOLOWERLIM, RHOUPPERLIM}. */
+float dsh_model_update(int nx, int ny, const float *vs, const float *rho, const float *d_vs, const float *d_rho,
+                       float eps_scale, float scalerho, int iter, int inv_vs_iter, int inv_rho_iter,
+                       const float limits[4], float *vs_new, float *rho_new, float *eps_rho);
 double dsh_calc_energy(const float *obs, int ntr, int ns, float dt, float energy_in);
 
 #ifdef __cplusplus

@@ -446,3 +446,20 @@ def calc_energy(obs, dt, energy_in=0.0):
     lib.refh_calc_energy.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_float]
     o = _f32(obs)
     return lib.refh_calc_energy(o.ctypes.data, o.shape[0], o.shape[1], dt, energy_in)
+
+
+def model_update(vs, rho, d_vs, d_rho, eps_scale, scalerho, it, inv_vs_iter, inv_rho_iter, limits):
+    """The reference's model update (src/calc_mat_change_test.c, itest = 1):
+    returns vs_new, rho_new, eps_u, eps_rho."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_model_update.restype = C.c_float
+    lib.refh_model_update.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_float, C.c_float, C.c_int, C.c_int,
+                                                                              C.c_int] + [C.c_void_p] * 4
+    a = [_f32(x) for x in (vs, rho, d_vs, d_rho)]
+    ny, nx = a[0].shape
+    lim = _f32(limits)
+    vn, rn = np.zeros_like(a[0]), np.zeros_like(a[0])
+    er = C.c_float()
+    eu = lib.refh_model_update(nx, ny, *[x.ctypes.data for x in a], eps_scale, scalerho, it, inv_vs_iter,
+                               inv_rho_iter, lim.ctypes.data, vn.ctypes.data, rn.ctypes.data, C.addressof(er))
+    return vn, rn, np.float32(eu), np.float32(er.value)

@@ -954,3 +954,40 @@ double refh_calc_energy(const float *obs, int ntr, int ns, float dt, float energ
     free_matrix(d, 1, ntr, 1, ns);
     return r;
 }
+
+/* The reference's model update (src/calc_mat_change_test.c, itest = 1) on
+ * dense [ny][nx] fields; returns eps_true, *eps_rho = EPSILON_rho. */
+float calc_mat_change_test(float **waveconv_rho, float **waveconv_u, float **rho, float **rhonp1, float **u,
+                           float **unp1, int iter, int epstest, int INVMAT, float eps_scale, int itest, int nfstart);
+extern float SCALERHO, EPSILON_u, EPSILON_rho, VSUPPERLIM, VSLOWERLIM, RHOUPPERLIM, RHOLOWERLIM;
+extern int INV_RHO_ITER, INV_VS_ITER;
+static float **field_in(const float *a, int nx, int ny)
+{
+    int i, j;
+    float **m = matrix(1, ny, 1, nx);
+    for (j = 1; j <= ny; j++) for (i = 1; i <= nx; i++) m[j][i] = a[(j - 1) * nx + i - 1];
+    return m;
+}
+float refh_model_update(int nx, int ny, const float *vs, const float *rho, const float *d_vs, const float *d_rho,
+                        float eps_scale, float scalerho, int iter, int inv_vs_iter, int inv_rho_iter,
+                        const float *limits, float *vs_new, float *rho_new, float *eps_rho)
+{
+    int i, j;
+    const int nx0 = NX, ny0 = NY, myid0 = MYID, inv0 = INVMAT1;
+    NX = nx; NY = ny; MYID = 0; INVMAT1 = 1;
+    SCALERHO = scalerho; INV_VS_ITER = inv_vs_iter; INV_RHO_ITER = inv_rho_iter;
+    VSLOWERLIM = limits[0]; VSUPPERLIM = limits[1]; RHOLOWERLIM = limits[2]; RHOUPPERLIM = limits[3];
+    float **u = field_in(vs, nx, ny), **r = field_in(rho, nx, ny), **gu = field_in(d_vs, nx, ny),
+          **gr = field_in(d_rho, nx, ny), **un = matrix(1, ny, 1, nx), **rn = matrix(1, ny, 1, nx);
+    const float eps = calc_mat_change_test(gr, gu, r, rn, u, un, iter, 1, 0, eps_scale, 1, 0);
+    for (j = 1; j <= ny; j++)
+        for (i = 1; i <= nx; i++) {
+            vs_new[(j - 1) * nx + i - 1] = un[j][i];
+            rho_new[(j - 1) * nx + i - 1] = rn[j][i];
+        }
+    *eps_rho = EPSILON_rho;
+    free_matrix(u, 1, ny, 1, nx); free_matrix(r, 1, ny, 1, nx); free_matrix(gu, 1, ny, 1, nx);
+    free_matrix(gr, 1, ny, 1, nx); free_matrix(un, 1, ny, 1, nx); free_matrix(rn, 1, ny, 1, nx);
+    NX = nx0; NY = ny0; MYID = myid0; INVMAT1 = inv0;
+    return eps;
+}
