@@ -6,6 +6,7 @@
 
 #include <math.h>
 #include <stddef.h>
+#include <stdlib.h>
 
 static double dot(long long n, const float *a, const float *b)
 {
@@ -257,4 +258,49 @@ float dsh_model_update(int nx, int ny, const float *vs, const float *rho, const 
         }
     if (eps_rho) *eps_rho = eps_r;
     return eps_u;
+}
+
+/* dotp.c:12-40: float sum in index order */
+static float dotp_f(const float *a, const float *b, long long n)
+{
+    float tmp = 0.0f;
+    long long i;
+    for (i = 0; i < n; i++) tmp += a[i] * b[i];
+    return tmp;
+}
+
+/* LBFGS.c:25-104 */
+int dsh_lbfgs_ring(int iter, const float *y, const float *s, float *q, float *r, int pointer, int nlbfgs,
+                   long long nvec)
+{
+    float *rho, *alpha, gamma;
+    long long i;
+    int k;
+    if (!y || !s || !q || !r || nlbfgs < 1 || nvec < 1 || pointer < 1 || pointer > nlbfgs) return -1;
+    if (iter <= 1) return 0;
+    rho = (float *)malloc(2 * (size_t)nlbfgs * sizeof(float));
+    if (!rho) return -3;
+    alpha = rho + nlbfgs;
+    {
+        const float *yp = y + (size_t)(pointer - 1) * nvec, *sp = s + (size_t)(pointer - 1) * nvec;
+        const float sum_nom = dotp_f(yp, sp, nvec), sum_denom = dotp_f(yp, yp, nvec);
+        gamma = sum_nom / sum_denom;
+    }
+    for (k = 1; k <= nlbfgs; k++) {
+        const float sum_nom = dotp_f(y + (size_t)(k - 1) * nvec, s + (size_t)(k - 1) * nvec, nvec);
+        rho[k - 1] = fabs(sum_nom) > 0.0 ? 1.0 / sum_nom : 0.0;
+    }
+    for (k = nlbfgs; k >= 1; k--) {
+        const float *yk = y + (size_t)(k - 1) * nvec, *sk = s + (size_t)(k - 1) * nvec;
+        alpha[k - 1] = rho[k - 1] * dotp_f(sk, q, nvec);
+        for (i = 0; i < nvec; i++) q[i] = q[i] - alpha[k - 1] * yk[i];
+    }
+    for (i = 0; i < nvec; i++) r[i] = gamma * q[i];
+    for (k = 1; k <= nlbfgs; k++) {
+        const float *yk = y + (size_t)(k - 1) * nvec, *sk = s + (size_t)(k - 1) * nvec;
+        const float beta = rho[k - 1] * dotp_f(yk, r, nvec);
+        for (i = 0; i < nvec; i++) r[i] = r[i] + sk[i] * (alpha[k - 1] - beta);
+    }
+    free(rho);
+    return 0;
 }

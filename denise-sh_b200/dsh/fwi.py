@@ -45,8 +45,26 @@ def _setup():
         L.dsh_model_update.restype = C.c_float
         L.dsh_model_update.argtypes = [C.c_int, C.c_int] + [C.c_void_p] * 4 + [C.c_float, C.c_float, C.c_int,
                                                                                 C.c_int, C.c_int] + [C.c_void_p] * 4
+        L.dsh_lbfgs_ring.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
+                                     C.c_longlong]
         L._fwi_ready = True
     return L
+
+
+def lbfgs_ring(it: int, y, s, q, pointer: int):
+    """The reference's own L-BFGS step (src/LBFGS.c) on its ring buffers y, s
+    [nlbfgs, nvec] (newest pair in slot `pointer`, 1-based): returns
+    (q after the first loop, r = H q), slot order and float sums as the
+    reference; r = 0 and q unchanged for it <= 1."""
+    y = np.ascontiguousarray(y, np.float32)
+    s = np.ascontiguousarray(s, np.float32)
+    q = np.array(q, np.float32, copy=True).ravel()
+    if y.shape != s.shape or y.ndim != 2 or y.shape[1] != q.size:
+        raise ValueError("y and s must be [nlbfgs, nvec] with nvec = q.size")
+    r = np.zeros_like(q)
+    _check(_setup().dsh_lbfgs_ring(it, y.ctypes.data, s.ctypes.data, q.ctypes.data, r.ctypes.data, pointer,
+                                   y.shape[0], q.size), "dsh_lbfgs_ring")
+    return q, r
 
 
 def model_update(vs, rho, d_vs, d_rho, eps_scale: float, scalerho: float = 1.0, it: int = 1, inv_vs_iter: int = 0,

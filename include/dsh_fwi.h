@@ -26,6 +26,17 @@ extern "C" {
  * Dot products in double. */
 int dsh_lbfgs_direction(long long n, int count, const float *S, const float *Y, const float *q, float *r);
 
+/* The reference's own L-BFGS step (src/LBFGS.c:12-107) on its ring buffers:
+ * y and s hold nlbfgs slots of nvec values (slot k, 1-based, at
+ * (k-1)*nvec), the newest pair in slot `pointer`; q is the preconditioned
+ * gradient vector (overwritten, as the reference overwrites q_LBFGS) and r
+ * receives H q.  As the reference: nothing is done for iter <= 1; gamma from
+ * slot `pointer`; the two loops run over the slots in slot order (k = nlbfgs
+ * .. 1, then 1 .. nlbfgs) whatever their age, empty slots included (their
+ * rho is 0); every dot product is a float sum in index order (src/dotp.c). */
+int dsh_lbfgs_ring(int iter, const float *y, const float *s, float *q, float *r, int pointer, int nlbfgs,
+                   long long nvec);
+
 /* Conjugate-gradient direction (src/PCG.c:10-107, called at
  * src/denise.c:1850-1871 on the steepest-descent directions of vs and rho):
  * the vectors hold nclass parameter classes of n values each, class after

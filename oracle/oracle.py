@@ -463,3 +463,15 @@ def model_update(vs, rho, d_vs, d_rho, eps_scale, scalerho, it, inv_vs_iter, inv
     eu = lib.refh_model_update(nx, ny, *[x.ctypes.data for x in a], eps_scale, scalerho, it, inv_vs_iter,
                                inv_rho_iter, lim.ctypes.data, vn.ctypes.data, rn.ctypes.data, C.addressof(er))
     return vn, rn, np.float32(eu), np.float32(er.value)
+
+
+def lbfgs_ring(it, y, s, q, pointer, nlbfgs):
+    """The reference's L-BFGS step (src/LBFGS.c) on ring buffers y, s
+    [nlbfgs, nvec]; returns (q after the first loop, r)."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_lbfgs.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int]
+    y, s = _f32(y), _f32(s)
+    q = _f32(q).copy()
+    r = np.zeros_like(q)
+    lib.refh_lbfgs(it, y.ctypes.data, s.ctypes.data, q.ctypes.data, r.ctypes.data, pointer, nlbfgs, q.size)
+    return q, r

@@ -991,3 +991,24 @@ float refh_model_update(int nx, int ny, const float *vs, const float *rho, const
     NX = nx0; NY = ny0; MYID = myid0; INVMAT1 = inv0;
     return eps;
 }
+
+/* The reference's L-BFGS step (src/LBFGS.c) on its ring buffers y, s
+ * [nlbfgs*nvec] and the vector q [nvec] (overwritten); r [nvec] out. */
+void LBFGS(int iter, float *y_LBFGS, float *s_LBFGS, float *rho_LBFGS, float *alpha_LBFGS, float *q_LBFGS,
+           float *r_LBFGS, float *beta_LBFGS, int LBFGS_pointer, int NLBFGS, int NLBFGS_vec);
+int refh_lbfgs(int iter, const float *y, const float *s, float *q, float *r, int pointer, int nlbfgs, int nvec)
+{
+    int i;
+    const int n = nlbfgs * nvec, myid0 = MYID;
+    float *yv = vector(1, n), *sv = vector(1, n), *qv = vector(1, nvec), *rv = vector(1, nvec);
+    float *rho = vector(1, nlbfgs), *alpha = vector(1, nlbfgs), *beta = vector(1, nlbfgs);
+    for (i = 1; i <= n; i++) { yv[i] = y[i - 1]; sv[i] = s[i - 1]; }
+    for (i = 1; i <= nvec; i++) { qv[i] = q[i - 1]; rv[i] = r[i - 1]; }
+    MYID = 1;                                    /* no per-slot printout */
+    LBFGS(iter, yv, sv, rho, alpha, qv, rv, beta, pointer, nlbfgs, nvec);
+    MYID = myid0;
+    for (i = 1; i <= nvec; i++) { q[i - 1] = qv[i]; r[i - 1] = rv[i]; }
+    free_vector(yv, 1, n); free_vector(sv, 1, n); free_vector(qv, 1, nvec); free_vector(rv, 1, nvec);
+    free_vector(rho, 1, nlbfgs); free_vector(alpha, 1, nlbfgs); free_vector(beta, 1, nlbfgs);
+    return 0;
+}

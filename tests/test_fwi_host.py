@@ -130,3 +130,24 @@ def test_line_search_gives_up_without_descent():
 def test_line_search_terminates_on_non_finite_misfits():
     eps, tests = fwi.line_search(lambda e: float("nan"), 1.0, eps_scale=0.01, scalefac=2.0, stepmax=3)
     assert eps == 0.0 and tests == 4
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference build not present")
+@pytest.mark.parametrize("it,pointer,filled", [(2, 1, 1), (3, 2, 2), (6, 3, 5), (9, 5, 5), (1, 1, 1)])
+def test_lbfgs_ring_matches_reference(it, pointer, filled):
+    """dsh_lbfgs_ring against the reference's LBFGS.c compiled into the oracle:
+    ring buffers of 5 slots, some empty, the newest pair anywhere in the ring
+    (after wrap-around the reference's slot order differs from age order)."""
+    rng = np.random.default_rng(it * 10 + pointer)
+    nl, n = 5, 301
+    y = np.zeros((nl, n), np.float32)
+    s = np.zeros((nl, n), np.float32)
+    for k in range(filled):
+        s[k] = rng.standard_normal(n).astype(np.float32) * np.float32(1e-2)
+        y[k] = (s[k] * np.float32(3.0) + rng.standard_normal(n).astype(np.float32) * np.float32(1e-3))
+    q = rng.standard_normal(n).astype(np.float32)
+    got_q, got_r = fwi.lbfgs_ring(it, y, s, q, pointer)
+    ref_q, ref_r = O.lbfgs_ring(it, y, s, q, pointer, nl)
+    assert np.array_equal(got_q, ref_q) and np.array_equal(got_r, ref_r)
+    if it > 1:
+        assert np.abs(got_r).max() > 0
