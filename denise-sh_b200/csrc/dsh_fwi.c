@@ -304,3 +304,32 @@ int dsh_lbfgs_ring(int iter, const float *y, const float *s, float *q, float *r,
     free(rho);
     return 0;
 }
+
+/* calc_opt_step.c:61-103 with solvelin.c:29-52 (method 1) in float */
+float dsh_opt_step_ref(const float L2t[3], const float epst[3])
+{
+    float A[3][3], b[3], x[3], a, c, opteps;
+    int k, m, n;
+    for (k = 0; k < 3; k++) {
+        A[k][2] = (epst[k] * epst[k]);
+        A[k][1] = (epst[k]);
+        A[k][0] = (1.0);
+        b[k] = L2t[k];
+    }
+    for (k = 0; k < 2; k++)
+        for (n = k; n < 2; n++) {
+            a = A[n + 1][k] / A[k][k];
+            for (m = 0; m < 3; m++) A[n + 1][m] = A[n + 1][m] - a * A[k][m];
+            b[n + 1] = b[n + 1] - a * b[k];
+        }
+    for (k = 2; k >= 0; k--) {
+        c = b[k];
+        for (m = 2; m >= k + 1; m--) c = c - A[k][m] * x[m];
+        x[k] = c / A[k][k];
+    }
+    opteps = -x[1] / (2.0 * x[2]);
+    if (((2.0 * x[2]) < 0.0) && (L2t[1] > L2t[2])) opteps = epst[2];
+    if (opteps > epst[2]) opteps = epst[2];
+    if (opteps < 0.0) opteps = epst[0];
+    return opteps;
+}

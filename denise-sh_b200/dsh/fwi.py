@@ -47,8 +47,18 @@ def _setup():
                                                                                 C.c_int, C.c_int] + [C.c_void_p] * 4
         L.dsh_lbfgs_ring.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int,
                                      C.c_longlong]
+        L.dsh_opt_step_ref.restype = C.c_float
+        L.dsh_opt_step_ref.argtypes = [C.c_void_p, C.c_void_p]
         L._fwi_ready = True
     return L
+
+
+def opt_step_ref(L2t, epst):
+    """The parabolic step exactly as src/calc_opt_step.c computes it (float
+    Gauss elimination of src/solvelin.c)."""
+    a = np.ascontiguousarray(L2t, np.float32)
+    e = np.ascontiguousarray(epst, np.float32)
+    return np.float32(_setup().dsh_opt_step_ref(a.ctypes.data, e.ctypes.data))
 
 
 def lbfgs_ring(it: int, y, s, q, pointer: int):

@@ -57,6 +57,12 @@ int dsh_pcg_direction(long long n, int nclass, const float *g_new, const float *
 
 /* epst[0..2], L2t[0..2]: test step lengths (epst[0] = 0) and their misfits */
 float dsh_opt_step(const float L2t[3], const float epst[3]);
+/* The same step as src/calc_opt_step.c:20-111 computes it, bit for bit: the
+ * 3 x 3 system [1, eps, eps^2] x = L2 solved by the reference's float Gauss
+ * elimination without pivoting (src/solvelin.c:9-60); a singular system gives
+ * what the reference gives (a non-finite step).  dsh_opt_step (used by
+ * dsh_line_search_next) solves in double and guards the singular case. */
+float dsh_opt_step_ref(const float L2t[3], const float epst[3]);
 
 /* Line-search state of src/line_search.c: feed the misfits of the steps the
  * previous call asked for; returns 1 while another test forward is needed

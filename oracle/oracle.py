@@ -475,3 +475,12 @@ def lbfgs_ring(it, y, s, q, pointer, nlbfgs):
     r = np.zeros_like(q)
     lib.refh_lbfgs(it, y.ctypes.data, s.ctypes.data, q.ctypes.data, r.ctypes.data, pointer, nlbfgs, q.size)
     return q, r
+
+
+def opt_step(l2t, epst):
+    """The reference's parabolic step (src/calc_opt_step.c, src/solvelin.c)."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_opt_step.restype = C.c_float
+    lib.refh_opt_step.argtypes = [C.c_void_p, C.c_void_p]
+    a, e = _f32(l2t), _f32(epst)
+    return np.float32(lib.refh_opt_step(a.ctypes.data, e.ctypes.data))

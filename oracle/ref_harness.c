@@ -1012,3 +1012,14 @@ int refh_lbfgs(int iter, const float *y, const float *s, float *q, float *r, int
     free_vector(rho, 1, nlbfgs); free_vector(alpha, 1, nlbfgs); free_vector(beta, 1, nlbfgs);
     return 0;
 }
+
+/* The reference's parabolic step (src/calc_opt_step.c with src/solvelin.c)
+ * for test misfits L2t[3] at steps epst[3]. */
+float calc_opt_step(float *L2t, float **waveconv, float **gradg, float *epst, int sws, float C_vp);
+float refh_opt_step(const float *l2t, const float *epst)
+{
+    float L[5] = {0}, E[5] = {0};
+    int i;
+    for (i = 0; i < 3; i++) { L[i + 1] = l2t[i]; E[i + 1] = epst[i]; }
+    return calc_opt_step(L, NULL, NULL, E, 1, 0.0f);
+}

@@ -151,3 +151,26 @@ def test_lbfgs_ring_matches_reference(it, pointer, filled):
     assert np.array_equal(got_q, ref_q) and np.array_equal(got_r, ref_r)
     if it > 1:
         assert np.abs(got_r).max() > 0
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference build not present")
+def test_opt_step_ref_matches_reference():
+    """dsh_opt_step_ref against calc_opt_step.c + solvelin.c compiled into the
+    oracle, bit for bit: line-search triples (first step 0), convex and
+    concave fits, clipping to the third step, negative extrema, and a singular
+    system (two equal steps), which is non-finite in both; dsh_opt_step, the
+    double solve the line search uses, agrees to float rounding."""
+    rng = np.random.default_rng(11)
+    for k in range(400):
+        e = np.sort(rng.uniform(0, 1, 3)).astype(np.float32)
+        if k % 2 == 0:
+            e[0] = 0
+        l2 = rng.uniform(0.5, 2.0, 3).astype(np.float32)
+        got, ref = fwi.opt_step_ref(l2, e), O.opt_step(l2, e)
+        assert got == ref or (np.isnan(got) and np.isnan(ref)), (l2, e)
+        dbl = np.float32(fwi.opt_step(l2, e))
+        assert abs(float(dbl) - float(got)) <= 1e-3 * max(1.0, abs(float(got))), (l2, e, dbl, got)
+    e = np.array([0.0, 0.3, 0.3], np.float32)
+    l2 = np.array([1.0, 0.8, 0.9], np.float32)
+    got, ref = fwi.opt_step_ref(l2, e), O.opt_step(l2, e)
+    assert (got == ref) or (np.isnan(got) and np.isnan(ref))
