@@ -7,6 +7,7 @@
 #include <math.h>
 #include <stddef.h>
 #include <stdlib.h>
+#include <string.h>
 
 static double dot(long long n, const float *a, const float *b)
 {
@@ -332,4 +333,52 @@ float dsh_opt_step_ref(const float L2t[3], const float epst[3])
     if (opteps > epst[2]) opteps = epst[2];
     if (opteps < 0.0) opteps = epst[0];
     return opteps;
+}
+
+/* smooth_model.c:25-121 with median.c:12-38 (k successive first minima) */
+static void median_field(int nx, int ny, int hfs, const float *in, float *out, float *win)
+{
+    const int side = 2 * hfs + 1, k = side * side;
+    int i, j, ii, jj, a;
+    for (j = 0; j < ny; j++)
+        for (i = 0; i < nx; i++) {
+            int n = 0;
+            for (jj = -hfs; jj <= hfs; jj++)
+                for (ii = -hfs; ii <= hfs; ii++) {
+                    int y = j + jj, x = i + ii;
+                    y = y < 0 ? 0 : (y >= ny ? ny - 1 : y);
+                    x = x < 0 ? 0 : (x >= nx ? nx - 1 : x);
+                    const float v = in[(size_t)y * nx + x];
+                    /* stable insertion: equal values keep their window order, as
+                       repeated first-minimum selection orders them */
+                    for (a = n; a > 0 && v < win[a - 1]; a--) win[a] = win[a - 1];
+                    win[a] = v;
+                    n++;
+                }
+            out[(size_t)j * nx + i] = win[(k + 1) / 2 - 1];
+        }
+}
+
+int dsh_smooth_model_median(int nx, int ny, int filt_size, const float *vs, const float *rho, float *vs_out,
+                            float *rho_out, int *filt_size_used)
+{
+    int fs = filt_size, hfs;
+    float *win;
+    if (nx < 1 || ny < 1 || !vs || !rho || !vs_out || !rho_out) return -1;
+    if (fs == 0) {
+        memcpy(vs_out, vs, (size_t)nx * ny * sizeof(float));
+        memcpy(rho_out, rho, (size_t)nx * ny * sizeof(float));
+        if (filt_size_used) *filt_size_used = 0;
+        return 0;
+    }
+    if (!(fs % 2)) fs = fs > 0 ? fs + 1 : fs - 1;
+    hfs = abs(fs) / 2;
+    if (hfs > 64) return -1;
+    win = (float *)malloc((size_t)(2 * hfs + 1) * (2 * hfs + 1) * sizeof(float));
+    if (!win) return -3;
+    median_field(nx, ny, hfs, vs, vs_out, win);
+    median_field(nx, ny, hfs, rho, rho_out, win);
+    free(win);
+    if (filt_size_used) *filt_size_used = fs;
+    return 0;
 }

@@ -49,8 +49,24 @@ def _setup():
                                      C.c_longlong]
         L.dsh_opt_step_ref.restype = C.c_float
         L.dsh_opt_step_ref.argtypes = [C.c_void_p, C.c_void_p]
+        L.dsh_smooth_model_median.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                              C.c_void_p, C.POINTER(C.c_int)]
         L._fwi_ready = True
     return L
+
+
+def smooth_model_median(vs, rho, filt_size: int):
+    """Median smoothing of the model (MODEL_FILTER=1, src/smooth_model.c):
+    returns vs, rho and the window side used (an even FILT_SIZE grows by one)."""
+    v = np.ascontiguousarray(vs, np.float32)
+    r = np.ascontiguousarray(rho, np.float32)
+    if v.shape != r.shape or v.ndim != 2:
+        raise ValueError("vs and rho must be [ny, nx] of one shape")
+    vo, ro = np.empty_like(v), np.empty_like(r)
+    used = C.c_int()
+    _check(_setup().dsh_smooth_model_median(v.shape[1], v.shape[0], filt_size, v.ctypes.data, r.ctypes.data,
+                                            vo.ctypes.data, ro.ctypes.data, C.byref(used)), "dsh_smooth_model_median")
+    return vo, ro, used.value
 
 
 def opt_step_ref(L2t, epst):

@@ -37,6 +37,17 @@ int dsh_lbfgs_direction(long long n, int count, const float *S, const float *Y, 
 int dsh_lbfgs_ring(int iter, const float *y, const float *s, float *q, float *r, int pointer, int nlbfgs,
                    long long nvec);
 
+/* Median smoothing of the updated model (MODEL_FILTER=1, src/smooth_model.c,
+ * called at src/denise.c:1948, with the median of src/median.c): each point
+ * of vs and rho [ny][nx] becomes the median of its window of side |FILT_SIZE|
+ * (an even FILT_SIZE grows by one away from 0, as the reference does),
+ * edges replicated; the window values are taken depth offset outer, x offset
+ * inner, and the median is element (k+1)/2 of their ascending order, ties in
+ * that order.  filt_size = 0 copies the fields.  Writes *filt_size_used
+ * (optional): the reference keeps the grown size in FILT_SIZE. */
+int dsh_smooth_model_median(int nx, int ny, int filt_size, const float *vs, const float *rho, float *vs_out,
+                            float *rho_out, int *filt_size_used);
+
 /* Conjugate-gradient direction (src/PCG.c:10-107, called at
  * src/denise.c:1850-1871 on the steepest-descent directions of vs and rho):
  * the vectors hold nclass parameter classes of n values each, class after

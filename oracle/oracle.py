@@ -484,3 +484,19 @@ def opt_step(l2t, epst):
     lib.refh_opt_step.argtypes = [C.c_void_p, C.c_void_p]
     a, e = _f32(l2t), _f32(epst)
     return np.float32(lib.refh_opt_step(a.ctypes.data, e.ctypes.data))
+
+
+def smooth_model(vs, rho, filt_size):
+    """The reference's median model smoothing (src/smooth_model.c with
+    src/median.c, MODEL_FILTER=1): returns vs, rho and FILT_SIZE after it."""
+    import tempfile
+
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_smooth_model.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    v, r = _f32(vs).copy(), _f32(rho).copy()
+    ny, nx = v.shape
+    with tempfile.TemporaryDirectory(dir="/tmp") as d:      # a short path: the reference's names are char[74]
+        fs = lib.refh_smooth_model(d.encode(), nx, ny, filt_size, v.ctypes.data, r.ctypes.data)
+    if fs == -999:
+        raise RuntimeError("refh_smooth_model failed")
+    return v, r, fs

@@ -1023,3 +1023,40 @@ float refh_opt_step(const float *l2t, const float *epst)
     for (i = 0; i < 3; i++) { L[i + 1] = l2t[i]; E[i + 1] = epst[i]; }
     return calc_opt_step(L, NULL, NULL, E, 1, 0.0f);
 }
+
+/* The reference's model smoothing (src/smooth_model.c, MODEL_FILTER=1, with
+ * src/median.c) of dense [ny][nx] vs, rho in place; its model files go to
+ * dir (INV_MODELFILE = dir/inv).  Returns FILT_SIZE after the call. */
+void smooth_model(float **pu, float **prho, int iter);
+extern int MODEL_FILTER, FILT_SIZE;
+int refh_smooth_model(const char *dir, int nx, int ny, int filt_size, float *vs, float *rho)
+{
+    if (strlen(dir) + 4 + 12 >= STRING_SIZE) return -999;
+    const int nx0 = NX, ny0 = NY, nxg0 = NXG, nyg0 = NYG, myid0 = MYID;
+    FILE *fp0 = FP, *quiet = fopen("/dev/null", "w");
+    char path[STRING_SIZE + 16];
+    int i, j, rc;
+    NX = NXG = nx; NY = NYG = ny; POS[1] = POS[2] = 0; NPROCX = NPROCY = 1; MYID = 0;
+    FP = quiet ? quiet : stderr;
+    MODEL_FILTER = 1; FILT_SIZE = filt_size;
+    snprintf(INV_MODELFILE, STRING_SIZE, "%s/inv", dir);
+    float **u = matrix(1, ny, 1, nx), **r = matrix(1, ny, 1, nx);
+    for (j = 1; j <= ny; j++) for (i = 1; i <= nx; i++) { u[j][i] = vs[(j - 1) * nx + i - 1]; r[j][i] = rho[(j - 1) * nx + i - 1]; }
+    /* the model files it reads: x outer, depth inner */
+    snprintf(path, sizeof path, "%s_vs.bin", INV_MODELFILE);
+    FILE *f = fopen(path, "wb");
+    for (i = 1; i <= nx; i++) for (j = 1; j <= ny; j++) fwrite(&u[j][i], sizeof(float), 1, f);
+    fclose(f);
+    snprintf(path, sizeof path, "%s_rho.bin", INV_MODELFILE);
+    f = fopen(path, "wb");
+    for (i = 1; i <= nx; i++) for (j = 1; j <= ny; j++) fwrite(&r[j][i], sizeof(float), 1, f);
+    fclose(f);
+    smooth_model(u, r, 1);
+    for (j = 1; j <= ny; j++) for (i = 1; i <= nx; i++) { vs[(j - 1) * nx + i - 1] = u[j][i]; rho[(j - 1) * nx + i - 1] = r[j][i]; }
+    free_matrix(u, 1, ny, 1, nx); free_matrix(r, 1, ny, 1, nx);
+    rc = FILT_SIZE;
+    MODEL_FILTER = 0;
+    NX = nx0; NY = ny0; NXG = nxg0; NYG = nyg0; MYID = myid0; FP = fp0;
+    if (quiet) fclose(quiet);
+    return rc;
+}

@@ -174,3 +174,25 @@ def test_opt_step_ref_matches_reference():
     l2 = np.array([1.0, 0.8, 0.9], np.float32)
     got, ref = fwi.opt_step_ref(l2, e), O.opt_step(l2, e)
     assert (got == ref) or (np.isnan(got) and np.isnan(ref))
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference build not present")
+@pytest.mark.parametrize("filt_size", [4, 5, 2, 7, 0, -4])
+def test_smooth_model_median_matches_reference(filt_size):
+    """dsh_smooth_model_median against the reference's smooth_model.c with
+    median.c compiled into the oracle (model files in a temporary directory):
+    identical fields and the same grown FILT_SIZE, for even and odd sizes,
+    with ties (a layered model) and edge replication."""
+    rng = np.random.default_rng(abs(filt_size) + 3)
+    ny, nx = 23, 31
+    vs = rng.uniform(100, 400, (ny, nx)).astype(np.float32)
+    vs[5:9, :] = np.float32(250.0)                       # ties inside windows
+    rho = np.round(rng.uniform(1500, 2200, (ny, nx)) / 50).astype(np.float32) * np.float32(50)
+    v, r, used = fwi.smooth_model_median(vs, rho, filt_size)
+    if filt_size == 0:
+        assert used == 0 and np.array_equal(v, vs) and np.array_equal(r, rho)
+        return
+    rv, rr, rfs = O.smooth_model(vs, rho, filt_size)
+    assert used == rfs
+    assert np.array_equal(v, rv) and np.array_equal(r, rr)
+    assert not np.array_equal(v, vs)
