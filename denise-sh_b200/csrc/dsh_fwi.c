@@ -382,3 +382,18 @@ int dsh_smooth_model_median(int nx, int ny, int filt_size, const float *vs, cons
     if (filt_size_used) *filt_size_used = fs;
     return 0;
 }
+
+/* calc_mres.c:12-24 */
+float dsh_calc_mres(int nx, int ny, const float *u, const float *u0)
+{
+    float M2tmp = 0.0f, m20 = 0.0f;
+    int i, j;
+    if (nx < 1 || ny < 1 || !u || !u0) return NAN;
+    for (j = 0; j < ny; j++)
+        for (i = 0; i < nx; i++) {
+            const size_t k = (size_t)j * nx + i;
+            M2tmp += (u[k] - u0[k]) * (u[k] - u0[k]);
+            m20 += u0[k] * u0[k];
+        }
+    return M2tmp / m20;
+}

@@ -51,8 +51,19 @@ def _setup():
         L.dsh_opt_step_ref.argtypes = [C.c_void_p, C.c_void_p]
         L.dsh_smooth_model_median.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                               C.c_void_p, C.POINTER(C.c_int)]
+        L.dsh_calc_mres.restype = C.c_float
+        L.dsh_calc_mres.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L._fwi_ready = True
     return L
+
+
+def calc_mres(u, u0):
+    """Relative model change sum (u-u0)^2 / sum u0^2 (src/calc_mres.c)."""
+    a = np.ascontiguousarray(u, np.float32)
+    b = np.ascontiguousarray(u0, np.float32)
+    if a.shape != b.shape or a.ndim != 2:
+        raise ValueError("u and u0 must be [ny, nx] of one shape")
+    return np.float32(_setup().dsh_calc_mres(a.shape[1], a.shape[0], a.ctypes.data, b.ctypes.data))
 
 
 def smooth_model_median(vs, rho, filt_size: int):

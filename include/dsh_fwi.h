@@ -118,6 +118,11 @@ float dsh_model_update(int nx, int ny, const float *vs, const float *rho, const 
                        float eps_scale, float scalerho, int iter, int inv_vs_iter, int inv_rho_iter,
                        const float limits[4], float *vs_new, float *rho_new, float *eps_rho);
 double dsh_calc_energy(const float *obs, int ntr, int ns, float dt, float energy_in);
+/* Relative model change sum (u - u0)^2 / sum u0^2 over dense [ny][nx]
+ * fields, float sums in the reference's order (src/calc_mres.c:7-25; the FWI
+ * loop reports it for vs and rho against the starting model,
+ * src/denise.c:1733-1738). */
+float dsh_calc_mres(int nx, int ny, const float *u, const float *u0);
 
 #ifdef __cplusplus
 }

@@ -500,3 +500,12 @@ def smooth_model(vs, rho, filt_size):
     if fs == -999:
         raise RuntimeError("refh_smooth_model failed")
     return v, r, fs
+
+
+def calc_mres(u, u0):
+    """The reference's relative model change (src/calc_mres.c)."""
+    lib = C.CDLL(os.path.join(REF_DIR, "libdenise_ref.so"))
+    lib.refh_calc_mres.restype = C.c_float
+    lib.refh_calc_mres.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+    a, b = _f32(u), _f32(u0)
+    return np.float32(lib.refh_calc_mres(a.shape[1], a.shape[0], a.ctypes.data, b.ctypes.data))

@@ -1060,3 +1060,13 @@ int refh_smooth_model(const char *dir, int nx, int ny, int filt_size, float *vs,
     if (quiet) fclose(quiet);
     return rc;
 }
+
+/* The reference's relative model change (src/calc_mres.c) of dense fields. */
+float calc_mres(int nx1, int nx2, int ny1, int ny2, float **u, float **u0);
+float refh_calc_mres(int nx, int ny, const float *u, const float *u0)
+{
+    float **a = field_in(u, nx, ny), **b = field_in(u0, nx, ny);
+    const float m = calc_mres(1, nx, 1, ny, a, b);
+    free_matrix(a, 1, ny, 1, nx); free_matrix(b, 1, ny, 1, nx);
+    return m;
+}

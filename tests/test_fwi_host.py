@@ -196,3 +196,14 @@ def test_smooth_model_median_matches_reference(filt_size):
     assert used == rfs
     assert np.array_equal(v, rv) and np.array_equal(r, rr)
     assert not np.array_equal(v, vs)
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference build not present")
+def test_calc_mres_matches_reference():
+    """dsh_calc_mres against src/calc_mres.c compiled into the oracle, bit for bit."""
+    rng = np.random.default_rng(5)
+    for ny, nx in [(1, 1), (17, 29), (200, 120)]:
+        u0 = rng.uniform(100, 500, (ny, nx)).astype(np.float32)
+        u = (u0 * rng.uniform(0.9, 1.1, (ny, nx))).astype(np.float32)
+        assert fwi.calc_mres(u, u0) == O.calc_mres(u, u0)
+    assert fwi.calc_mres(u0, u0) == 0.0
