@@ -396,6 +396,7 @@ static int check_params(const dsh_params *p)
     if (p->eprecond != 0 && p->eprecond != 1 && p->eprecond != 3 && p->eprecond != DSH_EPRECOND_ENERGY_ONLY)
         return DSH_ERR_PARAM;
     if (p->max_shots < 1 || p->max_shots > 65535) return DSH_ERR_PARAM;
+    if (p->ckpt_every < 0) return DSH_ERR_PARAM;
     if (p->nx > 65000 || p->ny > 65000) return DSH_ERR_PARAM;
     if (p->quellart != 1 && p->quellart != 2 && p->quellart != 3 && p->quellart != 4 && p->quellart != 5 &&
         p->quellart != 6)
@@ -1330,13 +1331,15 @@ int check_status(dsh_ctx *ctx)
  * step and shot) when it fits the budget (mem_budget, or the free device
  * memory less a 2 GiB reserve when mem_budget is 0); otherwise checkpoints
  * every C steps, C = sqrt(NT*(3+2L)/3) (minimises checkpoints + C-step buffer),
- * with one recomputed forward pass. */
+ * with one recomputed forward pass.  ckpt_every > 0 asks for checkpoints every
+ * ckpt_every steps whatever the budget. */
 static int ensure_storage(dsh_ctx *ctx)
 {
     const dsh_params &p = ctx->p;
     const size_t S = ctx->S, D = ctx->dstride, st = ctx->o_state_end;
     const size_t full = S * (size_t)p.nt * 3 * D * sizeof(float);
-    int C = (int)std::lround(std::sqrt((double)p.nt * (3.0 + 2.0 * p.l) / 3.0));
+    int C = p.ckpt_every > 0 ? p.ckpt_every
+                             : (int)std::lround(std::sqrt((double)p.nt * (3.0 + 2.0 * p.l) / 3.0));
     C = std::max(1, std::min(C, p.nt));
     const int nck = (p.nt + C - 1) / C - 1;
     const size_t ckpt_need = S * (size_t)C * 3 * D * sizeof(float) + (size_t)nck * S * st * sizeof(float) +
@@ -1354,7 +1357,7 @@ static int ensure_storage(dsh_ctx *ctx)
         budget = (long long)fr - (2LL << 30);
     }
     ctx->fwd_step_stride = 3 * D;
-    if ((long long)full <= budget) {
+    if (p.ckpt_every <= 0 && (long long)full <= budget) {
         if (cudaMalloc(&ctx->fwd, full) != cudaSuccess) { cudaGetLastError(); return DSH_ERR_OOM; }
         ctx->fwd_bytes = full;
         ctx->fwd_mod = p.nt;

@@ -17,6 +17,7 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
 #include <cstdio>
 #include <mutex>
 
@@ -30,16 +31,26 @@ constexpr int NA_MAX_DEVICES = 64;
  * DSH_NOALLOC_MAX_SHOTS shots (296 * 64 * 8 B = 151,552 B per device) */
 static __device__ __align__(256) double g_partials[DSH_NOALLOC_MAX_SHOTS * NA_BLOCKS];
 
-/* host-side device addresses of g_partials, looked up once per device */
+/* host-side device addresses of g_partials per device.  The address is
+ * looked up again on every call whose stream is not capturing (cheap once
+ * the module is loaded), so a device reset between calls, which unloads the
+ * module, cannot leave a stale address behind; a capturing call uses the
+ * address an earlier call on that device found. */
 std::mutex g_mu;
 double *g_partials_dev[NA_MAX_DEVICES] = {};
 
-int partials_address(double **out)
+int partials_address(cudaStream_t st, double **out)
 {
     int dev = -1;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NA_MAX_DEVICES) return DSH_ERR_CUDA;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) return DSH_ERR_CUDA;
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_partials_dev[dev]) {
+    if (cs != cudaStreamCaptureStatusNone && !g_partials_dev[dev]) {
+        fprintf(stderr, "dsh_residual_noalloc: the first call on device %d must come before any stream capture\n", dev);
+        return DSH_ERR_STATE;
+    }
+    if (cs == cudaStreamCaptureStatusNone) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_partials);
         if (e != cudaSuccess || !p) {
@@ -99,6 +110,13 @@ __global__ void reduce_static_kernel(const double *part, int nparts, double *l2)
     if (threadIdx.x == 0) l2[s] = sh[0];
 }
 
+/* whether the float ranges [a, a+n) and [b, b+n) share any element */
+bool overlap(const float *a, const float *b, long long n)
+{
+    const uintptr_t x = (uintptr_t)a, y = (uintptr_t)b, len = (uintptr_t)n * sizeof(float);
+    return x < y + len && y < x + len;
+}
+
 }  // namespace
 
 extern "C" int dsh_residual_noalloc(int nshots, int ntr, int nt, const float *syn, const float *obs, float *res,
@@ -110,15 +128,33 @@ extern "C" int dsh_residual_noalloc(int nshots, int ntr, int nt, const float *sy
                 nshots, DSH_NOALLOC_MAX_SHOTS);
         return DSH_ERR_PARAM;
     }
-    double *part = nullptr;
-    int rc = partials_address(&part);
-    if (rc != DSH_OK) return rc;
-    cudaStream_t st = (cudaStream_t)stream;
-    residual_static_kernel<<<dim3(NA_BLOCKS, nshots), NA_THREADS, 0, st>>>(nt, ntr, syn, obs, res, part);
-    reduce_static_kernel<<<nshots, NA_THREADS, 0, st>>>(part, NA_BLOCKS, l2);
+    /* each thread writes res[r][t-1] from syn/obs sample nt-t, which another
+       thread may be writing: the residual cannot be formed in place */
+    const long long total = (long long)nshots * ntr * nt;
+    if (overlap(res, syn, total) || overlap(res, obs, total)) {
+        fprintf(stderr, "dsh_residual_noalloc: res must not overlap syn or obs\n");
+        return DSH_ERR_PARAM;
+    }
+    /* an error left by earlier, unrelated work on this device is reported as
+       such, not as a failure of these launches */
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
-        fprintf(stderr, "dsh_residual_noalloc: launch failed (%s)\n", cudaGetErrorString(e));
+        fprintf(stderr, "dsh_residual_noalloc: a CUDA error from earlier work was pending (%s); nothing launched\n",
+                cudaGetErrorString(e));
+        return DSH_ERR_CUDA;
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    double *part = nullptr;
+    int rc = partials_address(st, &part);
+    if (rc != DSH_OK) return rc;
+    residual_static_kernel<<<dim3(NA_BLOCKS, nshots), NA_THREADS, 0, st>>>(nt, ntr, syn, obs, res, part);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        fprintf(stderr, "dsh_residual_noalloc: residual launch failed (%s)\n", cudaGetErrorString(e));
+        return DSH_ERR_CUDA;
+    }
+    reduce_static_kernel<<<nshots, NA_THREADS, 0, st>>>(part, NA_BLOCKS, l2);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        fprintf(stderr, "dsh_residual_noalloc: reduction launch failed (%s)\n", cudaGetErrorString(e));
         return DSH_ERR_CUDA;
     }
     return DSH_OK;

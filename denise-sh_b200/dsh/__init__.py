@@ -40,7 +40,8 @@ class Params(C.Structure):
                 ("fdorder", C.c_int), ("maxrelerror", C.c_int), ("fw", C.c_int), ("free_surf", C.c_int),
                 ("damping", C.c_float), ("fpml", C.c_float), ("npower", C.c_float), ("k_max_pml", C.c_float),
                 ("l", C.c_int), ("fl", C.c_float * 8), ("quellart", C.c_int), ("eprecond", C.c_int),
-                ("max_shots", C.c_int), ("compat_fd12", C.c_int), ("mem_budget", C.c_longlong)]
+                ("max_shots", C.c_int), ("compat_fd12", C.c_int), ("mem_budget", C.c_longlong),
+                ("ckpt_every", C.c_int)]
 
 
 class ShotC(C.Structure):

@@ -69,6 +69,9 @@ typedef struct dsh_params {
                                  when it fits, else checkpoints every
                                  C = sqrt(NT*(3+2L)/3) steps and one recomputed
                                  forward pass (DSH_ERR_OOM if even that does not fit) */
+    int ckpt_every;           /* > 0: always checkpoint-and-recompute, one checkpoint every
+                                 ckpt_every steps (e.g. ceil(sqrt(NT))), whatever the budget;
+                                 0 = the automatic choice above */
 } dsh_params;
 
 /* One shot (one source gather). */
@@ -180,7 +183,9 @@ int dsh_profile_fused(dsh_ctx *ctx, int pass, int nsteps, float *out_ms);
  * address (cudaGetSymbolAddress), so make the first call on each device before
  * any stream capture.  All calls on a device share the array and it keeps the
  * last call's contents; calls that overlap on the GPU race on it and must be
- * serialised by the caller. */
+ * serialised by the caller.  res must not overlap syn or obs (an in-place
+ * residual is rejected with DSH_ERR_PARAM); a CUDA error left pending by
+ * earlier work on the device is returned as DSH_ERR_CUDA before any launch. */
 #define DSH_NOALLOC_MAX_SHOTS 64
 int dsh_residual_noalloc(int nshots, int ntr, int nt, const float *syn, const float *obs, float *res, double *l2,
                          void *stream);

@@ -69,6 +69,40 @@ void refh_set_impl(void *v, void *s_el, void *s_visc, void *ep, void *ep1)
     impl_ep = (fn_ep_t)ep;
     impl_ep1 = (fn_ep1_t)ep1;
 }
+/* The same for the bookkeeping functions of the loops (seismo_ssg,
+ * hess_save, hessian, zero_fdveps, zero_fdveps_visc) and psource. */
+typedef void (*fn_seis_t)(int, int, int **, float **, float **, float **, float **, float *);
+typedef void (*fn_hsave_t)(int, float **, float **, float **, float ***, float ***, float ***);
+typedef void (*fn_hess_t)(int, float ***, float ***, float ***, float **, float **);
+typedef void (*fn_zero_t)(int, int, int, int, float **, float **, float **, float **, float **, float **, float **,
+                          float **, float **);
+typedef void (*fn_zerov_t)(int, int, int, int, float **, float **, float **, float **, float **, float **, float **,
+                           float **, float **, float ***, float ***, float ***);
+typedef void (*fn_psrc_t)(int, float **, float **, float **, float **, int);
+void psource(int nt, float **sxx, float **syy, float **srcpos_loc, float **signals, int nsrc);   /* src/psource.c:9; fd.h has no prototype */
+static fn_seis_t impl_seis = NULL;
+static fn_hsave_t impl_hsave = NULL;
+static fn_hess_t impl_hess = NULL;
+static fn_zero_t impl_zero = NULL;
+static fn_zerov_t impl_zerov = NULL;
+static fn_psrc_t impl_psrc = NULL;
+
+void refh_set_impl_aux(void *seis, void *hsave, void *hess, void *zero, void *zerov, void *psrc)
+{
+    impl_seis = (fn_seis_t)seis;
+    impl_hsave = (fn_hsave_t)hsave;
+    impl_hess = (fn_hess_t)hess;
+    impl_zero = (fn_zero_t)zero;
+    impl_zerov = (fn_zerov_t)zerov;
+    impl_psrc = (fn_psrc_t)psrc;
+}
+#define CALL_SEIS (impl_seis ? impl_seis : seismo_ssg)
+#define CALL_HSAVE (impl_hsave ? impl_hsave : hess_save)
+#define CALL_HESS (impl_hess ? impl_hess : hessian)
+#define CALL_ZERO (impl_zero ? impl_zero : zero_fdveps)
+#define CALL_ZEROV (impl_zerov ? impl_zerov : zero_fdveps_visc)
+#define CALL_PSRC (impl_psrc ? impl_psrc : psource)
+
 #define CALL_V (impl_v ? impl_v : update_v_PML)
 #define CALL_SE (impl_se ? impl_se : update_s_elastic_PML)
 #define CALL_SV (impl_sv ? impl_sv : update_s_visc_PML)
@@ -386,9 +420,9 @@ int refh_wavelet(int nsrc, const float *srcpos8, float *out)
 
 static void zero_state(void)
 {
-    if (L) zero_fdveps_visc(-nd + 1, NY + nd, -nd + 1, NX + nd, pvy, psyz, psxy, uy, pvyp1,
+    if (L) CALL_ZEROV(-nd + 1, NY + nd, -nd + 1, NX + nd, pvy, psyz, psxy, uy, pvyp1,
                             psi_sxy_x, psi_vyx, psi_syz_y, psi_vyy, pr, pp, pq);
-    else zero_fdveps(-nd + 1, NY + nd, -nd + 1, NX + nd, pvy, psyz, psxy, uy, pvyp1,
+    else CALL_ZERO(-nd + 1, NY + nd, -nd + 1, NX + nd, pvy, psyz, psxy, uy, pvyp1,
                      psi_sxy_x, psi_vyx, psi_syz_y, psi_vyy);
 }
 
@@ -465,20 +499,20 @@ int refh_forward(int nsrc, const float *srcpos8, const float *signals_in, int nt
                      hc, 0, 0, K_x, a_x, b_x, K_x_half, a_x_half, b_x_half, K_y, a_y, b_y, K_y_half, a_y_half,
                      b_y_half, psi_syz_y, psi_sxy_x);
         step_stress();
-        if (ntr > 0) seismo_ssg(nt, ntr, recpos_loc, sectionvy, pvy, psyz, pu, hc);
+        if (ntr > 0) CALL_SEIS(nt, ntr, recpos_loc, sectionvy, pvy, psyz, pu, hc);
         if (nt == hin1) {
             if (store) {                                  /* denise.c:1261-1301 */
                 for (i = 1; i <= NX; i++) for (j = 1; j <= NY; j++) fwd_rho_y[imat1++] = pvyp1[j][i];
                 for (i = 1; i <= NX; i++) for (j = 1; j <= NY; j++) fwd_y[imat++] = uy[j][i];
                 for (i = 1; i <= NX; i++) for (j = 1; j <= NY; j++) fwd_u[imat2++] = uyx[j][i];
             }
-            if (hessian_on) hess_save(hin, uy, uyx, pvyp1, hess_eyy, hess_eyx, hess_utty);
+            if (hessian_on) CALL_HSAVE(hin, uy, uyx, pvyp1, hess_eyy, hess_eyx, hess_utty);
             if ((EPRECOND == 1) || (EPRECOND == 3)) CALL_EP(Ws, pvy);
             hin++;
             hin1 = hin1 + DTINV;
         }
     }
-    if (hessian_on) hessian(nsteps, hess_eyy, hess_eyx, hess_utty, hessian_u, hessian_rho);
+    if (hessian_on) CALL_HESS(nsteps, hess_eyy, hess_eyx, hess_utty, hessian_u, hessian_rho);
     for (k = 1; k <= ntr; k++) for (nt = 1; nt <= NT; nt++) seis[(k - 1) * NT + nt - 1] = sectionvy[k][nt];
     free_matrix(signals, 1, nsrc, 1, NT);
     free_matrix(sp, 1, 8, 1, nsrc);
@@ -617,7 +651,7 @@ int refh_psource(int nt, float *sxx, float *syy, int nsrc, const float *srcpos8,
     for (j = 1; j <= NY; j++) for (i = 1; i <= NX; i++) { a[j][i] = sxx[(j - 1) * NX + i - 1]; b[j][i] = syy[(j - 1) * NX + i - 1]; }
     for (r = 1; r <= 8; r++) for (k = 1; k <= nsrc; k++) sp[r][k] = srcpos8[(r - 1) * nsrc + (k - 1)];
     for (k = 1; k <= nsrc; k++) for (n = 1; n <= NT; n++) sig[k][n] = signals_in[(k - 1) * NT + n - 1];
-    psource(nt, a, b, sp, sig, nsrc);
+    CALL_PSRC(nt, a, b, sp, sig, nsrc);
     for (j = 1; j <= NY; j++) for (i = 1; i <= NX; i++) { sxx[(j - 1) * NX + i - 1] = a[j][i]; syy[(j - 1) * NX + i - 1] = b[j][i]; }
     free_matrix(a, -nd + 1, NY + nd, -nd + 1, NX + nd); free_matrix(b, -nd + 1, NY + nd, -nd + 1, NX + nd);
     free_matrix(sp, 1, 8, 1, nsrc); free_matrix(sig, 1, nsrc, 1, NT);

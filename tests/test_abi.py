@@ -44,15 +44,16 @@ def test_every_declared_symbol_is_exported(header):
 
 def test_struct_layout():
     # dsh_params / dsh_shot / dsh_stats as the header lays them out on x86-64
-    assert C.sizeof(dsh.Params) == 112
+    assert C.sizeof(dsh.Params) == 120
     assert dsh.Params.mem_budget.offset == 104
+    assert dsh.Params.ckpt_every.offset == 112
     assert C.sizeof(dsh.ShotC) == 40
     assert C.sizeof(dsh.Stats) == 56
 
 
 @pytest.mark.parametrize("bad", [dict(fdorder=5), dict(fdorder=14), dict(maxrelerror=5), dict(l=5), dict(nx=0),
                                  dict(fw=-1), dict(fw=400), dict(dt=0.0), dict(eprecond=2), dict(max_shots=0),
-                                 dict(quellart=7), dict(l=2, fl=(10.0,))])
+                                 dict(quellart=7), dict(l=2, fl=(10.0,)), dict(ckpt_every=-1)])
 def test_invalid_params_rejected_before_device_use(bad):
     kw = dict(nx=64, ny=32, nt=10, dh=0.5, dt=1e-4, l=0)
     kw.update(bad)

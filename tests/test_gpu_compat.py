@@ -113,3 +113,30 @@ def test_compat_abort_mode_exits_like_the_reference():
     out = subprocess.run([sys.executable, "-c", code], cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 1, out.stdout[-2000:] + out.stderr[-2000:]
     assert "R U N - T I M E  E R R O R" in out.stdout and "Simulation is unstable" in out.stdout
+
+
+@pytest.mark.skipif(not O.available("ref"), reason="reference not compiled here")
+@pytest.mark.parametrize("name", ["elastic_fd4_fs", "visc_fd8_L2", "visc_fd6_L3_pml", "visc_fd10_L1"])
+def test_every_layer1_function_swapped_at_once(name):
+    """All of the layer's functions in the reference's loops at the same time
+    (velocity, stress, eprecond, eprecond1 on the GPU; seismo_ssg, hess_save,
+    hessian, zero_fdveps(_visc) on the host), including a forward pass with the
+    Hessian: bit-identical to the reference's own functions."""
+    from test_compat_host import _shot_loops, _swap
+
+    ref, comp = _libs()
+    d = golden(name)
+    ref.refh_set_impl(None, None, None, None, None)
+    _swap(ref, comp, False)
+    base = _shot_loops(d)
+    _use_compat(ref, comp)
+    _swap(ref, comp, True)
+    try:
+        gpu = _shot_loops(d)
+        assert comp.dsh_compat_status() == 0
+    finally:
+        ref.refh_set_impl(None, None, None, None, None)
+        _swap(ref, comp, False)
+    for k in base:
+        assert np.array_equal(gpu[k], base[k]), k
+    assert np.array_equal(gpu["hess_vs"], d["hess_vs"]) and np.array_equal(gpu["hess_rho"], d["hess_rho"])
