@@ -62,6 +62,8 @@ struct dsh_batch {
     double total_ms = 0;
     long long launches = 0, points = 0;
     int last_cuda = 0;
+    cudaEvent_t ev_wait = nullptr;         /* recorded by the bounded host waits */
+    double host_timeout_s = dsh::eng::HOST_TIMEOUT_DEFAULT_S;
 };
 
 static int bfail(dsh_batch *b, cudaError_t e)
@@ -74,6 +76,23 @@ static int bfail(dsh_batch *b, cudaError_t e)
     do {                                               \
         cudaError_t e_ = (x);                          \
         if (e_ != cudaSuccess) return bfail(b, e_);    \
+    } while (0)
+
+/* bounded host wait for the batch's stream (DSH_ERR_TIMEOUT after host_timeout_s) */
+static int bwait(dsh_batch *b)
+{
+    BK(cudaEventRecord(b->ev_wait, b->st));
+    const int rc = dsh::eng::wait_event(b->ev_wait, b->host_timeout_s);
+    if (rc == DSH_ERR_CUDA) return bfail(b, cudaGetLastError());
+    if (rc == DSH_ERR_TIMEOUT)
+        fprintf(stderr, "dsh batch: the device did not finish within %.3g s; the call returns DSH_ERR_TIMEOUT\n",
+                b->host_timeout_s);
+    return rc;
+}
+#define BWAIT(b)                                       \
+    do {                                               \
+        const int w_ = bwait(b);                       \
+        if (w_ != DSH_OK) return w_;                   \
     } while (0)
 
 static void drop_batch_graphs(dsh_batch *b)
@@ -98,6 +117,7 @@ extern "C" dsh_batch *dsh_batch_create(const dsh_params *p, int nmodels, int dev
     b->p.assign(p, p + nmodels);
     if (cudaSetDevice(device) != cudaSuccess) return fail(DSH_ERR_CUDA, b);
     if (cudaStreamCreateWithFlags(&b->own_st, cudaStreamNonBlocking) != cudaSuccess) return fail(DSH_ERR_CUDA, b);
+    if (cudaEventCreateWithFlags(&b->ev_wait, cudaEventDisableTiming) != cudaSuccess) return fail(DSH_ERR_CUDA, b);
     b->st = b->own_st;
     for (int k = 0; k < nmodels; k++) {
         int rc = DSH_OK;
@@ -127,11 +147,12 @@ extern "C" int dsh_batch_destroy(dsh_batch *b)
 {
     if (!b) return DSH_OK;
     cudaSetDevice(b->dev);
-    if (b->st) cudaStreamSynchronize(b->st);
+    if (b->st && b->ev_wait) bwait(b);
     drop_batch_graphs(b);
     for (dsh_ctx *c : b->ctx) dsh_destroy(c);
     cudaFree(b->d_nt); cudaFree(b->d_args); cudaFree(b->d_map);
     for (auto &e : b->ev) if (e) cudaEventDestroy(e);
+    if (b->ev_wait) cudaEventDestroy(b->ev_wait);
     if (b->own_st) cudaStreamDestroy(b->own_st);
     delete b;
     return DSH_OK;
@@ -146,10 +167,18 @@ extern "C" int dsh_batch_set_model(dsh_batch *b, int model, const float *vs, con
 extern "C" int dsh_batch_set_stream(dsh_batch *b, void *stream)
 {
     if (!b) return DSH_ERR_PARAM;
-    if (b->st) cudaStreamSynchronize(b->st);
+    if (b->st) BWAIT(b);
     b->st = stream ? (cudaStream_t)stream : b->own_st;
     for (dsh_ctx *c : b->ctx) dsh_set_stream(c, b->st);
     drop_batch_graphs(b);
+    return DSH_OK;
+}
+
+extern "C" int dsh_batch_set_host_timeout(dsh_batch *b, double host_seconds)
+{
+    if (!b) return DSH_ERR_PARAM;
+    b->host_timeout_s = host_seconds > 0 ? host_seconds : dsh::eng::HOST_TIMEOUT_DEFAULT_S;
+    for (dsh_ctx *c : b->ctx) dsh_set_wait_limits(c, c->device_polls, b->host_timeout_s);
     return DSH_OK;
 }
 
@@ -201,7 +230,7 @@ static int build_maps(dsh_batch *b)
         if (!maps[v].empty())
             BK(cudaMemcpyAsync(b->d_map + (size_t)v * b->map_cap, maps[v].data(), maps[v].size() * sizeof(int4),
                                cudaMemcpyHostToDevice, b->st));
-    BK(cudaStreamSynchronize(b->st));
+    BWAIT(b);
     drop_batch_graphs(b);
     b->sig = sig;
     b->var_v = b->var_s = -1;
@@ -218,7 +247,7 @@ static int upload_args(dsh_batch *b)
         a[k].nslots = b->nb[k];
     }
     BK(cudaMemcpyAsync(b->d_args, a.data(), a.size() * sizeof(StepArgs), cudaMemcpyHostToDevice, b->st));
-    BK(cudaStreamSynchronize(b->st));
+    BWAIT(b);
     return DSH_OK;
 }
 
@@ -339,7 +368,7 @@ static int tune(dsh_batch *b)
                 fn<<<nblk, dim3(BX, MULTI_ROWS[v], MULTI_SPB[v]), 0, b->st>>>(b->d_args, map, 0);
             }
             BK(cudaEventRecord(e1, b->st));
-            BK(cudaEventSynchronize(e1));
+            BWAIT(b);
             BK(cudaGetLastError());
             float ms = 0;
             cudaEventElapsedTime(&ms, e0, e1);
@@ -396,7 +425,7 @@ static int batch_forward(dsh_batch *b, const dsh_shot *shots, const int *nshots,
         b->launches += 1;
         b->points += (long long)b->p[k].nx * b->p[k].ny * b->p[k].nt * nshots[k];
     }
-    BK(cudaStreamSynchronize(b->st));
+    BWAIT(b);
     for (int k = 0; k < b->n; k++) {
         const size_t ph = std::lower_bound(b->phase_nt.begin(), b->phase_nt.end(), b->p[k].nt) - b->phase_nt.begin();
         float ms = 0;

@@ -353,6 +353,33 @@ static int fail_cuda(dsh_ctx *c, cudaError_t e)
         if (e_ != cudaSuccess) return fail_cuda(ctx, e_);  \
     } while (0)
 
+namespace dsh::eng {
+int wait_stream(dsh_ctx *ctx)
+{
+    CK(cudaEventRecord(ctx->ev_wait, ctx->st));
+    const int rc = wait_event(ctx->ev_wait, ctx->host_timeout_s);
+    if (rc == DSH_ERR_TIMEOUT)
+        fprintf(stderr, "dsh: the device did not finish within %.3g s; the call returns DSH_ERR_TIMEOUT\n",
+                ctx->host_timeout_s);
+    if (rc == DSH_ERR_CUDA) return fail_cuda(ctx, cudaGetLastError());
+    return rc;
+}
+}  // namespace dsh::eng
+
+/* bounded host waits (no cudaStreamSynchronize / cudaEventSynchronize): for
+ * the context's stream, and for an event already recorded on it */
+#define WAIT(c)                                            \
+    do {                                                   \
+        const int w_ = wait_stream(c);                     \
+        if (w_ != DSH_OK) return w_;                       \
+    } while (0)
+#define WAIT_EV(c, ev)                                     \
+    do {                                                   \
+        const int w_ = wait_event((ev), (c)->host_timeout_s); \
+        if (w_ == DSH_ERR_CUDA) return fail_cuda((c), cudaGetLastError()); \
+        if (w_ != DSH_OK) return w_;                       \
+    } while (0)
+
 extern "C" void dsh_params_default(dsh_params *p)
 {
     memset(p, 0, sizeof(*p));
@@ -416,6 +443,7 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     if (cudaStreamCreateWithFlags(&ctx->own_st, cudaStreamNonBlocking) != cudaSuccess) return bail(DSH_ERR_CUDA);
     ctx->st = ctx->own_st;
     for (int k = 0; k < 4; k++) cudaEventCreate(&ctx->ev[k]);
+    if (cudaEventCreateWithFlags(&ctx->ev_wait, cudaEventDisableTiming) != cudaSuccess) return bail(DSH_ERR_CUDA);
     const int nx = p->nx, ny = p->ny, L = p->l, fw = p->fw;
     ctx->H = p->fdorder / 2;
     ctx->hy = ctx->H;
@@ -496,7 +524,7 @@ extern "C" int dsh_destroy(dsh_ctx *ctx)
 {
     if (!ctx) return DSH_OK;
     cudaSetDevice(ctx->dev);
-    if (ctx->st) cudaStreamSynchronize(ctx->st);
+    if (ctx->st && ctx->ev_wait) wait_stream(ctx);     /* bounded: the device waits are bounded too */
     drop_graphs(ctx);
     cudaFree(ctx->slab); cudaFree(ctx->model); cudaFree(ctx->pml); cudaFree(ctx->sums); cudaFree(ctx->fwd);
     cudaFree(ctx->ckpt); cudaFree(ctx->shadow);
@@ -505,6 +533,7 @@ extern "C" int dsh_destroy(dsh_ctx *ctx)
     cudaFree(ctx->d_wemax);
     cudaFree(ctx->d_taper_box); cudaFree(ctx->d_taper_shot); cudaFree(ctx->d_tmap);
     for (int k = 0; k < 4; k++) if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
+    if (ctx->ev_wait) cudaEventDestroy(ctx->ev_wait);
     if (ctx->own_st) cudaStreamDestroy(ctx->own_st);
     delete ctx;
     return DSH_OK;
@@ -621,7 +650,7 @@ extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, co
         if ((rc = upload_field(ctx, ctx->m_tip, tip.data())) != DSH_OK) return rc;
         if ((rc = upload_field(ctx, ctx->m_taus, taus.data())) != DSH_OK) return rc;
     }
-    CK(cudaStreamSynchronize(ctx->st));   /* host staging vectors go out of scope */
+    WAIT(ctx);   /* host staging vectors go out of scope */
     ctx->model_set = 1;
     return DSH_OK;
 }
@@ -812,7 +841,7 @@ int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_h
     put(F + 4 * cp, gpk); put(F + 5 * cp, rpk); put(F + 6 * cp, rid);
     put(3 * (S + 1) + 3 * S * (T + 1), fvoff); put(F + 7 * cp, fvids);
     CK(cudaMemcpyAsync(ctx->d_geo, host.data(), (size_t)ctx->geo_cap * sizeof(int), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    WAIT(ctx);
 
     /* signals */
     if (nsig > ctx->cap_sig) {
@@ -832,7 +861,7 @@ int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_h
                 return DSH_ERR_PARAM;
         }
         CK(cudaMemcpyAsync(ctx->d_sig, sig.data(), (size_t)nsig * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
+        WAIT(ctx);
     }
     /* seismograms, residuals, observed data, transposed output */
     const long long nseis_cap = std::max(nseis, 1LL);
@@ -859,7 +888,7 @@ int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_h
     memcpy(&offs[2 * ctx->S], obs_off.data(), ctx->S * sizeof(long long));
     memcpy(&offs[3 * ctx->S], out_off.data(), ctx->S * sizeof(long long));
     CK(cudaMemcpyAsync(ctx->d_offs, offs.data(), offs.size() * sizeof(long long), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    WAIT(ctx);
     if (realloc) { drop_graphs(ctx); ctx->geo_version++; }
     return DSH_OK;
 }
@@ -922,6 +951,7 @@ StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.fwd_mod = ctx->fwd_mod > 0 ? ctx->fwd_mod : p.nt;
     a.fwd_step_stride = ctx->fwd_step_stride;
     a.status = ctx->d_status;
+    a.wait_polls = ctx->device_polls;
     if (ctx->tma_ok) {
         const CUtensorMap *tm = (const CUtensorMap *)ctx->d_tmap + (pass == P_RECOMP ? 2 : 0);
         a.tm_sxy = tm;
@@ -1316,11 +1346,12 @@ namespace dsh::eng {
 int check_status(dsh_ctx *ctx)
 {
     int h = 0;
+    WAIT(ctx);
     CK(cudaMemcpyAsync(&h, ctx->d_status, sizeof(int), cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    WAIT(ctx);
     if (h) {
         cudaMemsetAsync(ctx->d_status, 0, sizeof(int), ctx->st);
-        cudaStreamSynchronize(ctx->st);
+        WAIT(ctx);
         return (h & 2) ? DSH_ERR_TIMEOUT : DSH_ERR_UNSTABLE;   /* bit 2: a bounded grid barrier expired */
     }
     return DSH_OK;
@@ -1399,7 +1430,10 @@ int copy_seis_out(dsh_ctx *ctx, int nb, float *host_out, float *dev_out)
                                                              dst, ctx->d_offs + 3 * ctx->S);
     ctx->launches++;
     CK(cudaGetLastError());
-    if (host_out) CK(cudaMemcpyAsync(host_out, ctx->d_tmp, (size_t)tot * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    if (host_out) {
+        WAIT(ctx);     /* a copy to pageable host memory would wait for the stream without a limit */
+        CK(cudaMemcpyAsync(host_out, ctx->d_tmp, (size_t)tot * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
+    }
     return DSH_OK;
 }
 }  // namespace dsh::eng
@@ -1430,10 +1464,10 @@ static int forward_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *
         if ((rc = copy_seis_out(ctx, nb, seis_host ? seis_host + out : nullptr, seis_dev ? seis_dev + out : nullptr)) != DSH_OK)
             return rc;
         out += batch_seis_len(ctx, shots + b0, nb);
-        CK(cudaStreamSynchronize(ctx->st));
+        WAIT(ctx);
     }
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    CK(cudaEventSynchronize(ctx->ev[1]));
+    WAIT_EV(ctx, ctx->ev[1]);
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     ctx->stats.ms_forward = ms; ctx->stats.ms_adjoint = 0; ctx->stats.ms_total = ms;
@@ -1511,6 +1545,7 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
         if ((rc = adjoint_for_gradient(ctx, nb)) != DSH_OK) return rc;
         cudaEventRecord(e2, ctx->st);
         if (ws_host || wr_host) {
+            WAIT(ctx);
             for (int s = 0; s < nb; s++) {
                 if (ws_host) {
                     gather_dense_kernel<<<256, 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch,
@@ -1522,7 +1557,7 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
                                                                   ctx->slab + s * ctx->slot_stride + ctx->o_wr, ctx->d_out + n);
                     CK(cudaMemcpyAsync(wr_host + (size_t)(b0 + s) * n, ctx->d_out + n, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
                 }
-                CK(cudaStreamSynchronize(ctx->st));
+                WAIT(ctx);
             }
         }
         if (p.eprecond == 1 || p.eprecond == 3) {
@@ -1565,8 +1600,9 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
         }
         CK(cudaGetLastError());
         std::vector<double> l2b(nb);
+        WAIT(ctx);
         CK(cudaMemcpyAsync(l2b.data(), ctx->d_l2, nb * sizeof(double), cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
+        WAIT(ctx);
         for (int s = 0; s < nb; s++) { l2_total += l2b[s]; ctx->shot_l2.push_back(l2b[s]); }
         float a = 0, b = 0;
         cudaEventElapsedTime(&a, e0, e1);
@@ -1581,10 +1617,11 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
                                                           sum_r, gv, gr);
     ctx->launches++;
     CK(cudaGetLastError());
+    if (g_vs_host || g_rho_host) WAIT(ctx);
     if (g_vs_host) CK(cudaMemcpyAsync(g_vs_host, gv, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
     if (g_rho_host) CK(cudaMemcpyAsync(g_rho_host, gr, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    CK(cudaEventSynchronize(ctx->ev[1]));
+    WAIT_EV(ctx, ctx->ev[1]);
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     ctx->stats.ms_forward = ms_f; ctx->stats.ms_adjoint = ms_a; ctx->stats.ms_total = ms;
@@ -1611,6 +1648,28 @@ extern "C" int dsh_gradient_device(dsh_ctx *ctx, const dsh_shot *shots, int nsho
                          nullptr, nullptr);
 }
 
+extern "C" int dsh_set_wait_limits(dsh_ctx *ctx, long long device_polls, double host_seconds)
+{
+    if (!ctx) return DSH_ERR_PARAM;
+    const long long polls = device_polls > 0 ? device_polls : DEVICE_POLLS_DEFAULT;
+    if (polls != ctx->device_polls) drop_graphs(ctx);      /* the limit is baked into captured launches */
+    ctx->device_polls = polls;
+    ctx->host_timeout_s = host_seconds > 0 ? host_seconds : HOST_TIMEOUT_DEFAULT_S;
+    return DSH_OK;
+}
+
+extern "C" int dsh_set_step_variant(dsh_ctx *ctx, int variant)
+{
+    static const int sel[4][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};   /* staged, fused, persistent */
+    if (!ctx || variant < -1 || variant > 3) return DSH_ERR_PARAM;
+    if (variant == 2 && !ctx->fused_ok) return DSH_ERR_PARAM;
+    ctx->sel_staged = variant < 0 ? -1 : sel[variant][0];
+    ctx->sel_fused = variant < 0 ? -1 : sel[variant][1];
+    ctx->sel_persist = variant < 0 ? -1 : sel[variant][2];
+    drop_graphs(ctx);
+    return DSH_OK;
+}
+
 extern "C" int dsh_set_misfit(dsh_ctx *ctx, int lnorm)
 {
     if (!ctx || lnorm < 1 || lnorm > 5) return DSH_ERR_PARAM;
@@ -1632,7 +1691,7 @@ extern "C" int dsh_set_shot_taper(dsh_ctx *ctx, int enable, int srtshape, float 
     std::vector<float> box((size_t)g * g);
     dsh_setup_taper_box(srtshape, srtradius, ctx->p.dh, &g, &ijc, box.data());
     CK(cudaSetDevice(ctx->dev));
-    CK(cudaStreamSynchronize(ctx->st));
+    WAIT(ctx);
     ctx->taper_on = 0;
     cudaFree(ctx->d_taper_box);
     ctx->d_taper_box = nullptr;
@@ -1668,16 +1727,17 @@ extern "C" int dsh_hessian_diag(dsh_ctx *ctx, const dsh_shot *shots, int nshots,
         shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
                                                                ctx->slab + ctx->o_hu, ctx->slab + ctx->o_hrho, sum_u, sum_r);
         ctx->launches++;
-        CK(cudaStreamSynchronize(ctx->st));
+        WAIT(ctx);
     }
     hessian_convert_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->m_vs, ctx->m_rho, sum_u,
                                                                   sum_r, ctx->d_out, ctx->d_out + n);
     ctx->launches++;
     CK(cudaGetLastError());
+    if (h_vs || h_rho) WAIT(ctx);
     if (h_vs) CK(cudaMemcpyAsync(h_vs, ctx->d_out, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
     if (h_rho) CK(cudaMemcpyAsync(h_rho, ctx->d_out + n, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaEventRecord(ctx->ev[1], ctx->st));
-    CK(cudaEventSynchronize(ctx->ev[1]));
+    WAIT_EV(ctx, ctx->ev[1]);
     float ms = 0;
     cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
     ctx->stats.ms_forward = ms; ctx->stats.ms_adjoint = 0; ctx->stats.ms_total = ms;
@@ -1714,9 +1774,10 @@ extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
         else return DSH_ERR_PARAM;
     }
     }
+    WAIT(ctx);
     CK(cudaMemcpy2DAsync(out, (size_t)p.nx * sizeof(float), src + HX, (size_t)pitch * sizeof(float),
                          (size_t)p.nx * sizeof(float), p.ny, cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    WAIT(ctx);
     (void)n;
     return DSH_OK;
 }
@@ -1757,7 +1818,7 @@ extern "C" int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int
             CK(cudaEventRecord(e1, ctx->st));
         }
         if (rc != DSH_OK) break;
-        CK(cudaEventSynchronize(e1));
+        WAIT_EV(ctx, e1);
         cudaEventElapsedTime(&ms[v], e0, e1);
         ms[v] /= nsteps;
         if (ms[v] < ms[best]) best = v;
@@ -1804,7 +1865,7 @@ extern "C" int dsh_profile_fused(dsh_ctx *ctx, int pass, int nsteps, float *out_
         CK(cudaLaunchKernel((const void *)fk, grid, dim3(256), args, 0, ctx->st));
     }
     CK(cudaEventRecord(e1, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    WAIT(ctx);
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
@@ -1835,8 +1896,9 @@ extern "C" int dsh_get_energy_sums(dsh_ctx *ctx, float *ws_sum, float *wr_sum)
         if (!dst[k]) continue;
         gather_dense_kernel<<<256, 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, src[k], ctx->d_out);
         CK(cudaGetLastError());
+        WAIT(ctx);
         CK(cudaMemcpyAsync(dst[k], ctx->d_out, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
-        CK(cudaStreamSynchronize(ctx->st));
+        WAIT(ctx);
     }
     return DSH_OK;
 }
@@ -1852,7 +1914,7 @@ extern "C" int dsh_set_stream(dsh_ctx *ctx, void *stream)
 {
     if (!ctx) return DSH_ERR_PARAM;
     CK(cudaSetDevice(ctx->dev));
-    CK(cudaStreamSynchronize(ctx->st));
+    WAIT(ctx);
     ctx->st = stream ? (cudaStream_t)stream : ctx->own_st;
     return DSH_OK;
 }
@@ -1902,7 +1964,7 @@ extern "C" int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_m
         }
         CK(cudaEventRecord(ev[2 * q + 1], ctx->st));
     }
-    CK(cudaStreamSynchronize(ctx->st));
+    WAIT(ctx);
     double acc[3] = {0, 0, 0};
     for (int q = 0; q < 3; q++) {
         float ms = 0;

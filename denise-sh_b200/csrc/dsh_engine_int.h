@@ -5,7 +5,9 @@
 #include "dsh_dispatch.h"
 #include "dsh_setup.h"
 
+#include <chrono>
 #include <map>
+#include <thread>
 #include <vector>
 
 namespace dsh {
@@ -75,12 +77,40 @@ struct dsh_ctx {
     std::vector<double> shot_l2;          /* per-shot L2 misfits of the last gradient */
     std::map<long long, cudaGraphExec_t> graphs;
     cudaEvent_t ev[4];
+    cudaEvent_t ev_wait = nullptr;        /* recorded by the bounded host waits (timing disabled) */
+    double host_timeout_s = 1800.0;       /* wall-clock limit of every host wait (dsh_set_wait_limits) */
+    long long device_polls = 1LL << 24;   /* poll limit of the device's bounded waits (dsh_set_wait_limits) */
     dsh_stats stats;
     long long launches = 0;
     int last_cuda = 0;
 };
 
 namespace dsh::eng {
+constexpr double HOST_TIMEOUT_DEFAULT_S = 1800.0;
+constexpr long long DEVICE_POLLS_DEFAULT = 1LL << 24;
+
+/* Bounded host wait on a recorded event: polls it (yielding, then sleeping
+ * 20 us between polls) until it completes (DSH_OK), reports a device error
+ * (DSH_ERR_CUDA) or timeout_s seconds of wall-clock time pass
+ * (DSH_ERR_TIMEOUT; the device work goes on and a later call on the same
+ * stream waits behind it). */
+inline int wait_event(cudaEvent_t ev, double timeout_s)
+{
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int polls = 0;; polls++) {
+        const cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return DSH_OK;
+        if (e != cudaErrorNotReady) return DSH_ERR_CUDA;
+        if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > timeout_s)
+            return DSH_ERR_TIMEOUT;
+        if (polls < 512) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(20));
+    }
+}
+
+/* bounded wait for everything enqueued on the context's stream so far */
+int wait_stream(dsh_ctx *ctx);
+
 /* shots[0..nb) -> slots: sources, receivers, signals, optional observed data */
 int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_host, const float *obs_dev,
                  long long obs_dev_off);

@@ -111,6 +111,7 @@ struct StepArgs {
     /* compat outputs (Layer-1): explicit vyp1/uy/uyx haloed fields */
     float *out_acc, *out_uy, *out_uyx;
     int *status;                 /* device error word (non-finite detection) */
+    long long wait_polls;        /* poll limit of bounded device waits (the persistent launch's grid barrier) */
     const void *tm_sxy, *tm_syz;   /* tensor maps (CUtensorMap, device memory) of sxy / syz over all slots,
                                       for the TMA-staged velocity kernel; NULL when not built */
     TileLists tl;

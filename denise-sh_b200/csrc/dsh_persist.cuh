@@ -20,8 +20,6 @@
 
 namespace dsh {
 
-constexpr long long BARRIER_LIMIT = 1LL << 24;   /* polls of the generation word */
-
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 {
     unsigned v;
@@ -32,8 +30,8 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
 /* count[0]: arrivals of the current barrier, count[1]: generation.  The
  * block barrier before thread 0's fence makes the block's stores part of its
  * release (fences are cumulative); waiting threads poll the generation with
- * acquire loads. */
-__device__ __forceinline__ bool grid_barrier(unsigned *count, int *status)
+ * acquire loads, at most `limit` times (StepArgs::wait_polls). */
+__device__ __forceinline__ bool grid_barrier(unsigned *count, int *status, long long limit)
 {
     __shared__ int ok;
     __syncthreads();
@@ -48,7 +46,7 @@ __device__ __forceinline__ bool grid_barrier(unsigned *count, int *status)
         } else {
             long long it = 0;
             while (ld_acquire(count + 1) == g) {
-                if (++it > BARRIER_LIMIT) { atomicOr(status, 2); ok = 0; break; }
+                if (++it >= limit) { atomicOr(status, 2); ok = 0; break; }
             }
         }
         __threadfence();
@@ -69,13 +67,13 @@ __global__ void __launch_bounds__(BX *BY, 2) persist_fwd(StepArgs a, int nsteps,
             v_body<FDO, 0, P2, GlobalTaps<true>, true>(a, step, 1 + 4 * (bx * BX + threadIdx.x),
                                                        1 + by * BY + threadIdx.y, slot, tile);
         }
-        if (!grid_barrier(bar, a.status)) return;
+        if (!grid_barrier(bar, a.status, a.wait_polls)) return;
         for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
             const int slot = t / per_slot, tile = t % per_slot;
             const int bx = tile % gx, by = tile / gx;
             s_body<FDO, L, 0, true>(a, step, 1 + 4 * (bx * BX + threadIdx.x), 1 + by * BY + threadIdx.y, slot);
         }
-        if (!grid_barrier(bar, a.status)) return;
+        if (!grid_barrier(bar, a.status, a.wait_polls)) return;
     }
 }
 

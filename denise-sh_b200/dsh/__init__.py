@@ -102,6 +102,9 @@ def lib() -> C.CDLL:
         L.dsh_taper_apply.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_set_shot_taper.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]
         L.dsh_set_misfit.argtypes = [C.c_void_p, C.c_int]
+        L.dsh_set_wait_limits.argtypes = [C.c_void_p, C.c_longlong, C.c_double]
+        L.dsh_set_step_variant.argtypes = [C.c_void_p, C.c_int]
+        L.dsh_batch_set_host_timeout.argtypes = [C.c_void_p, C.c_double]
         L.dsh_autotune.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
         L.dsh_profile_fused.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_void_p]
         L.dsh_get_shot_misfits.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
@@ -314,6 +317,16 @@ class Engine:
         _check(rc, "dsh_profile_fused")
         return float(out[0])
 
+    def set_wait_limits(self, device_polls: int = 0, host_seconds: float = 0.0):
+        """Poll limit of the device's bounded waits and wall-clock limit of the
+        host's waits (0 = defaults); expiry returns DSH_ERR_TIMEOUT."""
+        _check(lib().dsh_set_wait_limits(self.h, C.c_longlong(int(device_polls)), C.c_double(float(host_seconds))),
+               "dsh_set_wait_limits")
+
+    def set_step_variant(self, variant: int):
+        """Pin a step-kernel variant (index into VARIANTS; -1 = defaults)."""
+        _check(lib().dsh_set_step_variant(self.h, int(variant)), "dsh_set_step_variant")
+
     LNORM = {"l1": 1, "l2": 2, "cauchy": 3, "sech": 4, "global_correlation": 5}
 
     def set_misfit(self, lnorm):
@@ -387,6 +400,10 @@ class Batch:
 
     def set_stream(self, stream_handle):
         _check(lib().dsh_batch_set_stream(self.h, stream_handle), "dsh_batch_set_stream")
+
+    def set_host_timeout(self, host_seconds: float):
+        """Wall-clock limit of the batch's host waits (0 = default); expiry returns DSH_ERR_TIMEOUT."""
+        _check(lib().dsh_batch_set_host_timeout(self.h, C.c_double(float(host_seconds))), "dsh_batch_set_host_timeout")
 
     def _flat(self, shots_per_model):
         flat = [s for group in shots_per_model for s in group]

@@ -217,6 +217,8 @@ int dsh_batch_forward_device(dsh_batch *b, const dsh_shot *shots, const int *nsh
 int dsh_batch_set_stream(dsh_batch *b, void *stream);
 /* tile-shape variants 0..2 for the velocity and stress launches; -1 = autotune */
 int dsh_batch_set_variant(dsh_batch *b, int v_variant, int s_variant);
+/* Wall-clock limit of the batch's host waits (as dsh_set_wait_limits; <= 0 restores 1800 s). */
+int dsh_batch_set_host_timeout(dsh_batch *b, double host_seconds);
 typedef struct dsh_batch_stats {
     double ms_total;                 /* device time of the last run (CUDA events) */
     long long kernel_launches;
@@ -309,6 +311,24 @@ int dsh_taper_apply(float *g_dev, int nx, int ny, const float *coeff_dev, const 
  * rejected: the reference reads integrated traces there that it allocates
  * only for LNORM=5 with GRAD_FORM=1 (src/calc_res.c:69-72,221). */
 int dsh_set_misfit(dsh_ctx *ctx, int lnorm);
+
+/* Limits of the context's waits (no counterpart in the reference, which
+ * blocks in MPI and has no device).  host_seconds: wall-clock limit of every
+ * host wait for the context's stream (default 1800 s; <= 0 restores it); when
+ * it passes the call returns DSH_ERR_TIMEOUT while the device work goes on, a
+ * later call on the stream waits behind that work, and outputs of the
+ * timed-out call are undefined.  device_polls: poll limit of the bounded
+ * device waits (the grid barrier of the persistent launch; default 2^24,
+ * <= 0 restores it); on expiry the kernel sets an error bit, leaves its time
+ * loop and the call returns DSH_ERR_TIMEOUT with the context still usable.
+ * Small limits exist to exercise those paths. */
+int dsh_set_wait_limits(dsh_ctx *ctx, long long device_polls, double host_seconds);
+
+/* Pins the step-kernel variant (0 kernel pair, 1 pair with shared-memory
+ * staged velocity taps, 2 fused step (FDORDER <= 8), 3 persistent launch of
+ * plain forward modelling when all tiles fit one wave, else the pair; -1 the
+ * defaults) — what dsh_autotune picks by timing. */
+int dsh_set_step_variant(dsh_ctx *ctx, int variant);
 
 /* Per-shot circular taper (SWS_TAPER_CIRCULAR_PER_SHOT, src/taper_grad_shot.c,
  * applied at src/denise.c:1681-1687): in dsh_gradient / dsh_gradient_device
