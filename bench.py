@@ -84,6 +84,8 @@ def args_parse():
     ap.add_argument("--ny", type=int, default=800, help="c2 only")
     ap.add_argument("--shots", type=int, default=64, help="c3 only: shots per GPU")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--c3-steps", type=int, default=2,
+                    help="c2 only: timed gradients of the 64-shot batched-gradient sub-measurement (0 = skip)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="c1-c3: keep the default kernel pair instead of timing the step-kernel variants "
                          "(for runs under a profiler)")
@@ -98,6 +100,15 @@ def peaks():
         d = json.load(open(p))
         return float(d["hbm_gbs"]), "measured"
     return FALLBACK_HBM_GBS, "fallback"
+
+
+def kernels_hash():
+    """sha256 of the step kernels' source (csrc/dsh_kernels.cuh): ties a
+    recorded ncu traffic figure to the build it was measured on."""
+    import hashlib
+
+    with open(os.path.join(ROOT, "denise-sh_b200", "csrc", "dsh_kernels.cuh"), "rb") as f:
+        return hashlib.sha256(f.read()).hexdigest()
 
 
 def bytes_per_point(l, nx, ny, fw, free_surf):
@@ -287,6 +298,79 @@ def reference_arm(a, rank, world):
 
 # ---------------------------------------------------------------------------
 
+def c3_sub(a, local):
+    """The batched multi-shot FWI gradient as the configuration states it:
+    NX=1000, NY=300, FDORDER 8, L=2, NT=4000, 64 shots advanced in one launch
+    per half-step, forward wavefield checkpointed every ceil(sqrt(NT)) = 64
+    steps and recomputed segment by segment for the adjoint.  Inputs resident
+    in HBM (observed data synthesised on the true model first); CUDA events on
+    the launching stream; one untimed gradient first.  Reports FWI gradients/s
+    (shots per second), Gpt/s counted over the two passes a gradient needs
+    and over the three passes it executes (the recompute included), and the
+    stress kernel's roofline."""
+    import torch
+
+    import dsh
+    from dsh import configs
+
+    nt = 4000
+    every = math.ceil(math.sqrt(nt))
+    cfg = configs.config3(nt=nt)
+    p, shots = cfg["params"], cfg["shots"]
+    nsh, nx, ny = len(shots), p["nx"], p["ny"]
+    n = nx * ny
+    eng = dsh.Engine(dsh.make_params(**p, max_shots=nsh, ckpt_every=every), device=local)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.set_model(cfg["true"], cfg["rho"], cfg["qs"])
+    seis = torch.empty(sum(sh.ntr for sh in shots) * nt, device="cuda", dtype=torch.float32)
+    eng.forward_device(shots, seis.data_ptr())
+    eng.set_model(cfg["vs"], cfg["rho"], cfg["qs"])
+    gv = torch.empty(n, device="cuda", dtype=torch.float32)
+    gr = torch.empty(n, device="cuda", dtype=torch.float32)
+    eng.gradient_device(shots, seis.data_ptr(), gv.data_ptr(), gr.data_ptr())
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches, ms_f, ms_a = 0, 0.0, 0.0
+    e0.record(stream)
+    for _ in range(a.c3_steps):
+        eng.gradient_device(shots, seis.data_ptr(), gv.data_ptr(), gr.data_ptr())
+        st = eng.stats()
+        launches += st["kernel_launches"]
+        ms_f += st["ms_forward"]
+        ms_a += st["ms_adjoint"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    st = eng.stats()
+    ms = e0.elapsed_time(e1) / a.c3_steps
+    prof = eng.profile_step("forward_store", a.profile_steps)
+    eng.close()
+    hbm, peak_kind = peaks()
+    kv, ks = kernel_bytes(2, store=True)
+    s_gbs = ks * n * nsh / (prof["s_step"] / 1e3) / 1e9
+    v_gbs = kv * n * nsh / (prof["v_step"] / 1e3) / 1e9
+    return {
+        "workload": f"batched-gradient-{nx}x{ny}-fd8-L2-{nsh}shots-nt{nt}", "steps": a.c3_steps, "warmup": 1,
+        "gradients_per_s": nsh / (ms / 1e3), "ms_per_gradient": ms,
+        "gpt_per_s": 2.0 * n * nt * nsh / (ms / 1e3) / 1e9,
+        "gpt_per_s_executed": 3.0 * n * nt * nsh / (ms / 1e3) / 1e9,
+        "counting": "gpt_per_s: forward + adjoint pass (2 x NX x NY x NT x shots per gradient); "
+                    "gpt_per_s_executed adds the recomputed forward pass of checkpointing",
+        "checkpoint_interval": st["checkpoint_interval"], "storage_gb": st["storage_bytes"] / 1e9,
+        "ms_forward_pass": ms_f / a.c3_steps, "ms_adjoint_and_recompute": ms_a / a.c3_steps,
+        "gpu_launches": launches,
+        "l2": f"inputs larger than L2 (state of {nsh} shots {(3 + 2 * 2) * n * 4 * nsh / 1e6:.0f} MB)",
+        "roofline": {"bound": "hbm", "achieved": s_gbs, "peak": hbm, "unit": "GB/s", "frac": s_gbs / hbm,
+                     "kernel": "s_step<8,2> (forward pass with storage, 64 slots)", "bytes_per_point": ks,
+                     "ms_per_launch": prof["s_step"], "peak_source": peak_kind},
+        "kernels_ms": prof, "v_step_gbs": v_gbs,
+        "clocks": clk,
+    }
+
+
 def main():
     a = args_parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -466,10 +550,14 @@ def main():
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath) and a.config == "c2":
+        # DRAM bytes of one launch from an ncu capture; reported only when the
+        # capture was taken on the step kernels' current source
         try:
+            rec = json.load(open(tpath))
             key = "fs_step_forward_store_bytes_per_launch" if fused_ms is not None else \
                 "s_step_forward_store_bytes_per_launch"
-            traffic = json.load(open(tpath)).get(key)
+            if rec.get("kernels_sha256") == kernels_hash():
+                traffic = rec.get(key)
         except Exception:
             traffic = None
 
@@ -516,8 +604,13 @@ def main():
         if gradient:
             line["gradients_per_s"] = world * nsh * a.steps / (ms / 1e3)
             line["l2_misfit"] = l2
-        print(json.dumps(line), flush=True)
     eng.close()
+    if rank == 0:
+        if a.config == "c2" and world == 1 and a.c3_steps > 0:
+            del seis, gv, gr
+            torch.cuda.empty_cache()
+            line["c3"] = c3_sub(a, local)
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
