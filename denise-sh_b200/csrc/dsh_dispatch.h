@@ -9,6 +9,7 @@ using KFn = void (*)(StepArgs, int);
     KFn v_kernel_fd##N(int flags, bool p2);    \
     KFn v_kernel_st_fd##N(int flags, bool p2); \
     KFn v_kernel_tp_fd##N(int flags, bool p2); \
+    KFn v_kernel_r2_fd##N(int flags, bool p2); \
     KFn s_kernel_fd##N(int l, int flags);
 DSH_DECLARE_FD(2)
 DSH_DECLARE_FD(4)
@@ -56,6 +57,20 @@ inline KFn v_kernel_tp(int fdo, int flags, bool p2)
     case 8: return v_kernel_tp_fd8(flags, p2);
     case 10: return v_kernel_tp_fd10(flags, p2);
     case 12: return v_kernel_tp_fd12(flags, p2);
+    default: return nullptr;
+    }
+}
+
+/* velocity step with two rows per thread (v_step_r2), block (32, 4) */
+inline KFn v_kernel_r2(int fdo, int flags, bool p2)
+{
+    switch (fdo) {
+    case 2: return v_kernel_r2_fd2(flags, p2);
+    case 4: return v_kernel_r2_fd4(flags, p2);
+    case 6: return v_kernel_r2_fd6(flags, p2);
+    case 8: return v_kernel_r2_fd8(flags, p2);
+    case 10: return v_kernel_r2_fd10(flags, p2);
+    case 12: return v_kernel_r2_fd12(flags, p2);
     default: return nullptr;
     }
 }

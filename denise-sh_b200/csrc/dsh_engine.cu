@@ -295,6 +295,29 @@ __global__ void convert_kernel(int nx, int ny, int pitch, float dt, const float 
     }
 }
 
+/* Qs gradient from the shot sums of the two correlations (no counterpart in
+ * the reference, which has no Q gradient): the stress multiplier of forward
+ * update k is (2/rho) times the back-propagated adjoint strain, so
+ * dJ/dtau_ipjp = -(2/rho) sum_x and dJ/dtau = -(2/rho) sum_y; tau_ipjp is the
+ * four-point average of tau (av_tau.c:12, one-rank periodic wrap) and
+ * tau = 2/Qs (readmod.c:99).  Double arithmetic in the oracle's order. */
+__global__ void q_convert_kernel(int nx, int ny, int pitch, const float *rho, const float *qs, const float *sum_x,
+                                 const float *sum_y, float *g_qs)
+{
+    const long long n = (long long)nx * ny;
+    for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n; idx += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(idx % nx) + 1, j = (int)(idx / nx) + 1;
+        const int im = i > 1 ? i - 1 : nx, jm = j > 1 ? j - 1 : ny;
+        const long long nb[4] = {(long long)(j - 1) * pitch + (i - 1 + HX), (long long)(j - 1) * pitch + (im - 1 + HX),
+                                 (long long)(jm - 1) * pitch + (i - 1 + HX), (long long)(jm - 1) * pitch + (im - 1 + HX)};
+        double gx = 0.0;
+        for (int k = 0; k < 4; k++) gx += -2.0 / (double)rho[nb[k]] * (double)sum_x[nb[k]];
+        const double gy = -2.0 / (double)rho[nb[0]] * (double)sum_y[nb[0]];
+        const double q = (double)qs[nb[0]];
+        g_qs[idx] = (float)((gy + 0.25 * gx) * (-2.0 / (q * q)));
+    }
+}
+
 /* hessian_out.c:20-31: H_rho += vs^4 H_mu; H_vs = 4 rho^2 vs^2 H_mu (double) */
 __global__ void hessian_convert_kernel(int nx, int ny, int pitch, const float *vs, const float *rho, const float *hu,
                                        const float *hr, float *h_vs, float *h_rho)
@@ -424,6 +447,7 @@ static int check_params(const dsh_params *p)
         return DSH_ERR_PARAM;
     if (p->max_shots < 1 || p->max_shots > 65535) return DSH_ERR_PARAM;
     if (p->ckpt_every < 0) return DSH_ERR_PARAM;
+    if (p->grad_q != 0 && (p->grad_q != 1 || p->l < 1)) return DSH_ERR_PARAM;   /* Qs gradient: viscoelastic only */
     if (p->nx > 65000 || p->ny > 65000) return DSH_ERR_PARAM;
     if (p->quellart != 1 && p->quellart != 2 && p->quellart != 3 && p->quellart != 4 && p->quellart != 5 &&
         p->quellart != 6)
@@ -479,10 +503,16 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     ctx->o_grho = o; o += ctx->dstride;
     ctx->o_hu = o; o += ctx->dstride;
     ctx->o_hrho = o; o += ctx->dstride;
+    if (p->grad_q) {                      /* Qs gradient: adjoint strains and correlation sums */
+        ctx->o_exy = o; o += ctx->dstride;
+        ctx->o_eyz = o; o += ctx->dstride;
+        ctx->o_gqx = o; o += ctx->dstride;
+        ctx->o_gqy = o; o += ctx->dstride;
+    }
     ctx->slot_stride = o;
     if (cudaMalloc(&ctx->slab, (size_t)ctx->S * ctx->slot_stride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     build_tmaps(ctx);
-    const long long nmodel = 9LL * ctx->dstride;
+    const long long nmodel = 10LL * ctx->dstride;
     if (cudaMalloc(&ctx->model, (size_t)nmodel * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     cudaMemset(ctx->model, 0, (size_t)nmodel * sizeof(float));
     float *m = ctx->model;
@@ -494,9 +524,12 @@ extern "C" dsh_ctx *dsh_create(const dsh_params *p, int device, int *status)
     ctx->m_tip = m; m += ctx->dstride;
     ctx->m_taus = m; m += ctx->dstride;
     ctx->m_vs = m; m += ctx->dstride;
-    ctx->m_rho = m;
+    ctx->m_rho = m; m += ctx->dstride;
+    ctx->m_qs = m;
     if (cudaMalloc(&ctx->pml, 12 * (size_t)(2 * DSH_MAX_FW + 1) * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
-    if (cudaMalloc(&ctx->sums, 6 * (size_t)ctx->dstride * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
+    if (cudaMalloc(&ctx->sums, (p->grad_q ? 8 : 6) * (size_t)ctx->dstride * sizeof(float)) != cudaSuccess)
+        return bail(DSH_ERR_OOM);
+    if (p->grad_q && cudaMalloc(&ctx->d_gq, (size_t)nx * ny * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     if (cudaMalloc(&ctx->d_out, 2 * (size_t)nx * ny * sizeof(float)) != cudaSuccess) return bail(DSH_ERR_OOM);
     if (cudaMalloc(&ctx->d_nt, 4 * sizeof(int)) != cudaSuccess) return bail(DSH_ERR_OOM);
     ctx->d_status = ctx->d_nt + 1;
@@ -530,7 +563,7 @@ extern "C" int dsh_destroy(dsh_ctx *ctx)
     cudaFree(ctx->ckpt); cudaFree(ctx->shadow);
     cudaFree(ctx->d_geo); cudaFree(ctx->d_offs); cudaFree(ctx->d_sig); cudaFree(ctx->d_seis); cudaFree(ctx->d_res);
     cudaFree(ctx->d_obs); cudaFree(ctx->d_tmp); cudaFree(ctx->d_out); cudaFree(ctx->d_nt); cudaFree(ctx->d_part); cudaFree(ctx->d_l2);
-    cudaFree(ctx->d_wemax);
+    cudaFree(ctx->d_wemax); cudaFree(ctx->d_gq);
     cudaFree(ctx->d_taper_box); cudaFree(ctx->d_taper_shot); cudaFree(ctx->d_tmap);
     for (int k = 0; k < 4; k++) if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     if (ctx->ev_wait) cudaEventDestroy(ctx->ev_wait);
@@ -649,7 +682,10 @@ extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, co
         if ((rc = upload_field(ctx, ctx->m_mujp, mujp.data())) != DSH_OK) return rc;
         if ((rc = upload_field(ctx, ctx->m_tip, tip.data())) != DSH_OK) return rc;
         if ((rc = upload_field(ctx, ctx->m_taus, taus.data())) != DSH_OK) return rc;
+        if ((rc = upload_field(ctx, ctx->m_qs, qs)) != DSH_OK) return rc;
+        ctx->sumu = dsh_setup_sumu(L, p.fl);
     }
+    ctx->gq_valid = 0;
     WAIT(ctx);   /* host staging vectors go out of scope */
     ctx->model_set = 1;
     return DSH_OK;
@@ -946,6 +982,10 @@ StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.muip = ctx->m_muip; a.mujp = ctx->m_mujp; a.tausipjp = ctx->m_tip; a.taus = ctx->m_taus;
     for (int l = 0; l < 4; l++) a.eta[l] = ctx->eta[l];
     a.lf = (float)p.l;
+    a.sumu = ctx->sumu;
+    if (p.grad_q) {
+        a.exy = sl + ctx->o_exy; a.eyz = sl + ctx->o_eyz; a.gqx = sl + ctx->o_gqx; a.gqy = sl + ctx->o_gqy;
+    }
     for (int l = 0; l < 4; l++) { a.bip[l] = ctx->bip[l]; a.bjm[l] = ctx->bjm[l]; a.cip[l] = ctx->cip[l]; a.cjm[l] = ctx->cjm[l]; }
     a.fwd_slot_stride = ctx->fwd_slot_stride;
     a.fwd_mod = ctx->fwd_mod > 0 ? ctx->fwd_mod : p.nt;
@@ -1050,10 +1090,13 @@ static VPick pick_v(const dsh_ctx *ctx, int fdo, int vflags, bool p2)
 {
     static const int env = env_flag("DSH_VSTAGE");
     static const int env_tma = env_flag("DSH_VTMA");
+    static const int env_rows = getenv("DSH_VROWS") ? atoi(getenv("DSH_VROWS")) : 1;
     const bool staged = ctx->sel_staged >= 0 ? ctx->sel_staged != 0 : env != 0;
     KFn k = staged ? v_kernel_st(fdo, vflags, p2) : nullptr;
     if (k) return {k, 1};
     if (env_tma && ctx->tma_ok && (k = v_kernel_tp(fdo, vflags, p2))) return {k, 2};
+    const bool rows2 = ctx->sel_rows >= 0 ? ctx->sel_rows != 0 : env_rows == 2;
+    if (rows2 && (k = v_kernel_r2(fdo, vflags, p2))) return {k, 3};
     return {v_kernel(fdo, vflags, p2), 0};
 }
 
@@ -1071,7 +1114,7 @@ static void v_shape(const dsh_ctx *ctx, const VPick &v, int nb, dim3 *grid, dim3
         *block = dim3(BX, BY + 1, 1);           /* 8 computing warps + 1 producer warp */
     } else {
         *grid = dim3(gx, gy, (unsigned)nb);
-        *block = dim3(BX, BY, 1);
+        *block = dim3(BX, v.code == 3 ? BY / 2 : BY, 1);
     }
 }
 
@@ -1085,7 +1128,7 @@ static bool use_fused(dsh_ctx *ctx, Pass pass)
 {
     static const int env = env_flag("DSH_FUSED");
     const bool on = ctx->sel_fused >= 0 ? ctx->sel_fused != 0 : env != 0;
-    return on && ctx->fused_ok && ctx->fused_inject && pass != P_FWD_HESS;
+    return on && ctx->fused_ok && ctx->fused_inject && pass != P_FWD_HESS && !ctx->p.grad_q;
 }
 
 static int fused_mode(Pass pass)
@@ -1135,6 +1178,8 @@ static int launch_step_chunk(dsh_ctx *ctx, Pass pass, int nb, int nsteps_in_chun
     case P_FWD_CKPT: break;
     case P_RECOMP: sflags = SF_STRAIN_OUT; break;
     }
+    if (p.grad_q && (sflags == SF_STRAIN_OUT || sflags == SF_CORR))   /* the Qs gradient's two halves */
+        sflags |= sflags == SF_CORR ? SF_CORRQ : SF_QSENS;
     const VPick vp = pick_v(ctx, p.fdorder, vflags, dh_pow2(p.dh));
     KFn vk = vp.k, sk = s_kernel(p.fdorder, p.l, sflags);
     if (!vk || !sk) return DSH_ERR_PARAM;
@@ -1368,12 +1413,13 @@ static int ensure_storage(dsh_ctx *ctx)
 {
     const dsh_params &p = ctx->p;
     const size_t S = ctx->S, D = ctx->dstride, st = ctx->o_state_end;
-    const size_t full = S * (size_t)p.nt * 3 * D * sizeof(float);
+    const size_t NS = p.grad_q ? 5 : 3;   /* stored fields per step: acc, uy, uyx (+ the two tau sensitivities) */
+    const size_t full = S * (size_t)p.nt * NS * D * sizeof(float);
     int C = p.ckpt_every > 0 ? p.ckpt_every
                              : (int)std::lround(std::sqrt((double)p.nt * (3.0 + 2.0 * p.l) / 3.0));
     C = std::max(1, std::min(C, p.nt));
     const int nck = (p.nt + C - 1) / C - 1;
-    const size_t ckpt_need = S * (size_t)C * 3 * D * sizeof(float) + (size_t)nck * S * st * sizeof(float) +
+    const size_t ckpt_need = S * (size_t)C * NS * D * sizeof(float) + (size_t)nck * S * st * sizeof(float) +
                              S * (size_t)ctx->slot_stride * sizeof(float);
     if (ctx->fwd && ((ctx->ckpt_c == 0 && ctx->fwd_bytes >= full) || (ctx->ckpt_c == C && ctx->ckpt))) return DSH_OK;
     cudaFree(ctx->fwd); cudaFree(ctx->ckpt); cudaFree(ctx->shadow);
@@ -1387,7 +1433,7 @@ static int ensure_storage(dsh_ctx *ctx)
         CK(cudaMemGetInfo(&fr, &tot));
         budget = (long long)fr - (2LL << 30);
     }
-    ctx->fwd_step_stride = 3 * D;
+    ctx->fwd_step_stride = NS * D;
     if (p.ckpt_every <= 0 && (long long)full <= budget) {
         if (cudaMalloc(&ctx->fwd, full) != cudaSuccess) { cudaGetLastError(); return DSH_ERR_OOM; }
         ctx->fwd_bytes = full;
@@ -1395,7 +1441,7 @@ static int ensure_storage(dsh_ctx *ctx)
         ctx->ckpt_c = 0;
     } else {
         if ((long long)ckpt_need > budget) return DSH_ERR_OOM;
-        const size_t seg = S * (size_t)C * 3 * D * sizeof(float);
+        const size_t seg = S * (size_t)C * NS * D * sizeof(float);
         if (cudaMalloc(&ctx->fwd, seg) != cudaSuccess) { cudaGetLastError(); return DSH_ERR_OOM; }
         if (nck > 0 && cudaMalloc(&ctx->ckpt, (size_t)nck * S * st * sizeof(float)) != cudaSuccess) {
             cudaGetLastError(); return DSH_ERR_OOM;
@@ -1504,6 +1550,8 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
     const bool energies = p.eprecond == 1 || p.eprecond == 3 || p.eprecond == DSH_EPRECOND_ENERGY_ONLY;
     CK(cudaMemsetAsync(ctx->sums, 0, 2 * (size_t)ctx->dstride * sizeof(float), ctx->st));
     CK(cudaMemsetAsync(esum_s, 0, 2 * (size_t)ctx->dstride * sizeof(float), ctx->st));
+    if (p.grad_q) CK(cudaMemsetAsync(ctx->sums + 6 * ctx->dstride, 0, 2 * (size_t)ctx->dstride * sizeof(float), ctx->st));
+    ctx->gq_valid = 0;
     ctx->launches = 0;
     ctx->shot_l2.clear();
     double l2_total = 0.0;
@@ -1592,6 +1640,13 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
                                                                    sum_u, sum_r);
         }
         ctx->launches++;
+        if (p.grad_q) {            /* shot sums of the Qs-gradient correlations */
+            shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
+                                                                   ctx->slab + ctx->o_gqx, ctx->slab + ctx->o_gqy,
+                                                                   ctx->sums + 6 * ctx->dstride,
+                                                                   ctx->sums + 7 * ctx->dstride);
+            ctx->launches++;
+        }
         if (energies) {            /* shot sums of Ws and Wr (dsh_get_energy_sums) */
             shot_sum_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->slot_stride, nb,
                                                                    ctx->slab + ctx->o_ws, ctx->slab + ctx->o_wr,
@@ -1616,6 +1671,12 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
     convert_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, p.dt, ctx->m_vs, ctx->m_rho, sum_u,
                                                           sum_r, gv, gr);
     ctx->launches++;
+    if (p.grad_q) {
+        q_convert_kernel<<<epi_grid(ctx, 1), 256, 0, ctx->st>>>(p.nx, p.ny, ctx->pitch, ctx->m_rho, ctx->m_qs,
+                                                                ctx->sums + 6 * ctx->dstride,
+                                                                ctx->sums + 7 * ctx->dstride, ctx->d_gq);
+        ctx->launches++;
+    }
     CK(cudaGetLastError());
     if (g_vs_host || g_rho_host) WAIT(ctx);
     if (g_vs_host) CK(cudaMemcpyAsync(g_vs_host, gv, n * sizeof(float), cudaMemcpyDeviceToHost, ctx->st));
@@ -1630,7 +1691,24 @@ static int gradient_impl(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const 
     ctx->stats.storage_bytes = (long long)(ctx->fwd_bytes + ctx->ckpt_bytes);
     ctx->stats.checkpoint_interval = ctx->ckpt_c;
     if (l2) *l2 = l2_total;
-    return check_status(ctx);
+    const int st = check_status(ctx);
+    ctx->gq_valid = p.grad_q && st == DSH_OK;
+    return st;
+}
+
+extern "C" int dsh_get_gradient_q(dsh_ctx *ctx, float *g_qs_host, float *g_qs_dev)
+{
+    if (!ctx || (!g_qs_host && !g_qs_dev)) return DSH_ERR_PARAM;
+    if (!ctx->p.grad_q || !ctx->gq_valid) return DSH_ERR_STATE;
+    CK(cudaSetDevice(ctx->dev));
+    const size_t bytes = (size_t)ctx->p.nx * ctx->p.ny * sizeof(float);
+    if (g_qs_dev) CK(cudaMemcpyAsync(g_qs_dev, ctx->d_gq, bytes, cudaMemcpyDeviceToDevice, ctx->st));
+    if (g_qs_host) {
+        WAIT(ctx);
+        CK(cudaMemcpyAsync(g_qs_host, ctx->d_gq, bytes, cudaMemcpyDeviceToHost, ctx->st));
+    }
+    WAIT(ctx);
+    return DSH_OK;
 }
 
 extern "C" int dsh_gradient(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const float *obs, float *g_vs,

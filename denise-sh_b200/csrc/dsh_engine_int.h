@@ -26,14 +26,19 @@ struct dsh_ctx {
     long long fstride = 0, dstride = 0, slot_stride = 0;
     long long o_vy, o_sxy, o_syz, o_r, o_q, o_pvxx, o_psxx, o_pvyy, o_psyy, o_state_end;
     long long o_ws, o_wr, o_we, o_gu, o_grho, o_hu, o_hrho;
+    long long o_exy = 0, o_eyz = 0, o_gqx = 0, o_gqy = 0;   /* Qs gradient (params.grad_q) */
     long long o_vy_b = 0, o_sxy_b = 0, o_syz_b = 0, o_pvxx_b = 0, o_pvyy_b = 0;   /* fused step's second buffers */
     int fused_ok = 0;                     /* FDORDER <= 8: the fused step kernel can run this context */
     int state_b = 0;                      /* the slab's current state is in the second buffers */
     int sel_staged = -1, sel_fused = -1, sel_persist = -1;   /* step-kernel variants chosen by dsh_autotune
                                                                (-1: the DSH_VSTAGE / DSH_FUSED / DSH_PERSIST defaults) */
+    int sel_rows = -1;                    /* 1: the velocity kernel with two rows per thread (-1: DSH_VROWS=2) */
     float *slab = nullptr;
-    float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho */
-    float *m_brho, *m_uip, *m_ujp, *m_muip, *m_mujp, *m_tip, *m_taus, *m_vs, *m_rho;
+    float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho qs */
+    float *m_brho, *m_uip, *m_ujp, *m_muip, *m_mujp, *m_tip, *m_taus, *m_vs, *m_rho, *m_qs;
+    float sumu = 0.0f;                    /* SLS sum of prepare_update_s (Qs gradient) */
+    float *d_gq = nullptr;                /* dJ/dQs of the last gradient (dense [ny][nx]) */
+    int gq_valid = 0;
     float eta[4] = {0};
     float *pml = nullptr;
     float *sums = nullptr;                /* sum_u, sum_rho, out_a, out_b (dense pitched) */

@@ -41,6 +41,17 @@
         }                                                                                     \
     }                                                                                         \
     KFn v_kernel_tp_fd##N(int flags, bool p2) { return p2 ? v_pick_tp_##N<true>(flags) : v_pick_tp_##N<false>(flags); } \
+    template <bool P2>                                                                        \
+    static KFn v_pick_r2_##N(int flags)                                                       \
+    {                                                                                         \
+        switch (flags) {                                                                      \
+        case 0: return v_step_r2<N, 0, P2>;                                                   \
+        case VF_HESS: return v_step_r2<N, VF_HESS, P2>;                                       \
+        case VF_ADJOINT | VF_CORR: return v_step_r2<N, VF_ADJOINT | VF_CORR, P2>;             \
+        default: return nullptr;                                                              \
+        }                                                                                     \
+    }                                                                                         \
+    KFn v_kernel_r2_fd##N(int flags, bool p2) { return p2 ? v_pick_r2_##N<true>(flags) : v_pick_r2_##N<false>(flags); } \
     template <int L>                                                                          \
     static KFn s_pick_##N(int flags)                                                          \
     {                                                                                         \
@@ -50,6 +61,12 @@
         case SF_HESS: return s_step<N, L, SF_HESS>;                                           \
         case SF_CORR: return s_step<N, L, SF_CORR>;                                           \
         case SF_STRAIN_OUT | SF_PARAMS: return s_step<N, L, SF_STRAIN_OUT | SF_PARAMS>;       \
+        case SF_STRAIN_OUT | SF_QSENS:                                                        \
+            if constexpr (L > 0) return s_step<N, L, SF_STRAIN_OUT | SF_QSENS>;               \
+            else return nullptr;                                                              \
+        case SF_CORR | SF_CORRQ:                                                              \
+            if constexpr (L > 0) return s_step<N, L, SF_CORR | SF_CORRQ>;                     \
+            else return nullptr;                                                              \
         default: return nullptr;                                                              \
         }                                                                                     \
     }                                                                                         \

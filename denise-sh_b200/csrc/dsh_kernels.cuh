@@ -48,6 +48,9 @@ constexpr int SF_CORR = 4;       /* g_u += uyx_fwd*sxy + uy_fwd*syz (denise.c:16
 constexpr int SF_HESS = 8;       /* H_u += uy^2 + (0.5 uyx)^2 (hessian.c:92) */
 constexpr int SF_PARAMS = 16;    /* viscoelastic: read precomputed fipjp, f, dip_l, d_l (the compat layer)
                                     instead of forming them from muip, mujp, tausipjp, taus */
+constexpr int SF_QSENS = 32;     /* with SF_STRAIN_OUT: also store the step's stress-increment
+                                    sensitivities to tau (the Qs gradient's forward part) */
+constexpr int SF_CORRQ = 64;     /* with SF_CORR: accumulate the Qs-gradient correlation */
 
 struct PmlCoef {                 /* device copies, index 1..2fw */
     const float *K_x, *a_x, *b_x, *K_x_half, *a_x_half, *b_x_half;
@@ -101,6 +104,8 @@ struct StepArgs {
     const float *muip, *mujp, *tausipjp, *taus;   /* viscoelastic base factors */
     float eta[4];                /* DT / tau_l */
     float lf;                    /* L as a float */
+    float sumu;                  /* sum_l w^2 tau_l^2 / (1 + w^2 tau_l^2) (prepare_update_s.c:29-32) */
+    float *exy, *eyz, *gqx, *gqy;   /* Qs gradient (per slot): adjoint strains, correlation sums */
     float bip[4], bjm[4], cip[4], cjm[4];
     /* stored forward wavefields: slot s, stored step k (0-based) at
        fwd + s*fwd_slot_stride + k*fwd_step_stride (+ 0/1/2 * dstride for acc/uy/uyx) */
@@ -431,6 +436,194 @@ __global__ void __launch_bounds__(BX *BY, (FLAGS & (VF_CORR | VF_HESS)) ? VSTEP_
                            blockIdx.z, blockIdx.y * gridDim.x + blockIdx.x);
 }
 
+/*
+ * The velocity step for R vertically adjacent rows per thread (j0 .. j0+R-1,
+ * the same 4 points in x): the syz column window of the rows overlaps, so R
+ * rows need 2H+R-1 syz rows instead of 2H*R, and every load of all R rows is
+ * issued before the first computation.  Per point the arithmetic, CPML,
+ * injection, sampling and stores are those of v_body (bit-identical).  The
+ * rows lie in one 128 x 8 tile of the injection / sampling lists.
+ */
+template <int FDO, int FLAGS, bool P2, int R>
+__device__ __forceinline__ void v_body_rows(const StepArgs &a, int nt_off, int i0, int j0, int slot)
+{
+    constexpr int H = FDO / 2;
+    constexpr int NL = (H + 3) / 4;
+    constexpr int NR = (H - 1 + 3) / 4;
+    constexpr int NXS = 4 * (NL + 1 + NR);
+    if (i0 > a.nx || j0 > a.ny) return;
+    const int nt = *a.nt_base + nt_off;
+    const long long so = (long long)slot * a.slot_stride;
+    const int pitch = a.pitch;
+    const int col0 = i0 - 1 + HX;
+    const int tile = ((j0 - 1) / BY) * a.tl.ntx + (i0 - 1) / (4 * BX);
+    const int nrows = min(R, a.ny - j0 + 1);
+
+    /* ---- loads of data the preceding stress kernel does not write ---- */
+    float4 b4[R], vy4[R], g4[R], h4[R], f4[R];
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        if (r < nrows) {
+            const long long drow = (long long)(j0 + r - 1) * pitch;
+            b4[r] = ldg4(a.brho + drow + col0);
+            vy4[r] = ld4(a.vy + so + (long long)(j0 + r - 1 + a.hy) * pitch + col0);
+            if (FLAGS & VF_CORR) g4[r] = ld4(a.grho + so + drow + col0);
+            if (FLAGS & VF_HESS) h4[r] = ld4(a.hrho + so + drow + col0);
+        }
+    }
+    int tg0 = 0, tg1 = 0, tr0 = 0, tr1 = 0;
+    if (a.tl.on) {
+        const int *go = a.tl.goff + (long long)slot * (a.tl.ntiles + 1) + tile;
+        tg0 = __ldg(go); tg1 = __ldg(go + 1);
+        if (a.tl.sample) {
+            const int *ro = a.tl.roff + (long long)slot * (a.tl.ntiles + 1) + tile;
+            tr0 = __ldg(ro); tr1 = __ldg(ro + 1);
+        }
+    }
+    if (nt > a.nt_last) return;
+    if (FLAGS & VF_CORR) {
+        const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
+        const float *fb = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + col0;
+#pragma unroll
+        for (int r = 0; r < R; r++)
+            if (r < nrows) f4[r] = ldcs4(fb + (long long)(j0 + r - 1) * pitch);
+    }
+    pdl_wait();
+    pdl_trigger();
+
+    /* ---- stress taps: sxy of each row, the shared syz column window ---- */
+    float xs[R][NXS];
+    float4 ys[2 * H + R - 1];                /* syz rows j0-H .. j0+H+R-2 */
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        if (r < nrows) {
+            const float *row = a.sxy + so + (long long)(j0 + r - 1 + a.hy) * pitch + col0 - 4 * NL;
+#pragma unroll
+            for (int v = 0; v < NL + 1 + NR; v++) {
+                const float4 t = ld4(row + 4 * v);
+                xs[r][4 * v] = t.x; xs[r][4 * v + 1] = t.y; xs[r][4 * v + 2] = t.z; xs[r][4 * v + 3] = t.w;
+            }
+        }
+    }
+    {
+        const float *col = a.syz + so + (long long)(j0 - 1 + a.hy - H) * pitch + col0;
+#pragma unroll
+        for (int q = 0; q < 2 * H + R - 1; q++)
+            if (q < 2 * H + nrows - 1) ys[q] = ld4(col + (long long)q * pitch);
+    }
+
+    const int nvalid = min(4, a.nx - i0 + 1);
+#pragma unroll
+    for (int r = 0; r < R; r++) {
+        if (r >= nrows) break;
+        const int j = j0 + r;
+        const long long hrow = (long long)(j - 1 + a.hy) * pitch;
+        const long long drow = (long long)(j - 1) * pitch;
+        float4 acc4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 old4 = vy4[r];
+        const bool in_pml = a.fw > 0 && (i0 <= a.fw || i0 + 3 >= a.nx - a.fw + 1 || (!a.free_surf && j <= a.fw) ||
+                                         j >= a.ny - a.fw + 1);
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int i = i0 + k;
+            float sxy_x, syy_y;
+#pragma unroll
+            for (int m = 1; m <= H; m++) {
+                const int my = (FDO == 12 && m == 6 && a.fd12_compat) ? 5 : m;
+                float tx = a.hc[m] * (xs[r][4 * NL + k + m - 1] - xs[r][4 * NL + k - m]);
+                float ty = a.hc[my] * (get(ys[r + H + m - 1], k) - get(ys[r + H - m], k));
+                if (m == 1) { sxy_x = tx; syy_y = ty; }
+                else { sxy_x = sxy_x + tx; syy_y = syy_y + ty; }
+            }
+            const int fw = a.fw;
+            if (in_pml && i <= a.nx) {
+                if (i <= fw) {
+                    float *p = a.psi_vxx + so + (long long)(j - 1) * 2 * fw + (i - 1);
+                    float ps = __ldg(a.pml.b_x + i) * *p + __ldg(a.pml.a_x + i) * sxy_x;
+                    *p = ps;
+                    sxy_x = sxy_x / __ldg(a.pml.K_x + i) + ps;
+                }
+                if (i >= a.nx - fw + 1) {
+                    const int h1 = i - a.nx + 2 * fw;
+                    float *p = a.psi_vxx + so + (long long)(j - 1) * 2 * fw + (h1 - 1);
+                    float ps = __ldg(a.pml.b_x + h1) * *p + __ldg(a.pml.a_x + h1) * sxy_x;
+                    *p = ps;
+                    sxy_x = sxy_x / __ldg(a.pml.K_x + h1) + ps;
+                }
+                if (!a.free_surf && j <= fw) {
+                    float *p = a.psi_vyy_v + so + (long long)(j - 1) * pitch + (col0 + k);
+                    float ps = __ldg(a.pml.b_y + j) * *p + __ldg(a.pml.a_y + j) * syy_y;
+                    *p = ps;
+                    syy_y = syy_y / __ldg(a.pml.K_y + j) + ps;
+                }
+                if (j >= a.ny - fw + 1) {
+                    const int h1 = j - a.ny + 2 * fw;
+                    float *p = a.psi_vyy_v + so + (long long)(h1 - 1) * pitch + (col0 + k);
+                    float ps = __ldg(a.pml.b_y + h1) * *p + __ldg(a.pml.a_y + h1) * syy_y;
+                    *p = ps;
+                    syy_y = syy_y / __ldg(a.pml.K_y + h1) + ps;
+                }
+            }
+            const float b = get(b4[r], k);
+            const float s = sxy_x + syy_y;
+            if (!(FLAGS & VF_ADJOINT)) set(acc4, k, div_dh<P2>(b * s, a));
+            set(vy4[r], k, get(vy4[r], k) + div_dh<P2>(b * a.dt * s, a));
+        }
+
+        for (int g = tg0; g < tg1; g++) {
+            const int pk = __ldg(a.tl.gpt + g);
+            const int gi = pk & 0xffff, gj = pk >> 16;
+            if (gj == j && gi >= i0 && gi < i0 + 4) {
+                float v = lane(vy4[r], gi - i0);
+                const float *sg = a.tl.sig + a.tl.sig_off[slot] + (long long)(nt - 1) * a.tl.sig_ts;
+                for (int e = __ldg(a.tl.gbeg + g); e < __ldg(a.tl.gbeg + g + 1); e++)
+                    v = v + sg[(long long)__ldg(a.tl.src_id + e) * a.tl.sig_ss];
+                set_lane(vy4[r], gi - i0, v);
+            }
+        }
+        if (tr1 > tr0) {
+            const int r0 = a.tl.rec_off[slot], ntr = a.tl.rec_off[slot + 1] - r0;
+            float *sm = a.tl.seis + a.tl.seis_off[slot] + (long long)(nt - 1) * ntr;
+            for (int e = tr0; e < tr1; e++) {
+                const int pk = __ldg(a.tl.rpt + e);
+                const int ri = pk & 0xffff, rj = pk >> 16;
+                if (rj == j && ri >= i0 && ri < i0 + 4) sm[__ldg(a.tl.rid + e)] = lane(vy4[r], ri - i0);
+            }
+        }
+
+        st4m(a.vy + so + hrow + col0, vy4[r], nvalid);
+        if (FLAGS & VF_ACC_OUT) st4m(a.out_acc + so + hrow + col0, (FLAGS & VF_ADJOINT) ? old4 : acc4, nvalid);
+        if (FLAGS & VF_CORR) {
+            float4 g = g4[r];
+            const float4 f = f4[r];
+            g.x = g.x + (old4.x * f.x); g.y = g.y + (old4.y * f.y);
+            g.z = g.z + (old4.z * f.z); g.w = g.w + (old4.w * f.w);
+            st4m(a.grho + so + drow + col0, g, nvalid);
+        }
+        if (!(FLAGS & VF_ADJOINT) && a.fwd && !(FLAGS & VF_CORR)) {
+            const long long k = store_idx(nt - 1, a.fwd_mod);
+            st4ms(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0, acc4, nvalid);
+        }
+        if ((FLAGS & VF_HESS) && nt < a.nt_total) {
+            float4 h = h4[r];
+            h.x = h.x + (acc4.x * acc4.x); h.y = h.y + (acc4.y * acc4.y);
+            h.z = h.z + (acc4.z * acc4.z); h.w = h.w + (acc4.w * acc4.w);
+            st4m(a.hrho + so + drow + col0, h, nvalid);
+        }
+    }
+}
+
+/* R rows per thread: a block of 32 x (8/R) threads covers a 128 x 8 tile */
+#ifndef VSTEP_R2_MIN_BLOCKS
+#define VSTEP_R2_MIN_BLOCKS 5
+#endif
+template <int FDO, int FLAGS, bool P2>
+__global__ void __launch_bounds__(BX *BY / 2, VSTEP_R2_MIN_BLOCKS) v_step_r2(StepArgs a, int nt_off)
+{
+    v_body_rows<FDO, FLAGS, P2, 2>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x),
+                                   1 + blockIdx.y * BY + 2 * threadIdx.y, blockIdx.z);
+}
+
 /* The velocity step with the block's stress taps staged in shared memory
  * first: 8 sxy rows of 128 + 4*(NL+NR) points and 8+2H-1 syz rows of 128
  * points, loaded once per block (about 3 float4 loads per thread instead of
@@ -506,6 +699,8 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     float4 c1, c2;                           /* uip/ujp (elastic) or fipjp/f (visc) */
     float4 rr[LL], qq[LL], dip4[LL], d4[LL];
     float4 mi4, mj4, ti4, tj4;               /* muip, mujp, tausipjp, taus */
+    float4 sold_r, sold_q, qsx, qsy;         /* Qs gradient: memory sums before the update, sensitivities */
+    float4 ex4, ey4, gx4, gy4, dsx4, dsy4;   /* Qs gradient, adjoint: strains, sums, stored sensitivities */
     if (L == 0) {
         c1 = ldg4(a.uip + drow + col0);
         c2 = ldg4(a.ujp + drow + col0);
@@ -540,6 +735,16 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
         const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
         fy = ldcs4(base + a.dstride);
         fu = ldcs4(base + 2 * a.dstride);
+        if (FLAGS & SF_CORRQ) {
+            dsx4 = ldcs4(base + 3 * a.dstride);
+            dsy4 = ldcs4(base + 4 * a.dstride);
+        }
+    }
+    if (FLAGS & SF_CORRQ) {
+        ex4 = ld4(a.exy + so + drow + col0);
+        ey4 = ld4(a.eyz + so + drow + col0);
+        gx4 = ld4(a.gqx + so + drow + col0);
+        gy4 = ld4(a.gqy + so + drow + col0);
     }
     pdl_wait();                              /* velocities of this step are complete */
     pdl_trigger();
@@ -649,6 +854,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
             set(sxy4, k, get(sxy4, k) + ((get(c1, k) * get(vyx4, k)) + (a.dthalbe * get(sumr4, k))));
             set(syz4, k, get(syz4, k) + ((get(c2, k) * get(vyy4, k)) + (a.dthalbe * get(sumq4, k))));
         }
+        if (FLAGS & SF_QSENS) { sold_r = sumr4; sold_q = sumq4; }
         sumr4 = make_float4(0.f, 0.f, 0.f, 0.f);
         sumq4 = sumr4;
 #pragma unroll
@@ -670,6 +876,22 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
         for (int k = 0; k < 4; k++) {
             set(sxy4, k, get(sxy4, k) + (a.dthalbe * get(sumr4, k)));
             set(syz4, k, get(syz4, k) + (a.dthalbe * get(sumq4, k)));
+        }
+        if (FLAGS & SF_QSENS) {
+            /* d(stress increment)/d(tau) with the strain history held fixed:
+               dfipjp/dtau = muip DT (L - sumu) / (1 + sumu tau), and every memory
+               variable scales with its dip_l, whose log-derivative is
+               1 / (tau (1 + sumu tau)) (prepare_update_s.c:40-55) */
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const float tx = get(ti4, k), ty = get(tj4, k);
+                const float denx = 1.0f + a.sumu * tx, deny = 1.0f + a.sumu * ty;
+                const float ax = ((get(mi4, k) * a.dt) * (a.lf - a.sumu)) / denx;
+                const float ay = ((get(mj4, k) * a.dt) * (a.lf - a.sumu)) / deny;
+                const float kx = a.dthalbe / (tx * denx), ky = a.dthalbe / (ty * deny);
+                set(qsx, k, (ax * get(vyx4, k)) + (kx * (get(sold_r, k) + get(sumr4, k))));
+                set(qsy, k, (ay * get(vyy4, k)) + (ky * (get(sold_q, k) + get(sumq4, k))));
+            }
         }
     }
 
@@ -696,6 +918,10 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
             float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
             st4ms(base + a.dstride, vyy4, nvalid);
             st4ms(base + 2 * a.dstride, vyx4, nvalid);
+            if ((FLAGS & SF_QSENS) && L > 0) {
+                st4ms(base + 3 * a.dstride, qsx, nvalid);
+                st4ms(base + 4 * a.dstride, qsy, nvalid);
+            }
         }
     }
     if (a.ws) {                       /* energy W += vy^2 (eprecond.c:11); vy at the point is xs[4NL+k] */
@@ -711,6 +937,20 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
         for (int kk = 0; kk < 4; kk++)
             set(g4, kk, get(g4, kk) + ((get(fu, kk) * get(sxy4, kk)) + (get(fy, kk) * get(syz4, kk))));
         st4m(a.gu + so + drow + col0, g4, nvalid);
+    }
+    if (FLAGS & SF_CORRQ) {           /* Qs gradient: adjoint strain of the earlier adjoint steps times the
+                                         stored sensitivity of forward step NT-nt+1, then this step's strain */
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            set(gx4, k, get(gx4, k) + (get(ex4, k) * get(dsx4, k)));
+            set(gy4, k, get(gy4, k) + (get(ey4, k) * get(dsy4, k)));
+            set(ex4, k, get(ex4, k) + (get(vyx4, k) * a.dt));
+            set(ey4, k, get(ey4, k) + (get(vyy4, k) * a.dt));
+        }
+        st4m(a.gqx + so + drow + col0, gx4, nvalid);
+        st4m(a.gqy + so + drow + col0, gy4, nvalid);
+        st4m(a.exy + so + drow + col0, ex4, nvalid);
+        st4m(a.eyz + so + drow + col0, ey4, nvalid);
     }
     if ((FLAGS & SF_HESS) && nt < a.nt_total) {
 #pragma unroll

@@ -341,6 +341,18 @@ int dsh_setup_visc_base(int nx, int ny, int l, const float *fl, float dt, const 
     return 0;
 }
 
+float dsh_setup_sumu(int l, const float *fl)
+{
+    float tau_sls[DSH_MAX_L], omega, sumu = 0.0;
+    int m;
+    if (l < 1 || l > DSH_MAX_L) return 0.0f;
+    for (m = 0; m < l; m++) tau_sls[m] = 1.0 / (2.0 * DSH_PI * fl[m]);
+    omega = 2.0 * DSH_PI * fl[0];
+    for (m = 0; m < l; m++)
+        sumu = sumu + ((omega * omega * tau_sls[m] * tau_sls[m]) / (1.0 + omega * omega * tau_sls[m] * tau_sls[m]));
+    return sumu;
+}
+
 int dsh_setup_wavelet(int quellart, int nt, float dt, int nsrc, const float *srcpos8, float *out)
 {
     int it, s;

@@ -41,6 +41,9 @@ int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const floa
                     const float *qs, float *brho, float *uip, float *ujp, float *fipjp, float *f, float *dip,
                     float *d, float *bip, float *bjm, float *cip, float *cjm, float *cnorm);
 
+/* sum_l w^2 tau_l^2 / (1 + w^2 tau_l^2), w = 2 pi FL[1] (prepare_update_s.c:24-32), as
+ * dsh_setup_visc_base forms it */
+float dsh_setup_sumu(int l, const float *fl);
 /* The per-point factors from which every viscoelastic coefficient is a
  * product (src/prepare_update_s.c:43-57): relaxed moduli muip/mujp at the
  * two stress positions, tau at (i+1/2, j+1/2) and (i, j+1/2) (av_tau), and

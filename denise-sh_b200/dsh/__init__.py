@@ -41,7 +41,7 @@ class Params(C.Structure):
                 ("damping", C.c_float), ("fpml", C.c_float), ("npower", C.c_float), ("k_max_pml", C.c_float),
                 ("l", C.c_int), ("fl", C.c_float * 8), ("quellart", C.c_int), ("eprecond", C.c_int),
                 ("max_shots", C.c_int), ("compat_fd12", C.c_int), ("mem_budget", C.c_longlong),
-                ("ckpt_every", C.c_int)]
+                ("ckpt_every", C.c_int), ("grad_q", C.c_int)]
 
 
 class ShotC(C.Structure):
@@ -103,6 +103,7 @@ def lib() -> C.CDLL:
         L.dsh_set_shot_taper.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_float, C.c_int]
         L.dsh_set_misfit.argtypes = [C.c_void_p, C.c_int]
         L.dsh_set_wait_limits.argtypes = [C.c_void_p, C.c_longlong, C.c_double]
+        L.dsh_get_gradient_q.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         L.dsh_set_step_variant.argtypes = [C.c_void_p, C.c_int]
         L.dsh_batch_set_host_timeout.argtypes = [C.c_void_p, C.c_double]
         L.dsh_autotune.argtypes = [C.c_void_p, C.POINTER(ShotC), C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int)]
@@ -257,6 +258,12 @@ class Engine:
             out["seis"] = _split(seis, shots, self.p.nt)
         if want_energy:
             out["Ws"], out["Wr"] = ws, wr
+        return out
+
+    def gradient_q(self):
+        """dJ/dQs [ny, nx] of the last gradient (params.grad_q = 1; J = the returned L2 misfit)."""
+        out = np.zeros(self.shape, np.float32)
+        _check(lib().dsh_get_gradient_q(self.h, out.ctypes.data, None), "dsh_get_gradient_q")
         return out
 
     def gradient_device(self, shots, obs_dev_ptr: int, g_vs_ptr: int, g_rho_ptr: int) -> float:

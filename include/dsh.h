@@ -72,6 +72,9 @@ typedef struct dsh_params {
     int ckpt_every;           /* > 0: always checkpoint-and-recompute, one checkpoint every
                                  ckpt_every steps (e.g. ceil(sqrt(NT))), whatever the budget;
                                  0 = the automatic choice above */
+    int grad_q;               /* 1: dsh_gradient also forms the gradient with respect to Qs
+                                 (L > 0 only; read it with dsh_get_gradient_q).  The forward
+                                 pass then stores 5 fields per step instead of 3 */
 } dsh_params;
 
 /* One shot (one source gather). */
@@ -129,6 +132,21 @@ int dsh_hessian_diag(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *h_v
  * host data as above (uploaded once per distinct geometry). */
 int dsh_gradient_device(dsh_ctx *ctx, const dsh_shot *shots, int nshots, const float *obs_dev, float *g_vs_dev,
                         float *g_rho_dev, double *l2);
+
+/* Gradient of the misfit J = sum over shots, traces and samples of res^2 (the
+ * L2 value dsh_gradient returns, LNORM=2) with respect to the quality factor
+ * Qs at every grid point, from the last dsh_gradient / dsh_gradient_device
+ * call of a context created with grad_q = 1.  No counterpart in the
+ * reference, which inverts vs and rho only.  It is the exact sensitivity of
+ * the discrete viscoelastic update (prepare_update_s.c:40-55 through
+ * tau = 2/Qs, readmod.c:99, and the four-point tau average, av_tau.c:12) to
+ * the back-propagated wavefield: per forward step the stress increment's
+ * derivative with respect to tau, with the strain history held fixed, is
+ * stored next to the strains, and the adjoint pass correlates it with the
+ * adjoint strain; it is neither energy-preconditioned nor scaled.  g_qs_host
+ * and/or g_qs_dev receive [ny][nx] floats.  DSH_ERR_STATE when there is no
+ * such gradient yet. */
+int dsh_get_gradient_q(dsh_ctx *ctx, float *g_qs_host, float *g_qs_dev);
 
 /* Device-resident forward: seis_dev receives [nshots][ntr][nt]. */
 int dsh_forward_device(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *seis_dev);

@@ -64,7 +64,10 @@ static struct {
     float K_y[64 + 1], a_y[64 + 1], b_y[64 + 1], K_y_half[64 + 1], a_y_half[64 + 1], b_y_half[64 + 1];
     float d_x[64 + 1], d_x_half[64 + 1], d_y[64 + 1], d_y_half[64 + 1];
     float *vs, *rho, *uip, *ujp, *taus, *tausipjp, *fipjp, *f, *dip, *d; /* dense [NY][NX] ([L][NY][NX]) */
+    float *muip, *mujp, *qs;                    /* relaxed-modulus factors and Qs (Q gradient) */
     float bip[8], bjm[8], cip[8], cjm[8], eta[8];
+    float sumu;                                 /* prepare_update_s.c:29-32 */
+    int grad_q;                                 /* accumulate the Qs gradient (dsho_set_grad_q) */
     float c_vs, c_rho;
     int ntr, *recpos;
 } G = {.fd12_compat = 1, .lnorm = 2};
@@ -81,6 +84,7 @@ static struct {
 #undef SFX
 
 void dsho_set_fd12_compat(int on) { G.fd12_compat = on; }
+void dsho_set_grad_q(int on) { G.grad_q = on; }
 int dsho_set_lnorm(int lnorm)
 {
     if (lnorm < 1 || lnorm > 5) return -1;
@@ -94,7 +98,9 @@ void dsho_free(void)
     state_free_f64();
     free(G.vs); free(G.rho); free(G.uip); free(G.ujp); free(G.taus); free(G.tausipjp);
     free(G.fipjp); free(G.f); free(G.dip); free(G.d); free(G.recpos);
+    free(G.muip); free(G.mujp); free(G.qs);
     G.vs = G.rho = G.uip = G.ujp = G.taus = G.tausipjp = G.fipjp = G.f = G.dip = G.d = NULL;
+    G.muip = G.mujp = G.qs = NULL;
     G.recpos = NULL;
     G.alive = 0;
 }
@@ -298,6 +304,8 @@ int dsho_init(const dsho_params *p, const float *vs, const float *rho, const flo
         G.taus = malloc(n * sizeof(float)); G.tausipjp = malloc(n * sizeof(float));
         G.fipjp = malloc(n * sizeof(float)); G.f = malloc(n * sizeof(float));
         G.dip = malloc(n * G.l * sizeof(float)); G.d = malloc(n * G.l * sizeof(float));
+        G.muip = malloc(n * sizeof(float)); G.mujp = malloc(n * sizeof(float)); G.qs = malloc(n * sizeof(float));
+        memcpy(G.qs, qs, n * sizeof(float));
         for (k = 0; k < (int)n; k++) G.taus[k] = 2.0 / qs[k];                 /* readmod.c:99 */
         for (l = 0; l < G.l; l++) {                                            /* readmod.c:30-33 */
             float p_ = 1.0 / (2.0 * ORACLE_PI * G.fl[l]);
@@ -317,9 +325,12 @@ int dsho_init(const dsho_params *p, const float *vs, const float *rho, const flo
             G.cip[l] = 1.0 - (G.eta[l] * 0.5);
             G.cjm[l] = 1.0 - (G.eta[l] * 0.5);
         }
+        G.sumu = sumu;
         for (k = 0; k < (int)n; k++) {
             float mujp = G.ujp[k] / (1.0 + sumu * G.taus[k]);
             float muip = G.uip[k] / (1.0 + sumu * G.tausipjp[k]);
+            G.muip[k] = muip;
+            G.mujp[k] = mujp;
             G.fipjp[k] = muip * G.dt * (1.0 + G.l * G.tausipjp[k]);
             G.f[k] = mujp * G.dt * (1.0 + G.l * G.taus[k]);
             for (l = 0; l < G.l; l++) {
@@ -559,6 +570,36 @@ int dsho_convert(const float *wu, const float *wrho, float *g_vs, float *g_rho)
             waveconv_rho = (G.vs[o] * G.vs[o] * waveconv_mu) + waveconv_rho_s;
             g_vs[o] = waveconv_u;
             g_rho[o] = waveconv_rho;
+        }
+    return 0;
+}
+
+/* Gradient of the misfit J = sum res^2 with respect to Qs after one shot's
+ * forward (stored) + residual + adjoint with dsho_set_grad_q(1) (no
+ * counterpart in the reference, which has no Q gradient).  The velocity-stress
+ * Lagrangian gives the stress multiplier of forward update k as (2/rho) times
+ * the back-propagated adjoint strain e, so dJ/dtau_ipjp = -(2/rho) sum e dsx
+ * and dJ/dtau = -(2/rho) sum e dsy; tau_ipjp is the four-point average of tau
+ * (av_tau.c:12, one-rank periodic wrap), and tau = 2/Qs (readmod.c:99). */
+int dsho_get_grad_q(double *g_qs)
+{
+    const int NX = G.nx, NY = G.ny;
+    int i, j;
+    if (!G.alive || G.l < 1 || !G.grad_q) return -1;
+    for (j = 1; j <= NY; j++)
+        for (i = 1; i <= NX; i++) {
+            const int im = i > 1 ? i - 1 : NX, jm = j > 1 ? j - 1 : NY;
+            const size_t o = (size_t)(j - 1) * NX + (i - 1);
+            const size_t nb[4] = {o, (size_t)(j - 1) * NX + (im - 1), (size_t)(jm - 1) * NX + (i - 1),
+                                  (size_t)(jm - 1) * NX + (im - 1)};
+            double gx = 0.0, gy;
+            int k;
+            for (k = 0; k < 4; k++) {
+                const double q = G.fp64 ? st_f64.gqx[nb[k]] : (double)st_f32.gqx[nb[k]];
+                gx += -2.0 / (double)G.rho[nb[k]] * q;
+            }
+            gy = -2.0 / (double)G.rho[o] * (G.fp64 ? st_f64.gqy[o] : (double)st_f32.gqy[o]);
+            g_qs[o] = (gy + 0.25 * gx) * (-2.0 / ((double)G.qs[o] * (double)G.qs[o]));
         }
     return 0;
 }

@@ -49,6 +49,10 @@ int dsho_adjoint(const float *adj, int nsteps);
 int dsho_eprecond_scale(void);
 int dsho_convert(const float *wu, const float *wrho, float *g_vs, float *g_rho);
 int dsho_hessian_out(float *h_vs, float *h_rho);
+/* Qs gradient (no counterpart in the reference): set before dsho_init, read
+ * after the adjoint of one shot (dJ/dQs, J = sum res^2, double [NY][NX]) */
+void dsho_set_grad_q(int on);
+int dsho_get_grad_q(double *g_qs);
 int dsho_psource(int nt, float *sxx, float *syy, int nsrc, const float *srcpos8, const float *signals);
 
 /* SPATFILTER=3 gradient smoothing (src/gauss_filt.c) */

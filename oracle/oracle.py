@@ -106,7 +106,8 @@ def _ptr(a, t=C.c_float):
 class Oracle:
     """A CPU oracle session for one model (one process-wide session per backend)."""
 
-    def __init__(self, model: Model, kind: str = "ref", fp64: bool = False, fd12_compat: bool = True):
+    def __init__(self, model: Model, kind: str = "ref", fp64: bool = False, fd12_compat: bool = True,
+                 grad_q: bool = False):
         self.kind, self.fp64, self.m = kind, fp64, model
         lib = {"ref": "libdenise_ref.so", "ref_fast": "libdenise_ref_fast.so", "port": "libdsh_oracle.so"}[kind]
         path = os.path.join(REF_DIR, lib)
@@ -122,8 +123,11 @@ class Oracle:
         qs = _f32(model.qs) if model.qs is not None else np.ones_like(vs)
         self._keep = (vs, rho, qs)
         self.params = model.params()
+        if grad_q and self.pre != "dsho_":
+            raise ValueError("the Qs gradient exists only in the restatement (the reference has none)")
         if self.pre == "dsho_":
             self.lib.dsho_set_fd12_compat(int(fd12_compat))
+            self.lib.dsho_set_grad_q(int(grad_q))
             rc = self.lib.dsho_init(C.byref(self.params), _ptr(vs), _ptr(rho), _ptr(qs), int(fp64))
         else:
             rc = self.lib.refh_init(C.byref(self.params), _ptr(vs), _ptr(rho), _ptr(qs))
@@ -236,6 +240,14 @@ class Oracle:
         gv, gr = np.zeros_like(a), np.zeros_like(b)
         self._fn("convert")(_ptr(a), _ptr(b), _ptr(gv), _ptr(gr))
         return gv, gr
+
+    def grad_q(self):
+        """dJ/dQs (J = sum res^2) of the last shot's adjoint, float64 [NY, NX]
+        (restatement only; the reference computes no Q gradient)."""
+        out = np.zeros((self.m.ny, self.m.nx), np.float64)
+        if self.lib.dsho_get_grad_q(_ptr(out, C.c_double)) != 0:
+            raise RuntimeError("no Qs gradient (needs L > 0 and grad_q=True)")
+        return out
 
     def hessian_out(self):
         hv = np.zeros((self.m.ny, self.m.nx), np.float32)
