@@ -764,17 +764,6 @@ def bench_batch(a, rank, world, local):
         dist.destroy_process_group()
 
 
-def time_to_reach(hist, target):
-    """GPU-seconds after which the misfit is <= target: iteration k's model
-    update is done at hist[k]['gpu_s'] and its misfit is hist[k+1]['misfit']."""
-    if hist[0]["misfit"] <= target:
-        return 0.0
-    for k in range(len(hist) - 1):
-        if hist[k + 1]["misfit"] <= target:
-            return hist[k]["gpu_s"]
-    return None
-
-
 def bench_learned(a, rank, world, local):
     """C5: training set from the solver, U-Net training, plain vs learned FWI."""
     import numpy as np
@@ -848,7 +837,7 @@ def bench_learned(a, rank, world, local):
         for key, m, net in runs:
             ws = time.time()
             hl, _ = fwi.run(prob, a.fwi_iters, method=m, net=net, torch=torch, target_misfit=target, log=log)
-            t = time_to_reach(hl, target)
+            t = fwi.time_to_reach(hl, target)
             res[key] = {"final_misfit": hl[-1]["misfit"], "gpu_s_to_target": t, "gpu_s_total": hl[-1]["gpu_s"],
                         "ratio": (t / t_plain) if t is not None else None,
                         "wall_ratio": ((time.time() - ws) / (w1 - w0)) if t is not None else None,

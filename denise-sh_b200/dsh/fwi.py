@@ -53,6 +53,12 @@ def _setup():
                                               C.c_void_p, C.POINTER(C.c_int)]
         L.dsh_calc_mres.restype = C.c_float
         L.dsh_calc_mres.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
+        L.dsh_vec_work_doubles.restype = C.c_longlong
+        L.dsh_vec_work_doubles.argtypes = [C.c_int]
+        L.dsh_lbfgs_direction_device.argtypes = [C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
+                                                 C.c_void_p, C.c_void_p, C.c_void_p]
+        L.dsh_pcg_direction_device.argtypes = [C.c_longlong, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                               C.c_void_p, C.c_void_p, C.c_void_p]
         L._fwi_ready = True
     return L
 
@@ -157,6 +163,40 @@ def lbfgs_direction(S, Y, q):
 PCG_BETA = {"fletcher_reeves": 1, "polak_ribiere": 2, "hestenes_stiefel": 3, "dai_yuan": 4}
 
 
+def _work(torch, count):
+    n = int(_setup().dsh_vec_work_doubles(count))
+    return torch.empty(n, dtype=torch.float64, device="cuda")
+
+
+def lbfgs_direction_device(torch, S, Y, q, stream=None):
+    """The two-loop recursion on the device (dsh_lbfgs_direction_device):
+    S, Y are float32 CUDA tensors [count][n] (oldest first, may be empty), q
+    [n]; returns r = H q as a new tensor on q's device."""
+    q = q.contiguous().view(-1)
+    count = int(S.shape[0]) if S is not None and S.dim() == 2 else 0
+    r = torch.empty_like(q)
+    w = _work(torch, count)
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    _check(_setup().dsh_lbfgs_direction_device(q.numel(), count, S.contiguous().data_ptr() if count else None,
+                                               Y.contiguous().data_ptr() if count else None, q.data_ptr(),
+                                               r.data_ptr(), w.data_ptr(), st), "dsh_lbfgs_direction_device")
+    return r
+
+
+def pcg_direction_device(torch, g_new, g_old, direction, beta="polak_ribiere", stream=None):
+    """The conjugate-gradient direction on the device (dsh_pcg_direction_device):
+    float32 CUDA tensors [nclass][...]; direction is updated in place; returns
+    (direction, beta per class as a CUDA tensor)."""
+    nclass = int(g_new.shape[0])
+    betas = torch.zeros(nclass, dtype=torch.float32, device=g_new.device)
+    w = _work(torch, 0)
+    st = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    _check(_setup().dsh_pcg_direction_device(g_new.numel() // nclass, nclass, g_new.contiguous().data_ptr(),
+                                             g_old.contiguous().data_ptr(), direction.data_ptr(), PCG_BETA[beta],
+                                             betas.data_ptr(), w.data_ptr(), st), "dsh_pcg_direction_device")
+    return direction, betas
+
+
 def pcg_direction(g_new, g_old, direction, beta="polak_ribiere"):
     """Conjugate-gradient direction (src/PCG.c): g_new, g_old, direction are
     [nclass][...] arrays (one parameter class per leading index, e.g. vs and
@@ -196,6 +236,18 @@ def line_search(misfit, L2_now, eps_scale=0.01, scalefac=2.0, stepmax=6):
         if rc == 1:
             continue
         return (float(eps.value) if rc == 0 else 0.0), tests
+
+
+def time_to_reach(hist, target):
+    """GPU-seconds after which the misfit of a run() history is <= target:
+    iteration k's model update is done at hist[k]['gpu_s'] and its misfit is
+    hist[k+1]['misfit']; None when the run never gets there."""
+    if hist[0]["misfit"] <= target:
+        return 0.0
+    for k in range(len(hist) - 1):
+        if hist[k + 1]["misfit"] <= target:
+            return hist[k]["gpu_s"]
+    return None
 
 
 def l2_misfit(syn, obs):
@@ -270,7 +322,7 @@ METHODS = ("plain", "learned", "learned_sym", "hessian", "energy_src")
 
 
 def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, scalefac=2.0, stepmax=6, nlbfgs=5,
-        vmin=None, vmax=None, target_misfit=None, log=None):
+        vmin=None, vmax=None, target_misfit=None, log=None, device_vectors=False):
     """FWI iterations; returns the history [{iter, misfit, gpu_s, eps, tests, fallback}].
     method
       "plain"        EPRECOND=1 gradient (per-shot g / (sqrt(Ws Wr) + 0.005 max), src/eprecond1.c)
@@ -283,9 +335,16 @@ def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, sc
       "energy_src"   raw gradient / (Ws + 0.005 max Ws): the forward energy alone in place
                      of the Hessian (what a "log_h_over_ws" network corrects; no network)
     The learned methods fall back to a plain gradient when the line search
-    rejects their step."""
+    rejects their step.
+    device_vectors (plain method, needs torch): the observed data stay in HBM,
+    the gradient is formed by dsh_gradient_device and the L-BFGS pairs and the
+    two-loop recursion run on the device (dsh_lbfgs_direction_device); only
+    the search direction is copied to the host, once per iteration, for the
+    model update that dsh_set_model takes from host memory."""
     if method not in METHODS:
         raise ValueError(method)
+    if device_vectors and (method != "plain" or torch is None):
+        raise ValueError("device_vectors needs the plain method and torch")
     if problem.obs is None:
         problem.observe()
     shots, obs = problem.shots, problem.obs
@@ -300,7 +359,22 @@ def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, sc
     hist = []
     fwd_eng = problem.engine(1)
 
+    if device_vectors:
+        obs_dev = torch.from_numpy(np.ascontiguousarray(np.concatenate([o.ravel() for o in obs]))).cuda()
+        g_dev = torch.empty(vs.size, dtype=torch.float32, device="cuda")
+        gr_dev = torch.empty_like(g_dev)
+
+    def gradient_dev():
+        eng = problem.engine(1)
+        eng.set_model(vs, problem.rho, problem.qs)
+        l2 = eng.gradient_device(shots, obs_dev.data_ptr(), g_dev.data_ptr(), gr_dev.data_ptr())
+        clock.add_engine(eng)
+        l2_test = float(eng.shot_misfits(len(shots))[test].sum())
+        return g_dev.clone(), l2, l2_test
+
     def gradient(kind):
+        if device_vectors:
+            return gradient_dev()
         eng = problem.engine(1 if kind == "plain" else 10)
         eng.set_model(vs, problem.rho, problem.qs)
         out = eng.gradient(shots, obs)
@@ -344,6 +418,19 @@ def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, sc
         q, l2, l2_test = gradient(kind)
         fallback = False
         for attempt in range(2):
+            if device_vectors:           # pairs, recursion and descent test on the device
+                qn = c_vs * q.view(-1)
+                if prev is not None:
+                    S.append(((torch.from_numpy(vs).cuda() - prev[0]).view(-1) / c_vs).contiguous())
+                    Y.append((qn - prev[1]).contiguous())
+                    S, Y = S[-nlbfgs:], Y[-nlbfgs:]
+                d = lbfgs_direction_device(torch, torch.stack(S) if S else None, torch.stack(Y) if Y else None, qn)
+                if float(torch.dot(d.double(), qn.double())) <= 0.0:
+                    S, Y = [], []
+                    d = qn.clone()
+                d = d.cpu().numpy().reshape(vs.shape)
+                eps, tests = line_search(test_misfit(d), l2_test, eps_scale, scalefac, stepmax)
+                break
             qn = c_vs * q.ravel()
             if prev is not None and prev[2] == kind:
                 S.append(((vs - prev[0]).ravel() / c_vs).astype(np.float32))
@@ -364,7 +451,10 @@ def run(problem, niter, method="plain", net=None, torch=None, eps_scale=0.01, sc
             fallback, kind = True, "plain"
             S, Y = [], []
             q, l2, l2_test = gradient("plain")
-        prev = (vs.copy(), c_vs * q.ravel(), kind)
+        if device_vectors:
+            prev = (torch.from_numpy(vs.copy()).cuda(), c_vs * q.view(-1), kind)
+        else:
+            prev = (vs.copy(), c_vs * q.ravel(), kind)
         if eps > 0.0:
             vs = step_model(d, eps)
         rec = {"iter": it, "misfit": l2, "gpu_s": clock.seconds, "eps": eps, "tests": tests, "fallback": fallback,

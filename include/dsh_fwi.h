@@ -66,6 +66,24 @@ int dsh_smooth_model_median(int nx, int ny, int filt_size, const float *vs, cons
 int dsh_pcg_direction(long long n, int nclass, const float *g_new, const float *g_old, float *dir, int beta_kind,
                       float *beta_out);
 
+/* Device versions of dsh_lbfgs_direction and dsh_pcg_direction (no
+ * counterpart in the reference, whose optimiser runs on the host): every
+ * vector is a device array, the work runs on `stream` (a cudaStream_t as
+ * void*, NULL = the default stream) and nothing is allocated or copied to the
+ * host.  Same steps as the host functions; each dot product is a double sum
+ * over a fixed partition of the vector (296 blocks, then a fixed tree), so
+ * results are reproducible and agree with the host versions to float
+ * rounding.  work: dsh_vec_work_doubles(count) doubles of device memory that
+ * the call owns until its stream reaches the end of it (count = the L-BFGS
+ * pairs; also enough for any nclass of the PCG step).  The PCG betas go to
+ * beta_dev (nclass floats on the device) or, when NULL, stay in work.
+ * Returns DSH_ERR_PARAM for invalid arguments, DSH_ERR_CUDA when a launch fails. */
+long long dsh_vec_work_doubles(int count);
+int dsh_lbfgs_direction_device(long long n, int count, const float *S, const float *Y, const float *q, float *r,
+                               double *work, void *stream);
+int dsh_pcg_direction_device(long long n, int nclass, const float *g_new, const float *g_old, float *dir,
+                             int beta_kind, float *beta_dev, double *work, void *stream);
+
 /* epst[0..2], L2t[0..2]: test step lengths (epst[0] = 0) and their misfits */
 float dsh_opt_step(const float L2t[3], const float epst[3]);
 /* The same step as src/calc_opt_step.c:20-111 computes it, bit for bit: the

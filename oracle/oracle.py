@@ -26,6 +26,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
+# the reference source tree: $DSH_REFERENCE, by default a directory named
+# "reference" next to this repository's root
+DEFAULT_REFERENCE = os.path.abspath(os.path.join(HERE, "..", "..", "reference"))
 
 FIELD = {"vy": 0, "sxy": 1, "syz": 2, "vyp1": 3, "uy": 4, "uyx": 5, "uip": 6, "ujp": 7, "rho": 8, "vs": 9,
          "fipjp": 10, "f": 11, "Ws": 12, "Wr": 13, "We": 14, "g_u": 15, "g_rho": 16, "hess_u": 17,
@@ -82,7 +85,7 @@ class Model:
 def build(reference: str | None = None, quiet: bool = True) -> None:
     """Build the oracle libraries (the reference part only if its tree exists)."""
     targets = ["port"]
-    ref = reference or os.environ.get("DSH_REFERENCE", "/root/reference")
+    ref = reference or os.environ.get("DSH_REFERENCE", DEFAULT_REFERENCE)
     if os.path.isdir(os.path.join(ref, "src")):
         targets.insert(0, "ref")
     out = subprocess.run(["make", "-C", HERE, f"REF={ref}", *targets], capture_output=True, text=True)

@@ -87,3 +87,39 @@ def test_training_pairs_and_learned_fwi():
     assert hist[-1]["misfit"] < hist[0]["misfit"]
     assert hist_res[-1]["misfit"] < hist_res[0]["misfit"]
     assert all(np.isfinite(h["misfit"]) for h in hist_ws)     # a diagnostic; no descent guarantee
+
+
+def test_learned_preconditioner_against_plain_on_held_out_problem():
+    """A U-Net trained on solver-generated pairs of 16 models (seeds 100-115)
+    preconditions L-BFGS on a problem it has not seen (seed 41): it must reach
+    the plain EPRECOND=1 method's final misfit (within 1 %) in at most 0.7x
+    the plain method's GPU-seconds.  The network's prior without the network
+    (energy_src: g / (Ws + 0.005 max Ws)) is run on the same problem and its
+    ratio printed beside the learned one: the gain of the Hessian-shaped
+    preconditioner over plain comes mostly from that prior, and the network
+    (trained on the correction log(H / Ws)) is held to the bound, not to a
+    margin over the prior."""
+    from dsh import nn
+
+    cfg = _small_problem(nshots=8, nt=600, seed=41)
+    p = cfg["params"]
+    models = list(configs.training_models(count=16, first_seed=100, nx=p["nx"], ny=p["ny"]))
+    xs, ts = fwi.training_pairs(torch, models, p, cfg["shots"][::2])
+    net = nn.UNet(torch, seed=3)
+    net.target = "log_h_over_ws"
+    fwi.train(net, torch, xs, nn.residual_targets(torch, xs, ts), p["ny"], p["nx"], epochs=25, batch=2, lr=2e-3)
+    prob = fwi.Problem(cfg, test_shots=3)
+    try:
+        plain, _ = fwi.run(prob, 8, method="plain", eps_scale=0.02)
+        target = plain[-1]["misfit"] * 1.01
+        t_plain = plain[-1]["gpu_s"]
+        learned, _ = fwi.run(prob, 8, method="learned", net=net, torch=torch, eps_scale=0.02, target_misfit=target)
+        prior, _ = fwi.run(prob, 8, method="energy_src", eps_scale=0.02, target_misfit=target)
+    finally:
+        prob.close()
+    t_learned, t_prior = fwi.time_to_reach(learned, target), fwi.time_to_reach(prior, target)
+    r_learned = None if t_learned is None else t_learned / t_plain
+    r_prior = None if t_prior is None else t_prior / t_plain
+    print(f"held-out seed 41: plain {len(plain) - 1} it, final misfit {plain[-1]['misfit']:.4g}, {t_plain:.3f} GPU-s; "
+          f"learned ratio {r_learned}, energy_src ratio {r_prior}")
+    assert r_learned is not None and r_learned <= 0.7
