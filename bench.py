@@ -137,6 +137,17 @@ def kernel_bytes(l, store=True):
     return v, s
 
 
+def kernel_bytes_adjoint(l):
+    """Per-point bytes of the adjoint pass's velocity and stress launches:
+    velocity vy R/W, sxy+syz R, 1/rho R, stored acceleration R, g_rho R/W;
+    stress sxy/syz R/W, r/q R/W, vy R, parameters, stored strains R, g_u R/W,
+    Wr R/W."""
+    v = 8 + 8 + 4 + 4 + 8
+    params = 8 if l == 0 else 16
+    s = 16 + 16 * l + 4 + params + 8 + 8 + 8
+    return v, s
+
+
 def fused_bytes(l, store=True):
     """Per-point bytes of one fused step (each array once): vy, sxy, syz and
     the 2L memory variables read and written, model parameters read (1/rho,
@@ -537,29 +548,45 @@ def main():
     pname = "forward_store" if gradient else "forward"
     fused_ms = eng.profile_fused(pname, a.profile_steps)
     prof = eng.profile_step(pname, a.profile_steps)
-    if fused_ms is not None:        # one fused kernel per step: it is the dominant (only) step kernel
-        ks = fused_bytes(L, store=gradient)
-        kname = f"fs_step<{fdo},{L}> (fused velocity+stress, forward pass{' with storage' if gradient else ''})"
-        kms = fused_ms
-        prof["fs_step"] = fused_ms
-    else:
-        kv, ks = kernel_bytes(L, store=gradient)
-        kname = f"s_step<{fdo},{L}> (forward pass{' with storage' if gradient else ''})"
-        kms = prof["s_step"]
-    s_gbs = ks * n * nsh / (kms / 1e3) / 1e9
-    traffic = None
+    trec = {}
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath) and a.config == "c2":
         # DRAM bytes of one launch from an ncu capture; reported only when the
         # capture was taken on the step kernels' current source
         try:
             rec = json.load(open(tpath))
-            key = "fs_step_forward_store_bytes_per_launch" if fused_ms is not None else \
-                "s_step_forward_store_bytes_per_launch"
             if rec.get("kernels_sha256") == kernels_hash():
-                traffic = rec.get(key)
+                trec = rec
         except Exception:
-            traffic = None
+            trec = {}
+    if fused_ms is not None:        # one fused kernel per step: it is the dominant (only) step kernel
+        ks = fused_bytes(L, store=gradient)
+        kname = f"fs_step<{fdo},{L}> (fused velocity+stress, forward pass{' with storage' if gradient else ''})"
+        kms = fused_ms
+        prof["fs_step"] = fused_ms
+        traffic = trec.get("fs_step_forward_store_bytes_per_launch")
+        rooflines = {}
+    else:
+        # the stress kernels of the forward pass (with storage) and of the
+        # adjoint pass launch once per step each; the dominant one is the
+        # slower of the two
+        kv, ks = kernel_bytes(L, store=gradient)
+        rooflines = {"forward": {"kernel": f"s_step<{fdo},{L}> (forward pass{' with storage' if gradient else ''})",
+                                 "bytes_per_point": ks, "ms_per_launch": prof["s_step"],
+                                 "traffic": trec.get("s_step_forward_store_bytes_per_launch")}}
+        if gradient:
+            pa = eng.profile_step("adjoint", a.profile_steps)
+            prof["v_step_adjoint"], prof["s_step_adjoint"] = pa["v_step"], pa["s_step"]
+            rooflines["adjoint"] = {"kernel": f"s_step<{fdo},{L}> (adjoint pass with correlation)",
+                                    "bytes_per_point": kernel_bytes_adjoint(L)[1], "ms_per_launch": pa["s_step"],
+                                    "traffic": trec.get("s_step_adjoint_bytes_per_launch")}
+        for r in rooflines.values():
+            r["achieved"] = r["bytes_per_point"] * n * nsh / (r["ms_per_launch"] / 1e3) / 1e9
+            r["frac"] = r["achieved"] / hbm
+        dom = max(rooflines, key=lambda k: rooflines[k]["ms_per_launch"])
+        kname, ks, kms = rooflines[dom]["kernel"], rooflines[dom]["bytes_per_point"], rooflines[dom]["ms_per_launch"]
+        traffic = rooflines[dom]["traffic"]
+    s_gbs = ks * n * nsh / (kms / 1e3) / 1e9
 
     cpu = None
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
@@ -590,6 +617,7 @@ def main():
             "roofline": {"bound": "hbm", "achieved": s_gbs, "peak": hbm, "unit": "GB/s", "frac": s_gbs / hbm,
                          "traffic": traffic, "kernel": kname, "bytes_per_point": ks, "ms_per_launch": kms,
                          "peak_source": peak_kind},
+            "stress_kernel_rooflines": rooflines,
             "step_roofline": {"achieved": step_gbs, "frac": step_gbs / hbm, "bytes_per_point_fwd": bf,
                               "bytes_per_point_adj": ba if gradient else None,
                               "ms_forward_pass": ms_f / a.steps,
@@ -824,6 +852,8 @@ def bench_learned(a, rank, world, local):
             runs.append((m, m, None))
     seeds = [int(x) for x in a.problem_seeds.split(",") if x]
     per_seed = []
+    clocks = Clocks(local)            # clocks over the FWI runs the ratios come from
+    clocks.start()
     for seed in seeds:
         pcfg = configs.config5(seed=seed, **({"nt": a.nt} if a.nt else {}))
         prob = fwi.Problem(pcfg, test_shots=4)
@@ -847,6 +877,7 @@ def bench_learned(a, rank, world, local):
         per_seed.append({"seed": seed, "plain": {"final_misfit": hp[-1]["misfit"], "gpu_s": t_plain,
                                                  "iterations": len(hp) - 1, "curve": curve(hp)},
                          "methods": res})
+    clk = clocks.stop()
     primary = a.methods.split(",")[0]
 
     def median_ratio(key, field="ratio"):
@@ -877,6 +908,7 @@ def bench_learned(a, rank, world, local):
         "e2e": {"value": median_ratio(primary, "wall_ratio"), "unit": "ratio (host wall-clock of the FWI runs)",
                 "h2d_bytes_per_step": None, "d2h_bytes_per_step": None},
         "wall_s": time.time() - t0,
+        "clocks": clk,
     }
     print(json.dumps(line), flush=True)
 
