@@ -624,6 +624,56 @@ __global__ void __launch_bounds__(BX *BY / 2, VSTEP_R2_MIN_BLOCKS) v_step_r2(Ste
                                    1 + blockIdx.y * BY + 2 * threadIdx.y, blockIdx.z);
 }
 
+/* Experimental velocity-kernel variants (FDORDER 8 only, DSH_VVAR=1..4),
+ * bit-identical to v_step, kept to measure what limits the velocity kernel:
+ *   1  stress taps through the read-only path (ld.global.nc) with the L2 hint
+ *   2  stress taps as plain loads without an L2 policy
+ *   3  128 x 16 points per 512-thread block (more vertical reuse of the syz rows in L1)
+ */
+struct GlobalTapsNC {
+    template <int H, int NL, int NR>
+    __device__ __forceinline__ void load(const StepArgs &a, long long so, long long hrow, int col0, int j, float *xs,
+                                         float4 *ys) const
+    {
+        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
+#pragma unroll
+        for (int v = 0; v < NL + 1 + NR; v++) {
+            float4 t = ldg4(row + 4 * v);
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * a.pitch + col0;
+#pragma unroll
+        for (int r = 0; r < 2 * H; r++) ys[r] = ldg4(col + (long long)r * a.pitch);
+    }
+};
+struct GlobalTapsPlain {
+    template <int H, int NL, int NR>
+    __device__ __forceinline__ void load(const StepArgs &a, long long so, long long hrow, int col0, int j, float *xs,
+                                         float4 *ys) const
+    {
+        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
+#pragma unroll
+        for (int v = 0; v < NL + 1 + NR; v++) {
+            float4 t = *reinterpret_cast<const float4 *>(row + 4 * v);
+            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
+        }
+        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * a.pitch + col0;
+#pragma unroll
+        for (int r = 0; r < 2 * H; r++) ys[r] = *reinterpret_cast<const float4 *>(col + (long long)r * a.pitch);
+    }
+};
+template <int FDO, int FLAGS, bool P2, int VAR>
+__global__ void __launch_bounds__(VAR == 3 ? 512 : 256, VAR == 3 ? 2 : ((FLAGS & (VF_CORR | VF_HESS)) ? VSTEP_MIN_BLOCKS : VSTEP_MIN_BLOCKS_FWD))
+    v_step_x(StepArgs a, int nt_off)
+{
+    const int i0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x);
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    const int tile = ((j - 1) / BY) * a.tl.ntx + (i0 - 1) / (4 * BX);
+    if (VAR == 1) v_body<FDO, FLAGS, P2, GlobalTapsNC>(a, nt_off, i0, j, blockIdx.z, tile);
+    else if (VAR == 2) v_body<FDO, FLAGS, P2, GlobalTapsPlain>(a, nt_off, i0, j, blockIdx.z, tile);
+    else v_body<FDO, FLAGS, P2>(a, nt_off, i0, j, blockIdx.z, tile);
+}
+
 /* The velocity step with the block's stress taps staged in shared memory
  * first: 8 sxy rows of 128 + 4*(NL+NR) points and 8+2H-1 syz rows of 128
  * points, loaded once per block (about 3 float4 loads per thread instead of
