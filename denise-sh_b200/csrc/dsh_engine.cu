@@ -1114,6 +1114,9 @@ static void v_shape(const dsh_ctx *ctx, const VPick &v, int nb, dim3 *grid, dim3
         const unsigned per = (unsigned)std::max(1, 2 * nsm / std::max(1, nb));
         *grid = dim3(std::min(per, gx * gy), (unsigned)nb, 1);
         *block = dim3(BX, BY + 1, 1);           /* 8 computing warps + 1 producer warp */
+    } else if (v.code == 14) {                  /* one x-point, 4 rows per thread: 32 x 32 points per block */
+        *grid = dim3((unsigned)((p.nx + 31) / 32), (unsigned)((p.ny + 31) / 32), (unsigned)nb);
+        *block = dim3(32, 8, 1);
     } else if (v.code == 13) {                  /* 128 x 16 points per block */
         *grid = dim3(gx, (unsigned)((p.ny + 15) / 16), (unsigned)nb);
         *block = dim3(BX, 16, 1);

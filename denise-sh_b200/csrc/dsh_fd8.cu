@@ -19,6 +19,11 @@ KFn v_kernel_exp_fd8(int var, int flags, bool p2)
     case 1: return p2 ? v_exp_pick<1, true>(flags) : v_exp_pick<1, false>(flags);
     case 2: return p2 ? v_exp_pick<2, true>(flags) : v_exp_pick<2, false>(flags);
     case 3: return p2 ? v_exp_pick<3, true>(flags) : v_exp_pick<3, false>(flags);
+    case 4:
+        if (flags == 0) return p2 ? v_step_col<8, 0, true> : v_step_col<8, 0, false>;
+        if (flags == (VF_ADJOINT | VF_CORR))
+            return p2 ? v_step_col<8, VF_ADJOINT | VF_CORR, true> : v_step_col<8, VF_ADJOINT | VF_CORR, false>;
+        return nullptr;
     default: return nullptr;
     }
 }
