@@ -61,9 +61,6 @@ inline KFn v_kernel_tp(int fdo, int flags, bool p2)
     }
 }
 
-/* experimental velocity-kernel variants of FDORDER 8 (v_step_x, DSH_VVAR=1..3) */
-KFn v_kernel_exp_fd8(int var, int flags, bool p2);
-
 /* velocity step with two rows per thread (v_step_r2), block (32, 4) */
 inline KFn v_kernel_r2(int fdo, int flags, bool p2)
 {

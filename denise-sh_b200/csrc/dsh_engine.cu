@@ -1095,8 +1095,6 @@ static VPick pick_v(const dsh_ctx *ctx, int fdo, int vflags, bool p2)
     KFn k = staged ? v_kernel_st(fdo, vflags, p2) : nullptr;
     if (k) return {k, 1};
     if (env_tma && ctx->tma_ok && (k = v_kernel_tp(fdo, vflags, p2))) return {k, 2};
-    static const int env_var = getenv("DSH_VVAR") ? atoi(getenv("DSH_VVAR")) : 0;
-    if (env_var > 0 && fdo == 8 && (k = v_kernel_exp_fd8(env_var, vflags, p2))) return {k, 10 + env_var};
     const bool rows2 = ctx->sel_rows >= 0 ? ctx->sel_rows != 0 : env_rows == 2;
     if (rows2 && (k = v_kernel_r2(fdo, vflags, p2))) return {k, 3};
     return {v_kernel(fdo, vflags, p2), 0};
@@ -1114,12 +1112,6 @@ static void v_shape(const dsh_ctx *ctx, const VPick &v, int nb, dim3 *grid, dim3
         const unsigned per = (unsigned)std::max(1, 2 * nsm / std::max(1, nb));
         *grid = dim3(std::min(per, gx * gy), (unsigned)nb, 1);
         *block = dim3(BX, BY + 1, 1);           /* 8 computing warps + 1 producer warp */
-    } else if (v.code == 14) {                  /* one x-point, 4 rows per thread: 32 x 32 points per block */
-        *grid = dim3((unsigned)((p.nx + 31) / 32), (unsigned)((p.ny + 31) / 32), (unsigned)nb);
-        *block = dim3(32, 8, 1);
-    } else if (v.code == 13) {                  /* 128 x 16 points per block */
-        *grid = dim3(gx, (unsigned)((p.ny + 15) / 16), (unsigned)nb);
-        *block = dim3(BX, 16, 1);
     } else {
         *grid = dim3(gx, gy, (unsigned)nb);
         *block = dim3(BX, v.code == 3 ? BY / 2 : BY, 1);

@@ -624,235 +624,6 @@ __global__ void __launch_bounds__(BX *BY / 2, VSTEP_R2_MIN_BLOCKS) v_step_r2(Ste
                                    1 + blockIdx.y * BY + 2 * threadIdx.y, blockIdx.z);
 }
 
-/* Experimental velocity-kernel variants (FDORDER 8 only, DSH_VVAR=1..4),
- * bit-identical to v_step, kept to measure what limits the velocity kernel:
- *   1  stress taps through the read-only path (ld.global.nc) with the L2 hint
- *   2  stress taps as plain loads without an L2 policy
- *   3  128 x 16 points per 512-thread block (more vertical reuse of the syz rows in L1)
- */
-struct GlobalTapsNC {
-    template <int H, int NL, int NR>
-    __device__ __forceinline__ void load(const StepArgs &a, long long so, long long hrow, int col0, int j, float *xs,
-                                         float4 *ys) const
-    {
-        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
-#pragma unroll
-        for (int v = 0; v < NL + 1 + NR; v++) {
-            float4 t = ldg4(row + 4 * v);
-            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
-        }
-        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * a.pitch + col0;
-#pragma unroll
-        for (int r = 0; r < 2 * H; r++) ys[r] = ldg4(col + (long long)r * a.pitch);
-    }
-};
-struct GlobalTapsPlain {
-    template <int H, int NL, int NR>
-    __device__ __forceinline__ void load(const StepArgs &a, long long so, long long hrow, int col0, int j, float *xs,
-                                         float4 *ys) const
-    {
-        const float *row = a.sxy + so + hrow + col0 - 4 * NL;
-#pragma unroll
-        for (int v = 0; v < NL + 1 + NR; v++) {
-            float4 t = *reinterpret_cast<const float4 *>(row + 4 * v);
-            xs[4 * v] = t.x; xs[4 * v + 1] = t.y; xs[4 * v + 2] = t.z; xs[4 * v + 3] = t.w;
-        }
-        const float *col = a.syz + so + (long long)(j - 1 + a.hy - H) * a.pitch + col0;
-#pragma unroll
-        for (int r = 0; r < 2 * H; r++) ys[r] = *reinterpret_cast<const float4 *>(col + (long long)r * a.pitch);
-    }
-};
-template <int FDO, int FLAGS, bool P2, int VAR>
-__global__ void __launch_bounds__(VAR == 3 ? 512 : 256, VAR == 3 ? 2 : ((FLAGS & (VF_CORR | VF_HESS)) ? VSTEP_MIN_BLOCKS : VSTEP_MIN_BLOCKS_FWD))
-    v_step_x(StepArgs a, int nt_off)
-{
-    const int i0 = 1 + 4 * (blockIdx.x * BX + threadIdx.x);
-    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
-    const int tile = ((j - 1) / BY) * a.tl.ntx + (i0 - 1) / (4 * BX);
-    if (VAR == 1) v_body<FDO, FLAGS, P2, GlobalTapsNC>(a, nt_off, i0, j, blockIdx.z, tile);
-    else if (VAR == 2) v_body<FDO, FLAGS, P2, GlobalTapsPlain>(a, nt_off, i0, j, blockIdx.z, tile);
-    else v_body<FDO, FLAGS, P2>(a, nt_off, i0, j, blockIdx.z, tile);
-}
-
-/*
- * Velocity step with one x-point and RY = 4 consecutive rows per thread
- * (experimental, DSH_VVAR=4): a warp covers 32 consecutive points of 4 rows;
- * the x-taps of sxy come from the neighbouring lanes by warp shuffles (each
- * lane loads its own value and, the first 2H-1 lanes, one of the right halo),
- * the syz column window of the 4 rows (2H+3 rows) is loaded once.  Every
- * load is a coalesced 128-byte row segment per warp.  Per point the
- * arithmetic, CPML, injection, sampling and stores are those of v_body.
- */
-constexpr int VC_RY = 4;
-template <int FDO, int FLAGS, bool P2>
-__global__ void __launch_bounds__(256, 4) v_step_col(StepArgs a, int nt_off)
-{
-    constexpr int H = FDO / 2;
-    constexpr int NZ = 2 * H + VC_RY - 1;            /* syz rows j0-H .. j0+RY+H-2 */
-    const int lane = threadIdx.x;
-    const int i = 1 + blockIdx.x * 32 + lane;
-    const int j0 = 1 + (blockIdx.y * blockDim.y + threadIdx.y) * VC_RY;
-    const int slot = blockIdx.z;
-    const int nt = *a.nt_base + nt_off;
-    const long long so = (long long)slot * a.slot_stride;
-    const int pitch = a.pitch;
-    const int rows_total = a.ny + 2 * a.hy;
-    const bool active = i <= a.nx && j0 <= a.ny;       /* the warp's shuffles need every lane */
-    const int col = i - 1 + HX;
-    const int tile = ((j0 - 1) / BY) * a.tl.ntx + (i - 1) / (4 * BX);
-
-    float b[VC_RY], vy[VC_RY], g[VC_RY], hh[VC_RY], f[VC_RY];
-#pragma unroll
-    for (int r = 0; r < VC_RY; r++) {
-        const int j = j0 + r;
-        const bool ok = active && j <= a.ny;
-        const long long drow = (long long)(j - 1) * pitch;
-        b[r] = ok ? __ldg(a.brho + drow + col) : 0.0f;
-        vy[r] = ok ? a.vy[so + (long long)(j - 1 + a.hy) * pitch + col] : 0.0f;
-        if (FLAGS & VF_CORR) g[r] = ok ? a.grho[so + drow + col] : 0.0f;
-        if (FLAGS & VF_HESS) hh[r] = ok ? a.hrho[so + drow + col] : 0.0f;
-    }
-    int tg0 = 0, tg1 = 0, tr0 = 0, tr1 = 0;
-    if (a.tl.on && active) {
-        const int *go = a.tl.goff + (long long)slot * (a.tl.ntiles + 1) + tile;
-        tg0 = __ldg(go); tg1 = __ldg(go + 1);
-        if (a.tl.sample) {
-            const int *ro = a.tl.roff + (long long)slot * (a.tl.ntiles + 1) + tile;
-            tr0 = __ldg(ro); tr1 = __ldg(ro + 1);
-        }
-    }
-    if (nt > a.nt_last) return;                        /* uniform over the grid */
-    if (FLAGS & VF_CORR) {
-        const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
-        const float *fb = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + col;
-#pragma unroll
-        for (int r = 0; r < VC_RY; r++)
-            f[r] = (active && j0 + r <= a.ny) ? __ldcs(fb + (long long)(j0 + r - 1) * pitch) : 0.0f;
-    }
-    pdl_wait();
-    pdl_trigger();
-
-    /* sxy x-window per row: w0 = sxy[x0-H+lane], w1 = sxy[x0-H+32+lane] (lanes < 2H-1) */
-    float w0[VC_RY], w1[VC_RY], zs[NZ];
-    const int c0 = col - H;                            /* column of w0 */
-#pragma unroll
-    for (int r = 0; r < VC_RY; r++) {
-        const int row = j0 + r - 1 + a.hy;
-        const bool rok = row < rows_total;
-        const float *rp = a.sxy + so + (long long)row * pitch;
-        w0[r] = (rok && c0 < pitch) ? rp[c0] : 0.0f;
-        w1[r] = (rok && lane < 2 * H - 1 && c0 + 32 < pitch) ? rp[c0 + 32] : 0.0f;
-    }
-#pragma unroll
-    for (int q = 0; q < NZ; q++) {
-        const int row = j0 - H + q - 1 + a.hy;
-        zs[q] = (row < rows_total && col < pitch) ? a.syz[so + (long long)row * pitch + col] : 0.0f;
-    }
-
-    float acc[VC_RY];
-#pragma unroll
-    for (int r = 0; r < VC_RY; r++) {
-        /* x-taps: t[d + H] = sxy[i + d], d = -H .. H-1, from lane + H + d of the window */
-        float t[2 * H];
-#pragma unroll
-        for (int d = -H; d < H; d++) {
-            const int src = lane + H + d;
-            const float lo = __shfl_sync(0xffffffffu, w0[r], src & 31);
-            const float hi = __shfl_sync(0xffffffffu, w1[r], src & 31);
-            t[d + H] = src < 32 ? lo : hi;
-        }
-        const int j = j0 + r;
-        float sxy_x, syy_y;
-#pragma unroll
-        for (int m = 1; m <= H; m++) {
-            const int my = (FDO == 12 && m == 6 && a.fd12_compat) ? 5 : m;
-            float tx = a.hc[m] * (t[H + m - 1] - t[H - m]);
-            float ty = a.hc[my] * (zs[r + H + m - 1] - zs[r + H - m]);
-            if (m == 1) { sxy_x = tx; syy_y = ty; }
-            else { sxy_x = sxy_x + tx; syy_y = syy_y + ty; }
-        }
-        const int fw = a.fw;
-        if (active && j <= a.ny && fw > 0 && (i <= fw || i >= a.nx - fw + 1 || (!a.free_surf && j <= fw) ||
-                                             j >= a.ny - fw + 1)) {
-            if (i <= fw) {
-                float *p = a.psi_vxx + so + (long long)(j - 1) * 2 * fw + (i - 1);
-                float ps = __ldg(a.pml.b_x + i) * *p + __ldg(a.pml.a_x + i) * sxy_x;
-                *p = ps;
-                sxy_x = sxy_x / __ldg(a.pml.K_x + i) + ps;
-            }
-            if (i >= a.nx - fw + 1) {
-                const int h1 = i - a.nx + 2 * fw;
-                float *p = a.psi_vxx + so + (long long)(j - 1) * 2 * fw + (h1 - 1);
-                float ps = __ldg(a.pml.b_x + h1) * *p + __ldg(a.pml.a_x + h1) * sxy_x;
-                *p = ps;
-                sxy_x = sxy_x / __ldg(a.pml.K_x + h1) + ps;
-            }
-            if (!a.free_surf && j <= fw) {
-                float *p = a.psi_vyy_v + so + (long long)(j - 1) * pitch + col;
-                float ps = __ldg(a.pml.b_y + j) * *p + __ldg(a.pml.a_y + j) * syy_y;
-                *p = ps;
-                syy_y = syy_y / __ldg(a.pml.K_y + j) + ps;
-            }
-            if (j >= a.ny - fw + 1) {
-                const int h1 = j - a.ny + 2 * fw;
-                float *p = a.psi_vyy_v + so + (long long)(h1 - 1) * pitch + col;
-                float ps = __ldg(a.pml.b_y + h1) * *p + __ldg(a.pml.a_y + h1) * syy_y;
-                *p = ps;
-                syy_y = syy_y / __ldg(a.pml.K_y + h1) + ps;
-            }
-        }
-        const float s = sxy_x + syy_y;
-        acc[r] = (FLAGS & VF_ADJOINT) ? vy[r] : div_dh<P2>(b[r] * s, a);
-        vy[r] = vy[r] + div_dh<P2>(b[r] * a.dt * s, a);
-    }
-    if (!active) return;
-
-    /* injection (sources in order per point), then sampling */
-    for (int gi = tg0; gi < tg1; gi++) {
-        const int pk = __ldg(a.tl.gpt + gi);
-        const int px = pk & 0xffff, py = pk >> 16;
-        if (px == i && py >= j0 && py < j0 + VC_RY) {
-            const int r = py - j0;
-            float v = vy[0];
-#pragma unroll
-            for (int q = 1; q < VC_RY; q++) if (q == r) v = vy[q];
-            const float *sg = a.tl.sig + a.tl.sig_off[slot] + (long long)(nt - 1) * a.tl.sig_ts;
-            for (int e = __ldg(a.tl.gbeg + gi); e < __ldg(a.tl.gbeg + gi + 1); e++)
-                v = v + sg[(long long)__ldg(a.tl.src_id + e) * a.tl.sig_ss];
-#pragma unroll
-            for (int q = 0; q < VC_RY; q++) if (q == r) vy[q] = v;
-        }
-    }
-    if (tr1 > tr0) {
-        const int r0 = a.tl.rec_off[slot], ntr = a.tl.rec_off[slot + 1] - r0;
-        float *sm = a.tl.seis + a.tl.seis_off[slot] + (long long)(nt - 1) * ntr;
-        for (int e = tr0; e < tr1; e++) {
-            const int pk = __ldg(a.tl.rpt + e);
-            const int px = pk & 0xffff, py = pk >> 16;
-            if (px == i && py >= j0 && py < j0 + VC_RY) {
-                float v = vy[0];
-#pragma unroll
-                for (int q = 1; q < VC_RY; q++) if (q == py - j0) v = vy[q];
-                sm[__ldg(a.tl.rid + e)] = v;
-            }
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < VC_RY; r++) {
-        const int j = j0 + r;
-        if (j > a.ny) break;
-        const long long drow = (long long)(j - 1) * pitch;
-        a.vy[so + (long long)(j - 1 + a.hy) * pitch + col] = vy[r];
-        if (FLAGS & VF_ACC_OUT) a.out_acc[so + (long long)(j - 1 + a.hy) * pitch + col] = acc[r];
-        if (FLAGS & VF_CORR) a.grho[so + drow + col] = g[r] + (acc[r] * f[r]);
-        if (!(FLAGS & VF_ADJOINT) && a.fwd && !(FLAGS & VF_CORR)) {
-            const long long k = store_idx(nt - 1, a.fwd_mod);
-            __stcs(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col, acc[r]);
-        }
-        if ((FLAGS & VF_HESS) && nt < a.nt_total) a.hrho[so + drow + col] = hh[r] + (acc[r] * acc[r]);
-    }
-}
-
 /* The velocity step with the block's stress taps staged in shared memory
  * first: 8 sxy rows of 128 + 4*(NL+NR) points and 8+2H-1 syz rows of 128
  * points, loaded once per block (about 3 float4 loads per thread instead of
