@@ -18,7 +18,8 @@
  *                        TMEM lanes 32w..32w+31 = tile rows), bias, ReLU,
  *                        FP32 or BF16 stores
  * Every mbarrier wait is bounded; on expiry the CTA records an error code,
- * stops issuing work and frees its tensor memory.
+ * stops issuing work, waits (with a separate bound) for the copies and
+ * matrix-multiply operations it already issued, and frees its tensor memory.
  */
 #include "dsh_nn.h"
 
@@ -33,7 +34,9 @@
 namespace {
 
 constexpr int BM = 128, BK = 64, STAGES = 4, THREADS = 128;
-constexpr long long WAIT_LIMIT = 1LL << 22;       /* mbarrier.try_wait polls before giving up */
+constexpr long long WAIT_LIMIT = 1LL << 22;       /* mbarrier.try_wait polls before giving up (default) */
+constexpr long long DRAIN_LIMIT = 1LL << 24;      /* polls while draining work in flight after an expiry */
+long long g_wait_polls = WAIT_LIMIT;              /* dsh_nn_set_wait_limit */
 
 struct GemmArgs {
     int M, N, K;
@@ -45,6 +48,7 @@ struct GemmArgs {
     const float *bias;
     int relu;
     int *err;                                    /* set to DSH_NN_ERR_TIMEOUT by a CTA whose wait expired */
+    long long wait_polls;                        /* poll limit of the pipeline's mbarrier waits */
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -73,12 +77,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *b, uint32_t parity)
 }
 
 /* bounded wait for the phase of the given parity; false on expiry or abort */
-__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort)
+__device__ __forceinline__ bool mbar_wait(uint64_t *b, uint32_t parity, volatile int *abort, long long limit)
 {
-    for (long long it = 0; it < WAIT_LIMIT; it++) {
+    for (long long it = 0; it < limit; it++) {
         if (mbar_try_wait(b, parity)) return true;
         if (*abort) return false;
     }
+    return false;
+}
+
+/* bounded wait that ignores the abort flag: after an expiry, for the copies
+   and multiply operations the CTA already issued to finish before it frees
+   its tensor memory and exits */
+__device__ __forceinline__ bool mbar_drain(uint64_t *b, uint32_t parity)
+{
+    for (long long it = 0; it < DRAIN_LIMIT; it++)
+        if (mbar_try_wait(b, parity)) return true;
     return false;
 }
 
@@ -188,21 +202,27 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     if (nk > 0) {
         if (warp == 0 && lane == 0) {                 /* TMA producer */
+            int issued = 0;
             for (int i = 0; i < nk; i++) {
                 const int s = i % STAGES;
                 const uint32_t ph = (uint32_t)(i / STAGES) & 1u;
-                if (!mbar_wait(&empty[s], ph ^ 1u, &abort_flag)) { abort_flag = 1; break; }
+                if (!mbar_wait(&empty[s], ph ^ 1u, &abort_flag, g.wait_polls)) { abort_flag = 1; break; }
                 uint8_t *sa = smem + s * STAGE;
                 mbar_expect_tx(&full[s], STAGE);
                 tma_load_2d(sa, &ta, &full[s], (kt0 + i) * BK, m0);
                 tma_load_2d(sa + A_BYTES, &tb, &full[s], (kt0 + i) * BK, n0);
+                issued = i + 1;
+            }
+            if (abort_flag) {                         /* the last load of each stage lands before the CTA exits */
+                for (int i = issued > STAGES ? issued - STAGES : 0; i < issued; i++)
+                    mbar_drain(&full[i % STAGES], (uint32_t)(i / STAGES) & 1u);
             }
         } else if (warp == 1 && lane == 0) {          /* MMA issuer */
             const uint32_t idesc = idesc_bf16<BN>();
             for (int i = 0; i < nk; i++) {
                 const int s = i % STAGES;
                 const uint32_t ph = (uint32_t)(i / STAGES) & 1u;
-                if (!mbar_wait(&full[s], ph, &abort_flag)) { abort_flag = 1; break; }
+                if (!mbar_wait(&full[s], ph, &abort_flag, g.wait_polls)) { abort_flag = 1; break; }
                 tc_fence_after();
                 const uint32_t sa = smem_u32(smem + s * STAGE), sb = sa + A_BYTES;
                 const uint64_t da = sw128_desc(sa), db = sw128_desc(sb);
@@ -211,11 +231,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                     umma_bf16(tmem, da + 2 * kk, db + 2 * kk, idesc, (i > 0 || kk > 0) ? 1u : 0u);
                 umma_commit(&empty[s]);
             }
-            umma_commit(&done);
+            umma_commit(&done);                       /* also after an expiry: tracks every issued MMA */
         }
         __syncwarp();
         /* epilogue: every thread one row of the tile */
-        const bool ok = mbar_wait(&done, 0, &abort_flag) && !abort_flag;
+        bool ok = mbar_wait(&done, 0, &abort_flag, g.wait_polls) && !abort_flag;
+        ok = __all_sync(0xffffffffu, ok);             /* tcgen05.ld below is warp-collective */
+        if (!ok) mbar_drain(&done, 0);                /* the issued MMAs finish before TMEM is freed */
         tc_fence_after();
         const int row = m0 + warp * 32 + lane;
         if (ok) {
@@ -237,7 +259,7 @@ __global__ void __launch_bounds__(THREADS, 1)
                     if (g.c16) g.c16[(long long)row * g.ldc + n] = __float2bfloat16_rn(x);
                 }
             }
-        } else if (threadIdx.x == 0) {
+        } else if (lane == 0) {                      /* any warp whose wait expired reports it */
             atomicExch(g.err, DSH_NN_ERR_TIMEOUT);
         }
     }
@@ -310,6 +332,12 @@ int launch(const CUtensorMap &ta, const CUtensorMap &tb, const GemmArgs &g, int 
 
 }  // namespace
 
+extern "C" int dsh_nn_set_wait_limit(long long polls)
+{
+    g_wait_polls = polls > 0 ? polls : WAIT_LIMIT;
+    return DSH_NN_OK;
+}
+
 extern "C" int dsh_nn_gemm(int M, int N, int K, const void *A, long long lda, const void *B, long long ldb, float *C32,
                            void *C16, long long ldc, const float *bias, int relu, int splits, float *partial,
                            int accumulate, int *err, void *stream)
@@ -336,6 +364,7 @@ extern "C" int dsh_nn_gemm(int M, int N, int K, const void *A, long long lda, co
     g.bias = bias;
     g.relu = relu;
     g.err = err;
+    g.wait_polls = g_wait_polls;
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
     switch (BN) {

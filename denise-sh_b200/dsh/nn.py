@@ -39,6 +39,7 @@ def nnlib() -> C.CDLL:
         L = C.CDLL(NN_LIB_PATH)
         v, i, ll, f = C.c_void_p, C.c_int, C.c_longlong, C.c_float
         L.dsh_nn_gemm.argtypes = [i, i, i, v, ll, v, ll, v, v, ll, v, i, i, v, i, v, v]
+        L.dsh_nn_set_wait_limit.argtypes = [ll]
         L.dsh_nn_im2col.argtypes = [v, i, i, i, i, v, ll, v]
         L.dsh_nn_im2col_t.argtypes = [v, i, i, i, i, v, ll, v]
         L.dsh_nn_transpose.argtypes = [v, ll, i, v, ll, v]
@@ -76,6 +77,12 @@ def _p(t):
 
 def _rup(x, m):
     return (x + m - 1) // m * m
+
+
+def set_wait_limit(polls: int = 0):
+    """Poll limit of the tensor-core GEMM's mbarrier waits (0 = default);
+    an expired wait is reported through Ctx.check (DSH_NN_ERR_TIMEOUT)."""
+    _ck(nnlib().dsh_nn_set_wait_limit(int(polls)), "dsh_nn_set_wait_limit")
 
 
 class Ctx:

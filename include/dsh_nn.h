@@ -34,6 +34,14 @@ extern "C" {
  * splits > 1 divides K over CTAs (FP32 partials in `partial`, splits*M*ldc
  * floats, then summed into C32; no bias/ReLU/C16 then); accumulate = 1 adds
  * the product to C32 (uses `partial` for M*ldc floats). */
+/* Poll limit of the GEMM pipeline's mbarrier waits for the following
+ * launches (process-wide; default 2^22, <= 0 restores it).  On expiry a CTA
+ * records DSH_NN_ERR_TIMEOUT in the caller's err word, stops issuing, waits
+ * for the copies and multiply operations it already issued, frees its tensor
+ * memory and exits; a small limit exercises that path on a healthy run.  No
+ * counterpart in the reference. */
+int dsh_nn_set_wait_limit(long long polls);
+
 int dsh_nn_gemm(int M, int N, int K, const void *A, long long lda, const void *B, long long ldb, float *C32, void *C16,
                 long long ldc, const float *bias, int relu, int splits, float *partial, int accumulate, int *err,
                 void *stream);

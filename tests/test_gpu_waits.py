@@ -77,3 +77,33 @@ def test_batch_host_wait_limit_expires_and_batch_recovers():
         out = b.forward(shots)
     for k in range(2):
         assert np.array_equal(out[k][0], ref[k][0])
+
+
+def test_gemm_mbarrier_limit_expires_and_next_call_is_exact():
+    """The tensor-core GEMM's pipeline waits (TMA producer, MMA issuer,
+    epilogue) poll an mbarrier at most a run-time number of times.  With one
+    poll they expire on a healthy run: the CTAs record DSH_NN_ERR_TIMEOUT,
+    stop issuing, let the copies and multiply operations already issued
+    finish, free their tensor memory and exit.  A following call with the
+    default limit gives the exact product."""
+    torch = pytest.importorskip("torch")
+    from dsh import nn
+
+    rng = np.random.default_rng(3)
+    M, N, K = 512, 128, 2048
+    A = torch.tensor(rng.standard_normal((M, K)), dtype=torch.float32).to(torch.bfloat16).cuda()
+    B = torch.tensor(rng.standard_normal((N, K)), dtype=torch.float32).to(torch.bfloat16).cuda()
+    ctx = nn.Ctx(torch)
+    c = torch.zeros(M, N, device="cuda")
+    try:
+        nn.set_wait_limit(1)
+        ctx.gemm(M, N, K, A, K, B, K, c32=c)
+        torch.cuda.synchronize()
+        assert int(ctx.err.item()) == TIMEOUT
+    finally:
+        nn.set_wait_limit(0)
+    ctx.err.zero_()
+    ctx.gemm(M, N, K, A, K, B, K, c32=c)
+    ctx.check()
+    ref = A.float() @ B.float().t()
+    assert float((c - ref).abs().max()) <= 1e-5 * float(ref.abs().max())
