@@ -563,7 +563,7 @@ extern "C" int dsh_destroy(dsh_ctx *ctx)
     cudaFree(ctx->ckpt); cudaFree(ctx->shadow);
     cudaFree(ctx->d_geo); cudaFree(ctx->d_offs); cudaFree(ctx->d_sig); cudaFree(ctx->d_seis); cudaFree(ctx->d_res);
     cudaFree(ctx->d_obs); cudaFree(ctx->d_tmp); cudaFree(ctx->d_out); cudaFree(ctx->d_nt); cudaFree(ctx->d_part); cudaFree(ctx->d_l2);
-    cudaFree(ctx->d_wemax); cudaFree(ctx->d_gq);
+    cudaFree(ctx->d_wemax); cudaFree(ctx->d_gq); cudaFree(ctx->d_flags);
     cudaFree(ctx->d_taper_box); cudaFree(ctx->d_taper_shot); cudaFree(ctx->d_tmap);
     for (int k = 0; k < 4; k++) if (ctx->ev[k]) cudaEventDestroy(ctx->ev[k]);
     if (ctx->ev_wait) cudaEventDestroy(ctx->ev_wait);
@@ -1278,8 +1278,20 @@ static int run_persistent(dsh_ctx *ctx, Pass pass, int nb, int n0, int count, in
     StepArgs sa = step_args(ctx, pass);
     sa.nslots = nb;
     set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, n0);
-    CK(cudaMemsetAsync(ctx->d_bar, 0, 2 * sizeof(unsigned), ctx->st));
-    unsigned *bar = ctx->d_bar;
+    /* completion flags of the tiles (velocity and stress step per tile and slot) */
+    const long long nflags = 2LL * grid;
+    if (nflags > ctx->flags_cap) {
+        cudaFree(ctx->d_flags);
+        ctx->d_flags = nullptr;
+        ctx->flags_cap = 0;
+        if (cudaMalloc(&ctx->d_flags, (size_t)nflags * sizeof(unsigned)) != cudaSuccess) {
+            cudaGetLastError();
+            return DSH_ERR_OOM;
+        }
+        ctx->flags_cap = nflags;
+    }
+    CK(cudaMemsetAsync(ctx->d_flags, 0, (size_t)nflags * sizeof(unsigned), ctx->st));
+    unsigned *bar = ctx->d_flags;
     void *args[3] = {&sa, &count, &bar};
     CK(cudaLaunchCooperativeKernel((const void *)fk, dim3(grid), dim3(BX, BY), args, 0, ctx->st));
     ctx->launches += 2;

@@ -66,7 +66,9 @@ struct dsh_ctx {
     long long cap_sig = 0, cap_seis = 0, cap_obs = 0;
     int geo_version = 0;
     int *d_nt = nullptr, *d_status = nullptr;
-    unsigned *d_bar = nullptr;            /* grid barrier of the persistent kernel: count, generation */
+    unsigned *d_bar = nullptr;            /* (unused spare words after the status word) */
+    unsigned *d_flags = nullptr;          /* tile completion flags of the persistent launch */
+    long long flags_cap = 0;
     double *d_part = nullptr, *d_l2 = nullptr;
     unsigned *d_wemax = nullptr;
     std::vector<int> ntr_b;

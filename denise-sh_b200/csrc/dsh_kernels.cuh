@@ -318,18 +318,20 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
             tr0 = __ldg(ro); tr1 = __ldg(ro + 1);
         }
     }
-    if (nt > a.nt_last) return;
-    if (FLAGS & VF_CORR) {                   /* stored forward acceleration of step NT-nt+1 */
-        const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
+    if (FLAGS & VF_CORR) {                   /* stored forward acceleration of step NT-nt+1 (the address
+                                                clamped so that a step beyond the pass stays in range) */
+        const long long k = store_idx(max(a.nt_total - nt, 0), a.fwd_mod);
         f4 = ldcs4(a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0);
     }
     pdl_wait();                              /* stresses of the previous step are complete */
     pdl_trigger();
 
-    /* ---- stress taps ---- */
+    /* ---- stress taps (issued before the step test below: their addresses do not
+       depend on the step, so they need not wait for the step counter) ---- */
     float xs[NXS];                           /* xs[p] = sxy[i0 - 4*NL + p] */
     float4 ys[2 * H];                        /* syz rows j-H .. j+H-1 */
     taps.template load<H, NL, NR>(a, so, hrow, col0, j, xs, ys);
+    if (nt > a.nt_last) return;
 
     /* ---- compute ---- */
     float4 acc4 = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -729,9 +731,8 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     if (a.ws) w4 = ld4(a.ws + so + drow + col0);
     if (FLAGS & SF_CORR) g4 = ld4(a.gu + so + drow + col0);
     if (FLAGS & SF_HESS) h4 = ld4(a.hu + so + drow + col0);
-    if (nt > a.nt_last) return;
-    if (FLAGS & SF_CORR) {
-        const long long k = store_idx(a.nt_total - nt, a.fwd_mod);
+    if (FLAGS & SF_CORR) {                   /* (address clamped as in v_body) */
+        const long long k = store_idx(max(a.nt_total - nt, 0), a.fwd_mod);
         const float *base = a.fwd + (long long)slot * a.fwd_slot_stride + k * a.fwd_step_stride + drow + col0;
         fy = ldcs4(base + a.dstride);
         fu = ldcs4(base + 2 * a.dstride);
@@ -765,6 +766,7 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
 #pragma unroll
         for (int r = 0; r < 2 * H; r++) ys[r] = lds4<CG>(col + (long long)r * pitch);
     }
+    if (nt > a.nt_last) return;              /* after every load: none depends on the step test */
 
     /* ---- derivatives and CPML ---- */
     const float dhi = (L > 0) ? a.dhi_visc : a.dhi_el;

@@ -239,12 +239,13 @@ def test_unstable_model_reports_error():
         assert np.all(np.isfinite(e.forward(shots)[0]))
 
 
-@pytest.mark.parametrize("nx,ny", [(70, 40), (1100, 300)])
+@pytest.mark.parametrize("nx,ny", [(70, 40), (500, 200), (1100, 300)])
 def test_forward_persistent_and_pair_paths(nx, ny):
     """With DSH_PERSIST=1 (set for the GPU test run), plain forward modelling
     takes the one-launch persistent kernel when all tiles fit in one wave
-    (70 x 40: 5 tiles) and the per-step kernel pair otherwise (1100 x 300:
-    342 tiles); both are bit-identical to the oracle."""
+    (70 x 40: 5 tiles, 500 x 200: 100 tiles whose completion flags order
+    the neighbouring tiles) and the per-step kernel pair otherwise (1100 x
+    300: 342 tiles); both are bit-identical to the oracle."""
     d, shots = _case(500 + nx, nx=nx, ny=ny, nt=90, fdo=8, L=2, fs=1, fw=10)
     rec = shots[0].recpos.copy()
     rec[1] = np.clip(rec[1], 1, ny)              # all receivers inside the grid: fused sampling lists
