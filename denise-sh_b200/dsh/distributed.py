@@ -50,15 +50,20 @@ class GradientResult:
     g_rho: np.ndarray
     l2: float
     my_shots: list[int]
+    g_qs: np.ndarray | None = None
 
 
 def distributed_gradient(local_gradient: Callable[[list[int]], dict], nshots: int, shape: tuple[int, int],
-                         costs: Sequence[float] | None = None, group=None, device=None) -> GradientResult:
+                         costs: Sequence[float] | None = None, group=None, device=None,
+                         with_q: bool = False) -> GradientResult:
     """Sum of per-shot gradients over all ranks of `group`.
 
-    local_gradient(indices) must return {"g_vs", "g_rho", "l2"} for the given
-    shot indices (e.g. a closure over dsh.Engine.gradient); a rank with no
-    shots contributes zeros.  Every rank takes the same collective steps."""
+    local_gradient(indices) must return {"g_vs", "g_rho", "l2"} (and "g_qs",
+    the Qs gradient, when with_q is set) for the given shot indices (e.g. a
+    closure over dsh.Engine.gradient and Engine.gradient_q); a rank with no
+    shots contributes zeros.  The Qs gradient is a plain sum over shots (no
+    preconditioning), so it travels in the same all-reduce.  Every rank takes
+    the same collective steps."""
     import torch
     import torch.distributed as dist
 
@@ -69,21 +74,25 @@ def distributed_gradient(local_gradient: Callable[[list[int]], dict], nshots: in
     if mine:
         out = local_gradient(mine)
         gv, gr, l2 = np.asarray(out["g_vs"], np.float32), np.asarray(out["g_rho"], np.float32), float(out["l2"])
+        gq = np.asarray(out["g_qs"], np.float32) if with_q else None
     else:
         gv = np.zeros(shape, np.float32)
         gr = np.zeros(shape, np.float32)
         l2 = 0.0
+        gq = np.zeros(shape, np.float32) if with_q else None
     if world == 1:
-        return GradientResult(gv, gr, l2, mine)
+        return GradientResult(gv, gr, l2, mine, gq)
     dev = device if device is not None else ("cuda" if torch.cuda.is_available() and dist.get_backend(group) == "nccl"
                                              else "cpu")
-    buf = torch.from_numpy(np.concatenate([gv.ravel(), gr.ravel()])).to(dev)
+    parts_ = [gv.ravel(), gr.ravel()] + ([gq.ravel()] if with_q else [])
+    buf = torch.from_numpy(np.concatenate(parts_)).to(dev)
     l2t = torch.tensor([l2], dtype=torch.float64, device=dev)
     dist.all_reduce(buf, group=group)
     dist.all_reduce(l2t, group=group)
     buf = buf.cpu().numpy()
     n = gv.size
-    return GradientResult(buf[:n].reshape(shape), buf[n:].reshape(shape), float(l2t.item()), mine)
+    return GradientResult(buf[:n].reshape(shape), buf[n:2 * n].reshape(shape), float(l2t.item()), mine,
+                          buf[2 * n:3 * n].reshape(shape) if with_q else None)
 
 
 def _device(group, device):

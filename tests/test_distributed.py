@@ -142,3 +142,78 @@ def test_rank_failure_is_detected_not_hung(tmp_path):
     err = (tmp_path / "err0.txt").read_text() if (tmp_path / "err0.txt").exists() else ""
     assert err, "surviving rank did not report the failed collective"
     assert (tmp_path / "err1.txt").exists()
+
+
+def _case_visc():
+    import oracle as O
+
+    rng = np.random.default_rng(9)
+    nx, ny, nt = 40, 30, 90
+    vs = (200 + 30 * rng.standard_normal((ny, nx))).clip(120, 300).astype(np.float32)
+    rho = (1800 + 60 * rng.standard_normal((ny, nx))).astype(np.float32)
+    qs = rng.uniform(20, 60, (ny, nx)).astype(np.float32)
+    m = O.Model(nx=nx, ny=ny, nt=nt, dh=0.5, dt=2e-4, vs=vs, rho=rho, qs=qs, fdorder=4, fw=6, fpml=30.0, l=2,
+                fl=(7.5, 30.0), damping=float(vs.max()))
+    shots = []
+    for k in range(4):
+        sp = np.zeros((8, 1), np.float32)
+        sp[:, 0] = [6 + 9 * k, 2, 0, -0.01, 60.0, 1.0, 0, 3]
+        shots.append((sp, np.array([[4, 14, 24, 34], [1, 1, 1, 1]], np.int32)))
+    obs = []
+    for sp, rec in shots:
+        o = O.Oracle(m, "port")
+        obs.append((o.forward(sp, rec) * np.float32(0.6)).astype(np.float32))
+        o.close()
+    return m, shots, obs
+
+
+def _local_gradient_q(m, shots, obs, idx):
+    import oracle as O
+
+    out = _local_gradient(m, shots, obs, idx)
+    gq = np.zeros((m.ny, m.nx), np.float64)
+    for k in idx:
+        o = O.Oracle(m, "port", grad_q=True)
+        o.forward(shots[k][0], shots[k][1], store=True)
+        o.residual(obs[k])
+        o.adjoint()
+        gq += o.grad_q()
+        o.close()
+    out["g_qs"] = gq
+    return out
+
+
+def _worker_q(rank, world, port, outdir):
+    import datetime
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path[:0] = [os.path.join(root, "denise-sh_b200"), os.path.join(root, "oracle")]
+    import torch.distributed as dist
+
+    from dsh.distributed import distributed_gradient
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=8))
+    m, shots, obs = _case_visc()
+    try:
+        res = distributed_gradient(lambda idx: _local_gradient_q(m, shots, obs, idx), len(shots), (m.ny, m.nx),
+                                   with_q=True)
+        np.savez(os.path.join(outdir, f"q{rank}.npz"), g_qs=res.g_qs, g_vs=res.g_vs, mine=np.array(res.my_shots))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_sum_the_qs_gradient(tmp_path):
+    """The Qs gradient travels in the same all-reduce as g_vs and g_rho: two
+    gloo ranks, each with half of the shots, give the single-process sum."""
+    port = _free_port()
+    mp.start_processes(_worker_q, args=(2, port, str(tmp_path)), nprocs=2, start_method="spawn")
+    m, shots, obs = _case_visc()
+    ref = _local_gradient_q(m, shots, obs, list(range(len(shots))))
+    outs = [np.load(tmp_path / f"q{r}.npz") for r in range(2)]
+    assert sorted(np.concatenate([o["mine"] for o in outs]).tolist()) == list(range(len(shots)))
+    for o in outs:
+        scale = np.abs(ref["g_qs"]).max()
+        assert scale > 0
+        assert np.allclose(o["g_qs"], ref["g_qs"], rtol=1e-5, atol=1e-6 * scale)
