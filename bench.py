@@ -86,6 +86,10 @@ def args_parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--c3-steps", type=int, default=2,
                     help="c2 only: timed gradients of the 64-shot batched-gradient sub-measurement (0 = skip)")
+    ap.add_argument("--c1-steps", type=int, default=5,
+                    help="c2 only: timed forward passes of the 500x200 elastic sub-measurement (0 = skip)")
+    ap.add_argument("--step-variant", type=int, default=-1,
+                    help="pin the step-kernel variant (index into dsh.Engine.VARIANTS) instead of autotuning")
     ap.add_argument("--no-autotune", action="store_true",
                     help="c1-c3: keep the default kernel pair instead of timing the step-kernel variants "
                          "(for runs under a profiler)")
@@ -309,6 +313,54 @@ def reference_arm(a, rank, world):
 
 # ---------------------------------------------------------------------------
 
+def c1_sub(a, local):
+    """Plain elastic forward modelling as its configuration states it:
+    NX=500, NY=200, FDORDER 4, NT=2000, one shot, 96 receivers, through the
+    device API with the step-kernel variant the autotuner picks for this grid
+    (the one-launch cluster-resident kernel where the device offers 16-CTA
+    clusters).  CUDA events on the launching stream, three untimed passes
+    first.  The state (1.2 MB) stays on chip in the cluster variant, so the
+    effective bandwidth below (the kernel pair's algorithmic 36 B per point
+    and step over the measured time) is not bounded by HBM."""
+    import torch
+
+    import dsh
+    from dsh import configs
+
+    cfg = configs.config1()
+    p, shots = cfg["params"], cfg["shots"]
+    nx, ny, nt = p["nx"], p["ny"], p["nt"]
+    eng = dsh.Engine(dsh.make_params(**p), device=local)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+    eng.set_model(cfg["vs"], cfg["rho"], None)
+    variant, variant_ms = eng.autotune(shots, nsteps=64)
+    seis = torch.empty(sum(sh.ntr for sh in shots) * nt, device="cuda", dtype=torch.float32)
+    for _ in range(3):
+        eng.forward_device(shots, seis.data_ptr())
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    launches = 0
+    e0.record(stream)
+    for _ in range(a.c1_steps):
+        eng.forward_device(shots, seis.data_ptr())
+        launches += eng.stats()["kernel_launches"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    eng.close()
+    ms = e0.elapsed_time(e1) / a.c1_steps
+    gpt = nx * ny * nt / (ms / 1e3) / 1e9
+    return {"workload": f"elastic-forward-{nx}x{ny}-fd4-nt{nt}", "steps": a.c1_steps, "warmup": 3,
+            "gpt_per_s": gpt, "ms_per_forward": ms, "us_per_time_step": 1e3 * ms / nt,
+            "step_variant": variant, "autotune_ms_per_step": variant_ms, "gpu_launches": launches,
+            "effective_gbs": 36.0 * nx * ny * nt / (ms / 1e3) / 1e9,
+            "l2": "state 1.2 MB: resident on chip; bytes counted algorithmically (kernel pair's 36 B/pt)",
+            "clocks": clk}
+
+
 def c3_sub(a, local):
     """The batched multi-shot FWI gradient as the configuration states it:
     NX=1000, NY=300, FDORDER 8, L=2, NT=4000, 64 shots advanced in one launch
@@ -428,7 +480,10 @@ def main():
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
     eng.set_model(cfg["vs"], cfg["rho"], cfg["qs"])
-    if a.no_autotune:            # profiling runs: a profiler's serialised timings would mislead the tuner
+    if a.step_variant >= 0:
+        eng.set_step_variant(a.step_variant)
+        variant, variant_ms = f"{dsh.Engine.VARIANTS[a.step_variant]} (pinned)", None
+    elif a.no_autotune:          # profiling runs: a profiler's serialised timings would mislead the tuner
         variant, variant_ms = "kernel pair (autotuner skipped)", None
     else:
         variant, variant_ms = eng.autotune(shots, nsteps=min(64, nt))   # step-kernel variant for this grid
@@ -638,6 +693,8 @@ def main():
             del seis, gv, gr
             torch.cuda.empty_cache()
             line["c3"] = c3_sub(a, local)
+        if a.config == "c2" and world == 1 and a.c1_steps > 0:
+            line["c1"] = c1_sub(a, local)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -18,6 +18,7 @@
 #include "dsh_engine_int.h"
 #include "dsh_fs.h"
 #include "dsh_pf.h"
+#include "dsh_cl.h"
 #include "dsh_fused.cuh"
 #include "dsh_setup.h"
 
@@ -814,6 +815,13 @@ int upload_batch(dsh_ctx *ctx, const dsh_shot *shots, int nb, const float *obs_h
         }
     }
     rec_off[S] = (int)rec_pt.size();
+    ctx->geo_max_groups = ctx->geo_max_members = ctx->geo_max_ntr = 0;
+    for (int s = 0; s < nb; s++) {
+        ctx->geo_max_groups = std::max(ctx->geo_max_groups, fgrp_off[s + 1] - fgrp_off[s]);
+        for (int g = fgrp_off[s]; g < fgrp_off[s + 1]; g++)
+            ctx->geo_max_members = std::max(ctx->geo_max_members, grp_beg[g + 1] - grp_beg[g]);
+        ctx->geo_max_ntr = std::max(ctx->geo_max_ntr, ctx->ntr_b[s]);
+    }
 
     /* fused step: per slot and 128 x 16 tile, the groups whose point lies in
      * the tile's velocity region (the tile grown by H-1 points left / above
@@ -1299,11 +1307,45 @@ static int run_persistent(dsh_ctx *ctx, Pass pass, int nb, int n0, int count, in
     return DSH_OK;
 }
 
+/* Small elastic grids, plain forward modelling: the whole pass in one launch
+ * of cl_fwd (dsh_cluster.cuh), one thread-block cluster per shot slot that
+ * holds the slot's wavefield and the model in its CTAs' shared memory.  On
+ * by DSH_CLUSTER=1 or the autotuner's choice; false when it does not apply
+ * (viscoelastic, FDORDER > 8, positions outside the grid, strips too large
+ * for one CTA's shared memory). */
+static bool cluster_cfg(dsh_ctx *ctx, Pass pass, int nb, ClCfg *cfg)
+{
+    static const int env = env_flag("DSH_CLUSTER");
+    const bool on = ctx->sel_cluster >= 0 ? ctx->sel_cluster != 0 : env != 0;
+    const dsh_params &p = ctx->p;
+    if (!on || pass != P_FWD_PLAIN || !ctx->fused_inject || p.l != 0 || p.fdorder > 8) return false;
+    ClProblem pb;
+    pb.fdorder = p.fdorder; pb.p2 = dh_pow2(p.dh) ? 1 : 0; pb.nx = p.nx; pb.ny = p.ny; pb.pitch = ctx->pitch;
+    pb.fw = p.fw; pb.free_surf = p.free_surf; pb.nb = nb;
+    pb.max_groups = ctx->geo_max_groups; pb.max_members = ctx->geo_max_members;
+    pb.max_receivers = ctx->geo_max_ntr;
+    return cl_config(pb, cfg);
+}
+
+static int run_cluster(dsh_ctx *ctx, Pass pass, int nb, int n0, int count, const ClCfg &cfg)
+{
+    const dsh_params &p = ctx->p;
+    StepArgs sa = step_args(ctx, pass);
+    sa.nslots = nb;
+    set_int_kernel<<<1, 1, 0, ctx->st>>>(ctx->d_nt, n0);
+    CK(cl_launch(cfg, p.fdorder, dh_pow2(p.dh), sa, count, nb, ctx->st));
+    ctx->launches += 2;
+    ctx->state_b = 0;
+    return DSH_OK;
+}
+
 /* Steps n0 .. n0+count-1 of a pass: graphs of `chunk` steps replayed
  * count/chunk times, then one graph for the remaining steps. */
 static int run_steps(dsh_ctx *ctx, Pass pass, int nb, int n0, int count)
 {
     if (count <= 0) return DSH_OK;
+    ClCfg ccfg;
+    if (cluster_cfg(ctx, pass, nb, &ccfg)) return run_cluster(ctx, pass, nb, n0, count, ccfg);
     if (const int grid = persistent_grid(ctx, pass, nb)) return run_persistent(ctx, pass, nb, n0, count, grid);
     const int K = std::min(ctx->chunk, count);
     const int nfull = count / K, rem = count % K;
@@ -1748,14 +1790,23 @@ extern "C" int dsh_set_wait_limits(dsh_ctx *ctx, long long device_polls, double 
     return DSH_OK;
 }
 
+/* step-kernel variants: staged velocity taps, fused step, persistent launch, cluster-resident launch */
+static const int VARIANT_SEL[DSH_STEP_VARIANTS][4] = {
+    {0, 0, 0, 0}, {1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+
+static void select_variant(dsh_ctx *ctx, int v)
+{
+    ctx->sel_staged = v < 0 ? -1 : VARIANT_SEL[v][0];
+    ctx->sel_fused = v < 0 ? -1 : VARIANT_SEL[v][1];
+    ctx->sel_persist = v < 0 ? -1 : VARIANT_SEL[v][2];
+    ctx->sel_cluster = v < 0 ? -1 : VARIANT_SEL[v][3];
+}
+
 extern "C" int dsh_set_step_variant(dsh_ctx *ctx, int variant)
 {
-    static const int sel[4][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};   /* staged, fused, persistent */
-    if (!ctx || variant < -1 || variant > 3) return DSH_ERR_PARAM;
+    if (!ctx || variant < -1 || variant >= DSH_STEP_VARIANTS) return DSH_ERR_PARAM;
     if (variant == 2 && !ctx->fused_ok) return DSH_ERR_PARAM;
-    ctx->sel_staged = variant < 0 ? -1 : sel[variant][0];
-    ctx->sel_fused = variant < 0 ? -1 : sel[variant][1];
-    ctx->sel_persist = variant < 0 ? -1 : sel[variant][2];
+    select_variant(ctx, variant);
     drop_graphs(ctx);
     return DSH_OK;
 }
@@ -1874,10 +1925,11 @@ extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
 
 /* Times plain forward steps of each step-kernel variant the context can run
  * on these shots — kernel pair (v_step), pair with v_step_st, fused step,
- * persistent launch — and keeps the fastest for the context's later calls
- * (the fused choice also serves the gradient passes, the persistent one only
- * plain forward modelling).  ms_per_step[4] (optional): mean device ms per
- * step of each variant, 0 where it does not apply. */
+ * persistent launch, cluster-resident launch — and keeps the fastest for the
+ * context's later calls (the fused choice also serves the gradient passes,
+ * the persistent and cluster ones only plain forward modelling).
+ * ms_per_step[DSH_STEP_VARIANTS] (optional): mean device ms per step of each
+ * variant, 0 where it does not apply. */
 extern "C" int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int nsteps, float *ms_per_step,
                             int *choice)
 {
@@ -1888,19 +1940,18 @@ extern "C" int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int
     int rc = upload_batch(ctx, shots, nb, nullptr, nullptr, 0);
     if (rc != DSH_OK) return rc;
     nsteps = std::min(nsteps, ctx->p.nt);
-    const int sel[4][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}};   /* staged, fused, persistent */
-    float ms[4] = {0, 0, 0, 0};
+    float ms[DSH_STEP_VARIANTS] = {0};
     int best = 0;
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    for (int v = 0; v < 4; v++) {
-        ctx->sel_staged = sel[v][0];
-        ctx->sel_fused = sel[v][1];
-        ctx->sel_persist = sel[v][2];
+    for (int v = 0; v < DSH_STEP_VARIANTS; v++) {
+        select_variant(ctx, v);
         drop_graphs(ctx);                              /* graphs hold the previous variant's kernels */
+        ClCfg ccfg;
         if (v == 2 && !use_fused(ctx, P_FWD_PLAIN)) continue;
         if (v == 3 && !persistent_grid(ctx, P_FWD_PLAIN, nb)) continue;
+        if (v == 4 && !cluster_cfg(ctx, P_FWD_PLAIN, nb, &ccfg)) continue;
         for (int rep = 0; rep < 2; rep++) {            /* first round warms up (graphs, lazy loading) */
             if ((rc = zero_slots(ctx, nb, false)) != DSH_OK) break;
             CK(cudaEventRecord(e0, ctx->st));
@@ -1915,11 +1966,9 @@ extern "C" int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    ctx->sel_staged = sel[best][0];
-    ctx->sel_fused = sel[best][1];
-    ctx->sel_persist = sel[best][2];
+    select_variant(ctx, best);
     drop_graphs(ctx);
-    if (ms_per_step) for (int v = 0; v < 4; v++) ms_per_step[v] = ms[v];
+    if (ms_per_step) for (int v = 0; v < DSH_STEP_VARIANTS; v++) ms_per_step[v] = ms[v];
     if (choice) *choice = best;
     if (rc != DSH_OK) return rc;
     return check_status(ctx);

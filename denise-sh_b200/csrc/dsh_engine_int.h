@@ -32,6 +32,7 @@ struct dsh_ctx {
     int state_b = 0;                      /* the slab's current state is in the second buffers */
     int sel_staged = -1, sel_fused = -1, sel_persist = -1;   /* step-kernel variants chosen by dsh_autotune
                                                                (-1: the DSH_VSTAGE / DSH_FUSED / DSH_PERSIST defaults) */
+    int sel_cluster = -1;                 /* cluster-resident forward modelling (-1: the DSH_CLUSTER default) */
     int sel_rows = -1;                    /* 1: the velocity kernel with two rows per thread (-1: DSH_VROWS=2) */
     float *slab = nullptr;
     float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho qs */
@@ -72,6 +73,8 @@ struct dsh_ctx {
     double *d_part = nullptr, *d_l2 = nullptr;
     unsigned *d_wemax = nullptr;
     std::vector<int> ntr_b;
+    int geo_max_groups = 0, geo_max_members = 0, geo_max_ntr = 0;   /* last batch, per slot: forward source
+                                                                       points, sources at one point, receivers */
     int lnorm = 2;                        /* misfit norm of the residual (dsh_set_misfit) */
     void *d_tmap = nullptr;               /* 4 CUtensorMap: sxy, syz of the slab, then of the shadow state */
     int tma_ok = 0;                       /* the maps are built (the TMA-staged velocity kernel can run) */

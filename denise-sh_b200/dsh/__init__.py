@@ -305,11 +305,12 @@ class Engine:
         _check(lib().dsh_profile_step(self.h, self.PASSES[pass_name], nsteps, out.ctypes.data), "dsh_profile_step")
         return {"v_step": float(out[0]), "inject_sample": float(out[1]), "s_step": float(out[2])}
 
-    VARIANTS = ("kernel pair", "kernel pair, staged velocity taps", "fused step", "persistent launch")
+    VARIANTS = ("kernel pair", "kernel pair, staged velocity taps", "fused step", "persistent launch",
+                "cluster-resident launch")
 
     def autotune(self, shots, nsteps=64):
         """Times each step-kernel variant on these shots, keeps the fastest; returns (name, ms per step each)."""
-        ms = np.zeros(4, np.float32)
+        ms = np.zeros(len(self.VARIANTS), np.float32)
         ch = C.c_int(0)
         _check(lib().dsh_autotune(self.h, _shots_c(list(shots)), len(shots), nsteps, ms.ctypes.data, C.byref(ch)),
                "dsh_autotune")

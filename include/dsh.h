@@ -170,13 +170,21 @@ int dsh_set_stream(dsh_ctx *ctx, void *stream);
  * wavefield state, which is rebuilt by the next call. */
 int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
 
+/* Step-kernel variants (dsh_autotune, dsh_set_step_variant): 0 kernel pair,
+ * 1 pair with the shared-memory staged velocity kernel, 2 fused
+ * velocity+stress step (FDORDER <= 8), 3 one persistent launch per pass of
+ * plain forward modelling for grids whose tiles fit one wave, 4 one launch
+ * per pass of plain elastic forward modelling with the wavefield and model
+ * held in the shared memory of one 16-CTA (or 8-CTA) thread-block cluster
+ * per shot (FDORDER <= 8, grids whose ceil(NY/16)-row strips fit one CTA's
+ * shared memory, e.g. 500 x 200). */
+#define DSH_STEP_VARIANTS 5
+
 /* Step-kernel autotuner: times nsteps plain forward steps of every variant
- * this context can run on these shots (0 kernel pair, 1 pair with the
- * shared-memory staged velocity kernel, 2 fused velocity+stress step,
- * 3 one persistent launch per pass for grids that fit one wave), keeps the
- * fastest for the context's later calls and reports ms_per_step[4] (0 where a
- * variant does not apply) and *choice.  Results do not depend on the choice
- * (all variants are bit-identical). */
+ * this context can run on these shots, keeps the fastest for the context's
+ * later calls and reports ms_per_step[DSH_STEP_VARIANTS] (0 where a variant
+ * does not apply) and *choice.  Results do not depend on the choice (all
+ * variants are bit-identical). */
 int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int nsteps, float *ms_per_step, int *choice);
 
 /* The same for the fused step kernel (one launch per time step; used when
@@ -342,10 +350,9 @@ int dsh_set_misfit(dsh_ctx *ctx, int lnorm);
  * Small limits exist to exercise those paths. */
 int dsh_set_wait_limits(dsh_ctx *ctx, long long device_polls, double host_seconds);
 
-/* Pins the step-kernel variant (0 kernel pair, 1 pair with shared-memory
- * staged velocity taps, 2 fused step (FDORDER <= 8), 3 persistent launch of
- * plain forward modelling when all tiles fit one wave, else the pair; -1 the
- * defaults) — what dsh_autotune picks by timing. */
+/* Pins the step-kernel variant (0 .. DSH_STEP_VARIANTS-1 as listed at
+ * DSH_STEP_VARIANTS; 3 and 4 fall back to the pair where they do not apply;
+ * -1 the defaults) — what dsh_autotune picks by timing. */
 int dsh_set_step_variant(dsh_ctx *ctx, int variant);
 
 /* Per-shot circular taper (SWS_TAPER_CIRCULAR_PER_SHOT, src/taper_grad_shot.c,
