@@ -633,6 +633,55 @@ static void build_tmaps(dsh_ctx *ctx)
     ctx->tma_ok = 1;
 }
 
+/* The per-point model coefficients on the device: the loops of
+ * dsh_setup_model (brho, the harmonic averages uip/ujp with the periodic
+ * one-rank neighbour) and dsh_setup_visc_base (taus = 2/Qs, its four-point
+ * average tausipjp, the relaxed moduli muip/mujp) in csrc/dsh_setup.c, with
+ * the same float/double expressions in the same order and no multiply-add
+ * contraction, so every field is identical to the host's.  Inputs and
+ * outputs are [ny][pitch] fields, point (i, j) at (j-1)*pitch + i-1+HX. */
+struct ModelArgs {
+    int nx, ny, pitch, l;
+    float sumu;
+    const float *vs, *rho, *qs;
+    float *brho, *uip, *ujp, *muip, *mujp, *tip, *taus;
+};
+
+static __global__ void model_coef_kernel(ModelArgs m)
+{
+    const long long n = (long long)m.nx * m.ny;
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        const int j = (int)(q / m.nx) + 1, i = (int)(q % m.nx) + 1;
+        const int ie = i < m.nx ? i + 1 : 1, je = j < m.ny ? j + 1 : 1;   /* periodic neighbour (one rank) */
+        const long long c = (long long)(j - 1) * m.pitch + (i - 1 + HX), e = (long long)(j - 1) * m.pitch + (ie - 1 + HX);
+        const long long sx = (long long)(je - 1) * m.pitch + (i - 1 + HX);
+        const float rho_c = m.rho[c], vs_c = m.vs[c];
+        float b = 1.0 / rho_c;
+        if (rho_c < 1e-20) b = 0.0;
+        m.brho[c] = b;
+        const float mu_c = rho_c * vs_c * vs_c;
+        const float mu_e = m.rho[e] * m.vs[e] * m.vs[e];
+        const float mu_s = m.rho[sx] * m.vs[sx] * m.vs[sx];
+        float ui = 2.0 / ((1.0 / mu_c) + (1.0 / mu_e));
+        float uj = 2.0 / ((1.0 / mu_c) + (1.0 / mu_s));
+        if ((mu_c == 0.0) || (mu_e == 0.0)) ui = 0.0;
+        if ((mu_c == 0.0) || (mu_s == 0.0)) uj = 0.0;
+        m.uip[c] = ui;
+        m.ujp[c] = uj;
+        if (m.l > 0) {
+            const long long se = (long long)(je - 1) * m.pitch + (ie - 1 + HX);
+            const float t_c = 2.0 / m.qs[c], t_e = 2.0 / m.qs[e], t_s = 2.0 / m.qs[sx], t_se = 2.0 / m.qs[se];
+            const float t_ip = 0.25 * (t_c + t_e + t_s + t_se);
+            const float u_jp = uj / (1.0 + m.sumu * t_c);
+            const float u_ip = ui / (1.0 + m.sumu * t_ip);
+            m.taus[c] = t_c;
+            m.tip[c] = t_ip;
+            m.mujp[c] = u_jp;
+            m.muip[c] = u_ip;
+        }
+    }
+}
+
 static int upload_field(dsh_ctx *ctx, float *dst, const float *src)
 {
     CK(cudaMemcpy2DAsync(dst + HX, (size_t)ctx->pitch * sizeof(float), src, (size_t)ctx->p.nx * sizeof(float),
@@ -654,14 +703,11 @@ extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, co
         if (L > 0 && !(qs[k] > 0)) bad |= 1;
     }
     if (bad) return DSH_ERR_PARAM;
-    std::vector<float> brho(n), uip(n), ujp(n), muip(L ? n : 1), mujp(L ? n : 1), tip(L ? n : 1), taus(L ? n : 1);
     if (dsh_setup_holberg(p.fdorder, p.maxrelerror, ctx->hc) != 0) return DSH_ERR_PARAM;
-    if (dsh_setup_model(p.nx, p.ny, L, p.fl, p.dt, vs, rho, qs, brho.data(), uip.data(), ujp.data(), nullptr, nullptr,
-                        nullptr, nullptr, ctx->bip, ctx->bjm, ctx->cip, ctx->cjm, ctx->cnorm) != 0)
-        return DSH_ERR_PARAM;
-    if (L > 0 && dsh_setup_visc_base(p.nx, p.ny, L, p.fl, p.dt, vs, rho, qs, muip.data(), mujp.data(), tip.data(),
-                                     taus.data(), ctx->eta) != 0)
-        return DSH_ERR_PARAM;
+    if (L > 0) {
+        if (dsh_setup_sls(L, p.fl, p.dt, ctx->eta, ctx->bip, ctx->bjm, ctx->cip, ctx->cjm) != 0) return DSH_ERR_PARAM;
+        ctx->sumu = dsh_setup_sumu(L, p.fl);
+    }
     dsh_pml pml;
     float damping = p.damping;
     if (!(damping > 0)) damping = *std::max_element(vs, vs + n);
@@ -672,22 +718,22 @@ extern "C" int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, co
     std::vector<float> pmlh(12 * vlen);
     for (int k = 0; k < 12; k++) memcpy(&pmlh[k * vlen], vecs[k], vlen * sizeof(float));
     CK(cudaMemcpyAsync(ctx->pml, pmlh.data(), pmlh.size() * sizeof(float), cudaMemcpyHostToDevice, ctx->st));
+    /* the model in, the coefficient fields formed on the device */
     int rc;
-    if ((rc = upload_field(ctx, ctx->m_brho, brho.data())) != DSH_OK) return rc;
-    if ((rc = upload_field(ctx, ctx->m_uip, uip.data())) != DSH_OK) return rc;
-    if ((rc = upload_field(ctx, ctx->m_ujp, ujp.data())) != DSH_OK) return rc;
     if ((rc = upload_field(ctx, ctx->m_vs, vs)) != DSH_OK) return rc;
     if ((rc = upload_field(ctx, ctx->m_rho, rho)) != DSH_OK) return rc;
-    if (L > 0) {
-        if ((rc = upload_field(ctx, ctx->m_muip, muip.data())) != DSH_OK) return rc;
-        if ((rc = upload_field(ctx, ctx->m_mujp, mujp.data())) != DSH_OK) return rc;
-        if ((rc = upload_field(ctx, ctx->m_tip, tip.data())) != DSH_OK) return rc;
-        if ((rc = upload_field(ctx, ctx->m_taus, taus.data())) != DSH_OK) return rc;
-        if ((rc = upload_field(ctx, ctx->m_qs, qs)) != DSH_OK) return rc;
-        ctx->sumu = dsh_setup_sumu(L, p.fl);
-    }
+    if (L > 0 && (rc = upload_field(ctx, ctx->m_qs, qs)) != DSH_OK) return rc;
+    ModelArgs ma;
+    ma.nx = p.nx; ma.ny = p.ny; ma.pitch = ctx->pitch; ma.l = L; ma.sumu = ctx->sumu;
+    ma.vs = ctx->m_vs; ma.rho = ctx->m_rho; ma.qs = ctx->m_qs;
+    ma.brho = ctx->m_brho; ma.uip = ctx->m_uip; ma.ujp = ctx->m_ujp;
+    ma.muip = ctx->m_muip; ma.mujp = ctx->m_mujp; ma.tip = ctx->m_tip; ma.taus = ctx->m_taus;
+    model_coef_kernel<<<(unsigned)std::min<long long>(((long long)n + 255) / 256, 148LL * 8), 256, 0, ctx->st>>>(ma);
+    CK(cudaGetLastError());
+    /* meanwhile on the host: the vs/rho means (a sequential float sum in the reference's order) */
+    dsh_setup_cnorm(p.nx, p.ny, vs, rho, ctx->cnorm);
     ctx->gq_valid = 0;
-    WAIT(ctx);   /* host staging vectors go out of scope */
+    WAIT(ctx);   /* the caller's arrays and the staging vector are free again once this returns */
     ctx->model_set = 1;
     return DSH_OK;
 }
@@ -1907,6 +1953,13 @@ extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
     case 16: src = base + ctx->o_grho; break;
     case 17: src = base + ctx->o_hu; break;
     case 18: src = base + ctx->o_hrho; break;
+    case 300: src = ctx->m_brho; break;
+    case 301: src = ctx->m_uip; break;
+    case 302: src = ctx->m_ujp; break;
+    case 303: case 304: case 305: case 306:
+        if (p.l < 1) return DSH_ERR_PARAM;
+        src = which == 303 ? ctx->m_muip : which == 304 ? ctx->m_mujp : which == 305 ? ctx->m_tip : ctx->m_taus;
+        break;
     default: {
         const int l = which % 100;
         if (l >= p.l) return DSH_ERR_PARAM;

@@ -290,19 +290,45 @@ int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const floa
     if (!uip) free(mu_ip);
     if (!ujp) free(mu_jp);
 
-    if (cnorm) {   /* means in the reference's loop order (x outer, depth inner) */
-        float vs_sum = 0.0, rho_sum = 0.0;
-        int cnt = 0;
-        for (i = 1; i <= nx; i++)
-            for (j = 1; j <= ny; j++) {
-                vs_sum += vs[(size_t)(j - 1) * nx + i - 1];
-                rho_sum += rho[(size_t)(j - 1) * nx + i - 1];
-                cnt++;
-            }
-        vs_sum /= cnt;
-        rho_sum /= cnt;
-        cnorm[0] = vs_sum;
-        cnorm[1] = rho_sum;
+    if (cnorm) dsh_setup_cnorm(nx, ny, vs, rho, cnorm);
+    (void)i;
+    (void)j;
+    return 0;
+}
+
+void dsh_setup_cnorm(int nx, int ny, const float *vs, const float *rho, float *cnorm)
+{
+    /* means in the reference's loop order (x outer, depth inner) */
+    float vs_sum = 0.0, rho_sum = 0.0;
+    int cnt = 0;
+    int i, j;
+    for (i = 1; i <= nx; i++)
+        for (j = 1; j <= ny; j++) {
+            vs_sum += vs[(size_t)(j - 1) * nx + i - 1];
+            rho_sum += rho[(size_t)(j - 1) * nx + i - 1];
+            cnt++;
+        }
+    vs_sum /= cnt;
+    rho_sum /= cnt;
+    cnorm[0] = vs_sum;
+    cnorm[1] = rho_sum;
+}
+
+int dsh_setup_sls(int l, const float *fl, float dt, float *eta, float *bip, float *bjm, float *cip, float *cjm)
+{
+    float tau_sls[DSH_MAX_L], e[DSH_MAX_L];
+    int m;
+    if (l < 1 || l > DSH_MAX_L) return -1;
+    for (m = 0; m < l; m++) {
+        tau_sls[m] = 1.0 / (2.0 * DSH_PI * fl[m]);
+        e[m] = dt / tau_sls[m];
+    }
+    for (m = 0; m < l; m++) {
+        if (eta) eta[m] = e[m];
+        if (bip) bip[m] = 1.0 / (1.0 + (e[m] * 0.5));
+        if (bjm) bjm[m] = 1.0 / (1.0 + (e[m] * 0.5));
+        if (cip) cip[m] = 1.0 - (e[m] * 0.5);
+        if (cjm) cjm[m] = 1.0 - (e[m] * 0.5);
     }
     return 0;
 }

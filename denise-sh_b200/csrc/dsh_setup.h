@@ -41,6 +41,16 @@ int dsh_setup_model(int nx, int ny, int l, const float *fl, float dt, const floa
                     const float *qs, float *brho, float *uip, float *ujp, float *fipjp, float *f, float *dip,
                     float *d, float *bip, float *bjm, float *cip, float *cjm, float *cnorm);
 
+/* C_vs, C_rho: the means of vs and rho as float sums in the reference's loop
+ * order (x outer, depth inner), as dsh_setup_model forms cnorm */
+void dsh_setup_cnorm(int nx, int ny, const float *vs, const float *rho, float *cnorm);
+
+/* The per-mechanism scalars of dsh_setup_model / dsh_setup_visc_base for
+ * l >= 1 relaxation mechanisms: eta_l = DT/tau_l (readmod.c:30-33) and the
+ * memory-variable factors bip, bjm, cip, cjm (prepare_update_s.c:52-55);
+ * NULL outputs are skipped. */
+int dsh_setup_sls(int l, const float *fl, float dt, float *eta, float *bip, float *bjm, float *cip, float *cjm);
+
 /* sum_l w^2 tau_l^2 / (1 + w^2 tau_l^2), w = 2 pi FL[1] (prepare_update_s.c:24-32), as
  * dsh_setup_visc_base forms it */
 float dsh_setup_sumu(int l, const float *fl);

@@ -25,7 +25,8 @@ ERRORS = {-1: "invalid parameter", -2: "CUDA error", -3: "out of device memory o
 ERR_PARAM, ERR_CUDA, ERR_OOM, ERR_UNSTABLE, ERR_STATE, ERR_TIMEOUT = -1, -2, -3, -4, -5, -6
 
 FIELD = {"vy": 0, "sxy": 1, "syz": 2, "Ws": 12, "Wr": 13, "We": 14, "g_u": 15, "g_rho": 16, "hess_u": 17,
-         "hess_rho": 18}
+         "hess_rho": 18, "brho": 300, "uip": 301, "ujp": 302, "muip": 303, "mujp": 304, "tausipjp": 305,
+         "taus": 306}
 
 
 class DshError(RuntimeError):
@@ -123,6 +124,7 @@ def lib() -> C.CDLL:
         L.dsh_setup_pml.argtypes = [C.c_int, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float, C.c_float,
                                     C.c_float, C.c_float, C.c_void_p]
         L.dsh_setup_model.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_float] + [C.c_void_p] * 15
+        L.dsh_setup_visc_base.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_float] + [C.c_void_p] * 8
         L.dsh_setup_wavelet.argtypes = [C.c_int, C.c_int, C.c_float, C.c_int, C.c_void_p, C.c_void_p]
         L.dsh_setup_dt_limit.restype = C.c_double
         L.dsh_setup_dt_limit.argtypes = [C.c_int, C.c_int, C.c_float, C.c_float]
@@ -587,6 +589,24 @@ def model_coefficients(vs, rho, qs=None, l=0, fl=(), dt=1e-4) -> dict:
                                *[x.ctypes.data for x in sls], cn.ctypes.data)
     _check(rc, "dsh_setup_model")
     out.update(dip=dip[:l], d=d[:l], bip=sls[0][:l], bjm=sls[1][:l], cip=sls[2][:l], cjm=sls[3][:l], cnorm=cn)
+    return out
+
+
+def visc_base(vs, rho, qs, l, fl, dt) -> dict:
+    """dsh_setup_visc_base on the host: relaxed moduli muip, mujp, tausipjp, taus and eta."""
+    vs = np.ascontiguousarray(vs, np.float32)
+    rho = np.ascontiguousarray(rho, np.float32)
+    qs = np.ascontiguousarray(qs, np.float32)
+    ny, nx = vs.shape
+    flv = np.zeros(8, np.float32)
+    flv[:len(fl)] = fl
+    out = {k: np.zeros((ny, nx), np.float32) for k in ("muip", "mujp", "tausipjp", "taus")}
+    eta = np.zeros(8, np.float32)
+    _check(lib().dsh_setup_visc_base(nx, ny, l, flv.ctypes.data, dt, vs.ctypes.data, rho.ctypes.data,
+                                     qs.ctypes.data, out["muip"].ctypes.data, out["mujp"].ctypes.data,
+                                     out["tausipjp"].ctypes.data, out["taus"].ctypes.data, eta.ctypes.data),
+           "dsh_setup_visc_base")
+    out["eta"] = eta[:l]
     return out
 
 

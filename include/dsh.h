@@ -153,7 +153,10 @@ int dsh_forward_device(dsh_ctx *ctx, const dsh_shot *shots, int nshots, float *s
 
 /* Inspection of the last run (tests and tools): copies a wavefield of shot
  * slot `shot` to host [ny][nx].  which: 0 vy, 1 sxy, 2 syz, 100+l r_l, 200+l q_l,
- * 12 Ws, 13 Wr, 14 We, 15 per-shot g_u (scaled), 16 per-shot g_rho (scaled). */
+ * 12 Ws, 13 Wr, 14 We, 15 per-shot g_u (scaled), 16 per-shot g_rho (scaled),
+ * 17 / 18 Hessian sums; the model coefficients that dsh_set_model forms on
+ * the device (any slot): 300 1/rho, 301 uip, 302 ujp, and for L > 0 the
+ * relaxed moduli 303 muip, 304 mujp and 305 tausipjp, 306 taus. */
 int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out);
 
 /* Runs the context's work on the caller's CUDA stream (a cudaStream_t passed

@@ -85,3 +85,15 @@ def test_dt_limit():
     hc = dsh.holberg(8, 1)
     expect = 0.25 / (np.sqrt(2.0) * np.abs(hc[1:]).astype(np.float64).sum() * 500.0)
     assert abs(dsh.dt_limit(8, 1, 0.25, 500.0) - expect) < 1e-12
+
+
+def test_visc_base_binding_runs_on_cpu():
+    """The host restatement the device coefficient kernel is checked against
+    (dsh_setup_visc_base) is callable and gives tau = 2/Qs."""
+    rng = np.random.default_rng(5)
+    vs = rng.uniform(150, 400, (9, 11)).astype(np.float32)
+    rho = rng.uniform(1800, 2100, (9, 11)).astype(np.float32)
+    qs = rng.uniform(20, 60, (9, 11)).astype(np.float32)
+    b = dsh.visc_base(vs, rho, qs, 3, (7.5, 30.0, 120.0), 2e-4)
+    assert np.array_equal(b["taus"], (2.0 / qs.astype(np.float64)).astype(np.float32))
+    assert np.all(b["muip"] > 0) and np.all(b["mujp"] > 0)
