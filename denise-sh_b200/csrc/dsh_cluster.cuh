@@ -11,9 +11,9 @@
  * j0[k] .. j0[k+1]-1 of vy, sxy, syz, of the model factors 1/rho, uip, ujp
  * and of the CPML memory in its shared memory for the whole pass, plus
  * H = FDORDER/2 halo rows of vy and syz above and below.  One time step is
- *     velocity update of the own rows -> injection, sampling (one warp) ->
- *     cluster barrier -> copy the neighbours' H boundary rows of vy into the
- *     halo (distributed shared memory) -> stress update of the own rows ->
+ *     velocity update of the own rows -> injection (one warp) -> cluster
+ *     barrier -> sampling; copy the neighbours' H boundary rows of vy into
+ *     the halo (distributed shared memory) -> stress update of the own rows ->
  *     cluster barrier -> copy the neighbours' boundary rows of syz
  * (sxy is only differentiated along x, inside a row, so it needs no halo).
  * The barriers are the hardware cluster barrier (arrive with release, wait
@@ -496,21 +496,23 @@ __global__ void __launch_bounds__(cl_max_threads(FDO), 1) cl_fwd(StepArgs a, int
             }
         }
         __syncthreads();
-        if (tid < 32) {                               /* injection (sources of a point in the reference's
-                                                         order), then sampling */
-            if (run && tid < ngrp) {
-                float x = vyf[gpt];
-                for (int m = 0; m < gn; m++) x = x + gnext[m];
-                vyf[gpt] = x;
-            }
-            __syncwarp();
+        if (run && tid < ngrp) {                      /* injection: sources of a point in the reference's order */
+            float x = vyf[gpt];
+            for (int m = 0; m < gn; m++) x = x + gnext[m];
+            vyf[gpt] = x;
+        }
+        cl.sync();                                    /* every velocity of the step is in place */
+        if (tid < 32) {
+            /* sampling and the next step's signals after the barrier, so that
+               these global accesses complete during the stress phase instead of
+               holding the barrier's release (own rows of vy stay unchanged
+               until the next velocity phase) */
             if (run && a.tl.sample)
                 for (int e = tid; e < nrec; e += 32) seis[(long long)(nt - 1) * ntr + rec[2 * e + 1]] = vyf[rec[2 * e]];
             if (tid < ngrp && nt + 1 <= a.nt_last)
                 for (int m = 0; m < gn; m++)
                     gnext[m] = sig[(long long)gsid[m] * a.tl.sig_ss + (long long)nt * a.tl.sig_ts];
         }
-        cl.sync();                                    /* every velocity of the step is in place */
         cl_halo(cl, cl_smem, L.vy, Lu.vy, Ld.vy, rank, has_up, has_dn, r, ru, H, p4);
         __syncthreads();
         if (run) {
