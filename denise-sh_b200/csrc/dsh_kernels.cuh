@@ -429,13 +429,15 @@ __device__ __forceinline__ void v_body(const StepArgs &a, int nt_off, int i0, in
     }
 }
 
-/* one thread block = 128 x 8 points of one shot slot (grid z) */
+/* one thread block = 128 x blockDim.y points of one shot slot (grid z),
+ * blockDim.y dividing the 8 rows of an injection / sampling list tile */
 template <int FDO, int FLAGS, bool P2>
 __global__ void __launch_bounds__(BX *BY, (FLAGS & (VF_CORR | VF_HESS)) ? VSTEP_MIN_BLOCKS : VSTEP_MIN_BLOCKS_FWD)
     v_step(StepArgs a, int nt_off)
 {
-    v_body<FDO, FLAGS, P2>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
-                           blockIdx.z, blockIdx.y * gridDim.x + blockIdx.x);
+    const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
+    v_body<FDO, FLAGS, P2>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), j, blockIdx.z,
+                           ((j - 1) / BY) * gridDim.x + blockIdx.x);
 }
 
 /*
@@ -964,11 +966,13 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     }
 }
 
-/* one thread block = 128 x 8 points of one shot slot (grid z) */
+/* one thread block = 128 x blockDim.y points of one shot slot (grid z);
+ * blockDim.y = 8, 4 or 2 (a shorter block lifetime shortens the last,
+ * partly idle wave of a launch) */
 template <int FDO, int L, int FLAGS>
 __global__ void __launch_bounds__(BX *BY, SSTEP_MIN_BLOCKS) s_step(StepArgs a, int nt_off)
 {
-    s_body<FDO, L, FLAGS>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * BY + threadIdx.y,
+    s_body<FDO, L, FLAGS>(a, nt_off, 1 + 4 * (blockIdx.x * BX + threadIdx.x), 1 + blockIdx.y * blockDim.y + threadIdx.y,
                           blockIdx.z);
 }
 
