@@ -281,6 +281,26 @@ def test_persistent_forward_in_subprocess():
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
 
 
+def test_other_block_heights_in_subprocess():
+    """The stress and velocity launches take 128 x 4-point blocks by default;
+    8- and 2-row blocks (DSH_SROWS / DSH_VBROWS, read once per process, so in
+    a child process) give the same results bit for bit: random cases,
+    multi-shot batches and checkpointed gradients."""
+    import subprocess
+    import sys
+
+    code = ("import sys; sys.argv=['x']; import pytest; "
+            "sys.exit(pytest.main(['-q', '-p', 'no:cacheprovider', '-m', 'gpu', "
+            "'tests/test_gpu_parity.py::test_random_cases_vs_oracle', "
+            "'tests/test_gpu_parity.py::test_multi_shot_batches', 'tests/test_gpu_checkpoint.py']))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for rows in (("8", "2"), ("2", "8")):
+        env = dict(os.environ, DSH_SROWS=rows[0], DSH_VBROWS=rows[1])
+        out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True,
+                             timeout=900)
+        assert out.returncode == 0, rows + (out.stdout[-2000:] + out.stderr[-2000:],)
+
+
 def test_tma_velocity_kernel_in_subprocess():
     """The opt-in persistent velocity kernel whose stress taps the tensor-memory
     accelerator stages in shared memory (DSH_VTMA=1, read once per process, so
