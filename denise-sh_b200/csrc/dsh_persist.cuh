@@ -34,9 +34,10 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p)
  * (H <= 6 points, less than a tile in either direction) and overwrites the
  * velocities they read in their stress update of step k-1, so it waits until
  * those tiles' stress flags reach k-1; the stress update of step k waits for
- * their velocity flags to reach k in the same way.  Thread 0 polls with
- * acquire loads, at most `limit` polls in all (StepArgs::wait_polls); on
- * expiry the block sets bit 2 of the status word and leaves its time loop,
+ * their velocity flags to reach k in the same way.  Eight threads poll the
+ * eight flags with acquire loads, at most `limit` polls each
+ * (StepArgs::wait_polls); on expiry the block sets bit 2 of the status word
+ * and leaves its time loop,
  * and the host reports DSH_ERR_TIMEOUT.  A tile publishes a flag after a
  * block barrier and a fence (cumulative: the block's stores are ordered
  * before the flag). */
@@ -48,19 +49,22 @@ __device__ __forceinline__ void st_release(unsigned *p, unsigned v)
 __device__ __forceinline__ bool wait_tiles(const unsigned *flags, int bx, int by, int gx, int gy, unsigned need,
                                            long long limit, int *status)
 {
+    /* the 8 neighbours' flags are polled at once, one thread each (each
+       acquire load is an L2 round trip; one thread polling them in turn paid
+       eight per phase); the block barrier then orders every thread's loads
+       after the acquiring loads */
     __shared__ int ok;
+    const int t = threadIdx.y * blockDim.x + threadIdx.x;
+    if (t == 0) ok = 1;
     __syncthreads();
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
-        ok = 1;
-        long long it = 0;
-        for (int dy = -1; dy <= 1 && ok; dy++)
-            for (int dx = -1; dx <= 1 && ok; dx++) {
-                const int x = bx + dx, y = by + dy;
-                if (x < 0 || x >= gx || y < 0 || y >= gy) continue;
-                const unsigned *f = flags + y * gx + x;
-                while (ld_acquire(f) < need)
-                    if (++it >= limit) { atomicOr(status, 2); ok = 0; break; }
-            }
+    if (t < 9 && t != 4) {
+        const int x = bx + t % 3 - 1, y = by + t / 3 - 1;
+        if (x >= 0 && x < gx && y >= 0 && y < gy) {
+            const unsigned *f = flags + y * gx + x;
+            long long it = 0;
+            while (ld_acquire(f) < need)
+                if (++it >= limit) { atomicOr(status, 2); ok = 0; break; }
+        }
     }
     __syncthreads();
     return ok != 0;
