@@ -26,6 +26,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <numeric>
 #include <vector>
 
@@ -45,6 +46,8 @@ struct dsh_batch {
     cudaStream_t st = nullptr, own_st = nullptr;
     int *d_nt = nullptr;
     StepArgs *d_args = nullptr;
+    std::unique_ptr<MultiParams> hp;       /* the same in the kernels' parameter space (batches of up to
+                                              MULTI_PARAM_MODELS models; DSH_MULTI_ARGS_DEVICE=1: never) */
     int4 *d_map = nullptr;                 /* MULTI_NVAR maps, each of map_cap entries */
     long long map_cap = 0;
     std::vector<int> order;                /* models by NT, longest first */
@@ -247,6 +250,14 @@ static int upload_args(dsh_batch *b)
         a[k].nslots = b->nb[k];
     }
     BK(cudaMemcpyAsync(b->d_args, a.data(), a.size() * sizeof(StepArgs), cudaMemcpyHostToDevice, b->st));
+    static const bool device_only = getenv("DSH_MULTI_ARGS_DEVICE") != nullptr;
+    if (b->n <= MULTI_PARAM_MODELS && !device_only) {
+        if (!b->hp) b->hp.reset(new MultiParams());
+        memset(b->hp.get(), 0, sizeof(MultiParams));
+        for (int k = 0; k < b->n; k++) b->hp->m[k] = a[k];
+    } else {
+        b->hp.reset();
+    }
     BWAIT(b);
     return DSH_OK;
 }
@@ -281,7 +292,8 @@ static int launch_chunk(dsh_batch *b, int ph, int K, long long *nl)
         cfg.stream = b->st;
         cfg.attrs = (use_pdl && k > 0) ? &attr : nullptr;
         cfg.numAttrs = (use_pdl && k > 0) ? 1 : 0;
-        BK(cudaLaunchKernelEx(&cfg, vk, args, map_v, off));
+        if (b->hp) BK(cudaLaunchKernelEx(&cfg, v_multi_p_kernel(b->var_v), *b->hp, map_v, off));
+        else BK(cudaLaunchKernelEx(&cfg, vk, args, map_v, off));
         for (auto &s : sep) {
             void *iargs[2] = {&s.second, &off};
             BK(cudaLaunchKernel((const void *)inject_sample, dim3(s.first), dim3(128), iargs, 0, b->st));
@@ -291,7 +303,8 @@ static int launch_chunk(dsh_batch *b, int ph, int K, long long *nl)
         cfg.gridDim = dim3((unsigned)nblk_s);
         cfg.attrs = use_pdl ? &attr : nullptr;
         cfg.numAttrs = use_pdl ? 1 : 0;
-        BK(cudaLaunchKernelEx(&cfg, sk, args, map_s, off));
+        if (b->hp) BK(cudaLaunchKernelEx(&cfg, s_multi_p_kernel(b->var_s), *b->hp, map_s, off));
+        else BK(cudaLaunchKernelEx(&cfg, sk, args, map_s, off));
         *nl += 2;
     }
     advance_step<<<1, 1, 0, b->st>>>(b->d_nt, K);
@@ -359,13 +372,15 @@ static int tune(dsh_batch *b)
             b->tune_ms[kind][v] = 0;
             if (forced >= 0 && v != forced) continue;
             MultiFn fn = kind ? s_multi_kernel(v) : v_multi_kernel(v);
+            MultiPFn fp = kind ? s_multi_p_kernel(v) : v_multi_p_kernel(v);
             const int4 *map = b->d_map + (size_t)v * b->map_cap;
             const unsigned nblk = (unsigned)b->prefix[v][0];
             if (nblk == 0) continue;
             batch_set_counter<<<1, 1, 0, b->st>>>(b->d_nt, 1);
             for (int r = 0; r < reps + 2; r++) {
                 if (r == 2) BK(cudaEventRecord(e0, b->st));
-                fn<<<nblk, dim3(BX, MULTI_ROWS[v], MULTI_SPB[v]), 0, b->st>>>(b->d_args, map, 0);
+                if (b->hp) fp<<<nblk, dim3(BX, MULTI_ROWS[v], MULTI_SPB[v]), 0, b->st>>>(*b->hp, map, 0);
+                else fn<<<nblk, dim3(BX, MULTI_ROWS[v], MULTI_SPB[v]), 0, b->st>>>(b->d_args, map, 0);
             }
             BK(cudaEventRecord(e1, b->st));
             BWAIT(b);

@@ -32,21 +32,23 @@ __host__ __device__ constexpr bool multi_supported(int fdo, int l)
     return (fdo == 4 || fdo == 6 || fdo == 8) && (l == 0 || l == 2);
 }
 
-/* Block prologue: the model's StepArgs into shared memory, then this
- * thread's point vector, row, slot and injection/sampling list tile.
- * Returns false for threads on slots the model does not use this run. */
+/* Batches of up to MULTI_PARAM_MODELS models pass every model's StepArgs in
+ * the kernel's parameter space (840 B each, within the 32 KB parameter
+ * limit): a block reads its model's fields there (constant cache) and starts
+ * its loads at once, instead of first copying the 840 B into shared memory
+ * behind a block barrier. */
+constexpr int MULTI_PARAM_MODELS = 36;
+struct MultiParams {
+    StepArgs m[MULTI_PARAM_MODELS];
+};
+static_assert(sizeof(MultiParams) + 16 <= 32764, "kernel parameter space");
+
+/* this thread's point vector, row, slot and injection/sampling list tile
+ * for map entry m; false for threads on slots the model does not use */
 template <int ROWS, int SPB>
-__device__ __forceinline__ bool multi_setup(StepArgs &sa, const StepArgs *__restrict__ args,
-                                            const int4 *__restrict__ map, int &i0, int &j, int &slot, int &tile)
+__device__ __forceinline__ bool multi_point(const StepArgs &sa, const int4 &m, int &i0, int &j, int &slot, int &tile)
 {
     static_assert(ROWS * SPB == BY, "256-thread blocks");
-    static_assert(sizeof(StepArgs) % 4 == 0, "word copy");
-    const int4 m = map[blockIdx.x];
-    const int tid = threadIdx.x + BX * (threadIdx.y + ROWS * threadIdx.z);
-    const int *src = reinterpret_cast<const int *>(args + m.x);
-    int *dst = reinterpret_cast<int *>(&sa);
-    for (int k = tid; k < (int)(sizeof(StepArgs) / 4); k += BX * BY) dst[k] = __ldg(src + k);
-    __syncthreads();
     i0 = 1 + 4 * (m.y * BX + threadIdx.x);
     j = 1 + m.z * ROWS + threadIdx.y;
     slot = m.w * SPB + threadIdx.z;
@@ -54,14 +56,25 @@ __device__ __forceinline__ bool multi_setup(StepArgs &sa, const StepArgs *__rest
     return slot < sa.nslots;
 }
 
-/* velocity half-step of plain forward modelling (flags 0) for all models */
+/* Block prologue of the device-array form: the model's StepArgs into shared
+ * memory, then multi_point. */
 template <int ROWS, int SPB>
-__global__ void __launch_bounds__(BX *BY, 3) v_multi(const StepArgs *__restrict__ args, const int4 *__restrict__ map,
-                                                     int nt_off)
+__device__ __forceinline__ bool multi_setup(StepArgs &sa, const StepArgs *__restrict__ args,
+                                            const int4 *__restrict__ map, int &i0, int &j, int &slot, int &tile)
 {
-    __shared__ StepArgs sa;
-    int i0, j, slot, tile;
-    if (!multi_setup<ROWS, SPB>(sa, args, map, i0, j, slot, tile)) return;
+    static_assert(sizeof(StepArgs) % 4 == 0, "word copy");
+    const int4 m = map[blockIdx.x];
+    const int tid = threadIdx.x + BX * (threadIdx.y + ROWS * threadIdx.z);
+    const int *src = reinterpret_cast<const int *>(args + m.x);
+    int *dst = reinterpret_cast<int *>(&sa);
+    for (int k = tid; k < (int)(sizeof(StepArgs) / 4); k += BX * BY) dst[k] = __ldg(src + k);
+    __syncthreads();
+    return multi_point<ROWS, SPB>(sa, m, i0, j, slot, tile);
+}
+
+/* the per-point bodies, picked from the model's FDORDER, L and DH */
+__device__ __forceinline__ void v_multi_body(const StepArgs &sa, int nt_off, int i0, int j, int slot, int tile)
+{
     switch (sa.fdo * 2 + sa.p2) {
     case 8: v_body<4, 0, false>(sa, nt_off, i0, j, slot, tile); break;
     case 9: v_body<4, 0, true>(sa, nt_off, i0, j, slot, tile); break;
@@ -72,15 +85,8 @@ __global__ void __launch_bounds__(BX *BY, 3) v_multi(const StepArgs *__restrict_
     default: break;
     }
 }
-
-/* stress half-step of plain forward modelling (flags 0) for all models */
-template <int ROWS, int SPB>
-__global__ void __launch_bounds__(BX *BY, 2) s_multi(const StepArgs *__restrict__ args, const int4 *__restrict__ map,
-                                                     int nt_off)
+__device__ __forceinline__ void s_multi_body(const StepArgs &sa, int nt_off, int i0, int j, int slot)
 {
-    __shared__ StepArgs sa;
-    int i0, j, slot, tile;
-    if (!multi_setup<ROWS, SPB>(sa, args, map, i0, j, slot, tile)) return;
     switch (sa.fdo * 8 + sa.l) {
     case 32: s_body<4, 0, 0>(sa, nt_off, i0, j, slot); break;
     case 34: s_body<4, 2, 0>(sa, nt_off, i0, j, slot); break;
@@ -92,8 +98,54 @@ __global__ void __launch_bounds__(BX *BY, 2) s_multi(const StepArgs *__restrict_
     }
 }
 
+/* velocity / stress half-step of plain forward modelling (flags 0) for all
+ * models: StepArgs from a device array ... */
+template <int ROWS, int SPB>
+__global__ void __launch_bounds__(BX *BY, 3) v_multi(const StepArgs *__restrict__ args, const int4 *__restrict__ map,
+                                                     int nt_off)
+{
+    __shared__ StepArgs sa;
+    int i0, j, slot, tile;
+    if (!multi_setup<ROWS, SPB>(sa, args, map, i0, j, slot, tile)) return;
+    v_multi_body(sa, nt_off, i0, j, slot, tile);
+}
+template <int ROWS, int SPB>
+__global__ void __launch_bounds__(BX *BY, 2) s_multi(const StepArgs *__restrict__ args, const int4 *__restrict__ map,
+                                                     int nt_off)
+{
+    __shared__ StepArgs sa;
+    int i0, j, slot, tile;
+    if (!multi_setup<ROWS, SPB>(sa, args, map, i0, j, slot, tile)) return;
+    s_multi_body(sa, nt_off, i0, j, slot);
+}
+
+/* ... or from the parameter space */
+template <int ROWS, int SPB>
+__global__ void __launch_bounds__(BX *BY, 3) v_multi_p(const __grid_constant__ MultiParams P,
+                                                       const int4 *__restrict__ map, int nt_off)
+{
+    const int4 m = map[blockIdx.x];
+    const StepArgs &sa = P.m[m.x];
+    int i0, j, slot, tile;
+    if (!multi_point<ROWS, SPB>(sa, m, i0, j, slot, tile)) return;
+    v_multi_body(sa, nt_off, i0, j, slot, tile);
+}
+template <int ROWS, int SPB>
+__global__ void __launch_bounds__(BX *BY, 2) s_multi_p(const __grid_constant__ MultiParams P,
+                                                       const int4 *__restrict__ map, int nt_off)
+{
+    const int4 m = map[blockIdx.x];
+    const StepArgs &sa = P.m[m.x];
+    int i0, j, slot, tile;
+    if (!multi_point<ROWS, SPB>(sa, m, i0, j, slot, tile)) return;
+    s_multi_body(sa, nt_off, i0, j, slot);
+}
+
 using MultiFn = void (*)(const StepArgs *, const int4 *, int);
+using MultiPFn = void (*)(const MultiParams, const int4 *, int);
 MultiFn v_multi_kernel(int variant);
 MultiFn s_multi_kernel(int variant);
+MultiPFn v_multi_p_kernel(int variant);
+MultiPFn s_multi_p_kernel(int variant);
 
 }  // namespace dsh

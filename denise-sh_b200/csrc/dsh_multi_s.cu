@@ -11,4 +11,13 @@ MultiFn s_multi_kernel(int variant)
     default: return nullptr;
     }
 }
+MultiPFn s_multi_p_kernel(int variant)
+{
+    switch (variant) {
+    case 0: return s_multi_p<8, 1>;
+    case 1: return s_multi_p<4, 2>;
+    case 2: return s_multi_p<2, 4>;
+    default: return nullptr;
+    }
+}
 }  // namespace dsh

@@ -11,4 +11,13 @@ MultiFn v_multi_kernel(int variant)
     default: return nullptr;
     }
 }
+MultiPFn v_multi_p_kernel(int variant)
+{
+    switch (variant) {
+    case 0: return v_multi_p<8, 1>;
+    case 1: return v_multi_p<4, 2>;
+    case 2: return v_multi_p<2, 4>;
+    default: return nullptr;
+    }
+}
 }  // namespace dsh
