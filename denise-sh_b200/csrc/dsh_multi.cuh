@@ -8,11 +8,13 @@
  * the model's FDORDER and L (uniform across the block, so no divergence).
  * Results are therefore bit-identical to the single-model kernels.
  *
- * Tile-shape variants: a block is always 256 threads, 32 along x (4 points
- * each, 128 points), ROWS rows and SPB shot slots of the same model
- * (ROWS * SPB = 8).  Blocks that share a model's coefficients across SPB shots
- * read them once from L2 per block instead of once per shot; the batch
- * autotuner times the variants on the actual batch and keeps the fastest.
+ * Tile-shape variants: a block is 32 threads along x (4 points each, 128
+ * points), ROWS rows and SPB shot slots of the same model: 256 threads
+ * (ROWS * SPB = 8) or, for 128 x 4 points of one shot, 128 threads (a
+ * shorter block lifetime, a shorter partly idle last wave).  Blocks that
+ * share a model's coefficients across SPB shots read them once from L2 per
+ * block instead of once per shot; the batch autotuner times the variants on
+ * the actual batch and keeps the fastest.
  *
  * Bodies compiled in: FDORDER 4, 6, 8 and L 0 (elastic), 2 (viscoelastic),
  * the operator and relaxation counts of uneven survey batches; the batch
@@ -23,9 +25,9 @@
 
 namespace dsh {
 
-constexpr int MULTI_NVAR = 3;
-constexpr int MULTI_ROWS[MULTI_NVAR] = {8, 4, 2};
-constexpr int MULTI_SPB[MULTI_NVAR] = {1, 2, 4};
+constexpr int MULTI_NVAR = 4;
+constexpr int MULTI_ROWS[MULTI_NVAR] = {8, 4, 2, 4};
+constexpr int MULTI_SPB[MULTI_NVAR] = {1, 2, 4, 1};
 
 __host__ __device__ constexpr bool multi_supported(int fdo, int l)
 {
@@ -48,7 +50,7 @@ static_assert(sizeof(MultiParams) + 16 <= 32764, "kernel parameter space");
 template <int ROWS, int SPB>
 __device__ __forceinline__ bool multi_point(const StepArgs &sa, const int4 &m, int &i0, int &j, int &slot, int &tile)
 {
-    static_assert(ROWS * SPB == BY, "256-thread blocks");
+    static_assert(ROWS * SPB == BY || (ROWS == 4 && SPB == 1), "256-thread blocks or 128 x 4 points");
     i0 = 1 + 4 * (m.y * BX + threadIdx.x);
     j = 1 + m.z * ROWS + threadIdx.y;
     slot = m.w * SPB + threadIdx.z;
@@ -67,7 +69,7 @@ __device__ __forceinline__ bool multi_setup(StepArgs &sa, const StepArgs *__rest
     const int tid = threadIdx.x + BX * (threadIdx.y + ROWS * threadIdx.z);
     const int *src = reinterpret_cast<const int *>(args + m.x);
     int *dst = reinterpret_cast<int *>(&sa);
-    for (int k = tid; k < (int)(sizeof(StepArgs) / 4); k += BX * BY) dst[k] = __ldg(src + k);
+    for (int k = tid; k < (int)(sizeof(StepArgs) / 4); k += BX * ROWS * SPB) dst[k] = __ldg(src + k);
     __syncthreads();
     return multi_point<ROWS, SPB>(sa, m, i0, j, slot, tile);
 }

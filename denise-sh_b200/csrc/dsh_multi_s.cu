@@ -8,6 +8,7 @@ MultiFn s_multi_kernel(int variant)
     case 0: return s_multi<8, 1>;
     case 1: return s_multi<4, 2>;
     case 2: return s_multi<2, 4>;
+    case 3: return s_multi<4, 1>;
     default: return nullptr;
     }
 }
@@ -17,6 +18,7 @@ MultiPFn s_multi_p_kernel(int variant)
     case 0: return s_multi_p<8, 1>;
     case 1: return s_multi_p<4, 2>;
     case 2: return s_multi_p<2, 4>;
+    case 3: return s_multi_p<4, 1>;
     default: return nullptr;
     }
 }

@@ -8,6 +8,7 @@ MultiFn v_multi_kernel(int variant)
     case 0: return v_multi<8, 1>;
     case 1: return v_multi<4, 2>;
     case 2: return v_multi<2, 4>;
+    case 3: return v_multi<4, 1>;
     default: return nullptr;
     }
 }
@@ -17,6 +18,7 @@ MultiPFn v_multi_p_kernel(int variant)
     case 0: return v_multi_p<8, 1>;
     case 1: return v_multi_p<4, 2>;
     case 2: return v_multi_p<2, 4>;
+    case 3: return v_multi_p<4, 1>;
     default: return nullptr;
     }
 }

@@ -371,7 +371,8 @@ class Batch:
     velocity and one stress launch per time step for every shot of every
     model; the block shape is chosen by the batch's autotuner."""
 
-    VARIANTS = ("128x8 points x 1 shot", "128x4 points x 2 shots", "128x2 points x 4 shots")
+    VARIANTS = ("128x8 points x 1 shot", "128x4 points x 2 shots", "128x2 points x 4 shots",
+                "128x4 points x 1 shot")
 
     def __init__(self, params_list, device: int = 0):
         self.params = list(params_list)
@@ -444,7 +445,8 @@ class Batch:
         _check(lib().dsh_batch_get_stats(self.h, ms.ctypes.data, C.byref(s)), "dsh_batch_get_stats")
         return {"ms_total": s.ms_total, "kernel_launches": s.kernel_launches, "point_updates": s.point_updates,
                 "v_variant": s.v_variant, "s_variant": s.s_variant, "phases": s.phases,
-                "v_ms": list(s.v_ms)[:3], "s_ms": list(s.s_ms)[:3], "model_ms": ms}
+                "v_ms": list(s.v_ms)[:len(self.VARIANTS)], "s_ms": list(s.s_ms)[:len(self.VARIANTS)],
+                "model_ms": ms}
 
 
 def smooth_gauss(grad, filt, stream=None):

@@ -244,7 +244,9 @@ int dsh_batch_set_model(dsh_batch *b, int model, const float *vs, const float *r
 int dsh_batch_forward(dsh_batch *b, const dsh_shot *shots, const int *nshots, float *seis_out);
 int dsh_batch_forward_device(dsh_batch *b, const dsh_shot *shots, const int *nshots, float *seis_dev);
 int dsh_batch_set_stream(dsh_batch *b, void *stream);
-/* tile-shape variants 0..2 for the velocity and stress launches; -1 = autotune */
+/* tile-shape variants for the velocity and stress launches: 0 128x8 points
+ * x 1 shot, 1 128x4 x 2 shots, 2 128x2 x 4 shots (256-thread blocks), 3 128x4
+ * x 1 shot (128 threads); -1 = autotune */
 int dsh_batch_set_variant(dsh_batch *b, int v_variant, int s_variant);
 /* Wall-clock limit of the batch's host waits (as dsh_set_wait_limits; <= 0 restores 1800 s). */
 int dsh_batch_set_host_timeout(dsh_batch *b, double host_seconds);

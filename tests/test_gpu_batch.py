@@ -86,8 +86,8 @@ def test_batch_matches_reference_oracle():
             assert np.array_equal(s_gpu, ref)
 
 
-@pytest.mark.parametrize("v", [0, 1, 2])
-@pytest.mark.parametrize("s", [0, 1, 2])
+@pytest.mark.parametrize("v", [0, 1, 2, 3])
+@pytest.mark.parametrize("s", [0, 1, 2, 3])
 def test_tile_variants_identical(v, s):
     models = _batch_models()
     base, _ = _run_batch(models, (0, 0))
