@@ -105,7 +105,9 @@ const char *dsh_error_string(int status);
  * harmonic shear-modulus averages with the one-rank periodic model halo
  * (src/matcopy_elastic.c, src/av_mue.c), tau averages (src/av_tau.c),
  * SLS coefficients (src/prepare_update_s.c) and the C_vs / C_rho means
- * (src/denise.c:778-816). */
+ * (src/denise.c:778-816).  Only vs, rho and qs are copied to the device;
+ * the per-point coefficients are formed there, identical to the host
+ * restatement.  The host arrays may be reused once the call returns. */
 int dsh_set_model(dsh_ctx *ctx, const float *vs, const float *rho, const float *qs);
 
 /* Forward modelling of nshots shots; seis_out receives the vertical-velocity
