@@ -117,7 +117,9 @@ bool cl_config(const ClProblem &pb, ClCfg *cfg)
         const int per = (items + maxthr - 1) / maxthr;
         c.nthr = std::max(32, ((items + per - 1) / per + 31) / 32 * 32);
         c.smem = smem;
-        if (cudaFuncSetAttribute((const void *)fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        /* the opt-in maximum, not this problem's size: contexts of other sizes
+           may launch the same kernel concurrently */
+        if (cudaFuncSetAttribute((const void *)fk, cudaFuncAttributeMaxDynamicSharedMemorySize, maxsm) !=
                 cudaSuccess ||
             (C > 8 && cudaFuncSetAttribute((const void *)fk, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
                           cudaSuccess)) {
