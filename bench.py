@@ -88,6 +88,8 @@ def args_parse():
                     help="c2 only: timed gradients of the 64-shot batched-gradient sub-measurement (0 = skip)")
     ap.add_argument("--c1-steps", type=int, default=5,
                     help="c2 only: timed forward passes of the 500x200 elastic sub-measurement (0 = skip)")
+    ap.add_argument("--c5-small", type=int, default=1,
+                    help="c2 only: 1 = add the reduced learned-vs-plain FWI sub-measurement (0 = skip)")
     ap.add_argument("--step-variant", type=int, default=-1,
                     help="pin the step-kernel variant (index into dsh.Engine.VARIANTS) instead of autotuning")
     ap.add_argument("--no-autotune", action="store_true",
@@ -359,6 +361,52 @@ def c1_sub(a, local):
             "effective_gbs": 36.0 * nx * ny * nt / (ms / 1e3) / 1e9,
             "l2": "state 1.2 MB: resident on chip; bytes counted algorithmically (kernel pair's 36 B/pt)",
             "clocks": clk}
+
+
+def c5_small_sub(a, local):
+    """The learned preconditioner against plain EPRECOND=1 L-BFGS on a reduced
+    problem that fits the default run (the c5 configuration itself, 1200x400
+    with 32 shots and a U-Net trained on 200 models, takes ~13 minutes and
+    runs as --config c5): 160x80 elastic FDORDER 4, 8 shots, NT 600, a U-Net
+    trained on solver-generated pairs of 16 models (seeds 100-115), FWI on a
+    problem it has not seen (seed 41), up to 8 iterations each.  Reports the
+    GPU-seconds each method needs to reach plain's final misfit (within 1 %)
+    over plain's GPU-seconds, for the network and for its prior without the
+    network (energy_src)."""
+    import torch
+
+    from dsh import configs, fwi
+    from dsh import nn as dnn
+
+    cfg = configs.config5(seed=41, nx=160, ny=80, nt=600, nshots=8, ntr=60)
+    cfg["params"].update(fdorder=4, l=0, fl=())
+    cfg["qs"] = None
+    p = cfg["params"]
+    t0 = time.time()
+    models = list(configs.training_models(count=16, first_seed=100, nx=p["nx"], ny=p["ny"]))
+    xs, ts = fwi.training_pairs(torch, models, p, cfg["shots"][::2])
+    net = dnn.UNet(torch, seed=3)
+    net.target = "log_h_over_ws"
+    fwi.train(net, torch, xs, dnn.residual_targets(torch, xs, ts), p["ny"], p["nx"], epochs=25, batch=2, lr=2e-3)
+    t_train = time.time() - t0
+    clocks = Clocks(local)
+    clocks.start()
+    prob = fwi.Problem(cfg, test_shots=3)
+    try:
+        plain, _ = fwi.run(prob, 8, method="plain", eps_scale=0.02)
+        target = plain[-1]["misfit"] * 1.01
+        t_plain = plain[-1]["gpu_s"]
+        learned, _ = fwi.run(prob, 8, method="learned", net=net, torch=torch, eps_scale=0.02, target_misfit=target)
+        prior, _ = fwi.run(prob, 8, method="energy_src", eps_scale=0.02, target_misfit=target)
+    finally:
+        prob.close()
+    clk = clocks.stop()
+    ratio = lambda run: (None if fwi.time_to_reach(run, target) is None else fwi.time_to_reach(run, target) / t_plain)
+    return {"workload": "learned-vs-plain-fwi-160x80-fd4-8shots-nt600 (reduced; the configuration is --config c5)",
+            "metric": "GPU-seconds to plain's final misfit (within 1 %) / plain's GPU-seconds (lower is better)",
+            "learned": ratio(learned), "energy_src_prior": ratio(prior),
+            "plain": {"iterations": len(plain) - 1, "final_misfit": plain[-1]["misfit"], "gpu_s": t_plain},
+            "training": {"models": 16, "epochs": 25, "wall_s": t_train}, "clocks": clk}
 
 
 def c3_sub(a, local):
@@ -719,6 +767,8 @@ def main():
             line["c3"] = c3_sub(a, local)
         if a.config == "c2" and world == 1 and a.c1_steps > 0:
             line["c1"] = c1_sub(a, local)
+        if a.config == "c2" and world == 1 and a.c5_small:
+            line["c5_small"] = c5_small_sub(a, local)
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
