@@ -123,3 +123,21 @@ def test_batch_reuse_and_fewer_shots():
             continue
         ref = _single(dict(m, shots=m["shots"][:1]))
         assert np.array_equal(out[k][0], ref[0])
+
+
+def test_device_array_arguments_in_subprocess():
+    """Batches of up to 36 models pass their StepArgs in the kernels'
+    parameter space; larger ones read them from a device array.  With
+    DSH_MULTI_ARGS_DEVICE=1 (read once per process, so in a child process)
+    every batch takes the device-array path: the same results bit for bit."""
+    import os
+    import subprocess
+    import sys
+
+    env = dict(os.environ, DSH_MULTI_ARGS_DEVICE="1")
+    code = ("import sys; sys.argv=['x']; import pytest; "
+            "sys.exit(pytest.main(['-q', '-p', 'no:cacheprovider', '-m', 'gpu', 'tests/test_gpu_batch.py', "
+            "'-k', 'not subprocess']))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True, timeout=900)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
