@@ -9,8 +9,12 @@
  * slot group) for each tile-shape variant.  Models are ordered by NT,
  * longest first, so the models still running at step n are a prefix of the
  * map: phase p (steps T_{p-1}+1 .. T_p of the sorted distinct NTs) launches
- * that prefix.  Steps are replayed from CUDA graphs of up to 32 steps per
- * phase; an event after each phase gives each model's completion time.
+ * that prefix.  With the StepArgs in the kernels' parameter space the map of
+ * each half-step is further grouped by register class (the model's body key,
+ * dsh_multi.cuh): one class kernel per key present, each over the NT-ordered
+ * prefix of its own group.  Steps are replayed from CUDA graphs of up to 32
+ * steps per phase; an event after each phase gives each model's completion
+ * time.
  *
  * Reference correspondence: every model runs the forward loop of
  * src/denise.c:1179-1346 (update_v_PML, source injection, update_s_*_PML,
@@ -48,11 +52,18 @@ struct dsh_batch {
     StepArgs *d_args = nullptr;
     std::unique_ptr<MultiParams> hp;       /* the same in the kernels' parameter space (batches of up to
                                               MULTI_PARAM_MODELS models; DSH_MULTI_ARGS_DEVICE=1: never) */
-    int4 *d_map = nullptr;                 /* MULTI_NVAR maps, each of map_cap entries */
+    int4 *d_map = nullptr;                 /* 2 x MULTI_NVAR maps (velocity, stress x tile-shape variant),
+                                              each of map_cap entries */
     long long map_cap = 0;
+    bool classed = false;                  /* class kernels, or the kernel with every body (key 0) */
     std::vector<int> order;                /* models by NT, longest first */
     std::vector<int> phase_nt;             /* distinct NTs ascending */
-    std::vector<long long> prefix[MULTI_NVAR];   /* per phase: map entries of the running models */
+    struct MapClass {
+        int key;                           /* body key; 0: every body */
+        long long start;                   /* first entry in the map */
+        std::vector<long long> count;      /* per phase: entries of the group's running models */
+    };
+    std::vector<MapClass> cls[2][MULTI_NVAR];
     std::vector<int> nb;                   /* shots per model of the current run */
     long long sig = -1;                    /* signature of the uploaded maps */
     long long geo = -1;                    /* sum of the models' geometry versions the graphs were made for */
@@ -195,44 +206,71 @@ extern "C" int dsh_batch_set_variant(dsh_batch *b, int v_variant, int s_variant)
     return DSH_OK;
 }
 
-/* block maps of every variant for the current shot counts; per phase the
- * number of entries of the models still running */
+/* block maps of both half-steps and every variant for the current shot
+ * counts, grouped by register class; per phase the number of entries of the
+ * models still running in each group */
+static int body_key(const dsh_batch *b, int kind, int k)
+{
+    if (!b->classed) return 0;
+    const dsh_params &q = b->p[k];
+    return kind ? multi_skey(q.fdorder, q.l) : multi_vkey(q.fdorder, dh_pow2(q.dh) ? 1 : 0);
+}
+
+static const int4 *map_of(const dsh_batch *b, int kind, int v)
+{
+    return b->d_map + ((size_t)kind * MULTI_NVAR + v) * b->map_cap;
+}
+
 static int build_maps(dsh_batch *b)
 {
     unsigned long long h = 1469598103934665603ULL;     /* FNV-1a over the shot counts */
     for (int k = 0; k < b->n; k++) h = (h ^ (unsigned)b->nb[k]) * 1099511628211ULL;
     const long long sig = (long long)(h >> 1);
     if (sig == b->sig) return DSH_OK;
-    std::vector<int4> maps[MULTI_NVAR];
+    static const bool mixed = getenv("DSH_MULTI_MIXED") != nullptr || getenv("DSH_MULTI_ARGS_DEVICE") != nullptr;
+    b->classed = !mixed && b->n <= MULTI_PARAM_MODELS;
+    std::vector<int4> maps[2][MULTI_NVAR];
     long long cap = 1;
-    for (int v = 0; v < MULTI_NVAR; v++) {
-        const int rows = MULTI_ROWS[v], spb = MULTI_SPB[v];
-        std::vector<long long> end_of(b->n, 0);
+    for (int kind = 0; kind < 2; kind++) {
+        std::vector<int> keys;             /* keys present, in the order of the models' first appearance */
         for (int k : b->order) {
-            const dsh_params &q = b->p[k];
-            const int gx = (q.nx + 4 * BX - 1) / (4 * BX), gy = (q.ny + rows - 1) / rows;
-            const int gz = (b->nb[k] + spb - 1) / spb;
-            for (int z = 0; z < gz; z++)
-                for (int y = 0; y < gy; y++)
-                    for (int x = 0; x < gx; x++) maps[v].push_back(make_int4(k, x, y, z));
-            end_of[k] = (long long)maps[v].size();
+            const int key = body_key(b, kind, k);
+            if (std::find(keys.begin(), keys.end(), key) == keys.end()) keys.push_back(key);
         }
-        b->prefix[v].assign(b->phase_nt.size(), 0);
-        for (size_t ph = 0; ph < b->phase_nt.size(); ph++)
-            for (int k = 0; k < b->n; k++)
-                if (b->p[k].nt >= b->phase_nt[ph]) b->prefix[v][ph] = std::max(b->prefix[v][ph], end_of[k]);
-        cap = std::max(cap, (long long)maps[v].size());
+        for (int v = 0; v < MULTI_NVAR; v++) {
+            const int rows = MULTI_ROWS[v], spb = MULTI_SPB[v];
+            std::vector<int4> &m = maps[kind][v];
+            b->cls[kind][v].clear();
+            for (int key : keys) {
+                dsh_batch::MapClass c{key, (long long)m.size(), std::vector<long long>(b->phase_nt.size(), 0)};
+                for (int k : b->order) {
+                    if (body_key(b, kind, k) != key) continue;
+                    const dsh_params &q = b->p[k];
+                    const int gx = (q.nx + 4 * BX - 1) / (4 * BX), gy = (q.ny + rows - 1) / rows;
+                    const int gz = (b->nb[k] + spb - 1) / spb;
+                    for (int z = 0; z < gz; z++)
+                        for (int y = 0; y < gy; y++)
+                            for (int x = 0; x < gx; x++) m.push_back(make_int4(k, x, y, z));
+                    const long long end = (long long)m.size() - c.start;
+                    for (size_t ph = 0; ph < b->phase_nt.size(); ph++)
+                        if (q.nt >= b->phase_nt[ph]) c.count[ph] = std::max(c.count[ph], end);
+                }
+                if ((long long)m.size() > c.start) b->cls[kind][v].push_back(c);
+            }
+            cap = std::max(cap, (long long)m.size());
+        }
     }
     if (cap > b->map_cap) {
         cudaFree(b->d_map);
         b->d_map = nullptr;
-        BK(cudaMalloc(&b->d_map, (size_t)MULTI_NVAR * cap * sizeof(int4)));
+        BK(cudaMalloc(&b->d_map, (size_t)2 * MULTI_NVAR * cap * sizeof(int4)));
         b->map_cap = cap;
     }
-    for (int v = 0; v < MULTI_NVAR; v++)
-        if (!maps[v].empty())
-            BK(cudaMemcpyAsync(b->d_map + (size_t)v * b->map_cap, maps[v].data(), maps[v].size() * sizeof(int4),
-                               cudaMemcpyHostToDevice, b->st));
+    for (int kind = 0; kind < 2; kind++)
+        for (int v = 0; v < MULTI_NVAR; v++)
+            if (!maps[kind][v].empty())
+                BK(cudaMemcpyAsync((int4 *)map_of(b, kind, v), maps[kind][v].data(),
+                                   maps[kind][v].size() * sizeof(int4), cudaMemcpyHostToDevice, b->st));
     BWAIT(b);
     drop_batch_graphs(b);
     b->sig = sig;
@@ -262,14 +300,57 @@ static int upload_args(dsh_batch *b)
     return DSH_OK;
 }
 
-/* K steps of phase ph: v_multi -> (separate injection for models whose
- * sources or receivers lie on the padding) -> s_multi, then the counter */
+/* the launches of one half-step (kind 0 velocity, 1 stress) over the
+ * running models of phase ph: one per register class, or one mixed launch;
+ * the first with programmatic serialization only if pdl_first */
+static int launch_half(dsh_batch *b, int kind, int var, int ph, int off, bool pdl_first, long long *nl)
+{
+    static const bool use_pdl = getenv("DSH_NO_PDL") == nullptr;
+    cudaLaunchAttribute attr;
+    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr.val.programmaticStreamSerializationAllowed = 1;
+    const int4 *map = map_of(b, kind, var);
+    bool first = true;
+    for (const auto &c : b->cls[kind][var]) {
+        const long long nblk = c.count[ph];
+        if (nblk == 0) continue;
+        const bool pdl = use_pdl && (pdl_first || !first);
+        first = false;
+        cudaLaunchConfig_t cfg = {};
+        cfg.blockDim = dim3(BX, MULTI_ROWS[var], MULTI_SPB[var]);
+        cfg.gridDim = dim3((unsigned)nblk);
+        cfg.stream = b->st;
+        cfg.attrs = pdl ? &attr : nullptr;
+        cfg.numAttrs = pdl ? 1 : 0;
+        const int4 *m = map + c.start;
+        if (b->classed) {
+            MultiPFn f = kind ? s_multi_k_kernel(var, c.key) : v_multi_k_kernel(var, c.key);
+            if (!f) return DSH_ERR_PARAM;
+            BK(cudaLaunchKernelEx(&cfg, f, *b->hp, m, off));
+        } else if (b->hp) {
+            BK(cudaLaunchKernelEx(&cfg, kind ? s_multi_p_kernel(var) : v_multi_p_kernel(var), *b->hp, m, off));
+        } else {
+            const StepArgs *args = b->d_args;
+            BK(cudaLaunchKernelEx(&cfg, kind ? s_multi_kernel(var) : v_multi_kernel(var), args, m, off));
+        }
+        *nl += 1;
+    }
+    return DSH_OK;
+}
+
+/* number of launches of one half-step in phase ph */
+static int half_launches(const dsh_batch *b, int kind, int var, int ph)
+{
+    int n = 0;
+    for (const auto &c : b->cls[kind][var]) n += c.count[ph] > 0;
+    return n;
+}
+
+/* K steps of phase ph: velocity launches -> (separate injection for models
+ * whose sources or receivers lie on the padding) -> stress launches, then
+ * the counter */
 static int launch_chunk(dsh_batch *b, int ph, int K, long long *nl)
 {
-    const long long nblk_v = b->prefix[b->var_v][ph], nblk_s = b->prefix[b->var_s][ph];
-    const int4 *map_v = b->d_map + (size_t)b->var_v * b->map_cap;
-    const int4 *map_s = b->d_map + (size_t)b->var_s * b->map_cap;
-    MultiFn vk = v_multi_kernel(b->var_v), sk = s_multi_kernel(b->var_s);
     std::vector<std::pair<int, InjectArgs>> sep;
     for (int k = 0; k < b->n; k++) {
         dsh_ctx *c = b->ctx[k];
@@ -278,34 +359,18 @@ static int launch_chunk(dsh_batch *b, int ph, int K, long long *nl)
         ia.nt_base = b->d_nt;
         sep.push_back({b->nb[k], ia});
     }
-    cudaLaunchAttribute attr;
-    attr.id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr.val.programmaticStreamSerializationAllowed = 1;
-    static const bool use_pdl = getenv("DSH_NO_PDL") == nullptr;
-    const StepArgs *args = b->d_args;
-    if (nblk_v == 0 || nblk_s == 0) return DSH_OK;     /* no shots in this phase */
+    if (half_launches(b, 0, b->var_v, ph) == 0 || half_launches(b, 1, b->var_s, ph) == 0)
+        return DSH_OK;                                 /* no shots in this phase */
+    int rc;
     for (int k = 0; k < K; k++) {
         int off = k;
-        cudaLaunchConfig_t cfg = {};
-        cfg.blockDim = dim3(BX, MULTI_ROWS[b->var_v], MULTI_SPB[b->var_v]);
-        cfg.gridDim = dim3((unsigned)nblk_v);
-        cfg.stream = b->st;
-        cfg.attrs = (use_pdl && k > 0) ? &attr : nullptr;
-        cfg.numAttrs = (use_pdl && k > 0) ? 1 : 0;
-        if (b->hp) BK(cudaLaunchKernelEx(&cfg, v_multi_p_kernel(b->var_v), *b->hp, map_v, off));
-        else BK(cudaLaunchKernelEx(&cfg, vk, args, map_v, off));
+        if ((rc = launch_half(b, 0, b->var_v, ph, off, k > 0, nl)) != DSH_OK) return rc;
         for (auto &s : sep) {
             void *iargs[2] = {&s.second, &off};
             BK(cudaLaunchKernel((const void *)inject_sample, dim3(s.first), dim3(128), iargs, 0, b->st));
             *nl += 1;
         }
-        cfg.blockDim = dim3(BX, MULTI_ROWS[b->var_s], MULTI_SPB[b->var_s]);
-        cfg.gridDim = dim3((unsigned)nblk_s);
-        cfg.attrs = use_pdl ? &attr : nullptr;
-        cfg.numAttrs = use_pdl ? 1 : 0;
-        if (b->hp) BK(cudaLaunchKernelEx(&cfg, s_multi_p_kernel(b->var_s), *b->hp, map_s, off));
-        else BK(cudaLaunchKernelEx(&cfg, sk, args, map_s, off));
-        *nl += 2;
+        if ((rc = launch_half(b, 1, b->var_s, ph, off, true, nl)) != DSH_OK) return rc;
     }
     advance_step<<<1, 1, 0, b->st>>>(b->d_nt, K);
     *nl += 1;
@@ -346,20 +411,23 @@ static int run_phase(dsh_batch *b, int ph)
             cudaGraphDestroy(g);
             it = b->graphs.emplace(key, ex).first;
         }
-        /* launches per chunk: 2 per step (+ separate injections) + the counter */
+        /* launches per chunk: the class launches of both half-steps per step
+           (+ separate injections) + the counter */
+        const int nv = half_launches(b, 0, b->var_v, ph), ns = half_launches(b, 1, b->var_s, ph);
         long long per = 0;
         for (int k = 0; k < b->n; k++)
             if (b->p[k].nt >= b->phase_nt[ph] && !b->ctx[k]->fused_inject && b->nb[k] > 0) per++;
-        b->launches += (2 + per) * len + 1;
+        b->launches += nv && ns ? (nv + ns + per) * len + 1 : 0;
         BK(cudaGraphLaunch(it->second, b->st));
     }
     return DSH_OK;
 }
 
-/* Autotuner: each velocity and stress variant launched back to back over
- * every model (phase 0 map), mean device time per launch; the fastest of
- * each kind is kept for this batch signature.  The wavefields it disturbs
- * are zeroed again before the run. */
+/* Autotuner: the launches of each velocity and stress variant (one per
+ * register class) repeated back to back over every model (phase 0), mean
+ * device time per half-step; the fastest of each kind is kept for this
+ * batch signature.  The wavefields it disturbs are zeroed again before the
+ * run. */
 static int tune(dsh_batch *b)
 {
     const int reps = 8;
@@ -371,16 +439,13 @@ static int tune(dsh_batch *b)
         for (int v = 0; v < MULTI_NVAR; v++) {
             b->tune_ms[kind][v] = 0;
             if (forced >= 0 && v != forced) continue;
-            MultiFn fn = kind ? s_multi_kernel(v) : v_multi_kernel(v);
-            MultiPFn fp = kind ? s_multi_p_kernel(v) : v_multi_p_kernel(v);
-            const int4 *map = b->d_map + (size_t)v * b->map_cap;
-            const unsigned nblk = (unsigned)b->prefix[v][0];
-            if (nblk == 0) continue;
+            if (half_launches(b, kind, v, 0) == 0) continue;
             batch_set_counter<<<1, 1, 0, b->st>>>(b->d_nt, 1);
+            long long nl = 0;
             for (int r = 0; r < reps + 2; r++) {
                 if (r == 2) BK(cudaEventRecord(e0, b->st));
-                if (b->hp) fp<<<nblk, dim3(BX, MULTI_ROWS[v], MULTI_SPB[v]), 0, b->st>>>(*b->hp, map, 0);
-                else fn<<<nblk, dim3(BX, MULTI_ROWS[v], MULTI_SPB[v]), 0, b->st>>>(b->d_args, map, 0);
+                int rc = launch_half(b, kind, v, 0, 0, false, &nl);
+                if (rc != DSH_OK) return rc;
             }
             BK(cudaEventRecord(e1, b->st));
             BWAIT(b);

@@ -143,11 +143,56 @@ __global__ void __launch_bounds__(BX *BY, 2) s_multi_p(const __grid_constant__ M
     s_multi_body(sa, nt_off, i0, j, slot);
 }
 
+/* Register classes.  A kernel that holds every body needs the registers of
+ * the largest one (FDORDER 8, L 2: 128 per thread, 16 warps per SM) for all
+ * its blocks, elastic FDORDER-4 tiles included.  A class kernel holds the
+ * body of one key alone and a register budget of its own (velocity: that of
+ * the single-model kernel, 64 registers, 32 warps per SM; stress: below),
+ * and the batch launches one per key present, back to back: every grid waits
+ * for its predecessor (pdl_wait) before it reads stresses or velocities, so
+ * the launches of one half-step run in order and the next one may begin its
+ * prologue during the previous one's tail.  Keys: velocity FDORDER x 2 + (DH
+ * a power of two), stress FDORDER x 8 + L. */
+__host__ __device__ constexpr int multi_vkey(int fdo, int p2) { return fdo * 2 + (p2 ? 1 : 0); }
+__host__ __device__ constexpr int multi_skey(int fdo, int l) { return fdo * 8 + l; }
+
+template <int ROWS, int SPB, int KEY>
+__global__ void __launch_bounds__(BX *BY, VSTEP_MIN_BLOCKS_FWD) v_multi_k(const __grid_constant__ MultiParams P,
+                                                                          const int4 *__restrict__ map, int nt_off)
+{
+    const int4 m = map[blockIdx.x];
+    const StepArgs &sa = P.m[m.x];
+    int i0, j, slot, tile;
+    if (!multi_point<ROWS, SPB>(sa, m, i0, j, slot, tile)) return;
+    v_body<KEY / 2, 0, (KEY & 1) != 0>(sa, nt_off, i0, j, slot, tile);
+}
+/* stress: a register cap per key rather than the single-model kernel's
+ * budget (a block of 128 threads resides 6 times per SM at <= 80 registers,
+ * 5 times at <= 96, 4 times at 128): elastic bodies 80 registers (FDORDER 4
+ * without spills, 6 and 8 a few words), viscoelastic 96 (a few words more);
+ * measured 6.8 % faster per stress half-step of the 32-model survey batch
+ * than the single-model budget, and the cap of 80 for the viscoelastic
+ * bodies too 1.5 % slower than 96 */
+__host__ __device__ constexpr int multi_sreg(int key) { return key % 8 ? 96 : 80; }
+template <int ROWS, int SPB, int KEY>
+__global__ void __maxnreg__(multi_sreg(KEY)) s_multi_k(const __grid_constant__ MultiParams P,
+                                                        const int4 *__restrict__ map, int nt_off)
+{
+    const int4 m = map[blockIdx.x];
+    const StepArgs &sa = P.m[m.x];
+    int i0, j, slot, tile;
+    if (!multi_point<ROWS, SPB>(sa, m, i0, j, slot, tile)) return;
+    s_body<KEY / 8, KEY % 8, 0>(sa, nt_off, i0, j, slot);
+}
+
 using MultiFn = void (*)(const StepArgs *, const int4 *, int);
 using MultiPFn = void (*)(const MultiParams, const int4 *, int);
 MultiFn v_multi_kernel(int variant);
 MultiFn s_multi_kernel(int variant);
 MultiPFn v_multi_p_kernel(int variant);
 MultiPFn s_multi_p_kernel(int variant);
+/* class kernels: nullptr for a key of a body that is not compiled in */
+MultiPFn v_multi_k_kernel(int variant, int key);
+MultiPFn s_multi_k_kernel(int variant, int key);
 
 }  // namespace dsh

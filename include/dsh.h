@@ -221,20 +221,22 @@ int dsh_profile_fused(dsh_ctx *ctx, int pass, int nsteps, float *out_ms);
 int dsh_residual_noalloc(int nshots, int ntr, int nt, const float *syn, const float *obs, float *res, double *l2,
                          void *stream);
 
-/* ---- Uneven batches: many models in one launch per half-step ----
+/* ---- Uneven batches: many models in few launches per half-step ----
  * A batch holds nmodels independent models, each with its own dsh_params
  * (grid, FDORDER, L, DT, NT, max_shots, ...).  dsh_batch_forward advances all
- * their shots together: one velocity and one stress kernel launch per time
- * step for the whole batch, each thread block working on one 128-point tile
- * of one model; models leave the launches once their NT is reached.  Results
- * are bit-identical to running each model through its own context (and so
- * to the reference's forward loop, src/denise.c:1179-1346); the reference
- * runs one model per program.  Supported per model: FDORDER 4, 6, 8 and
- * L 0 or 2 (other combinations: DSH_ERR_PARAM at creation).
- * Tile shape: each launch uses one of three block shapes (128 x 8 points x 1
- * shot, 128 x 4 x 2 shots, 128 x 2 x 4 shots); the first run of a batch times
- * them on the batch itself and keeps the fastest (dsh_batch_set_variant
- * fixes them instead). */
+ * their shots together: per time step one velocity and one stress kernel
+ * launch for all models of a register class (the same FDORDER and L; one
+ * launch holding every body for batches of more than 36 models), each thread
+ * block working on one 128-point tile of one model; models leave the
+ * launches once their NT is reached.  Results are bit-identical to running
+ * each model through its own context (and so to the reference's forward
+ * loop, src/denise.c:1179-1346); the reference runs one model per program.
+ * Supported per model: FDORDER 4, 6, 8 and L 0 or 2 (other combinations:
+ * DSH_ERR_PARAM at creation).
+ * Tile shape: each launch uses one of four block shapes (128 x 8 points x 1
+ * shot, 128 x 4 x 2 shots, 128 x 2 x 4 shots, 128 x 4 x 1 shot); the first
+ * run of a batch times them on the batch itself and keeps the fastest
+ * (dsh_batch_set_variant fixes them instead). */
 typedef struct dsh_batch dsh_batch;
 dsh_batch *dsh_batch_create(const dsh_params *p, int nmodels, int device, int *status);
 int dsh_batch_destroy(dsh_batch *b);

@@ -1,8 +1,9 @@
 """Uneven multi-model batches (dsh_batch): every model of a batch advanced by
-one velocity and one stress launch per step must give exactly the
-seismograms of its own single-model context, which the parity tests tie to
-the reference; every tile-shape variant must agree bit for bit; the
-autotuner must report its timings and pick the fastest."""
+one velocity and one stress launch per register class and step (or one
+launch holding every body) must give exactly the seismograms of its own
+single-model context, which the parity tests tie to the reference; every
+tile-shape variant must agree bit for bit; the autotuner must report its
+timings and pick the fastest."""
 import numpy as np
 import pytest
 
@@ -125,16 +126,20 @@ def test_batch_reuse_and_fewer_shots():
         assert np.array_equal(out[k][0], ref[0])
 
 
-def test_device_array_arguments_in_subprocess():
+@pytest.mark.parametrize("var", ["DSH_MULTI_ARGS_DEVICE", "DSH_MULTI_MIXED"])
+def test_other_launch_forms_in_subprocess(var):
     """Batches of up to 36 models pass their StepArgs in the kernels'
-    parameter space; larger ones read them from a device array.  With
-    DSH_MULTI_ARGS_DEVICE=1 (read once per process, so in a child process)
-    every batch takes the device-array path: the same results bit for bit."""
+    parameter space and launch one kernel per register class; larger ones
+    read them from a device array in one kernel holding every body.  With
+    DSH_MULTI_ARGS_DEVICE=1 every batch takes the device-array path, with
+    DSH_MULTI_MIXED=1 the parameter-space kernel holding every body (both
+    read once per process, so in a child process): the same results bit for
+    bit."""
     import os
     import subprocess
     import sys
 
-    env = dict(os.environ, DSH_MULTI_ARGS_DEVICE="1")
+    env = dict(os.environ, **{var: "1"})
     code = ("import sys; sys.argv=['x']; import pytest; "
             "sys.exit(pytest.main(['-q', '-p', 'no:cacheprovider', '-m', 'gpu', 'tests/test_gpu_batch.py', "
             "'-k', 'not subprocess']))")
