@@ -286,6 +286,7 @@ static int upload_args(dsh_batch *b)
         a[k] = step_args(b->ctx[k], P_FWD_PLAIN);
         a[k].nt_base = b->d_nt;
         a[k].nslots = b->nb[k];
+        a[k].l2_stream = 0;            /* the batch's working set is every model's */
     }
     BK(cudaMemcpyAsync(b->d_args, a.data(), a.size() * sizeof(StepArgs), cudaMemcpyHostToDevice, b->st));
     static const bool device_only = getenv("DSH_MULTI_ARGS_DEVICE") != nullptr;

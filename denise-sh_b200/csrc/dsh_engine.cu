@@ -996,6 +996,28 @@ bool dh_pow2(float dh)
 }  // namespace dsh::eng
 
 namespace dsh::eng {
+/* L2 policy of a pass (StepArgs::l2_stream): the fields the velocity kernel
+ * reads every half-step (vy, sxy, syz of every slot, 1/rho, and in the
+ * adjoint the g_rho, g_u and Wr sums) stay evict-last.  If they fit half the
+ * L2, the memory variables (read and written once per step, bit 0) are
+ * streamed evict-first so that they do not displace those fields, and with a
+ * single shot slot the stress model factors too (bit 1; with several slots
+ * every slot of the launch re-reads them).  A single-shot 2000 x 800
+ * viscoelastic gradient: 38.0 -> 42.0 Gpt/s.  With more (64 slots of
+ * 1000 x 300: 230 MB) everything keeps the evict-last policy, which measured
+ * faster there.  DSH_L2_STREAM=<mask> fixes the choice. */
+int l2_stream(const dsh_ctx *ctx, Pass pass)
+{
+    static const char *env = getenv("DSH_L2_STREAM");
+    if (env) return atoi(env) & 3;
+    int l2 = 0;
+    if (cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, ctx->dev) != cudaSuccess || l2 <= 0) return 0;
+    const long long per_slot = 3 * ctx->fstride + (pass == P_ADJ ? 3 * ctx->dstride : 0);
+    const long long bytes = 4 * ((long long)ctx->S * per_slot + ctx->dstride);
+    if (bytes > (long long)l2 / 2) return 0;
+    return ctx->S == 1 ? 3 : 1;
+}
+
 StepArgs step_args(dsh_ctx *ctx, Pass pass)
 {
     const dsh_params &p = ctx->p;
@@ -1004,6 +1026,7 @@ StepArgs step_args(dsh_ctx *ctx, Pass pass)
     a.nx = p.nx; a.ny = p.ny; a.pitch = ctx->pitch; a.hy = ctx->hy; a.fw = p.fw; a.free_surf = p.free_surf;
     a.l = p.l; a.fd12_compat = p.compat_fd12;
     a.fdo = p.fdorder; a.p2 = dh_pow2(p.dh) ? 1 : 0; a.nslots = ctx->S;
+    a.l2_stream = l2_stream(ctx, pass);
     a.nt_last = p.nt; a.nt_total = p.nt; a.nt_base = ctx->d_nt;
     a.chk_mask = 15;
     a.fstride = ctx->fstride; a.dstride = ctx->dstride; a.slot_stride = ctx->slot_stride;

@@ -130,6 +130,7 @@ int zero_slots(dsh_ctx *ctx, int nb, bool accumulators);
 int copy_seis_out(dsh_ctx *ctx, int nb, float *host_out, float *dev_out);
 int check_status(dsh_ctx *ctx);
 bool dh_pow2(float dh);
+int l2_stream(const dsh_ctx *ctx, Pass pass);
 long long batch_seis_len(dsh_ctx *ctx, const dsh_shot *shots, int nb);
 void drop_graphs(dsh_ctx *ctx);
 }  // namespace dsh::eng

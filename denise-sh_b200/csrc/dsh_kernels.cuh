@@ -85,6 +85,7 @@ struct StepArgs {
     int fd12_compat;
     int fdo, p2;                 /* FDORDER; DH a power of two (multi-model launches pick the body from these) */
     int nslots;                  /* shot slots allocated (multi-model launches skip slots >= nslots) */
+    int l2_stream;               /* evict-first in L2: bit 0 memory variables, bit 1 stress model factors */
     int nt_last;                 /* last valid step of this pass (1-based) */
     int nt_total;                /* NT of the pass (for the Hessian's nt < NTDTINV) */
     int chk_mask;                /* finite check of the updated fields on steps with (nt & chk_mask) == 0
@@ -175,6 +176,51 @@ __device__ __forceinline__ float4 ldg4(const float *p) { return __ldg(reinterpre
 __device__ __forceinline__ void st4(float *p, float4 v) { *reinterpret_cast<float4 *>(p) = v; }
 __device__ __forceinline__ void st1(float *p, float v) { *p = v; }
 #endif
+#if DSH_L2_KEEP
+/* The memory variables (StepArgs::l2_stream bit 0) and the stress kernel's
+ * model factors (bit 1) are loaded and stored evict-first when the host finds
+ * that the velocity kernel's read set then stays in L2 from one half-step to
+ * the next; otherwise they keep the evict-last policy. */
+__device__ __forceinline__ uint64_t l2_drop()
+{
+    uint64_t pol;
+    asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+__device__ __forceinline__ float4 ld4p(const float *p, uint64_t pol)
+{
+    float4 v;
+    asm volatile("ld.global.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float4 ldg4p(const float *p, uint64_t pol)
+{
+    float4 v;
+    asm volatile("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+                 : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+                 : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ void st4p(float *p, float4 v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.v4.f32 [%0], {%1, %2, %3, %4}, %5;" ::"l"(p), "f"(v.x), "f"(v.y),
+                 "f"(v.z), "f"(v.w), "l"(pol)
+                 : "memory");
+}
+__device__ __forceinline__ void st1p(float *p, float v, uint64_t pol)
+{
+    asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
+}
+#define DSH_L2_POL(a, bit) (((a).l2_stream & (bit)) ? l2_drop() : l2_keep())
+#else
+__device__ __forceinline__ float4 ld4p(const float *p, uint64_t) { return ld4(p); }
+__device__ __forceinline__ float4 ldg4p(const float *p, uint64_t) { return ldg4(p); }
+__device__ __forceinline__ void st4p(float *p, float4 v, uint64_t) { st4(p, v); }
+__device__ __forceinline__ void st1p(float *p, float v, uint64_t) { st1(p, v); }
+#define DSH_L2_POL(a, bit) 0ull
+#endif
 /* state loads of the persistent kernel: other blocks wrote them earlier in the
  * same launch, so they bypass L1 (ld.global.cg) */
 template <bool CG>
@@ -196,6 +242,13 @@ __device__ __forceinline__ void st4m(float *p, float4 v, int nvalid)
     if (nvalid > 0) st1(p, v.x);
     if (nvalid > 1) st1(p + 1, v.y);
     if (nvalid > 2) st1(p + 2, v.z);
+}
+__device__ __forceinline__ void st4mp(float *p, float4 v, int nvalid, uint64_t pol)
+{
+    if (nvalid >= 4) { st4p(p, v, pol); return; }
+    if (nvalid > 0) st1p(p, v.x, pol);
+    if (nvalid > 1) st1p(p + 1, v.y, pol);
+    if (nvalid > 2) st1p(p + 2, v.z, pol);
 }
 
 /* forward-storage traffic is written once per pass and read once by the
@@ -705,28 +758,29 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     float4 mi4, mj4, ti4, tj4;               /* muip, mujp, tausipjp, taus */
     float4 sold_r, sold_q, qsx, qsy;         /* Qs gradient: memory sums before the update, sensitivities */
     float4 ex4, ey4, gx4, gy4, dsx4, dsy4;   /* Qs gradient, adjoint: strains, sums, stored sensitivities */
+    const uint64_t pol_rq = DSH_L2_POL(a, 1), pol_f = DSH_L2_POL(a, 2);   /* memory variables, model factors */
     if (L == 0) {
-        c1 = ldg4(a.uip + drow + col0);
-        c2 = ldg4(a.ujp + drow + col0);
+        c1 = ldg4p(a.uip + drow + col0, pol_f);
+        c2 = ldg4p(a.ujp + drow + col0, pol_f);
     } else {
 #pragma unroll
         for (int l = 0; l < L; l++) {
-            rr[l] = ld4(a.r + so + l * a.dstride + drow + col0);
-            qq[l] = ld4(a.q + so + l * a.dstride + drow + col0);
+            rr[l] = ld4p(a.r + so + l * a.dstride + drow + col0, pol_rq);
+            qq[l] = ld4p(a.q + so + l * a.dstride + drow + col0, pol_rq);
         }
         if (FLAGS & SF_PARAMS) {
-            c1 = ldg4(a.fipjp + drow + col0);
-            c2 = ldg4(a.f + drow + col0);
+            c1 = ldg4p(a.fipjp + drow + col0, pol_f);
+            c2 = ldg4p(a.f + drow + col0, pol_f);
 #pragma unroll
             for (int l = 0; l < L; l++) {
-                dip4[l] = ldg4(a.dip + l * a.dstride + drow + col0);
-                d4[l] = ldg4(a.d + l * a.dstride + drow + col0);
+                dip4[l] = ldg4p(a.dip + l * a.dstride + drow + col0, pol_f);
+                d4[l] = ldg4p(a.d + l * a.dstride + drow + col0, pol_f);
             }
         } else {
-            mi4 = ldg4(a.muip + drow + col0);
-            mj4 = ldg4(a.mujp + drow + col0);
-            ti4 = ldg4(a.tausipjp + drow + col0);
-            tj4 = ldg4(a.taus + drow + col0);
+            mi4 = ldg4p(a.muip + drow + col0, pol_f);
+            mj4 = ldg4p(a.mujp + drow + col0, pol_f);
+            ti4 = ldg4p(a.tausipjp + drow + col0, pol_f);
+            tj4 = ldg4p(a.taus + drow + col0, pol_f);
         }
     }
     float4 w4, g4, h4, fy, fu;
@@ -904,8 +958,8 @@ __device__ __forceinline__ void s_body(const StepArgs &a, int nt_off, int i0, in
     st4m(syz_p, syz4, nvalid);
 #pragma unroll
     for (int l = 0; l < L; l++) {
-        st4m(a.r + so + l * a.dstride + drow + col0, rr[l], nvalid);
-        st4m(a.q + so + l * a.dstride + drow + col0, qq[l], nvalid);
+        st4mp(a.r + so + l * a.dstride + drow + col0, rr[l], nvalid, pol_rq);
+        st4mp(a.q + so + l * a.dstride + drow + col0, qq[l], nvalid, pol_rq);
     }
     /* a non-finite value never turns finite again in these updates, so a
        check every few steps and on the last one finds every instability */

@@ -301,6 +301,28 @@ def test_other_block_heights_in_subprocess():
         assert out.returncode == 0, rows + (out.stdout[-2000:] + out.stderr[-2000:],)
 
 
+@pytest.mark.parametrize("mask", ["0", "1", "3"])
+def test_l2_policies_in_subprocess(mask):
+    """The stress kernel streams the memory variables (bit 0 of the L2 policy
+    mask) and the model factors (bit 1) evict-first when the host finds that
+    the velocity kernel's read set then stays in L2; the cache hints change no
+    arithmetic.  Each mask forced through DSH_L2_STREAM (read once per
+    process, so in a child process): random cases, multi-shot batches and
+    checkpointed gradients bit-identical to the oracle."""
+    import subprocess
+    import sys
+
+    env = dict(os.environ, DSH_L2_STREAM=mask)
+    code = ("import sys; sys.argv=['x']; import pytest; "
+            "sys.exit(pytest.main(['-q', '-p', 'no:cacheprovider', '-m', 'gpu', "
+            "'tests/test_gpu_parity.py::test_random_cases_vs_oracle', "
+            "'tests/test_gpu_parity.py::test_multi_shot_batches', 'tests/test_gpu_checkpoint.py']))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True,
+                         timeout=900)
+    assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
+
+
 def test_tma_velocity_kernel_in_subprocess():
     """The opt-in persistent velocity kernel whose stress taps the tensor-memory
     accelerator stages in shared memory (DSH_VTMA=1, read once per process, so
