@@ -322,11 +322,11 @@ def c1_sub(a, local):
     """Plain elastic forward modelling as its configuration states it:
     NX=500, NY=200, FDORDER 4, NT=2000, one shot, 96 receivers, through the
     device API with the step-kernel variant the autotuner picks for this grid
-    (the one-launch cluster-resident kernel where the device offers 16-CTA
-    clusters).  CUDA events on the launching stream, three untimed passes
-    first.  The state (1.2 MB) stays on chip in the cluster variant, so the
-    effective bandwidth below (the kernel pair's algorithmic 36 B per point
-    and step over the measured time) is not bounded by HBM."""
+    (on a B200 the temporally blocked launches, four steps per launch).  CUDA
+    events on the launching stream, three untimed passes first.  The state
+    (1.2 MB) stays in L2 and shared memory, so the effective bandwidth below
+    (the kernel pair's algorithmic 36 B per point and step over the measured
+    time) is not bounded by HBM."""
     import torch
 
     import dsh

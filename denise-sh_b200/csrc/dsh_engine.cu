@@ -19,6 +19,7 @@
 #include "dsh_fs.h"
 #include "dsh_pf.h"
 #include "dsh_cl.h"
+#include "dsh_tb.h"
 #include "dsh_fused.cuh"
 #include "dsh_setup.h"
 
@@ -1436,6 +1437,37 @@ static int run_cluster(dsh_ctx *ctx, Pass pass, int nb, int n0, int count, const
     return DSH_OK;
 }
 
+/* Small elastic grids, plain forward modelling: k time steps per launch of
+ * tb_fwd (dsh_tblock.cuh), each CTA advancing its tile and a recomputed halo
+ * in shared memory.  On by DSH_TBLOCK=1 or the autotuner's choice; false
+ * when it does not apply (viscoelastic, FDORDER > 8, positions outside the
+ * grid, more sources or receivers per shot than its lists hold). */
+static bool tblock_cfg(dsh_ctx *ctx, Pass pass, int nb, TbCfg *cfg)
+{
+    static const int env = env_flag("DSH_TBLOCK");
+    const bool on = ctx->sel_tblock >= 0 ? ctx->sel_tblock != 0 : env != 0;
+    const dsh_params &p = ctx->p;
+    if (!on || pass != P_FWD_PLAIN || !ctx->fused_inject || p.l != 0 || p.fdorder > 8) return false;
+    TbProblem pb;
+    pb.fdorder = p.fdorder; pb.p2 = dh_pow2(p.dh) ? 1 : 0; pb.nx = p.nx; pb.ny = p.ny; pb.fw = p.fw; pb.nb = nb;
+    pb.max_groups = ctx->geo_max_groups; pb.max_members = ctx->geo_max_members;
+    pb.max_receivers = ctx->geo_max_ntr;
+    return tb_config(pb, cfg);
+}
+
+static int run_tblock(dsh_ctx *ctx, Pass pass, int nb, int n0, int count, const TbCfg &cfg)
+{
+    const dsh_params &p = ctx->p;
+    StepArgs sa = step_args(ctx, pass);
+    sa.nslots = nb;
+    long long nl = 0;
+    const cudaError_t e = tb_launch(cfg, p.fdorder, dh_pow2(p.dh), sa, n0, count, nb, ctx->st, &nl);
+    ctx->launches += nl;
+    CK(e);
+    ctx->state_b = 0;
+    return DSH_OK;
+}
+
 /* Steps n0 .. n0+count-1 of a pass: graphs of `chunk` steps replayed
  * count/chunk times, then one graph for the remaining steps. */
 static int run_steps(dsh_ctx *ctx, Pass pass, int nb, int n0, int count)
@@ -1443,6 +1475,8 @@ static int run_steps(dsh_ctx *ctx, Pass pass, int nb, int n0, int count)
     if (count <= 0) return DSH_OK;
     ClCfg ccfg;
     if (cluster_cfg(ctx, pass, nb, &ccfg)) return run_cluster(ctx, pass, nb, n0, count, ccfg);
+    TbCfg tcfg;
+    if (tblock_cfg(ctx, pass, nb, &tcfg)) return run_tblock(ctx, pass, nb, n0, count, tcfg);
     if (const int grid = persistent_grid(ctx, pass, nb)) return run_persistent(ctx, pass, nb, n0, count, grid);
     const int K = std::min(ctx->chunk, count);
     const int nfull = count / K, rem = count % K;
@@ -1887,9 +1921,10 @@ extern "C" int dsh_set_wait_limits(dsh_ctx *ctx, long long device_polls, double 
     return DSH_OK;
 }
 
-/* step-kernel variants: staged velocity taps, fused step, persistent launch, cluster-resident launch */
-static const int VARIANT_SEL[DSH_STEP_VARIANTS][4] = {
-    {0, 0, 0, 0}, {1, 0, 0, 0}, {0, 1, 0, 0}, {0, 0, 1, 0}, {0, 0, 0, 1}};
+/* step-kernel variants: staged velocity taps, fused step, persistent launch, cluster-resident launch,
+ * temporally blocked launches */
+static const int VARIANT_SEL[DSH_STEP_VARIANTS][5] = {
+    {0, 0, 0, 0, 0}, {1, 0, 0, 0, 0}, {0, 1, 0, 0, 0}, {0, 0, 1, 0, 0}, {0, 0, 0, 1, 0}, {0, 0, 0, 0, 1}};
 
 static void select_variant(dsh_ctx *ctx, int v)
 {
@@ -1897,6 +1932,7 @@ static void select_variant(dsh_ctx *ctx, int v)
     ctx->sel_fused = v < 0 ? -1 : VARIANT_SEL[v][1];
     ctx->sel_persist = v < 0 ? -1 : VARIANT_SEL[v][2];
     ctx->sel_cluster = v < 0 ? -1 : VARIANT_SEL[v][3];
+    ctx->sel_tblock = v < 0 ? -1 : VARIANT_SEL[v][4];
 }
 
 extern "C" int dsh_set_step_variant(dsh_ctx *ctx, int variant)
@@ -2029,9 +2065,9 @@ extern "C" int dsh_get_field(dsh_ctx *ctx, int shot, int which, float *out)
 
 /* Times plain forward steps of each step-kernel variant the context can run
  * on these shots — kernel pair (v_step), pair with v_step_st, fused step,
- * persistent launch, cluster-resident launch — and keeps the fastest for the
- * context's later calls (the fused choice also serves the gradient passes,
- * the persistent and cluster ones only plain forward modelling).
+ * persistent launch, cluster-resident launch, temporally blocked launches —
+ * and keeps the fastest for the context's later calls (the fused choice also
+ * serves the gradient passes, the last three only plain forward modelling).
  * ms_per_step[DSH_STEP_VARIANTS] (optional): mean device ms per step of each
  * variant, 0 where it does not apply. */
 extern "C" int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int nsteps, float *ms_per_step,
@@ -2056,6 +2092,8 @@ extern "C" int dsh_autotune(dsh_ctx *ctx, const dsh_shot *shots, int nshots, int
         if (v == 2 && !use_fused(ctx, P_FWD_PLAIN)) continue;
         if (v == 3 && !persistent_grid(ctx, P_FWD_PLAIN, nb)) continue;
         if (v == 4 && !cluster_cfg(ctx, P_FWD_PLAIN, nb, &ccfg)) continue;
+        TbCfg tcfg;
+        if (v == 5 && !tblock_cfg(ctx, P_FWD_PLAIN, nb, &tcfg)) continue;
         for (int rep = 0; rep < 2; rep++) {            /* first round warms up (graphs, lazy loading) */
             if ((rc = zero_slots(ctx, nb, false)) != DSH_OK) break;
             CK(cudaEventRecord(e0, ctx->st));

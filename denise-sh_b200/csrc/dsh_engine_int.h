@@ -33,6 +33,7 @@ struct dsh_ctx {
     int sel_staged = -1, sel_fused = -1, sel_persist = -1;   /* step-kernel variants chosen by dsh_autotune
                                                                (-1: the DSH_VSTAGE / DSH_FUSED / DSH_PERSIST defaults) */
     int sel_cluster = -1;                 /* cluster-resident forward modelling (-1: the DSH_CLUSTER default) */
+    int sel_tblock = -1;                  /* temporally blocked forward modelling (-1: the DSH_TBLOCK default) */
     int sel_rows = -1;                    /* 1: the velocity kernel with two rows per thread (-1: DSH_VROWS=2) */
     float *slab = nullptr;
     float *model = nullptr;               /* brho uip ujp muip mujp tausipjp taus vs rho qs */

@@ -308,7 +308,7 @@ class Engine:
         return {"v_step": float(out[0]), "inject_sample": float(out[1]), "s_step": float(out[2])}
 
     VARIANTS = ("kernel pair", "kernel pair, staged velocity taps", "fused step", "persistent launch",
-                "cluster-resident launch")
+                "cluster-resident launch", "temporally blocked launch")
 
     def autotune(self, shots, nsteps=64):
         """Times each step-kernel variant on these shots, keeps the fastest; returns (name, ms per step each)."""

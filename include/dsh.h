@@ -182,8 +182,12 @@ int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
  * per pass of plain elastic forward modelling with the wavefield and model
  * held in the shared memory of one 16-CTA (or 8-CTA) thread-block cluster
  * per shot (FDORDER <= 8, grids whose ceil(NY/16)-row strips fit one CTA's
- * shared memory, e.g. 500 x 200). */
-#define DSH_STEP_VARIANTS 5
+ * shared memory, e.g. 500 x 200), 5 plain elastic forward modelling with k
+ * time steps per launch (FDORDER 2/4/6/8: k = 8/4/3/2), each thread block
+ * advancing a 32 x 16-point tile and a recomputed halo of k*(FDORDER-1)
+ * points in its shared memory (FDORDER <= 8, NX and NY >= 2 FW, at most 32
+ * source points, 4 sources per point and 512 receivers per shot). */
+#define DSH_STEP_VARIANTS 6
 
 /* Step-kernel autotuner: times nsteps plain forward steps of every variant
  * this context can run on these shots, keeps the fastest for the context's
@@ -360,7 +364,7 @@ int dsh_set_misfit(dsh_ctx *ctx, int lnorm);
 int dsh_set_wait_limits(dsh_ctx *ctx, long long device_polls, double host_seconds);
 
 /* Pins the step-kernel variant (0 .. DSH_STEP_VARIANTS-1 as listed at
- * DSH_STEP_VARIANTS; 3 and 4 fall back to the pair where they do not apply;
+ * DSH_STEP_VARIANTS; 3, 4 and 5 fall back to the pair where they do not apply;
  * -1 the defaults) — what dsh_autotune picks by timing. */
 int dsh_set_step_variant(dsh_ctx *ctx, int variant);
 
