@@ -28,9 +28,10 @@ bool tb_config(const TbProblem &pb, TbCfg *cfg)
     if (!fk || pb.nb < 1 || pb.nx < 1 || pb.ny < 1 || pb.nx > 0xffff || pb.ny > 0x7fff) return false;
     if (pb.max_groups > TB_MAX_GRP || pb.max_members > TB_MAX_MEM || pb.max_receivers > TB_MAX_REC) return false;
     if (pb.fw > 0 && (pb.nx < 2 * pb.fw || pb.ny < 2 * pb.fw)) return false;
-    int dev = 0, maxsm = 0;
+    int dev = 0, maxsm = 0, nsm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
-        cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) {
+        cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
@@ -40,15 +41,37 @@ bool tb_config(const TbProblem &pb, TbCfg *cfg)
         const int v = atoi(e);
         if (v >= 1 && v <= 64) k = v;
     }
+    int rows = 0;                                    /* tile height pinned by DSH_TB_ROWS */
+    if (const char *e = getenv("DSH_TB_ROWS")) {
+        const int v = atoi(e);
+        if (v >= 1 && v <= 256) rows = v;
+    }
     TbCfg c;
     c.geo.tw = 32;
-    c.geo.th = 16;
-    for (; k >= 1; k--) {
-        c.geo.g = k * R;
+    auto shape = [&](int th, int kk) {
+        c.geo.th = th;
+        c.geo.g = kk * R;
         c.geo.ew = c.geo.tw + 2 * c.geo.g;
         c.geo.eh = c.geo.th + 2 * c.geo.g;
-        if (tb_smem_bytes(c.geo) <= maxsm) break;
+        return tb_smem_bytes(c.geo) <= maxsm;
+    };
+    /* tile height: the smallest multiple of 8 rows (up to 64) for which every
+       tile of every slot runs at once, one CTA per SM (a second wave, or SMs
+       holding two tiles beside SMs holding one, would double the time of the
+       slowest SM); 16 rows where no height does */
+    int th = 16;
+    if (rows) {
+        th = rows;
+    } else {
+        const int ntx = (pb.nx + c.geo.tw - 1) / c.geo.tw;
+        for (int t = 8; t <= 64; t += 8)
+            if ((long long)ntx * ((pb.ny + t - 1) / t) * pb.nb <= nsm && shape(t, k)) {
+                th = t;
+                break;
+            }
     }
+    for (; k >= 1; k--)
+        if (shape(th, k)) break;
     if (k < 1) return false;
     c.k = k;
     c.ntx = (pb.nx + c.geo.tw - 1) / c.geo.tw;

@@ -21,9 +21,12 @@ struct TbCfg {
     size_t smem = 0;             /* dynamic shared memory per CTA in bytes */
 };
 
-/* The launch shape on the current device: 32 x 16-point own tiles, k steps
- * per launch (FDORDER 2: 8, 4: 4, 6: 3, 8: 2; DSH_TB_STEPS overrides it),
- * k lowered until the tile fits the opt-in shared memory of one CTA.  false
+/* The launch shape on the current device: own tiles 32 points wide and as
+ * few rows high (a multiple of 8, up to 64) as lets every tile of every slot
+ * run at once with one CTA per SM, else 16 rows (DSH_TB_ROWS pins the
+ * height); k steps per launch (FDORDER 2: 8, 4: 4, 6: 3, 8: 2; DSH_TB_STEPS
+ * overrides it), k lowered until the tile fits the opt-in shared memory of
+ * one CTA.  false
  * when the kernel cannot serve the problem (FDORDER > 8, more sources or
  * receivers per slot than its lists hold, NX or NY below 2 FW). */
 bool tb_config(const TbProblem &pb, TbCfg *cfg);

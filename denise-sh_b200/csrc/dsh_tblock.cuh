@@ -44,7 +44,7 @@
 
 namespace dsh {
 
-constexpr int TB_THREADS = 256;  /* threads per CTA */
+constexpr int TB_THREADS = 512;  /* threads per CTA */
 constexpr int TB_MAX_GRP = 32;   /* source points (groups) of a slot */
 constexpr int TB_MAX_MEM = 4;    /* sources at one point */
 constexpr int TB_MAX_REC = 512;  /* receivers of a slot */
@@ -156,12 +156,23 @@ __global__ void __launch_bounds__(TB_THREADS) tb_fwd(StepArgs a, TbGeom geo, int
     }
     __syncthreads();
     const int ngrp = min(cnt[0], TB_MAX_GRP), nrec = min(cnt[1], TB_MAX_REC);
-    const int ntr = a.tl.on ? a.tl.rec_off[slot + 1] - a.tl.rec_off[slot] : 0;
+    const int ntr = nrec > 0 ? a.tl.rec_off[slot + 1] - a.tl.rec_off[slot] : 0;
+    float *seis = nrec > 0 ? a.tl.seis + a.tl.seis_off[slot] : nullptr;
+    const float *sig = ngrp > 0 ? a.tl.sig + a.tl.sig_off[slot] : nullptr;
 
     int bad = 0;
     for (int s = 0; s < ksteps; s++) {
         const int nt = n_first + s;
         const int e = (ksteps - 1 - s) * R;
+        /* this step's signals of the CTA's groups, fetched before the velocity
+           update so that their latency overlaps it */
+        float sv[TB_MAX_MEM];
+        if (tid < ngrp) {
+            const float *sg = sig + (long long)(nt - 1) * a.tl.sig_ts;
+#pragma unroll
+            for (int m = 0; m < TB_MAX_MEM; m++)
+                if (m < gl[TB_MAX_GRP + tid]) sv[m] = sg[(long long)gs[tid * TB_MAX_MEM + m] * a.tl.sig_ss];
+        }
 
         /* ---- velocity half-step (v_body) ---- */
         const int vx0 = max(1, ox - e - (H - 1)), vx1 = min(nx, ox1 + e + H);
@@ -212,9 +223,10 @@ __global__ void __launch_bounds__(TB_THREADS) tb_fwd(StepArgs a, TbGeom geo, int
             const int pk = gl[2 * TB_MAX_GRP + tid], gi = pk & 0xffff, gj = pk >> 16;
             if (gi >= vx0 && gi <= vx1 && gj >= vy0 && gj <= vy1) {
                 const int p = gl[tid], nm = gl[TB_MAX_GRP + tid];
-                const float *sg = a.tl.sig + a.tl.sig_off[slot] + (long long)(nt - 1) * a.tl.sig_ts;
                 float v = vy[p];
-                for (int m = 0; m < nm; m++) v = v + sg[(long long)gs[tid * TB_MAX_MEM + m] * a.tl.sig_ss];
+#pragma unroll
+                for (int m = 0; m < TB_MAX_MEM; m++)
+                    if (m < nm) v = v + sv[m];
                 vy[p] = v;
             }
         }
@@ -222,7 +234,7 @@ __global__ void __launch_bounds__(TB_THREADS) tb_fwd(StepArgs a, TbGeom geo, int
 
         /* ---- receiver samples (own points; vy after the injection) ---- */
         if (nrec > 0) {
-            float *sm = a.tl.seis + a.tl.seis_off[slot] + (long long)(nt - 1) * ntr;
+            float *sm = seis + (long long)(nt - 1) * ntr;
             for (int r = tid; r < nrec; r += TB_THREADS) sm[rl[TB_MAX_REC + r]] = vy[rl[r]];
         }
 

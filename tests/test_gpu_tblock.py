@@ -1,13 +1,15 @@
 """The temporally blocked forward-modelling launches (step variant 5): plain
 elastic forward modelling of a small grid with k time steps per launch, each
-thread block advancing its 32 x 16-point tile and a recomputed halo of
-k*(FDORDER-1) points in shared memory.
+thread block advancing its tile (32 points wide, 8-64 rows high so that all
+tiles run in one wave) and a recomputed halo of k*(FDORDER-1) points in
+shared memory.
 
 Bit-exact against the CPU oracle (pinned to the reference's
 update_v_PML.c / update_s_elastic_PML.c / seismo_ssg.c) over FDORDER 2-8,
 free surface on and off (CPML on all four sides), DH a power of two or not,
 grid widths that are not a multiple of the tile, steps per launch from 1 to
-7 (a pass whose NT is not a multiple of k ends with a shorter launch),
+7 (a pass whose NT is not a multiple of k ends with a shorter launch), tile
+heights of 5, 8, 16 and 24 rows,
 several shots in one launch and the 500 x 200 x 2000 benchmark case; the end
 state written back to the slots equals the kernel pair's; an unstable model
 reports DSH_ERR_UNSTABLE."""
@@ -62,6 +64,20 @@ def test_tblock_steps_per_launch(k, monkeypatch):
     seis, st, _ = _run(d, shots, TBLOCK)
     assert st["kernel_launches"] <= math.ceil(101 / k) + 8
     assert np.array_equal(seis[0], _oracle_forward(d, shots[0]))
+
+
+@pytest.mark.parametrize("rows", [16, 5])
+def test_tblock_pinned_tile_heights(rows, monkeypatch):
+    """Tile heights the single-wave choice does not pick here (DSH_TB_ROWS):
+    16 rows (two CTAs per SM on this grid) and an odd 5."""
+    monkeypatch.setenv("DSH_TB_ROWS", str(rows))
+    d, shots = _case(4150 + rows, nx=203, ny=97, nt=90, fdo=6, L=0, fs=0, fw=10)
+    shots = _inside(d, shots)
+    seis, _, end = _run(d, shots, TBLOCK)
+    assert np.array_equal(seis[0], _oracle_forward(d, shots[0]))
+    _, _, end_pair = _run(d, shots, 0)
+    for k in ("vy", "sxy", "syz"):
+        assert np.array_equal(end[0][k], end_pair[0][k]), k
 
 
 def test_tblock_several_shots_in_one_launch():
