@@ -184,9 +184,10 @@ int dsh_profile_step(dsh_ctx *ctx, int pass, int nsteps, float *out_ms3);
  * per shot (FDORDER <= 8, grids whose ceil(NY/16)-row strips fit one CTA's
  * shared memory, e.g. 500 x 200), 5 plain elastic forward modelling with k
  * time steps per launch (FDORDER 2/4/6/8: k = 8/4/3/2), each thread block
- * advancing a 32 x 16-point tile and a recomputed halo of k*(FDORDER-1)
- * points in its shared memory (FDORDER <= 8, NX and NY >= 2 FW, at most 32
- * source points, 4 sources per point and 512 receivers per shot). */
+ * advancing a tile 32 points wide (and 8-64 rows high, so that all tiles run
+ * in one wave where they can) and a recomputed halo of k*(FDORDER-1) points
+ * in its shared memory (FDORDER <= 8, NX and NY >= 2 FW, at most 32 source
+ * points, 4 sources per point and 512 receivers per shot). */
 #define DSH_STEP_VARIANTS 6
 
 /* Step-kernel autotuner: times nsteps plain forward steps of every variant
